@@ -1,0 +1,129 @@
+/* spaqr_b200.h -- C ABI of the B200 pspaQR factorize-and-solve path.
+ *
+ * One opaque handle per factorization.  Every call returns an int status
+ * (0 = success, negative = error; spq_last_error() gives the message) and no
+ * call exits the process.  Host pointers are never retained: matrices and
+ * coordinates are copied.  Device memory belongs to the handle.
+ *
+ * Each entry point names the reference interface it replaces
+ * (Abeynaya/pspaQR_public, paths relative to that project).
+ *
+ * Status codes: -1 bad argument, -2 unsupported input (non-square, levels),
+ * -3 coordinates missing or mismatched, -4 call out of order, -5 / -6 symbolic
+ * structure inconsistent, -10 CUDA error, -11 device memory exhausted,
+ * -12 device-side wait timed out / preconditioner failure.
+ */
+#ifndef SPAQR_B200_H
+#define SPAQR_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct spq_tree spq_tree;
+
+/* ParTree(int nlevels, int skip)  -- include/ptree.h:135-141 */
+int spq_create(int nlevels, int skip, spq_tree** out);
+/* ~ParTree()  -- include/ptree.h:160 */
+int spq_destroy(spq_tree* t);
+
+/* Tree::set_tol / set_skip / set_scale / set_order / set_hsl / set_square
+ * (src/tree.cpp:14-20) and ParTree::set_nthreads / set_verbose / set_ttor_log
+ * (src/ptree.cpp:21-23).  order, hsl, nthreads and ttor_log are accepted and
+ * recorded like the reference (ParTree never reads order; the rest steer its
+ * CPU runtime, which this path replaces).  set_skip follows the driver rule
+ * skip = nlevels-1 when tol == 0 (pspaQR.cpp:150) at partition time. */
+int spq_set_tol(spq_tree* t, double tol);
+int spq_set_skip(spq_tree* t, int skip);
+int spq_set_scale(spq_tree* t, int scale);
+int spq_set_order(spq_tree* t, float order);
+int spq_set_hsl(spq_tree* t, int hsl);
+int spq_set_nthreads(spq_tree* t, int n);
+int spq_set_verbose(spq_tree* t, int v);
+int spq_set_ttor_log(spq_tree* t, int l);
+int spq_set_square(spq_tree* t, int s);
+/* RRQR pivot tie rule (no reference counterpart; LAPACK's dgeqp3 breaks
+ * equal-norm ties by rounding noise): the pivot is the first column whose
+ * partial norm is within rtol of the largest.  0 = first maximum. Default 1e-6. */
+int spq_set_pivot_rtol(spq_tree* t, double rtol);
+
+/* Tree::set_Xcoo(MatrixXd*) (src/tree.cpp:21): coordinates, dim x n
+ * column-major (the reference borrows the pointer; this copies it). */
+int spq_set_coords(spq_tree* t, int dim, int n, const double* X);
+/* linspace_nd(n, d) + set_Xcoo (util.cpp:901-930, pspaQR.cpp:153-160). */
+int spq_set_coords_tensor(spq_tree* t, int n, int d);
+
+/* ParTree::partition(SpMat& A)  -- src/ptree.cpp:495-701.  A in CSC, 0-based,
+ * sorted row indices; copied. */
+int spq_partition(spq_tree* t, int nrows, int ncols, const int* colptr, const int* rowidx, const double* vals);
+/* ParTree::assemble(SpMat& A)  -- src/ptree.cpp:703-864 (uses the matrix given
+ * to spq_partition). */
+int spq_assemble(spq_tree* t);
+/* int ParTree::factorize()  -- src/ptree.cpp:873-2154 */
+int spq_factorize(spq_tree* t);
+
+/* void ParTree::solve(VectorXd& x) const  -- src/ptree.cpp:2788-3210.
+ * x (host pointer, length n, permuted order) is overwritten by M^{-1} x. */
+int spq_solve_inplace(spq_tree* t, double* x);
+/* Same, x is a device pointer (stream-ordered on the handle's stream). */
+int spq_solve_inplace_device(spq_tree* t, double* x);
+/* void ParTree::solve(VectorXd b, VectorXd& x) const  -- src/ptree.cpp:2268-2785
+ * (square branch): b and x in the original ordering. */
+int spq_solve_global(spq_tree* t, const double* b, double* x);
+/* VectorXd ParTree::spmv(VectorXd x) const  -- src/ptree.cpp:3212-3262 (permuted order). */
+int spq_spmv(spq_tree* t, const double* x, double* y);
+/* unsigned long dist_gmres(A, b, M, iter, tol, verb)  -- src/is.cpp:447-527.
+ * b (host, permuted order) is overwritten by the solution; iters = the
+ * reference's k; relres = true ||b - A x|| / ||b|| (pspaQR.cpp:264-268);
+ * hist (may be null) receives the preconditioned residual per step. */
+int spq_gmres(spq_tree* t, double* b, int maxit, double tol, int* iters, double* relres, double* hist, int hist_cap);
+/* Same with a device-resident right-hand side / solution. */
+int spq_gmres_device(spq_tree* t, double* b, int maxit, double tol, int* iters, double* relres, double* hist,
+                     int hist_cap);
+
+/* ParTree::distribute_x / extract_x (src/ptree.cpp:3264-3303), single rank:
+ * x_local = x[rperm]  and  x[cperm] = x_local. */
+int spq_distribute_x(spq_tree* t, const double* x, double* x_local);
+int spq_extract_x(spq_tree* t, const double* x_local, double* x);
+/* ParTree::nrows_local / ncols_local (src/ptree.cpp:25-26). */
+int spq_n(spq_tree* t);
+
+/* Stream the handle launches on (a cudaStream_t passed as void*); null = own stream. */
+int spq_set_stream(spq_tree* t, void* stream);
+
+/* Driver preprocessing (pspaQR.cpp:133-146): vals <- A diag(1/||A(:,j)||) * 10. */
+int spq_scale_columns(int ncols, const int* colptr, double* vals);
+/* util.cpp:992-1001 random(size, seed): mt19937 + uniform_real_distribution(-1,1). */
+int spq_random_reference(int n, int seed, double* out);
+
+/* Introspection for parity checks. */
+int spq_get_perm(spq_tree* t, int* cperm);
+int spq_num_clusters(spq_tree* t);
+int spq_num_levels(spq_tree* t);
+/* info[16]: lvl, merge_lvl, size (current), rank, parent, cstart, sep, l_lvl,
+ * l_sep, r_lvl, r_sep, section, size at creation, sparsified, nchildren, interior */
+int spq_cluster_info(spq_tree* t, int order, int* info);
+int spq_level_range(spq_tree* t, int lvl, int* first, int* count);
+int spq_num_edges(spq_tree* t);
+/* Index of the block A(n2 rows, n1 cols) in the symbolic structure, or -1. */
+int spq_find_edge(spq_tree* t, int n1, int n2);
+/* Final block A(n2 rows, n1 cols): shape[0..2] = rows, cols, ld; out may be null. */
+int spq_get_block(spq_tree* t, int n1, int n2, double* out, int* shape);
+/* Factors of cluster `order` (which: 0 = diagonal-QR T of an interior,
+ * 1 = scaling T, 2 = sparsification reflectors V (n x rank), 3 = their T);
+ * shape[0..2] = rows, cols, ld of the stored factor; out receives rows x cols. */
+int spq_get_factor(spq_tree* t, int order, int which, double* out, int* shape);
+/* times[0..4] = partition, assemble, factorize, last solve, last gmres (seconds). */
+int spq_times(spq_tree* t, double* times);
+/* Per level: elim, scale, spars, merge milliseconds (4 * nlevels values). */
+int spq_level_times(spq_tree* t, float* ms);
+/* Nominal FP64 flops of the last factorization (LAPACK Working Note 41 counts). */
+double spq_factor_flops(spq_tree* t);
+/* Bytes of device memory held by factor blocks. */
+double spq_pool_bytes(spq_tree* t);
+const char* spq_last_error(spq_tree* t);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

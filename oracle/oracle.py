@@ -31,6 +31,7 @@ def lib():
             "orc_create": (vp, [i32, i32, f64, i32]),
             "orc_destroy": (None, [vp]),
             "orc_set_threads": (i32, [vp, i32]),
+            "orc_set_pivot": (i32, [vp, i32, f64]),
             "orc_set_matrix": (i32, [vp, i32, i32, pi, pi, pd, i32]),
             "orc_get_matrix_values": (i32, [vp, pd]),
             "orc_set_coords_tensor": (i32, [vp, i32, i32]),
@@ -100,6 +101,11 @@ class OracleTree:
     def _chk(self, rc, what):
         if rc != 0:
             raise RuntimeError(f"oracle {what} failed with status {rc}")
+
+    def set_pivot(self, mode: int, rtol: float = 1e-6):
+        """mode 1 (default): restated dlaqp2, pivot = first column within rtol of the
+        largest partial norm; mode 0: LAPACK dgeqp3 exactly as the reference calls it."""
+        lib().orc_set_pivot(self.h, mode, rtol)
 
     def set_threads(self, t: int):
         lib().orc_set_threads(self.h, t)

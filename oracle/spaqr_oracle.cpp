@@ -237,6 +237,81 @@ struct Cluster {
   void reset_size(int r, int c) { rsize = r; csize = c; rank = c; }
 };
 
+// Column-pivoted Householder QR of C (m x w, col-major), restating LAPACK
+// dgeqp3's unblocked path dlaqp2 (pivot on the largest partial column norm,
+// LAWN 176 norm downdating with recomputation when temp2 <= sqrt(eps)), stopped
+// at the first i >= 1 with |R(i,i)|/|R(0,0)| < tol (util.cpp:830-851
+// choose_rank).  Pivot: the first column whose partial norm is within
+// pivot_rtol of the largest (pivot_rtol = 0 is LAPACK's idamax rule).
+// Returns the rank; tau[0:rank] and V (below the diagonal of the first rank
+// columns) as dgeqp3 leaves them.
+int geqp3_trunc(double* C, int m, int w, double tol, double pivot_rtol, std::vector<double>& tau) {
+  const int kmin = std::min(m, w);
+  tau.assign(std::max(kmin, 1), 0.0);
+  std::vector<double> vn1(w), vn2(w);
+  auto col = [&](int j) { return C + (size_t)j * m; };
+  for (int j = 0; j < w; ++j) {
+    double s = 0;
+    for (int r = 0; r < m; ++r) s += col(j)[r] * col(j)[r];
+    vn1[j] = vn2[j] = std::sqrt(s);
+  }
+  const double tol3z = std::sqrt(1.1102230246251565e-16);
+  double r00 = 0;
+  for (int i = 0; i < kmin; ++i) {
+    double mx = -1.0;
+    for (int j = i; j < w; ++j) mx = std::max(mx, vn1[j]);
+    const double thr = mx * (1.0 - pivot_rtol);
+    int pvt = i;
+    for (int j = i; j < w; ++j)
+      if (vn1[j] >= thr) { pvt = j; break; }
+    if (pvt != i) {
+      for (int r = 0; r < m; ++r) std::swap(col(i)[r], col(pvt)[r]);
+      vn1[pvt] = vn1[i];
+      vn2[pvt] = vn2[i];
+    }
+    double* ci = col(i);
+    double ss = 0;
+    for (int r = i + 1; r < m; ++r) ss += ci[r] * ci[r];
+    const double alpha = ci[i];
+    double beta = alpha, t = 0.0, scal = 0.0;
+    if (ss != 0.0) {
+      beta = -std::copysign(std::hypot(alpha, std::sqrt(ss)), alpha);
+      t = (beta - alpha) / beta;
+      scal = 1.0 / (alpha - beta);
+    }
+    const double absb = std::fabs(beta);
+    if (i == 0) r00 = absb;
+    else if (!(absb / r00 >= tol)) return i;
+    if (t != 0.0)
+      for (int r = i + 1; r < m; ++r) ci[r] *= scal;
+    ci[i] = beta;
+    tau[i] = t;
+    for (int j = i + 1; j < w; ++j) {
+      double* cj = col(j);
+      if (t != 0.0) {
+        double d = cj[i];
+        for (int r = i + 1; r < m; ++r) d += ci[r] * cj[r];
+        d *= t;
+        cj[i] -= d;
+        for (int r = i + 1; r < m; ++r) cj[r] -= ci[r] * d;
+      }
+      if (vn1[j] != 0.0) {
+        double temp = std::fabs(cj[i]) / vn1[j];
+        temp = std::max(1.0 - temp * temp, 0.0);
+        const double q = vn1[j] / vn2[j];
+        if (temp * q * q <= tol3z) {
+          double nn = 0;
+          for (int r = i + 1; r < m; ++r) nn += cj[r] * cj[r];
+          vn1[j] = vn2[j] = (i + 1 < m) ? std::sqrt(nn) : 0.0;
+        } else {
+          vn1[j] *= std::sqrt(temp);
+        }
+      }
+    }
+  }
+  return kmin;
+}
+
 struct Timers {
   double partition = 0, assemble = 0, factorize = 0, solve = 0, gmres = 0;
   std::vector<double> lvl_fill, lvl_elim, lvl_scale, lvl_spars, lvl_merge;
@@ -246,6 +321,8 @@ struct Oracle {
   int nlevels, skip;
   double tol;
   int nthreads = 1;
+  int pivot_mode = 1;          // 0: LAPACK dgeqp3 as the reference calls it; 1: restated dlaqp2 with tie rule
+  double pivot_rtol = 1e-6;
   int n = 0;
   CSC A;      // scaled input matrix (original order)
   CSC App;    // permuted matrix (rows rperm, cols cperm)
@@ -632,16 +709,20 @@ struct Oracle {
     int kmin = std::min(m, w);
     std::vector<int> jpvt(w, 0);
     std::vector<double> tau(kmin, 0.0);
-    if (m > 0 && w > 0) scipy_LAPACKE_dgeqp3(kColMajor, m, w, C.p(), m, jpvt.data(), tau.data());
-    // util.cpp:830-851 choose_rank (relative)
     int rank;
-    if (tol == 0) rank = kmin;
-    else if (tol >= 1.0) rank = 0;
-    else if (kmin <= 1) rank = kmin;
-    else {
-      double sref = std::fabs(C(0, 0));
-      rank = 1;
-      while (rank < kmin && std::fabs(C(rank, rank)) / sref >= tol) rank++;
+    if (pivot_mode == 1 && tol > 0 && tol < 1.0 && kmin > 1) {
+      rank = geqp3_trunc(C.p(), m, w, tol, pivot_rtol, tau);
+    } else {
+      if (m > 0 && w > 0) scipy_LAPACKE_dgeqp3(kColMajor, m, w, C.p(), m, jpvt.data(), tau.data());
+      // util.cpp:830-851 choose_rank (relative)
+      if (tol == 0) rank = kmin;
+      else if (tol >= 1.0) rank = 0;
+      else if (kmin <= 1) rank = kmin;
+      else {
+        double sref = std::fabs(C(0, 0));
+        rank = 1;
+        while (rank < kmin && std::fabs(C(rank, rank)) / sref >= tol) rank++;
+      }
     }
     Mat V(m, rank);
     for (int j = 0; j < rank; ++j)
@@ -1047,6 +1128,12 @@ void* orc_create(int nlevels, int skip, double tol, int nthreads) {
   return o;
 }
 void orc_destroy(void* h) { delete static_cast<Oracle*>(h); }
+int orc_set_pivot(void* h, int mode, double rtol) {
+  Oracle* o = static_cast<Oracle*>(h);
+  o->pivot_mode = mode;
+  o->pivot_rtol = rtol;
+  return 0;
+}
 int orc_set_threads(void* h, int t) {
   static_cast<Oracle*>(h)->nthreads = std::max(1, t);
   return 0;

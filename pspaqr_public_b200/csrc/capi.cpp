@@ -1,0 +1,226 @@
+// capi.cpp -- extern "C" boundary (include/spaqr_b200.h) over spq::Tree.
+#include <cmath>
+#include <cstring>
+#include <random>
+#include <string>
+#include <vector>
+
+#include "../../include/spaqr_b200.h"
+#include "engine.hpp"
+
+struct spq_tree {
+  spq::Tree* t;
+  std::string err;
+};
+
+namespace {
+int done(spq_tree* h, int rc) {
+  if (rc != 0) h->err = h->t->error;
+  return rc;
+}
+thread_local std::string g_err;
+}  // namespace
+
+extern "C" {
+
+int spq_create(int nlevels, int skip, spq_tree** out) {
+  if (!out) return -1;
+  *out = nullptr;
+  if (nlevels < 2 || skip < 0) return -1;
+  spq_tree* h = new spq_tree;
+  h->t = new spq::Tree(nlevels, skip);
+  *out = h;
+  return 0;
+}
+
+int spq_destroy(spq_tree* h) {
+  if (!h) return -1;
+  delete h->t;
+  delete h;
+  return 0;
+}
+
+#define SPQ_SETTER(name, type, field) \
+  int name(spq_tree* h, type v) {     \
+    if (!h) return -1;                \
+    h->t->field = v;                  \
+    return 0;                         \
+  }
+SPQ_SETTER(spq_set_tol, double, tol)
+SPQ_SETTER(spq_set_skip, int, skip)
+SPQ_SETTER(spq_set_scale, int, scale)
+SPQ_SETTER(spq_set_order, float, order)
+SPQ_SETTER(spq_set_hsl, int, hsl)
+SPQ_SETTER(spq_set_nthreads, int, nthreads)
+SPQ_SETTER(spq_set_verbose, int, verbose)
+SPQ_SETTER(spq_set_ttor_log, int, ttor_log)
+#undef SPQ_SETTER
+
+int spq_set_pivot_rtol(spq_tree* h, double r) {
+  if (!h || r < 0 || r >= 1) return -1;
+  h->t->pivot_rtol = r;
+  return 0;
+}
+
+int spq_set_square(spq_tree* h, int s) {
+  if (!h) return -1;
+  if (!s) {
+    h->err = "rectangular (least-squares) systems are not supported by this build";
+    return -2;
+  }
+  h->t->square = 1;
+  return 0;
+}
+
+int spq_set_coords(spq_tree* h, int dim, int n, const double* X) {
+  if (!h) return -1;
+  return done(h, h->t->set_coords(dim, n, X));
+}
+int spq_set_coords_tensor(spq_tree* h, int n, int d) {
+  if (!h) return -1;
+  return done(h, h->t->set_coords_tensor(n, d));
+}
+int spq_partition(spq_tree* h, int nrows, int ncols, const int* colptr, const int* rowidx, const double* vals) {
+  if (!h) return -1;
+  if (h->t->hsl) {
+    h->err = "bipartite matching (HSL MC64) is not part of this build";
+    return -2;
+  }
+  return done(h, h->t->partition(nrows, ncols, colptr, rowidx, vals));
+}
+int spq_assemble(spq_tree* h) { return h ? done(h, h->t->assemble()) : -1; }
+int spq_factorize(spq_tree* h) { return h ? done(h, h->t->factorize()) : -1; }
+int spq_solve_inplace(spq_tree* h, double* x) { return (h && x) ? done(h, h->t->solve_host(x)) : -1; }
+int spq_solve_inplace_device(spq_tree* h, double* x) { return (h && x) ? done(h, h->t->solve_device(x)) : -1; }
+int spq_solve_global(spq_tree* h, const double* b, double* x) {
+  return (h && b && x) ? done(h, h->t->solve_global(b, x)) : -1;
+}
+int spq_spmv(spq_tree* h, const double* x, double* y) { return (h && x && y) ? done(h, h->t->spmv_host(x, y)) : -1; }
+int spq_gmres(spq_tree* h, double* b, int maxit, double tol, int* iters, double* relres, double* hist, int hist_cap) {
+  if (!h || !b || !iters || !relres) return -1;
+  return done(h, h->t->gmres_host(b, maxit, tol, iters, relres, hist, hist_cap));
+}
+int spq_gmres_device(spq_tree* h, double* b, int maxit, double tol, int* iters, double* relres, double* hist,
+                     int hist_cap) {
+  if (!h || !b || !iters || !relres) return -1;
+  return done(h, h->t->gmres_device(b, maxit, tol, iters, relres, hist, hist_cap));
+}
+int spq_distribute_x(spq_tree* h, const double* x, double* xl) {
+  if (!h || !x || !xl) return -1;
+  const auto& s = h->t->structure();
+  if (s.rperm.empty()) return -4;
+  for (int i = 0; i < s.n; ++i) xl[i] = x[s.rperm[i]];
+  return 0;
+}
+int spq_extract_x(spq_tree* h, const double* xl, double* x) {
+  if (!h || !x || !xl) return -1;
+  const auto& s = h->t->structure();
+  if (s.cperm.empty()) return -4;
+  for (int i = 0; i < s.n; ++i) x[s.cperm[i]] = xl[i];
+  return 0;
+}
+int spq_n(spq_tree* h) { return h ? h->t->n() : -1; }
+int spq_set_stream(spq_tree* h, void* stream) {
+  return h ? done(h, h->t->set_stream(static_cast<cudaStream_t>(stream))) : -1;
+}
+
+int spq_scale_columns(int ncols, const int* colptr, double* vals) {
+  if (ncols < 0 || !colptr || !vals) return -1;
+  for (int j = 0; j < ncols; ++j) {
+    double s = 0.0;
+    for (int k = colptr[j]; k < colptr[j + 1]; ++k) s += vals[k] * vals[k];
+    const double d = 1.0 / std::sqrt(s);
+    for (int k = colptr[j]; k < colptr[j + 1]; ++k) vals[k] = (vals[k] * d) * 10.0;
+  }
+  return 0;
+}
+
+int spq_random_reference(int n, int seed, double* out) {
+  if (n < 0 || !out) return -1;
+  std::mt19937 rng;
+  rng.seed(seed);
+  std::uniform_real_distribution<double> dist(-1.0, 1.0);
+  for (int i = 0; i < n; ++i) out[i] = dist(rng);
+  return 0;
+}
+
+int spq_get_perm(spq_tree* h, int* cperm) {
+  if (!h || !cperm) return -1;
+  const auto& s = h->t->structure();
+  if (s.cperm.empty()) return -4;
+  std::memcpy(cperm, s.cperm.data(), sizeof(int) * s.n);
+  return 0;
+}
+int spq_num_clusters(spq_tree* h) { return h ? (int)h->t->structure().clusters.size() : -1; }
+int spq_num_levels(spq_tree* h) { return h ? h->t->structure().nlevels : -1; }
+int spq_cluster_info(spq_tree* h, int order, int* info) {
+  if (!h || !info) return -1;
+  const auto& s = h->t->structure();
+  if (order < 0 || order >= (int)s.clusters.size()) return -1;
+  const spq::Cluster& c = s.clusters[order];
+  auto sz = h->t->cluster_sizes();
+  auto so = h->t->cluster_sizes_org();
+  const bool have = !sz.empty();
+  info[0] = c.lvl;
+  info[1] = c.merge_lvl;
+  info[2] = have ? sz[order] : c.size0;
+  info[3] = have ? sz[order] : c.size0;
+  info[4] = c.parent;
+  info[5] = c.cstart;
+  info[6] = c.id.self.sep;
+  info[7] = c.id.l.lvl;
+  info[8] = c.id.l.sep;
+  info[9] = c.id.r.lvl;
+  info[10] = c.id.r.sep;
+  info[11] = c.id.section;
+  info[12] = have ? so[order] : c.size0;
+  info[13] = c.sparsify ? 1 : 0;
+  info[14] = c.child_end - c.child_begin;
+  info[15] = c.interior ? 1 : 0;
+  return 0;
+}
+int spq_level_range(spq_tree* h, int lvl, int* first, int* count) {
+  if (!h || !first || !count) return -1;
+  const auto& s = h->t->structure();
+  if (lvl < 0 || lvl >= (int)s.levels.size()) return -1;
+  *first = s.levels[lvl].first;
+  *count = s.levels[lvl].count;
+  return 0;
+}
+int spq_num_edges(spq_tree* h) { return h ? (int)h->t->structure().edges.size() : -1; }
+int spq_find_edge(spq_tree* h, int n1, int n2) { return h ? h->t->structure().find_edge(n1, n2) : -1; }
+int spq_get_block(spq_tree* h, int n1, int n2, double* out, int* shape) {
+  if (!h || !shape) return -1;
+  return h->t->get_block(n1, n2, out, shape, shape + 1, shape + 2);
+}
+int spq_get_factor(spq_tree* h, int order, int which, double* out, int* shape) {
+  if (!h || !shape) return -1;
+  return h->t->get_factor(order, which, out, shape);
+}
+int spq_times(spq_tree* h, double* times) {
+  if (!h || !times) return -1;
+  times[0] = h->t->t_partition;
+  times[1] = h->t->t_assemble;
+  times[2] = h->t->t_factorize;
+  times[3] = h->t->t_solve;
+  times[4] = h->t->t_gmres;
+  return 0;
+}
+int spq_level_times(spq_tree* h, float* ms) {
+  if (!h || !ms) return -1;
+  const auto& lt = h->t->level_timing();
+  for (size_t l = 0; l < lt.size(); ++l) {
+    ms[4 * l] = lt[l].elim_ms;
+    ms[4 * l + 1] = lt[l].scale_ms;
+    ms[4 * l + 2] = lt[l].spars_ms;
+    ms[4 * l + 3] = lt[l].merge_ms;
+  }
+  return 0;
+}
+double spq_factor_flops(spq_tree* h) { return h ? h->t->factor_flops() : -1.0; }
+double spq_pool_bytes(spq_tree* h) { return h ? (double)h->t->pool_bytes() : -1.0; }
+const char* spq_last_error(spq_tree* h) {
+  if (!h) return "null handle";
+  return h->err.c_str();
+}
+}

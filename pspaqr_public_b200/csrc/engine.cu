@@ -1,0 +1,918 @@
+// engine.cu -- host orchestration of the factorization, solve and GMRES.
+#include "engine.hpp"
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <numeric>
+
+#include "kernels.hpp"
+
+namespace spq {
+
+namespace {
+double wall() {
+  return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+constexpr size_t kAlign = 256;
+constexpr size_t kChunk = size_t(1) << 30;
+// bounded wait of the forward sweep: ~1 s at 2 GHz
+constexpr long long kSpinLimit = 2000000000LL;
+}  // namespace
+
+// ---------------------------------------------------------------- Arena
+Arena::~Arena() { release(); }
+
+void* Arena::alloc(size_t bytes) {
+  bytes = (bytes + kAlign - 1) / kAlign * kAlign;
+  if (bytes == 0) bytes = kAlign;
+  if (chunks_.empty() || chunks_.back().off + bytes > chunks_.back().size) {
+    size_t sz = std::max(kChunk, bytes);
+    void* p = nullptr;
+    if (cudaMalloc(&p, sz) != cudaSuccess) return nullptr;
+    chunks_.push_back({static_cast<char*>(p), sz, 0});
+    reserved_ += sz;
+  }
+  Chunk& c = chunks_.back();
+  void* r = c.base + c.off;
+  c.off += bytes;
+  used_ += bytes;
+  return r;
+}
+
+void Arena::release() {
+  for (auto& c : chunks_) cudaFree(c.base);
+  chunks_.clear();
+  used_ = reserved_ = 0;
+}
+
+// ---------------------------------------------------------------- Tree
+Tree::Tree(int L, int s) : nlevels(L), skip(s) {}
+
+Tree::~Tree() {
+  if (solve_exec_) cudaGraphExecDestroy(solve_exec_);
+  if (solve_graph_) cudaGraphDestroy(solve_graph_);
+  cudaFree(d_rank_);
+  cudaFree(d_rowptr_);
+  cudaFree(d_col_);
+  cudaFree(d_val_);
+  cudaFree(d_xw_);
+  cudaFree(d_turn_);
+  cudaFree(d_tickets_);
+  cudaFree(d_status_);
+  cudaFree(d_tmp_);
+  scratch_.release();
+  arena_.release();
+  if (own_stream_ && stream_) cudaStreamDestroy(stream_);
+}
+
+int Tree::check_cuda(cudaError_t e, const char* where) {
+  if (e == cudaSuccess) return 0;
+  error = std::string(where) + ": " + cudaGetErrorString(e);
+  return -10;
+}
+
+int Tree::set_stream(cudaStream_t s) {
+  if (own_stream_ && stream_) cudaStreamDestroy(stream_);
+  stream_ = s;
+  own_stream_ = false;
+  if (solve_exec_) {
+    cudaGraphExecDestroy(solve_exec_);
+    cudaGraphDestroy(solve_graph_);
+    solve_exec_ = nullptr;
+    solve_graph_ = nullptr;
+    if (factorized_) return build_solve_graph();
+  }
+  return 0;
+}
+
+int Tree::device_status() {
+  int s = 0;
+  if (d_status_) cudaMemcpy(&s, d_status_, sizeof(int), cudaMemcpyDeviceToHost);
+  return s;
+}
+
+void* Tree::upload(const void* host, size_t bytes) {
+  void* d = scratch_.alloc(bytes);
+  if (d && bytes) cudaMemcpyAsync(d, host, bytes, cudaMemcpyHostToDevice, stream_);
+  return d;
+}
+
+int Tree::set_coords(int dim, int n, const double* X) {
+  if (dim <= 0 || n <= 0 || !X) return fail(-1, "bad coordinates");
+  dim_ = dim;
+  X_.assign(X, X + (size_t)dim * n);
+  return 0;
+}
+
+// util.cpp:901-930 linspace_nd: node i0*n^(d-1) + ... + i_{d-1} at (i0, ..., i_{d-1})
+int Tree::set_coords_tensor(int n, int d) {
+  if (n <= 0 || d <= 0 || d > 3) return fail(-1, "tensor coordinates need n > 0 and 1 <= d <= 3");
+  int64_t N = 1;
+  for (int i = 0; i < d; ++i) N *= n;
+  dim_ = d;
+  X_.assign((size_t)N * d, 0.0);
+  for (int64_t id = 0; id < N; ++id) {
+    int64_t r = id;
+    for (int k = d - 1; k >= 0; --k) {
+      X_[(size_t)id * d + k] = (double)(r % n);
+      r /= n;
+    }
+  }
+  return 0;
+}
+
+int Tree::partition(int nrows, int ncols, const int* colptr, const int* rowidx, const double* val) {
+  double t0 = wall();
+  if (nrows != ncols) return fail(-2, "only square matrices are supported (rectangular path not built)");
+  if (!colptr || !rowidx || !val) return fail(-1, "null matrix pointer");
+  if (dim_ == 0) return fail(-3, "no coordinates: call set_coords or set_coords_tensor first");
+  if ((int64_t)X_.size() != (int64_t)dim_ * ncols) return fail(-3, "coordinates do not match the matrix size");
+  A_.nrows = nrows;
+  A_.ncols = ncols;
+  A_.colptr.assign(colptr, colptr + ncols + 1);
+  const int nnz = colptr[ncols];
+  A_.rowidx.assign(rowidx, rowidx + nnz);
+  A_.val.assign(val, val + nnz);
+  for (int j = 0; j < ncols; ++j)
+    if (colptr[j + 1] < colptr[j]) return fail(-1, "colptr is not monotone");
+  for (int k = 0; k < nnz; ++k)
+    if (rowidx[k] < 0 || rowidx[k] >= nrows) return fail(-1, "row index out of range");
+  int rc = build_structure(st_, A_, nlevels, skip, tol, X_, dim_);
+  if (rc != 0) return fail(rc, st_.error);
+  partitioned_ = true;
+  assembled_ = factorized_ = false;
+  t_partition = wall() - t0;
+  if (verbose) printf("Time to partition: %g\n", t_partition);
+  return 0;
+}
+
+int Tree::assemble() {
+  if (!partitioned_) return fail(-4, "assemble called before partition");
+  double t0 = wall();
+  if (!stream_) {
+    if (check_cuda(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "stream")) return -10;
+    own_stream_ = true;
+  }
+  const int n = st_.n;
+  const int ncl = (int)st_.clusters.size();
+  const int ned = (int)st_.edges.size();
+  size_.assign(ncl, 0);
+  size_org_.assign(ncl, 0);
+  rpos_.assign(ncl, 0);
+  T_.assign(ncl, nullptr);
+  Ts_.assign(ncl, nullptr);
+  Qsp_.assign(ncl, nullptr);
+  Tsp_.assign(ncl, nullptr);
+  ptr_.assign(ned, nullptr);
+  ld_.assign(ned, 0);
+  rows_.assign(ned, 0);
+  cols_.assign(ned, 0);
+  tsqrtT_.assign(ned, nullptr);
+  arena_.release();
+  const Level& L0 = st_.levels[0];
+  for (int o = L0.first; o < L0.first + L0.count; ++o) size_[o] = size_org_[o] = st_.clusters[o].size0;
+  // level-0 blocks, zeroed, then the nonzeros of App scattered in
+  size_t total = 0;
+  for (int e : L0.edges) {
+    const Edge& E = st_.edges[e];
+    rows_[e] = size_[E.n2];
+    cols_[e] = size_[E.n1];
+    ld_[e] = std::max(1, rows_[e]);
+    ptr_[e] = arena_.dalloc((size_t)ld_[e] * cols_[e]);
+    if (!ptr_[e]) return fail(-11, "out of device memory (level-0 blocks)");
+    total += (size_t)ld_[e] * cols_[e];
+  }
+  for (int e : L0.edges) cudaMemsetAsync(ptr_[e], 0, sizeof(double) * (size_t)ld_[e] * cols_[e], stream_);
+  (void)total;
+  const Csc& P = st_.App;
+  std::vector<int> leaf_of(n);
+  for (int o = L0.first; o < L0.first + L0.count; ++o)
+    for (int k = st_.clusters[o].cstart; k < st_.clusters[o].cstart + st_.clusters[o].size0; ++k) leaf_of[k] = o;
+  const int nnz = (int)P.rowidx.size();
+  std::vector<double*> dst(nnz);
+  for (int j = 0; j < n; ++j) {
+    const int cj = leaf_of[j];
+    for (int k = P.colptr[j]; k < P.colptr[j + 1]; ++k) {
+      const int i = P.rowidx[k];
+      const int ri = leaf_of[i];
+      const int e = st_.find_edge(cj, ri);
+      dst[k] = ptr_[e] + (i - st_.clusters[ri].cstart) + (size_t)(j - st_.clusters[cj].cstart) * ld_[e];
+    }
+  }
+  // CSR of App for the SpMV (y = App x)
+  std::vector<int> rowptr(n + 1, 0), col(nnz);
+  std::vector<double> val(nnz);
+  for (int k = 0; k < nnz; ++k) rowptr[P.rowidx[k] + 1]++;
+  std::partial_sum(rowptr.begin(), rowptr.end(), rowptr.begin());
+  {
+    std::vector<int> pos(rowptr.begin(), rowptr.end() - 1);
+    for (int j = 0; j < n; ++j)
+      for (int k = P.colptr[j]; k < P.colptr[j + 1]; ++k) {
+        int p = pos[P.rowidx[k]]++;
+        col[p] = j;
+        val[p] = P.val[k];
+      }
+  }
+  cudaFree(d_rowptr_);
+  cudaFree(d_col_);
+  cudaFree(d_val_);
+  cudaFree(d_rank_);
+  cudaFree(d_status_);
+  cudaFree(d_tmp_);
+  if (check_cuda(cudaMalloc(&d_rowptr_, sizeof(int) * (n + 1)), "malloc") ||
+      check_cuda(cudaMalloc(&d_col_, sizeof(int) * std::max(nnz, 1)), "malloc") ||
+      check_cuda(cudaMalloc(&d_val_, sizeof(double) * std::max(nnz, 1)), "malloc") ||
+      check_cuda(cudaMalloc(&d_rank_, sizeof(int) * ncl), "malloc") ||
+      check_cuda(cudaMalloc(&d_status_, sizeof(int)), "malloc") ||
+      check_cuda(cudaMalloc(&d_tmp_, sizeof(double) * 2 * n), "malloc"))
+    return -10;
+  cudaMemcpyAsync(d_rowptr_, rowptr.data(), sizeof(int) * (n + 1), cudaMemcpyHostToDevice, stream_);
+  cudaMemcpyAsync(d_col_, col.data(), sizeof(int) * nnz, cudaMemcpyHostToDevice, stream_);
+  cudaMemcpyAsync(d_val_, val.data(), sizeof(double) * nnz, cudaMemcpyHostToDevice, stream_);
+  cudaMemsetAsync(d_status_, 0, sizeof(int), stream_);
+  // scatter values of App (CSC order) into the blocks
+  std::vector<double> cval(P.val);
+  double* d_cval = static_cast<double*>(upload(cval.data(), sizeof(double) * nnz));
+  double** d_dst = static_cast<double**>(upload(dst.data(), sizeof(double*) * nnz));
+  if (!d_cval || !d_dst) return fail(-11, "out of device memory (assembly)");
+  launch_scatter(nnz, d_cval, d_dst, stream_);
+  if (check_cuda(cudaStreamSynchronize(stream_), "assemble")) return -10;
+  scratch_.release();
+  assembled_ = true;
+  factorized_ = false;
+  t_assemble = wall() - t0;
+  if (verbose) printf("Time to assemble: %g\n", t_assemble);
+  return 0;
+}
+
+int Tree::factorize() {
+  if (!assembled_) return fail(-4, "factorize called before assemble");
+  if (factorized_) return fail(-4, "factorize called twice; assemble again first");
+  double t0 = wall();
+  const int L = st_.nlevels;
+  lt_.assign(L, LevelTiming());
+  flops_ = 0;
+  cudaEvent_t ev[5];
+  for (auto& e : ev) cudaEventCreate(&e);
+  std::vector<int> host_rank(st_.clusters.size(), 0);
+  for (int lvl = 0; lvl < L; ++lvl) {
+    const Level& Lv = st_.levels[lvl];
+    cudaEventRecord(ev[0], stream_);
+    // ---------------- elimination: geqrt + tsqrt chains
+    std::vector<ElimTask> et;
+    std::vector<ElimOut> eo;
+    int nmax = 1;
+    for (size_t ii = 0; ii < Lv.interiors.size(); ++ii) {
+      const int c = Lv.interiors[ii];
+      const int nc = size_[c];
+      const int se = Lv.self_edge_of[c - Lv.first];
+      T_[c] = arena_.dalloc((size_t)nc * nc);
+      ElimTask t;
+      t.S = ptr_[se];
+      t.T = T_[c];
+      t.n = nc;
+      t.out_begin = (int)eo.size();
+      flops_ += 2.0 * nc * nc * (nc - nc / 3.0);
+      for (int q = Lv.out_begin[ii]; q < Lv.out_end[ii]; ++q) {
+        const int e = Lv.out_edges[q];
+        tsqrtT_[e] = arena_.dalloc((size_t)nc * nc);
+        ElimOut o;
+        o.B = ptr_[e];
+        o.T = tsqrtT_[e];
+        o.m = rows_[e];
+        eo.push_back(o);
+        flops_ += 2.0 * rows_[e] * nc * nc;
+      }
+      t.out_end = (int)eo.size();
+      et.push_back(t);
+      nmax = std::max(nmax, nc);
+    }
+    // trailing updates by column cluster
+    std::vector<UpdTask> ut;
+    std::vector<UpdOp> uo;
+    int kmax_upd = 1;
+    for (size_t ct = 0; ct < Lv.col_m.size(); ++ct) {
+      const int m = Lv.col_m[ct];
+      UpdTask t;
+      t.op_begin = (int)uo.size();
+      t.ncols = size_[m];
+      for (int q = Lv.col_begin[ct]; q < Lv.col_end[ct]; ++q) {
+        const int c = Lv.col_c[q];
+        const int ecm = Lv.col_ecm[q];
+        const int nc = size_[c];
+        const int se = Lv.self_edge_of[c - Lv.first];
+        UpdOp a;
+        a.kind = 0;
+        a.V = ptr_[se];
+        a.T = T_[c];
+        a.A = ptr_[ecm];
+        a.B = nullptr;
+        a.k = nc;
+        a.m = nc;
+        a.ldv = nc;
+        a.lda = ld_[ecm];
+        a.ldb = 0;
+        uo.push_back(a);
+        kmax_upd = std::max(kmax_upd, nc);
+        flops_ += 4.0 * nc * nc * t.ncols;
+        // interior's out-edges in chain order, aligned with col_emn
+        const int ii = (int)(std::lower_bound(Lv.interiors.begin(), Lv.interiors.end(), c) - Lv.interiors.begin());
+        int j = Lv.col_emn_begin[q];
+        for (int r = Lv.out_begin[ii]; r < Lv.out_end[ii]; ++r, ++j) {
+          const int ecn = Lv.out_edges[r];
+          const int emn = Lv.col_emn[j];
+          UpdOp b;
+          b.kind = 1;
+          b.V = ptr_[ecn];
+          b.T = tsqrtT_[ecn];
+          b.A = ptr_[ecm];
+          b.B = ptr_[emn];
+          b.k = nc;
+          b.m = rows_[ecn];
+          b.ldv = ld_[ecn];
+          b.lda = ld_[ecm];
+          b.ldb = ld_[emn];
+          uo.push_back(b);
+          flops_ += 4.0 * rows_[ecn] * nc * t.ncols;
+        }
+      }
+      t.op_end = (int)uo.size();
+      ut.push_back(t);
+    }
+    lt_[lvl].ntasks_elim = (int)et.size();
+    lt_[lvl].ntasks_upd = (int)ut.size();
+    {
+      auto* d_et = static_cast<ElimTask*>(upload(et.data(), sizeof(ElimTask) * et.size()));
+      auto* d_eo = static_cast<ElimOut*>(upload(eo.data(), sizeof(ElimOut) * std::max<size_t>(eo.size(), 1)));
+      auto* d_ut = static_cast<UpdTask*>(upload(ut.data(), sizeof(UpdTask) * std::max<size_t>(ut.size(), 1)));
+      auto* d_uo = static_cast<UpdOp*>(upload(uo.data(), sizeof(UpdOp) * std::max<size_t>(uo.size(), 1)));
+      if (!d_et || !d_eo || !d_ut || !d_uo) return fail(-11, "out of device memory (elimination descriptors)");
+      launch_elim(d_et, d_eo, (int)et.size(), nmax, stream_);
+      launch_update(d_ut, d_uo, (int)ut.size(), kmax_upd, stream_);
+    }
+    cudaEventRecord(ev[1], stream_);
+    // ---------------- scaling + sparsification
+    const bool spars = !Lv.spars_clusters.empty();
+    if (spars) {
+      std::vector<ScaleTask> sc;
+      int smax = 1;
+      for (int p : Lv.spars_clusters) {
+        const int np = size_[p];
+        Ts_[p] = arena_.dalloc((size_t)np * np);
+        ScaleTask t;
+        t.S = ptr_[Lv.self_edge_of[p - Lv.first]];
+        t.T = Ts_[p];
+        t.n = np;
+        sc.push_back(t);
+        smax = std::max(smax, np);
+        flops_ += 2.0 * np * np * (np - np / 3.0);
+      }
+      std::vector<ScaleEdgeTask> se;
+      int kmax_se = 1, kmax_sp = 1;
+      for (int e : Lv.spars_edges) {
+        const Edge& E = st_.edges[e];
+        const bool r = st_.clusters[E.n2].sparsify, c = st_.clusters[E.n1].sparsify;
+        if (!r && !c) continue;
+        ScaleEdgeTask t;
+        t.A = ptr_[e];
+        t.lda = ld_[e];
+        t.m = rows_[e];
+        t.nc = cols_[e];
+        t.Qr = r ? ptr_[Lv.self_edge_of[E.n2 - Lv.first]] : nullptr;
+        t.Tr = r ? Ts_[E.n2] : nullptr;
+        t.ldqr = size_[E.n2];
+        t.Qc = c ? ptr_[Lv.self_edge_of[E.n1 - Lv.first]] : nullptr;
+        t.ldqc = size_[E.n1];
+        se.push_back(t);
+        if (r) kmax_se = std::max(kmax_se, t.m);
+        if (r) flops_ += 4.0 * t.m * t.m * t.nc;
+        if (c) flops_ += (double)t.m * t.nc * t.nc;
+      }
+      std::vector<RrqrTask> rt;
+      std::vector<RrqrSrc> rs;
+      int mmax = 1;
+      for (size_t q = 0; q < Lv.spars_clusters.size(); ++q) {
+        const int p = Lv.spars_clusters[q];
+        const int mp = size_[p];
+        RrqrTask t;
+        t.m = mp;
+        t.src_begin = (int)rs.size();
+        int w = 0;
+        for (int k = Lv.sp_out_begin[q]; k < Lv.sp_out_end[q]; ++k) {
+          const int e = Lv.sp_out[k];
+          rs.push_back({ptr_[e], ld_[e], rows_[e], cols_[e], 1});
+          w += rows_[e];
+        }
+        for (int k = Lv.sp_in_begin[q]; k < Lv.sp_in_end[q]; ++k) {
+          const int e = Lv.sp_in[k];
+          rs.push_back({ptr_[e], ld_[e], rows_[e], cols_[e], 0});
+          w += cols_[e];
+        }
+        t.src_end = (int)rs.size();
+        t.w = w;
+        Qsp_[p] = arena_.dalloc((size_t)mp * std::max(w, 1));
+        Tsp_[p] = arena_.dalloc((size_t)mp * mp);
+        t.C = Qsp_[p];
+        t.T = Tsp_[p];
+        t.tau = scratch_.dalloc(std::max(mp, 1));
+        t.vn = scratch_.dalloc(2 * (size_t)std::max(w, 1));
+        t.jpvt = static_cast<int*>(scratch_.alloc(sizeof(int) * std::max(w, 1)));
+        t.rank = d_rank_ + p;
+        if (!t.C || !t.T || !t.tau || !t.vn || !t.jpvt) return fail(-11, "out of device memory (rrqr)");
+        rt.push_back(t);
+        mmax = std::max(mmax, mp);
+      }
+      std::vector<SparsEdgeTask> sp;
+      for (int e : Lv.spars_edges) {
+        const Edge& E = st_.edges[e];
+        const bool r = st_.clusters[E.n2].sparsify, c = st_.clusters[E.n1].sparsify;
+        if (!r && !c) continue;
+        SparsEdgeTask t;
+        t.A = ptr_[e];
+        t.lda = ld_[e];
+        t.m = rows_[e];
+        t.nc = cols_[e];
+        t.Vr = r ? Qsp_[E.n2] : nullptr;
+        t.Tr = r ? Tsp_[E.n2] : nullptr;
+        t.rank_r = d_rank_ + E.n2;
+        t.ldvr = size_[E.n2];
+        t.Vc = c ? Qsp_[E.n1] : nullptr;
+        t.Tc = c ? Tsp_[E.n1] : nullptr;
+        t.rank_c = d_rank_ + E.n1;
+        t.ldvc = size_[E.n1];
+        sp.push_back(t);
+        kmax_sp = std::max(kmax_sp, std::max(r ? t.ldvr : 1, c ? t.ldvc : 1));
+      }
+      auto* d_sc = static_cast<ScaleTask*>(upload(sc.data(), sizeof(ScaleTask) * sc.size()));
+      auto* d_se = static_cast<ScaleEdgeTask*>(upload(se.data(), sizeof(ScaleEdgeTask) * std::max<size_t>(se.size(), 1)));
+      auto* d_rt = static_cast<RrqrTask*>(upload(rt.data(), sizeof(RrqrTask) * rt.size()));
+      auto* d_rs = static_cast<RrqrSrc*>(upload(rs.data(), sizeof(RrqrSrc) * std::max<size_t>(rs.size(), 1)));
+      auto* d_sp = static_cast<SparsEdgeTask*>(upload(sp.data(), sizeof(SparsEdgeTask) * std::max<size_t>(sp.size(), 1)));
+      if (!d_sc || !d_se || !d_rt || !d_rs || !d_sp) return fail(-11, "out of device memory (sparsification)");
+      launch_scale(d_sc, (int)sc.size(), smax, stream_);
+      launch_scale_edge(d_se, (int)se.size(), kmax_se, stream_);
+      cudaEventRecord(ev[2], stream_);
+      launch_rrqr(d_rt, d_rs, (int)rt.size(), mmax, st_.tol, pivot_rtol, stream_);
+      launch_spars_edge(d_sp, (int)sp.size(), kmax_sp, stream_);
+      cudaEventRecord(ev[3], stream_);
+      if (check_cuda(cudaMemcpyAsync(host_rank.data(), d_rank_, sizeof(int) * host_rank.size(), cudaMemcpyDeviceToHost,
+                                     stream_),
+                     "rank readback") ||
+          check_cuda(cudaStreamSynchronize(stream_), "sparsification"))
+        return -10;
+      for (int p : Lv.spars_clusters) size_[p] = host_rank[p];
+      for (size_t q = 0; q < rt.size(); ++q) {
+        const double m = rt[q].m, w = rt[q].w, r = size_[Lv.spars_clusters[q]];
+        flops_ += 4.0 * m * w * r - 2.0 * r * r * (m + w) + 4.0 * r * r * r / 3.0 + m * r * r;
+      }
+      for (int e : Lv.spars_edges) {
+        rows_[e] = size_[st_.edges[e].n2];
+        cols_[e] = size_[st_.edges[e].n1];
+      }
+      lt_[lvl].nspars = (int)Lv.spars_clusters.size();
+    } else {
+      cudaEventRecord(ev[2], stream_);
+      cudaEventRecord(ev[3], stream_);
+    }
+    // ---------------- merge into the next level
+    if (lvl + 1 < L) {
+      const Level& N = st_.levels[lvl + 1];
+      for (int P = N.first; P < N.first + N.count; ++P) {
+        const Cluster& C = st_.clusters[P];
+        int off = 0;
+        for (int k = C.child_begin; k < C.child_end; ++k) {
+          const int ch = st_.children[k];
+          rpos_[ch] = off;
+          off += size_[ch];
+        }
+        size_[P] = size_org_[P] = off;
+      }
+      size_t region = 0;
+      for (int e : N.edges) {
+        const Edge& E = st_.edges[e];
+        rows_[e] = size_[E.n2];
+        cols_[e] = size_[E.n1];
+        ld_[e] = std::max(1, rows_[e]);
+        ptr_[e] = arena_.dalloc((size_t)ld_[e] * cols_[e]);
+        if (!ptr_[e]) return fail(-11, "out of device memory (level blocks)");
+        cudaMemsetAsync(ptr_[e], 0, sizeof(double) * (size_t)ld_[e] * cols_[e], stream_);
+        region += (size_t)ld_[e] * cols_[e];
+      }
+      (void)region;
+      std::vector<MergeTask> mt;
+      for (size_t q = 0; q < Lv.merge_src.size(); ++q) {
+        const int s = Lv.merge_src[q], d = Lv.merge_dst[q];
+        const Edge& E = st_.edges[s];
+        MergeTask t;
+        t.src = ptr_[s];
+        t.dst = ptr_[d];
+        t.ld_src = ld_[s];
+        t.ld_dst = ld_[d];
+        t.rows = size_[E.n2];
+        t.cols = size_[E.n1];
+        t.roff = rpos_[E.n2];
+        t.coff = rpos_[E.n1];
+        t.identity = (E.n1 == E.n2 && st_.clusters[E.n1].sparsify) ? 1 : 0;
+        if (t.rows > 0 && t.cols > 0) mt.push_back(t);
+      }
+      auto* d_mt = static_cast<MergeTask*>(upload(mt.data(), sizeof(MergeTask) * std::max<size_t>(mt.size(), 1)));
+      if (!d_mt) return fail(-11, "out of device memory (merge)");
+      launch_merge(d_mt, (int)mt.size(), stream_);
+    }
+    cudaEventRecord(ev[4], stream_);
+    if (check_cuda(cudaStreamSynchronize(stream_), "factorize level")) return -10;
+    cudaEventElapsedTime(&lt_[lvl].elim_ms, ev[0], ev[1]);
+    cudaEventElapsedTime(&lt_[lvl].scale_ms, ev[1], ev[2]);
+    cudaEventElapsedTime(&lt_[lvl].spars_ms, ev[2], ev[3]);
+    cudaEventElapsedTime(&lt_[lvl].merge_ms, ev[3], ev[4]);
+    scratch_.release();
+    if (verbose)
+      printf("%d    elim %.3f ms  scale %.3f ms  spars %.3f ms  merge %.3f ms  (interiors %zu, interfaces %zu)\n", lvl,
+             lt_[lvl].elim_ms, lt_[lvl].scale_ms, lt_[lvl].spars_ms, lt_[lvl].merge_ms, Lv.interiors.size(),
+             Lv.interfaces.size());
+  }
+  for (auto& e : ev) cudaEventDestroy(e);
+  factorized_ = true;
+  int rc = build_solve_graph();
+  if (rc) return rc;
+  t_factorize = wall() - t0;
+  if (verbose) {
+    printf("Tolerance set: %e\n", st_.tol);
+    printf("Time to factorize:  %g\n", t_factorize);
+  }
+  return 0;
+}
+
+// Cluster vectors: level-0 clusters at their permuted columns [0, n); every
+// later cluster gets its own segment of its level size.
+int Tree::build_solve_graph() {
+  const int L = st_.nlevels;
+  const int ncl = (int)st_.clusters.size();
+  xoff_.assign(ncl, 0);
+  int64_t off = st_.n;
+  const Level& L0 = st_.levels[0];
+  for (int o = L0.first; o < L0.first + L0.count; ++o) xoff_[o] = st_.clusters[o].cstart;
+  for (int o = L0.first + L0.count; o < ncl; ++o) {
+    xoff_[o] = off;
+    off += size_org_[o];
+  }
+  xw_size_ = off;
+  cudaFree(d_xw_);
+  cudaFree(d_turn_);
+  cudaFree(d_tickets_);
+  if (check_cuda(cudaMalloc(&d_xw_, sizeof(double) * std::max<int64_t>(xw_size_, 1)), "malloc") ||
+      check_cuda(cudaMalloc(&d_turn_, sizeof(int) * ncl), "malloc") ||
+      check_cuda(cudaMalloc(&d_tickets_, sizeof(int) * L), "malloc"))
+    return -10;
+  struct LevelSolve {
+    FwdElimTask* fe = nullptr;
+    FwdOut* fo = nullptr;
+    int nfe = 0, fe_nmax = 1, fe_mmax = 1;
+    FwdSparsTask* fs = nullptr;
+    int nfs = 0, fs_nmax = 1;
+    BwdElimTask* be = nullptr;
+    BwdIn* bi = nullptr;
+    int nbe = 0, be_nmax = 1;
+    int* gsrc = nullptr;
+    int* gdst = nullptr;
+    int ng = 0;
+  };
+  std::vector<LevelSolve> ls(L);
+  auto up = [&](const void* h, size_t bytes) -> void* {
+    void* d = arena_.alloc(std::max<size_t>(bytes, 1));
+    if (d && bytes) cudaMemcpyAsync(d, h, bytes, cudaMemcpyHostToDevice, stream_);
+    return d;
+  };
+  for (int lvl = 0; lvl < L; ++lvl) {
+    const Level& Lv = st_.levels[lvl];
+    LevelSolve& S = ls[lvl];
+    // turn order per neighbour: interiors ascending
+    std::vector<int> seen(Lv.count, 0);
+    std::vector<FwdElimTask> fe;
+    std::vector<FwdOut> fo;
+    for (size_t ii = 0; ii < Lv.interiors.size(); ++ii) {
+      const int c = Lv.interiors[ii];
+      FwdElimTask t;
+      t.S = ptr_[Lv.self_edge_of[c - Lv.first]];
+      t.T = T_[c];
+      t.x = d_xw_ + xoff_[c];
+      t.n = size_[c];
+      t.out_begin = (int)fo.size();
+      for (int q = Lv.out_begin[ii]; q < Lv.out_end[ii]; ++q) {
+        const int e = Lv.out_edges[q];
+        const int nb = st_.edges[e].n2;
+        FwdOut o;
+        o.V = ptr_[e];
+        o.T = tsqrtT_[e];
+        o.xn = d_xw_ + xoff_[nb];
+        o.turn = d_turn_ + nb;
+        o.m = rows_[e];
+        o.my_turn = seen[nb - Lv.first]++;
+        fo.push_back(o);
+        S.fe_mmax = std::max(S.fe_mmax, o.m);
+      }
+      t.out_end = (int)fo.size();
+      fe.push_back(t);
+      S.fe_nmax = std::max(S.fe_nmax, t.n);
+    }
+    std::vector<FwdSparsTask> fs;
+    for (int p : Lv.spars_clusters) {
+      FwdSparsTask t;
+      t.Qs = ptr_[Lv.self_edge_of[p - Lv.first]];
+      t.Ts = Ts_[p];
+      t.V = Qsp_[p];
+      t.T = Tsp_[p];
+      t.rank = d_rank_ + p;
+      t.x = d_xw_ + xoff_[p];
+      t.n = size_org_[p];
+      fs.push_back(t);
+      S.fs_nmax = std::max(S.fs_nmax, t.n);
+    }
+    std::vector<BwdElimTask> be;
+    std::vector<BwdIn> bi;
+    for (size_t ii = 0; ii < Lv.interiors.size(); ++ii) {
+      const int c = Lv.interiors[ii];
+      BwdElimTask t;
+      t.S = ptr_[Lv.self_edge_of[c - Lv.first]];
+      t.x = d_xw_ + xoff_[c];
+      t.n = size_[c];
+      t.in_begin = (int)bi.size();
+      for (int q = Lv.in_begin[ii]; q < Lv.in_end[ii]; ++q) {
+        const int e = Lv.in_edges[q];
+        BwdIn b;
+        b.R = ptr_[e];
+        b.ldr = ld_[e];
+        b.s = cols_[e];
+        b.xm = d_xw_ + xoff_[st_.edges[e].n1];
+        bi.push_back(b);
+      }
+      t.in_end = (int)bi.size();
+      be.push_back(t);
+      S.be_nmax = std::max(S.be_nmax, t.n);
+    }
+    std::vector<int> gs, gd;
+    if (lvl + 1 < L) {
+      const Level& N = st_.levels[lvl + 1];
+      for (int P = N.first; P < N.first + N.count; ++P) {
+        const Cluster& C = st_.clusters[P];
+        for (int k = C.child_begin; k < C.child_end; ++k) {
+          const int ch = st_.children[k];
+          for (int i = 0; i < size_[ch]; ++i) {
+            gs.push_back((int)(xoff_[ch] + i));
+            gd.push_back((int)(xoff_[P] + rpos_[ch] + i));
+          }
+        }
+      }
+    }
+    S.nfe = (int)fe.size();
+    S.nfs = (int)fs.size();
+    S.nbe = (int)be.size();
+    S.ng = (int)gs.size();
+    S.fe = static_cast<FwdElimTask*>(up(fe.data(), sizeof(FwdElimTask) * fe.size()));
+    S.fo = static_cast<FwdOut*>(up(fo.data(), sizeof(FwdOut) * fo.size()));
+    S.fs = static_cast<FwdSparsTask*>(up(fs.data(), sizeof(FwdSparsTask) * fs.size()));
+    S.be = static_cast<BwdElimTask*>(up(be.data(), sizeof(BwdElimTask) * be.size()));
+    S.bi = static_cast<BwdIn*>(up(bi.data(), sizeof(BwdIn) * bi.size()));
+    S.gsrc = static_cast<int*>(up(gs.data(), sizeof(int) * gs.size()));
+    S.gdst = static_cast<int*>(up(gd.data(), sizeof(int) * gd.size()));
+    if (!S.fe || !S.fo || !S.fs || !S.be || !S.bi || !S.gsrc || !S.gdst)
+      return fail(-11, "out of device memory (solve descriptors)");
+  }
+  if (check_cuda(cudaStreamSynchronize(stream_), "solve descriptors")) return -10;
+  // capture the sweep
+  if (solve_exec_) {
+    cudaGraphExecDestroy(solve_exec_);
+    cudaGraphDestroy(solve_graph_);
+    solve_exec_ = nullptr;
+  }
+  if (check_cuda(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal), "capture")) return -10;
+  cudaMemsetAsync(d_turn_, 0, sizeof(int) * ncl, stream_);
+  cudaMemsetAsync(d_tickets_, 0, sizeof(int) * L, stream_);
+  for (int lvl = 0; lvl < L; ++lvl) {
+    LevelSolve& S = ls[lvl];
+    launch_fwd_elim(S.fe, S.fo, S.nfe, S.fe_nmax, S.fe_mmax, d_tickets_ + lvl, d_status_, kSpinLimit, stream_);
+    launch_fwd_spars(S.fs, S.nfs, S.fs_nmax, stream_);
+    launch_copy_idx(S.ng, S.gsrc, S.gdst, d_xw_, stream_);
+  }
+  for (int lvl = L - 1; lvl >= 0; --lvl) {
+    LevelSolve& S = ls[lvl];
+    launch_bwd_spars(S.fs, S.nfs, S.fs_nmax, stream_);
+    launch_bwd_elim(S.be, S.bi, S.nbe, S.be_nmax, stream_);
+    if (lvl > 0) launch_copy_idx(ls[lvl - 1].ng, ls[lvl - 1].gdst, ls[lvl - 1].gsrc, d_xw_, stream_);
+  }
+  cudaError_t ce = cudaStreamEndCapture(stream_, &solve_graph_);
+  if (check_cuda(ce, "end capture")) return -10;
+  if (check_cuda(cudaGraphInstantiate(&solve_exec_, solve_graph_, 0), "instantiate")) return -10;
+  return 0;
+}
+
+int Tree::solve_device(double* x) {
+  if (!factorized_) return fail(-4, "solve called before factorize");
+  const int n = st_.n;
+  cudaMemcpyAsync(d_xw_, x, sizeof(double) * n, cudaMemcpyDeviceToDevice, stream_);
+  if (check_cuda(cudaGraphLaunch(solve_exec_, stream_), "solve graph")) return -10;
+  cudaMemcpyAsync(x, d_xw_, sizeof(double) * n, cudaMemcpyDeviceToDevice, stream_);
+  return 0;
+}
+
+int Tree::solve_host(double* x) {
+  double t0 = wall();
+  const int n = st_.n;
+  if (!factorized_) return fail(-4, "solve called before factorize");
+  cudaMemcpyAsync(d_tmp_, x, sizeof(double) * n, cudaMemcpyHostToDevice, stream_);
+  int rc = solve_device(d_tmp_);
+  if (rc) return rc;
+  cudaMemcpyAsync(x, d_tmp_, sizeof(double) * n, cudaMemcpyDeviceToHost, stream_);
+  if (check_cuda(cudaStreamSynchronize(stream_), "solve")) return -10;
+  if (device_status() != 0) return fail(-12, "forward sweep wait timed out on the device");
+  t_solve = wall() - t0;
+  return 0;
+}
+
+int Tree::solve_global(const double* b, double* x) {
+  const int n = st_.n;
+  std::vector<double> t(n);
+  for (int i = 0; i < n; ++i) t[i] = b[st_.rperm[i]];
+  int rc = solve_host(t.data());
+  if (rc) return rc;
+  for (int i = 0; i < n; ++i) x[st_.cperm[i]] = t[i];
+  return 0;
+}
+
+int Tree::spmv_device(const double* x, double* y) {
+  if (!assembled_) return fail(-4, "spmv called before assemble");
+  launch_spmv(st_.n, d_rowptr_, d_col_, d_val_, x, y, stream_);
+  return 0;
+}
+
+int Tree::spmv_host(const double* x, double* y) {
+  const int n = st_.n;
+  if (!assembled_) return fail(-4, "spmv called before assemble");
+  cudaMemcpyAsync(d_tmp_, x, sizeof(double) * n, cudaMemcpyHostToDevice, stream_);
+  spmv_device(d_tmp_, d_tmp_ + n);
+  cudaMemcpyAsync(y, d_tmp_ + n, sizeof(double) * n, cudaMemcpyDeviceToHost, stream_);
+  return check_cuda(cudaStreamSynchronize(stream_), "spmv");
+}
+
+// is.cpp:447-527: left-preconditioned, unrestarted GMRES with MGS Arnoldi,
+// x0 = 0, stopping on the preconditioned residual |beta(k+1)|/||M^-1 b||.
+// On exit b holds the solution; relres is the true ||b - A x|| / ||b||.
+int Tree::gmres_device(double* b, int maxit, double gtol, int* iters, double* relres, double* hist, int hist_cap) {
+  if (!factorized_) return fail(-4, "gmres called before factorize");
+  if (maxit < 1) return fail(-1, "maxit must be >= 1");
+  double t0 = wall();
+  const int n = st_.n;
+  const size_t ldq = (size_t)n;
+  double *Q = nullptr, *q = nullptr, *bsave = nullptr, *hcol = nullptr, *partial = nullptr;
+  unsigned int* done = nullptr;
+  const int grid = mgs_grid(n);
+  if (check_cuda(cudaMalloc(&Q, sizeof(double) * ldq * (maxit + 1)), "malloc Krylov basis") ||
+      check_cuda(cudaMalloc(&q, sizeof(double) * n), "malloc") ||
+      check_cuda(cudaMalloc(&bsave, sizeof(double) * n), "malloc") ||
+      check_cuda(cudaMalloc(&hcol, sizeof(double) * (maxit + 3)), "malloc") ||
+      check_cuda(cudaMalloc(&partial, sizeof(double) * grid), "malloc") ||
+      check_cuda(cudaMalloc(&done, sizeof(unsigned int)), "malloc")) {
+    cudaFree(Q);
+    cudaFree(q);
+    cudaFree(bsave);
+    cudaFree(hcol);
+    cudaFree(partial);
+    cudaFree(done);
+    return -10;
+  }
+  cudaMemsetAsync(done, 0, sizeof(unsigned int), stream_);
+  cudaMemcpyAsync(bsave, b, sizeof(double) * n, cudaMemcpyDeviceToDevice, stream_);
+  cudaMemcpyAsync(q, b, sizeof(double) * n, cudaMemcpyDeviceToDevice, stream_);
+  solve_device(q);
+  launch_mgs_step(n, q, nullptr, nullptr, nullptr, partial, done, hcol, 1, stream_);  // ||r||
+  launch_scale_copy(n, q, hcol, Q, stream_);
+  double r_norm = 0;
+  cudaMemcpyAsync(&r_norm, hcol, sizeof(double), cudaMemcpyDeviceToHost, stream_);
+  int rc = check_cuda(cudaStreamSynchronize(stream_), "gmres start");
+  std::vector<double> H((size_t)(maxit + 1) * maxit, 0.0), cs(maxit, 0.0), sn(maxit, 0.0), beta(maxit + 1, 0.0);
+  auto Hc = [&](int i, int j) -> double& { return H[(size_t)j * (maxit + 1) + i]; };
+  beta[0] = r_norm;
+  int k = 0;
+  std::vector<double> hk(maxit + 2);
+  int nh = 0;
+  if (!rc && (std::isnan(r_norm) || device_status() != 0)) rc = fail(-12, "preconditioner apply failed");
+  for (; !rc && k < maxit; ++k) {
+    spmv_device(Q + (size_t)k * ldq, q);
+    solve_device(q);
+    for (int i = 0; i <= k; ++i)
+      launch_mgs_step(n, q, i ? Q + (size_t)(i - 1) * ldq : nullptr, i ? hcol + (i - 1) : nullptr, Q + (size_t)i * ldq,
+                      partial, done, hcol + i, 0, stream_);
+    launch_mgs_step(n, q, Q + (size_t)k * ldq, hcol + k, nullptr, partial, done, hcol + k + 1, 1, stream_);
+    launch_scale_copy(n, q, hcol + k + 1, Q + (size_t)(k + 1) * ldq, stream_);
+    cudaMemcpyAsync(hk.data(), hcol, sizeof(double) * (k + 2), cudaMemcpyDeviceToHost, stream_);
+    if ((rc = check_cuda(cudaStreamSynchronize(stream_), "gmres iteration"))) break;
+    for (int i = 0; i <= k + 1; ++i) Hc(i, k) = hk[i];
+    for (int i = 0; i < k; ++i) {
+      const double temp = cs[i] * Hc(i, k) + sn[i] * Hc(i + 1, k);
+      Hc(i + 1, k) = -sn[i] * Hc(i, k) + cs[i] * Hc(i + 1, k);
+      Hc(i, k) = temp;
+    }
+    if (Hc(k, k) == 0) {
+      cs[k] = 0;
+      sn[k] = 1;
+    } else {
+      const double t = std::sqrt(Hc(k, k) * Hc(k, k) + Hc(k + 1, k) * Hc(k + 1, k));
+      cs[k] = std::fabs(Hc(k, k)) / t;
+      sn[k] = cs[k] * Hc(k + 1, k) / Hc(k, k);
+    }
+    Hc(k, k) = cs[k] * Hc(k, k) + sn[k] * Hc(k + 1, k);
+    Hc(k + 1, k) = 0.0;
+    beta[k + 1] = -sn[k] * beta[k];
+    beta[k] = cs[k] * beta[k];
+    const double err = std::fabs(beta[k + 1]) / r_norm;
+    if (hist && nh < hist_cap) hist[nh++] = err;
+    if (verbose) printf("GMRES: error at step %d is %e\n", k, err);
+    if (err <= gtol) break;
+  }
+  if (!rc) {
+    if (device_status() != 0) rc = fail(-12, "forward sweep wait timed out on the device");
+  }
+  if (!rc) {
+    k = std::min(k, maxit - 1);
+    std::vector<double> y(k + 1, 0.0);  // util.cpp:1019-1032 LUSolve
+    for (int i = k; i >= 0; --i) {
+      y[i] = beta[i];
+      for (int j = i + 1; j < k + 1; ++j) y[i] -= Hc(i, j) * y[j];
+      y[i] /= Hc(i, i);
+    }
+    double* dy = hcol;
+    cudaMemcpyAsync(dy, y.data(), sizeof(double) * (k + 1), cudaMemcpyHostToDevice, stream_);
+    launch_combine(n, k + 1, Q, ldq, dy, b, stream_);
+    spmv_device(b, q);
+    launch_sub(n, bsave, q, q, stream_);
+    launch_mgs_step(n, q, nullptr, nullptr, nullptr, partial, done, hcol, 1, stream_);
+    launch_mgs_step(n, bsave, nullptr, nullptr, nullptr, partial, done, hcol + 1, 1, stream_);
+    double nr[2];
+    cudaMemcpyAsync(nr, hcol, sizeof(double) * 2, cudaMemcpyDeviceToHost, stream_);
+    rc = check_cuda(cudaStreamSynchronize(stream_), "gmres finish");
+    *iters = k;
+    *relres = nr[0] / nr[1];
+    last_gmres_iters = k;
+  }
+  cudaFree(Q);
+  cudaFree(q);
+  cudaFree(bsave);
+  cudaFree(hcol);
+  cudaFree(partial);
+  cudaFree(done);
+  t_gmres = wall() - t0;
+  return rc;
+}
+
+int Tree::gmres_host(double* b, int maxit, double gtol, int* iters, double* relres, double* hist, int hist_cap) {
+  const int n = st_.n;
+  if (!factorized_) return fail(-4, "gmres called before factorize");
+  double* d = nullptr;
+  if (check_cuda(cudaMalloc(&d, sizeof(double) * n), "malloc")) return -10;
+  cudaMemcpyAsync(d, b, sizeof(double) * n, cudaMemcpyHostToDevice, stream_);
+  int rc = gmres_device(d, maxit, gtol, iters, relres, hist, hist_cap);
+  if (!rc) {
+    cudaMemcpyAsync(b, d, sizeof(double) * n, cudaMemcpyDeviceToHost, stream_);
+    rc = check_cuda(cudaStreamSynchronize(stream_), "gmres copy-out");
+  }
+  cudaFree(d);
+  return rc;
+}
+
+int Tree::get_block(int n1, int n2, double* out, int* rows, int* cols, int* ld) const {
+  const int e = st_.find_edge(n1, n2);
+  if (e < 0 || e >= (int)ptr_.size() || !ptr_[e]) return -1;
+  *rows = rows_[e];
+  *cols = cols_[e];
+  *ld = ld_[e];
+  if (out) cudaMemcpy(out, ptr_[e], sizeof(double) * (size_t)ld_[e] * cols_[e], cudaMemcpyDeviceToHost);
+  return 0;
+}
+
+// which: 0 = T of an interior's diagonal QR (n x n), 1 = scaling T (n x n),
+// 2 = sparsification reflectors V (n x rank), 3 = their T (rank x rank).
+int Tree::get_factor(int order, int which, double* out, int* shape) const {
+  if (!factorized_ || order < 0 || order >= (int)size_.size()) return -4;
+  const double* p = nullptr;
+  int r = 0, c = 0, ld = 0;
+  const int n = size_org_[order];
+  switch (which) {
+    case 0: p = T_[order]; r = c = ld = n; break;
+    case 1: p = Ts_[order]; r = c = ld = n; break;
+    case 2: p = Qsp_[order]; r = ld = n; c = size_[order]; break;
+    case 3: p = Tsp_[order]; r = c = size_[order]; ld = n; break;
+    default: return -1;
+  }
+  if (!p) return -1;
+  shape[0] = r;
+  shape[1] = c;
+  shape[2] = ld;
+  if (out)
+    for (int j = 0; j < c; ++j) cudaMemcpy(out + (size_t)j * r, p + (size_t)j * ld, sizeof(double) * r, cudaMemcpyDeviceToHost);
+  return 0;
+}
+
+}  // namespace spq

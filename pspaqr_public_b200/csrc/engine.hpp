@@ -1,0 +1,138 @@
+// engine.hpp -- the device factorization engine behind the C ABI.
+//
+// Tree owns one CUDA stream, a block arena in HBM and the symbolic structure.
+// factorize() runs the level loop: per level the host plans task descriptors
+// for the sizes it knows (level-0 sizes are static; later sizes follow from
+// the ranks read back after the previous level's sparsification), uploads
+// them in one copy and launches the grouped kernels.  The preconditioner apply
+// is captured once into a CUDA graph after the factorization.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "structure.hpp"
+#include "tasks.hpp"
+
+namespace spq {
+
+// Bump allocator over large cudaMalloc'd chunks.
+class Arena {
+ public:
+  ~Arena();
+  void* alloc(size_t bytes);
+  double* dalloc(size_t n) { return static_cast<double*>(alloc(n * sizeof(double))); }
+  void release();
+  size_t used() const { return used_; }
+  size_t reserved() const { return reserved_; }
+
+ private:
+  struct Chunk {
+    char* base;
+    size_t size, off;
+  };
+  std::vector<Chunk> chunks_;
+  size_t used_ = 0, reserved_ = 0;
+};
+
+struct LevelTiming {
+  float elim_ms = 0, scale_ms = 0, spars_ms = 0, merge_ms = 0;
+  int ntasks_elim = 0, ntasks_upd = 0, nspars = 0;
+};
+
+class Tree {
+ public:
+  Tree(int nlevels, int skip);
+  ~Tree();
+
+  // settings (ParTree setters, ptree.h:122-127 / tree.h:299-305)
+  int nlevels, skip;
+  double tol = 1e-1;
+  int scale = 1, hsl = 0, nthreads = 1, verbose = 0, ttor_log = 0, square = 1;
+  float order = 1.0f;
+  // RRQR pivot: first column whose partial norm is within pivot_rtol of the
+  // largest (0 = LAPACK's first maximum).  Equal norms in exact arithmetic
+  // (symmetric stencils) are otherwise resolved by rounding noise.
+  double pivot_rtol = 1e-6;
+
+  int set_coords(int dim, int n, const double* X);
+  int set_coords_tensor(int n, int d);
+  int partition(int nrows, int ncols, const int* colptr, const int* rowidx, const double* val);
+  int assemble();
+  int factorize();
+  // preconditioner apply, x in permuted order (device or host pointer)
+  int solve_device(double* x);
+  int solve_host(double* x);
+  int solve_global(const double* b, double* x);
+  int spmv_device(const double* x, double* y);
+  int spmv_host(const double* x, double* y);
+  int gmres_host(double* b, int maxit, double tol, int* iters, double* relres, double* hist, int hist_cap);
+  int gmres_device(double* b_dev, int maxit, double tol, int* iters, double* relres, double* hist, int hist_cap);
+
+  int set_stream(cudaStream_t s);
+  cudaStream_t stream() const { return stream_; }
+
+  // introspection
+  int n() const { return st_.n; }
+  const Structure& structure() const { return st_; }
+  std::vector<int> cluster_sizes() const { return size_; }
+  std::vector<int> cluster_sizes_org() const { return size_org_; }
+  int get_block(int n1, int n2, double* out, int* rows, int* cols, int* ld) const;
+  int get_factor(int order, int which, double* out, int* shape) const;
+  const std::vector<LevelTiming>& level_timing() const { return lt_; }
+  double t_partition = 0, t_assemble = 0, t_factorize = 0, t_solve = 0, t_gmres = 0;
+  int last_gmres_iters = 0;
+  std::string error;
+  size_t pool_bytes() const { return arena_.used(); }
+  double factor_flops() const { return flops_; }
+  int device_status();
+
+ private:
+  int fail(int code, const std::string& msg) {
+    error = msg;
+    return code;
+  }
+  int check_cuda(cudaError_t e, const char* where);
+  void* upload(const void* host, size_t bytes);   // into the per-level scratch arena
+  int build_solve_graph();
+
+  Structure st_;
+  Csc A_;
+  std::vector<double> X_;
+  int dim_ = 0;
+  bool partitioned_ = false, assembled_ = false, factorized_ = false;
+
+  cudaStream_t stream_ = nullptr;
+  bool own_stream_ = false;
+  Arena arena_;        // blocks and factors (lives until destruction)
+  Arena scratch_;      // descriptors of the factorization (released after it)
+
+  // per cluster
+  std::vector<int> size_, size_org_, rpos_;
+  std::vector<double*> T_, Ts_, Qsp_, Tsp_;
+  std::vector<int64_t> xoff_;
+  int* d_rank_ = nullptr;
+  // per edge
+  std::vector<double*> ptr_;
+  std::vector<int> ld_, rows_, cols_;
+  std::vector<double*> tsqrtT_;  // per out-edge of an interior: T of the chain step
+
+  // device copies for SpMV / GMRES
+  int* d_rowptr_ = nullptr;
+  int* d_col_ = nullptr;
+  double* d_val_ = nullptr;
+  double* d_xw_ = nullptr;     // solve workspace (all cluster vectors)
+  int64_t xw_size_ = 0;
+  int* d_turn_ = nullptr;      // per cluster turn counters
+  int* d_tickets_ = nullptr;   // per level
+  int* d_status_ = nullptr;
+  cudaGraphExec_t solve_exec_ = nullptr;
+  cudaGraph_t solve_graph_ = nullptr;
+  double* d_tmp_ = nullptr;    // 2 vectors for host-pointer entry points
+  std::vector<LevelTiming> lt_;
+  double flops_ = 0;
+};
+
+}  // namespace spq

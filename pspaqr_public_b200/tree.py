@@ -1,0 +1,332 @@
+"""Python mirror of the reference ParTree API over the C ABI (ctypes).
+
+``ParTree`` keeps the reference's call sequence and setter names
+(ptree.h:122-160, tree.h:299-305): construct with ``(nlevels, skip)``, set
+options, ``partition(A)`` -> ``assemble(A)`` -> ``factorize()`` ->
+``solve(...)``; ``dist_gmres`` mirrors is.cpp:447-527.  All numerics run in
+``libspaqr_b200.so`` on the GPU; there is no CPU fallback -- a missing or
+unloadable library raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from typing import Optional
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libspaqr_b200.so")
+_lib = None
+
+
+class SpqError(RuntimeError):
+    def __init__(self, what: str, status: int, msg: str):
+        super().__init__(f"{what} failed (status {status}): {msg}")
+        self.status = status
+
+
+def lib():
+    """Load the CUDA library (raises if it was not built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"{LIB_PATH} is missing: run `python -m pspaqr_public_b200.build` first")
+        L = C.CDLL(LIB_PATH)
+        vp, i32, f64, f32 = C.c_void_p, C.c_int, C.c_double, C.c_float
+        pi, pd, pf = C.POINTER(C.c_int), C.POINTER(C.c_double), C.POINTER(C.c_float)
+        sig = {
+            "spq_create": (i32, [i32, i32, C.POINTER(vp)]),
+            "spq_destroy": (i32, [vp]),
+            "spq_set_tol": (i32, [vp, f64]),
+            "spq_set_skip": (i32, [vp, i32]),
+            "spq_set_scale": (i32, [vp, i32]),
+            "spq_set_order": (i32, [vp, f32]),
+            "spq_set_hsl": (i32, [vp, i32]),
+            "spq_set_nthreads": (i32, [vp, i32]),
+            "spq_set_verbose": (i32, [vp, i32]),
+            "spq_set_ttor_log": (i32, [vp, i32]),
+            "spq_set_square": (i32, [vp, i32]),
+            "spq_set_pivot_rtol": (i32, [vp, f64]),
+            "spq_get_factor": (i32, [vp, i32, i32, pd, pi]),
+            "spq_set_coords": (i32, [vp, i32, i32, pd]),
+            "spq_set_coords_tensor": (i32, [vp, i32, i32]),
+            "spq_partition": (i32, [vp, i32, i32, pi, pi, pd]),
+            "spq_assemble": (i32, [vp]),
+            "spq_factorize": (i32, [vp]),
+            "spq_solve_inplace": (i32, [vp, pd]),
+            "spq_solve_inplace_device": (i32, [vp, vp]),
+            "spq_solve_global": (i32, [vp, pd, pd]),
+            "spq_spmv": (i32, [vp, pd, pd]),
+            "spq_gmres": (i32, [vp, pd, i32, f64, pi, pd, pd, i32]),
+            "spq_gmres_device": (i32, [vp, vp, i32, f64, pi, pd, pd, i32]),
+            "spq_distribute_x": (i32, [vp, pd, pd]),
+            "spq_extract_x": (i32, [vp, pd, pd]),
+            "spq_n": (i32, [vp]),
+            "spq_set_stream": (i32, [vp, vp]),
+            "spq_scale_columns": (i32, [i32, pi, pd]),
+            "spq_random_reference": (i32, [i32, i32, pd]),
+            "spq_get_perm": (i32, [vp, pi]),
+            "spq_num_clusters": (i32, [vp]),
+            "spq_num_levels": (i32, [vp]),
+            "spq_cluster_info": (i32, [vp, i32, pi]),
+            "spq_level_range": (i32, [vp, i32, pi, pi]),
+            "spq_num_edges": (i32, [vp]),
+            "spq_find_edge": (i32, [vp, i32, i32]),
+            "spq_get_block": (i32, [vp, i32, i32, pd, pi]),
+            "spq_times": (i32, [vp, pd]),
+            "spq_level_times": (i32, [vp, pf]),
+            "spq_factor_flops": (f64, [vp]),
+            "spq_pool_bytes": (f64, [vp]),
+            "spq_last_error": (C.c_char_p, [vp]),
+        }
+        for name, (res, args) in sig.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+def _pi(a):
+    return a.ctypes.data_as(C.POINTER(C.c_int))
+
+
+def _pd(a):
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def as_csc(A):
+    """Accept a scipy sparse matrix or a (colptr, rowidx, values) triple."""
+    if isinstance(A, tuple):
+        colptr, rowidx, vals = A
+        n = len(colptr) - 1
+        return (np.ascontiguousarray(colptr, np.int32), np.ascontiguousarray(rowidx, np.int32),
+                np.ascontiguousarray(vals, np.float64), n, n)
+    import scipy.sparse as sp
+
+    A = sp.csc_matrix(A)
+    A.sort_indices()
+    return (A.indptr.astype(np.int32), A.indices.astype(np.int32), A.data.astype(np.float64), A.shape[0], A.shape[1])
+
+
+def scale_columns(colptr, vals):
+    """The driver's column scaling (pspaQR.cpp:133-146), computed by the library."""
+    colptr = np.ascontiguousarray(colptr, np.int32)
+    out = np.array(vals, dtype=np.float64, copy=True)
+    rc = lib().spq_scale_columns(len(colptr) - 1, _pi(colptr), _pd(out))
+    if rc:
+        raise SpqError("scale_columns", rc, "bad arguments")
+    return out
+
+
+def random_reference(n: int, seed: int) -> np.ndarray:
+    """util.cpp:992-1001 ``random(size, seed)``: mt19937, U(-1, 1)."""
+    out = np.empty(n)
+    lib().spq_random_reference(n, seed, _pd(out))
+    return out
+
+
+INFO_FIELDS = ("lvl", "merge_lvl", "size", "rank", "parent", "cstart", "sep", "l_lvl", "l_sep", "r_lvl", "r_sep",
+               "section", "size_org", "sparsify", "nchildren", "interior")
+
+
+class ParTree:
+    """GPU ParTree: same construction, setters and call order as the reference."""
+
+    def __init__(self, nlevels: int, skip: int = 0):
+        h = C.c_void_p()
+        rc = lib().spq_create(nlevels, skip, C.byref(h))
+        if rc:
+            raise SpqError("ParTree", rc, "nlevels must be >= 2 and skip >= 0")
+        self._h = h
+        self.nlevels = nlevels
+        self._A = None
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().spq_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+    def _chk(self, rc: int, what: str):
+        if rc != 0:
+            raise SpqError(what, rc, (lib().spq_last_error(self._h) or b"").decode())
+
+    # -- setters (tree.cpp:14-21, ptree.cpp:21-23)
+    def set_tol(self, tol: float):
+        self._chk(lib().spq_set_tol(self._h, tol), "set_tol")
+
+    def set_skip(self, s: int):
+        self._chk(lib().spq_set_skip(self._h, s), "set_skip")
+
+    def set_scale(self, s: int):
+        self._chk(lib().spq_set_scale(self._h, s), "set_scale")
+
+    def set_order(self, o: float):
+        self._chk(lib().spq_set_order(self._h, o), "set_order")
+
+    def set_hsl(self, h: int):
+        self._chk(lib().spq_set_hsl(self._h, h), "set_hsl")
+
+    def set_nthreads(self, n: int):
+        self._chk(lib().spq_set_nthreads(self._h, n), "set_nthreads")
+
+    def set_verbose(self, v: int):
+        self._chk(lib().spq_set_verbose(self._h, v), "set_verbose")
+
+    def set_ttor_log(self, l: int):
+        self._chk(lib().spq_set_ttor_log(self._h, l), "set_ttor_log")
+
+    def set_square(self, s: int):
+        self._chk(lib().spq_set_square(self._h, s), "set_square")
+
+    def set_pivot_rtol(self, r: float):
+        self._chk(lib().spq_set_pivot_rtol(self._h, r), "set_pivot_rtol")
+
+    def set_Xcoo(self, X: np.ndarray):
+        """Coordinates as a dim x n array (tree.cpp:21)."""
+        X = np.asfortranarray(X, dtype=np.float64)
+        self._chk(lib().spq_set_coords(self._h, X.shape[0], X.shape[1], _pd(X)), "set_Xcoo")
+
+    def set_coords_tensor(self, n: int, d: int):
+        """linspace_nd(n, d) coordinates (util.cpp:901-930)."""
+        self._chk(lib().spq_set_coords_tensor(self._h, n, d), "set_coords_tensor")
+
+    def set_stream(self, stream_ptr: int):
+        self._chk(lib().spq_set_stream(self._h, C.c_void_p(stream_ptr)), "set_stream")
+
+    # -- pipeline
+    def partition(self, A):
+        colptr, rowidx, vals, nr, nc = as_csc(A)
+        self._A = (colptr, rowidx, vals)
+        self._chk(lib().spq_partition(self._h, nr, nc, _pi(colptr), _pi(rowidx), _pd(vals)), "partition")
+
+    def assemble(self, A=None):
+        self._chk(lib().spq_assemble(self._h), "assemble")
+
+    def factorize(self) -> int:
+        self._chk(lib().spq_factorize(self._h), "factorize")
+        return 0
+
+    def solve(self, b: np.ndarray, x: Optional[np.ndarray] = None) -> np.ndarray:
+        """One-shot solve with a global right-hand side (ptree.cpp:2268-2785)."""
+        b = np.ascontiguousarray(b, np.float64)
+        out = np.zeros_like(b) if x is None else x
+        self._chk(lib().spq_solve_global(self._h, _pd(b), _pd(out)), "solve")
+        return out
+
+    def solve_inplace(self, x: np.ndarray) -> np.ndarray:
+        """Preconditioner apply on a permuted local vector (ptree.cpp:2788-3210)."""
+        if x.dtype != np.float64 or not x.flags.c_contiguous:
+            raise TypeError("x must be a contiguous float64 array")
+        self._chk(lib().spq_solve_inplace(self._h, _pd(x)), "solve")
+        return x
+
+    def solve_inplace_device(self, ptr: int):
+        self._chk(lib().spq_solve_inplace_device(self._h, C.c_void_p(ptr)), "solve")
+
+    def spmv(self, x: np.ndarray) -> np.ndarray:
+        x = np.ascontiguousarray(x, np.float64)
+        y = np.empty_like(x)
+        self._chk(lib().spq_spmv(self._h, _pd(x), _pd(y)), "spmv")
+        return y
+
+    def nrows_local(self) -> int:
+        return lib().spq_n(self._h)
+
+    def ncols_local(self) -> int:
+        return lib().spq_n(self._h)
+
+    def distribute_x(self, x: np.ndarray, x_dist: np.ndarray):
+        x = np.ascontiguousarray(x, np.float64)
+        self._chk(lib().spq_distribute_x(self._h, _pd(x), _pd(x_dist)), "distribute_x")
+
+    def extract_x(self, x_local: np.ndarray) -> np.ndarray:
+        x_local = np.ascontiguousarray(x_local, np.float64)
+        out = np.empty_like(x_local)
+        self._chk(lib().spq_extract_x(self._h, _pd(x_local), _pd(out)), "extract_x")
+        return out
+
+    # -- introspection
+    def perm(self) -> np.ndarray:
+        p = np.empty(self.nrows_local(), np.int32)
+        self._chk(lib().spq_get_perm(self._h, _pi(p)), "perm")
+        return p
+
+    def num_clusters(self) -> int:
+        return lib().spq_num_clusters(self._h)
+
+    def level_range(self, lvl: int):
+        f, c = C.c_int(), C.c_int()
+        self._chk(lib().spq_level_range(self._h, lvl, C.byref(f), C.byref(c)), "level_range")
+        return f.value, c.value
+
+    def cluster(self, order: int) -> dict:
+        info = np.zeros(16, np.int32)
+        self._chk(lib().spq_cluster_info(self._h, order, _pi(info)), "cluster_info")
+        return dict(zip(INFO_FIELDS, info.tolist()))
+
+    def clusters(self):
+        return [self.cluster(o) for o in range(self.num_clusters())]
+
+    def num_edges(self) -> int:
+        return lib().spq_num_edges(self._h)
+
+    def find_edge(self, n1: int, n2: int) -> int:
+        return lib().spq_find_edge(self._h, n1, n2)
+
+    def block(self, n1: int, n2: int):
+        shape = np.zeros(3, np.int32)
+        if lib().spq_get_block(self._h, n1, n2, None, _pi(shape)) != 0:
+            return None
+        r, c, ld = (int(v) for v in shape)
+        buf = np.zeros(max(ld * c, 1))
+        lib().spq_get_block(self._h, n1, n2, _pd(buf), _pi(shape))
+        return buf[: ld * c].reshape(c, ld).T[:r, :]
+
+    def factor(self, order: int, which: int):
+        """0: diagonal-QR T, 1: scaling T, 2: sparsification V, 3: its T (None if absent)."""
+        shape = np.zeros(3, np.int32)
+        if lib().spq_get_factor(self._h, order, which, None, _pi(shape)) != 0:
+            return None
+        r, c = int(shape[0]), int(shape[1])
+        buf = np.zeros(max(r * c, 1))
+        lib().spq_get_factor(self._h, order, which, _pd(buf), _pi(shape))
+        return buf[: r * c].reshape(c, r).T
+
+    def times(self) -> dict:
+        t = np.zeros(5)
+        lib().spq_times(self._h, _pd(t))
+        return dict(zip(("partition", "assemble", "factorize", "solve", "gmres"), t.tolist()))
+
+    def level_times(self) -> np.ndarray:
+        out = np.zeros(4 * self.nlevels, np.float32)
+        lib().spq_level_times(self._h, out.ctypes.data_as(C.POINTER(C.c_float)))
+        return out.reshape(self.nlevels, 4)
+
+    def factor_flops(self) -> float:
+        return lib().spq_factor_flops(self._h)
+
+    def pool_bytes(self) -> float:
+        return lib().spq_pool_bytes(self._h)
+
+
+def dist_gmres(A, b: np.ndarray, M: ParTree, iters: int = 300, tol: float = 1e-12, verb: bool = True,
+               hist: Optional[list] = None):
+    """is.cpp:447-527: b (permuted local order) is overwritten by the solution.
+
+    Returns ``(k, relres)``: the reference's iteration index at the break and the
+    true relative residual ||b0 - A x|| / ||b0|| (pspaQR.cpp:264-268).
+    """
+    if b.dtype != np.float64 or not b.flags.c_contiguous:
+        raise TypeError("b must be a contiguous float64 array")
+    k = C.c_int()
+    rr = C.c_double()
+    h = np.zeros(iters)
+    M._chk(lib().spq_gmres(M._h, _pd(b), iters, tol, C.byref(k), C.byref(rr), _pd(h), iters), "gmres")
+    if hist is not None:
+        hist.extend(h[: k.value + 1].tolist())
+    return k.value, rr.value

@@ -1,0 +1,162 @@
+"""GPU path (C ABI) against the CPU oracle: ordering, kept ranks, factors, the
+preconditioner apply and GMRES.  Tolerances: FP64 factors and the solve agree to
+1e-10 relative (the kernels and LAPACK differ only in summation order); integer
+outputs (ranks, permutation, iteration counts) are exact."""
+import os
+
+import numpy as np
+import pytest
+
+from oracle.oracle import OracleTree, random_reference
+from pspaqr_public_b200 import ParTree, dist_gmres, scale_columns
+from pspaqr_public_b200 import matrices as M
+
+pytestmark = pytest.mark.gpu
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
+RTOL = 1e-10
+
+
+def _matrix(kind, n, d):
+    if kind == "lapl":
+        return M.laplacian(n, d)
+    if kind == "diff":
+        return M.diffusion_lognormal(n, d, seed=2)
+    if kind == "chan":
+        return M.diffusion_binary(n, d, seed=3)
+    return M.convection_diffusion_2d(n)
+
+
+def _pair(kind, n, d, L, tol, skip=0):
+    cp, ri, v = _matrix(kind, n, d)
+    t = ParTree(L, skip)
+    t.set_tol(tol)
+    t.set_coords_tensor(n, d)
+    t.partition((cp, ri, scale_columns(cp, v)))
+    t.assemble()
+    t.factorize()
+    o = OracleTree(L, skip, tol, 4)
+    o.set_matrix(cp, ri, v)
+    o.set_coords_tensor(n, d)
+    o.partition()
+    o.assemble()
+    o.factorize()
+    return t, o
+
+
+def _relerr(a, b):
+    return np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300)
+
+
+@pytest.mark.parametrize("kind,n,d,L", [("lapl", 16, 2, 4), ("lapl", 8, 3, 4), ("convdiff", 16, 2, 3)])
+def test_exact_without_sparsification(kind, n, d, L):
+    t, o = _pair(kind, n, d, L, 0.0)
+    N = n ** d
+    b = random_reference(N, 11)
+    x = t.solve_inplace(b.copy())
+    assert np.linalg.norm(b - t.spmv(x)) / np.linalg.norm(b) < 1e-12
+    assert _relerr(x, o.solve_inplace(b)) < 1e-12
+
+
+@pytest.mark.parametrize("kind,n,d,L,tol,skip", [
+    ("lapl", 64, 2, 6, 1e-2, 0),
+    ("lapl", 64, 2, 6, 1e-2, 1),
+    ("lapl", 32, 3, 8, 1e-2, 0),
+    ("diff", 16, 3, 6, 1e-2, 0),
+    ("chan", 16, 3, 6, 1e-2, 0),
+    ("convdiff", 64, 2, 6, 1e-2, 0),
+    ("lapl", 32, 2, 5, 1e-1, 0),
+])
+def test_factor_and_solve_parity(kind, n, d, L, tol, skip):
+    t, o = _pair(kind, n, d, L, tol, skip)
+    oc, tc = o.clusters(), t.clusters()
+    assert [c["rank"] for c in oc] == [c["rank"] for c in tc]
+    # R blocks of the level-0 interiors, and of the top separator
+    for q, c in enumerate(oc):
+        if c["merge_lvl"] == 0 and c["lvl"] == 0:
+            Ro, Rt = np.triu(o.block(q, q)), np.triu(t.block(q, q))
+            assert np.abs(Ro - Rt).max() <= RTOL * np.abs(Ro).max()
+    top = o.level(L - 1)[0][0]
+    Ro, Rt = np.triu(o.block(top, top)), np.triu(t.block(top, top))
+    assert np.abs(Ro - Rt).max() <= 1e-9 * np.abs(Ro).max()
+    # sparsification reflectors
+    for q, c in enumerate(oc):
+        if c["sparsified"]:
+            Vo, _ = o.qsp(q)
+            Vt = t.factor(q, 2)
+            assert Vo.shape == Vt.shape
+            np.testing.assert_allclose(np.tril(Vt, -1), np.tril(Vo, -1), rtol=0, atol=1e-9)
+    N = n ** d
+    b = random_reference(N, 2021)
+    xo = o.solve_inplace(b)
+    xt = t.solve_inplace(b.copy())
+    assert _relerr(xt, xo) < 1e-9
+    xg = b.copy()
+    k, rr = dist_gmres(None, xg, t, 300, 1e-12)
+    _, ko, rro, _ = o.gmres(b.copy(), 300, 1e-12)
+    assert k == ko
+    assert rr < 1e-10
+
+
+@pytest.mark.parametrize("name,case", [
+    ("lapl2d_16_l3", (16, 2, 3, 1e-2, 0)),
+    ("lapl2d_64_l6", (64, 2, 6, 1e-2, 0)),
+    ("lapl2d_64_l6_skip1", (64, 2, 6, 1e-2, 1)),
+    ("lapl3d_16_l6", (16, 3, 6, 1e-2, 0)),
+])
+def test_against_golden_fixtures(name, case):
+    g = np.load(os.path.join(GOLDEN, name + ".npz"))
+    n, d, L, tol, skip = case
+    cp, ri, v = M.laplacian(n, d)
+    t = ParTree(L, skip)
+    t.set_tol(tol)
+    t.set_coords_tensor(n, d)
+    t.partition((cp, ri, scale_columns(cp, v)))
+    t.assemble()
+    t.factorize()
+    assert np.array_equal(t.perm(), g["perm"])
+    assert np.array_equal(np.array([c["rank"] for c in t.clusters()]), g["rank"])
+    top = t.level_range(L - 1)[0]
+    np.testing.assert_allclose(np.abs(np.diag(t.block(top, top))), g["top_rdiag"], rtol=1e-9)
+    b = random_reference(n ** d, 2021)
+    x = t.solve_inplace(b.copy())
+    assert _relerr(x, g["precond_x"]) < 1e-9
+    k, rr = dist_gmres(None, b.copy(), t, 300, 1e-12)
+    assert k == int(g["gmres_iters"])
+    assert rr < 1e-10
+
+
+def test_global_solve_matches_permuted_solve():
+    n, d, L = 32, 2, 5
+    cp, ri, v = M.laplacian(n, d)
+    t = ParTree(L, 0)
+    t.set_tol(1e-2)
+    t.set_coords_tensor(n, d)
+    t.partition((cp, ri, scale_columns(cp, v)))
+    t.assemble()
+    t.factorize()
+    b = random_reference(n * n, 5)
+    xg = t.solve(b)
+    bl = np.zeros(n * n)
+    t.distribute_x(b, bl)
+    xl = t.solve_inplace(bl)
+    np.testing.assert_allclose(xg, t.extract_x(xl), rtol=0, atol=0)
+
+
+def test_gmres_64cube_manufactured_solution():
+    """Full-size property: A x = b with a known x is solved to the requested residual."""
+    n, d, L = 64, 3, 12
+    cp, ri, v = M.laplacian(n, d)
+    t = ParTree(L, 0)
+    t.set_tol(1e-2)
+    t.set_coords_tensor(n, d)
+    t.partition((cp, ri, scale_columns(cp, v)))
+    t.assemble()
+    t.factorize()
+    N = n ** d
+    x_true = np.random.default_rng(0).standard_normal(N)
+    b = t.spmv(x_true)
+    x = b.copy()
+    k, rr = dist_gmres(None, x, t, 100, 1e-12)
+    assert rr < 1e-10
+    assert k <= 20
+    assert _relerr(x, x_true) < 1e-6
