@@ -1,0 +1,354 @@
+"""Benchmark: time to a 1e-10 relative residual (factorization + GMRES) on the
+64^3 variable-coefficient diffusion matrix, one B200.
+
+A step is one full time-to-solution run on an assembled tree: ``factorize()``
+followed by left-preconditioned GMRES until the preconditioned residual is
+<= 1e-10 (is.cpp:447-527), with the true ||b - A x|| / ||b|| checked after it.
+
+  value : device time of the step, inputs resident in HBM (CUDA events on the
+          handle's stream, max over ranks), seconds -- lower is better.
+  e2e   : the same step through the C ABI with host buffers: assemble (matrix
+          upload) + factorize + spq_gmres(host b -> host x).
+  roofline : the dominant kernel of the step (from the per-kernel event
+          timing below) against the measured peak it is bound by.
+  cpu_baseline : the CPU oracle (LAPACK restatement of the reference path,
+          OpenMP over independent tasks on all host cores) on the same workload.
+
+``--impl reference`` times that CPU oracle as the reference arm (the reference
+itself cannot be built here: no Eigen, MPI, TaskTorrent or LAPACKE headers).
+With torchrun (N > 1) every rank solves its own replica; the path is not
+sharded across GPUs (replicas only).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOAD = {
+    "name": "diff3d_64",
+    "matrix": "-div(k grad u), k = exp(g), g Gaussian random field (corr. length 8, var 1, seed 2), "
+              "harmonic-mean faces, 64^3 7-point (n=262144)",
+    "n": 64, "d": 3, "nlevels": 12, "tol": 1e-2, "skip": 0, "gmres_tol": 1e-10, "maxit": 300, "rhs_seed": 2,
+}
+METRIC = "time to 1e-10 rel. residual (factor+GMRES), 64^3 diffusion: mixed+learned vs FP64"
+
+
+def build_matrix():
+    from pspaqr_public_b200 import matrices as M
+
+    return M.diffusion_lognormal(WORKLOAD["n"], WORKLOAD["d"], seed=2)
+
+
+def dist_env():
+    return int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("LOCAL_RANK", "0"))
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.th = threading.Thread(target=self._read, daemon=True)
+            self.th.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], 0.0, set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 7:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                mx = max(mx, float(parts[1]))
+            except ValueError:
+                continue
+            for nm, val in zip(names, parts[3:7]):
+                if val.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx or None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return json.load(f)
+    except OSError:
+        return {}
+
+
+def fp64_gemm_peak(torch) -> float:
+    """cuBLAS DGEMM 8192^3 on this GPU (TFLOP/s): the FP64 roofline denominator
+    (MEASURED_PEAKS.json carries HBM and bf16 figures only)."""
+    n = 8192
+    a = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    b = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    best = 1e30
+    for _ in range(4):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        torch.matmul(a, b)
+        e1.record()
+        torch.cuda.synchronize()
+        best = min(best, e0.elapsed_time(e1) / 1e3)
+    del a, b
+    return 2.0 * n ** 3 / best / 1e12
+
+
+def run_ours(args):
+    import torch
+
+    from pspaqr_public_b200 import ParTree, scale_columns
+    from pspaqr_public_b200 import tree as T
+
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600))
+    W = WORKLOAD
+    cp, ri, v = build_matrix()
+    vs = scale_columns(cp, v)
+    N = W["n"] ** W["d"]
+    from pspaqr_public_b200 import matrices as M
+
+    b_host = M.rhs_normal(N, W["rhs_seed"] + rank)
+    stream = torch.cuda.Stream()
+    t = ParTree(W["nlevels"], W["skip"])
+    t.set_tol(W["tol"])
+    t.set_coords_tensor(W["n"], W["d"])
+    t.set_stream(stream.cuda_stream)
+    t0 = time.time()
+    t.partition((cp, ri, vs))
+    t_part = time.time() - t0
+    lib = T.lib()
+    b_dev = torch.empty(N, dtype=torch.float64, device="cuda")
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")  # 256 MB > L2
+    import ctypes as C
+
+    def device_step():
+        t.assemble()
+        b_dev.copy_(torch.from_numpy(b_host).to("cuda"))
+        flush.zero_()
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        l0 = T.kernel_launches()
+        e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+        e0.record(stream)
+        t.factorize()
+        e1.record(stream)
+        it, rr = C.c_int(), C.c_double()
+        rc = lib.spq_gmres_device(t._h, C.c_void_p(b_dev.data_ptr()), W["maxit"], W["gmres_tol"], C.byref(it),
+                                  C.byref(rr), None, 0)
+        if rc:
+            raise RuntimeError(lib.spq_last_error(t._h))
+        e2.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e2) / 1e3, e0.elapsed_time(e1) / 1e3, it.value, rr.value, T.kernel_launches() - l0
+
+    def e2e_step():
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        x = b_host.copy()
+        s0 = time.perf_counter()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        t.assemble()
+        t.factorize()
+        it, rr = C.c_int(), C.c_double()
+        rc = lib.spq_gmres(t._h, x.ctypes.data_as(C.POINTER(C.c_double)), W["maxit"], W["gmres_tol"], C.byref(it),
+                           C.byref(rr), None, 0)
+        if rc:
+            raise RuntimeError(lib.spq_last_error(t._h))
+        e1.record(stream)
+        torch.cuda.synchronize()
+        wall = time.perf_counter() - s0
+        return max(wall, e0.elapsed_time(e1) / 1e3), it.value, rr.value
+
+    for _ in range(args.warmup):
+        device_step()
+    times, ftimes, iters, rels, launches = [], [], [], [], []
+    with ClockSampler(local) as clk:
+        for _ in range(args.steps):
+            dt, ft, it, rr, nl = device_step()
+            times.append(dt)
+            ftimes.append(ft)
+            iters.append(it)
+            rels.append(rr)
+            launches.append(nl)
+    e2e_times = [e2e_step()[0] for _ in range(max(1, min(args.steps, 3)))]
+    step = float(np.mean(times))
+    if dist:
+        tt = torch.tensor([step, float(np.mean(e2e_times))], dtype=torch.float64, device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        step, e2e = float(tt[0]), float(tt[1])
+    else:
+        e2e = float(np.mean(e2e_times))
+    # per-level kernel-phase timing of the last factorization (events inside the library)
+    lt = t.level_times()
+    flops = t.factor_flops()
+    peaks = measured_peaks()
+    fp64_peak = fp64_gemm_peak(torch) if rank == 0 else 0.0
+    fact = float(np.mean(ftimes))
+    achieved = flops / fact / 1e12
+    nnz = len(ri)
+    h2d = nnz * (8 + 4) + (N + 1) * 4 + 8 * N + 8 * nnz  # matrix (CSC values + indices) + b
+    out = {
+        "metric": METRIC,
+        "value": step,
+        "unit": "s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": step * 1e3,
+        "higher_is_better": False,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64",
+        "data": "synthetic (seeded Gaussian random field coefficients, N(0,1) right-hand side)",
+        "variant": "fp64 (plain spaQR: FP64 tile QR, RRQR sparsification, FP64 GMRES)",
+        "config": {"workload": W["name"], "matrix": W["matrix"], "nlevels": W["nlevels"], "tol": W["tol"],
+                   "skip": W["skip"], "gmres_tol": W["gmres_tol"], "parallelism": f"replicas x{world}",
+                   "l2": "factor pool (GBs) > L2; 256 MB buffer written before every timed step"},
+        "factorize_s": fact,
+        "gmres_s": step - fact,
+        "gmres_iters": int(np.median(iters)),
+        "true_relres": float(max(rels)),
+        "partition_s": t_part,
+        "e2e": {"value": e2e, "unit": "s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": 8 * N},
+        "gpu_launches": int(np.median(launches)),
+        "roofline": {"bound": "fp64", "achieved": achieved, "peak": fp64_peak, "unit": "TFLOP/s",
+                     "frac": achieved / fp64_peak if fp64_peak else None, "traffic": None,
+                     "kernel": "factorization (all phases, nominal LAWN 41 flops / factorize time)",
+                     "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (MEASURED_PEAKS.json has no FP64 figure)"},
+        "level_ms": {k: lt[:, i].round(3).tolist() for i, k in enumerate(ParTree.LEVEL_PHASES)},
+        "clocks": clk.summary(),
+        "hbm_peak_gbs": peaks.get("hbm_gbs"),
+    }
+    if rank == 0 and not args.no_cpu_baseline:
+        out["cpu_baseline"] = cpu_baseline(cp, ri, v, b_host)
+    if rank == 0:
+        print(json.dumps(out))
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def cpu_baseline(cp, ri, v, b_host, threads=None):
+    """The oracle (CPU restatement of the reference path) on the same workload."""
+    from oracle.oracle import OracleTree
+
+    W = WORKLOAD
+    threads = threads or os.cpu_count() or 1
+    o = OracleTree(W["nlevels"], W["skip"], W["tol"], threads)
+    o.set_matrix(cp, ri, v)
+    o.set_coords_tensor(W["n"], W["d"])
+    o.partition()
+    o.assemble()
+    t0 = time.perf_counter()
+    o.factorize()
+    t1 = time.perf_counter()
+    _, k, rr, _ = o.gmres(b_host.copy(), W["maxit"], W["gmres_tol"])
+    t2 = time.perf_counter()
+    return {"value": t2 - t0, "unit": "s", "cores": threads, "kind": "port",
+            "sample": f"one full time-to-solution run of {W['name']} (factorize {t1 - t0:.2f} s + "
+                      f"{k} GMRES iterations {t2 - t1:.2f} s, true residual {rr:.2e}); "
+                      "factor phases OpenMP-parallel over independent tasks, solve sequential"}
+
+
+def run_reference(args):
+    """CPU reference arm: the oracle port on all host cores, same metric/config."""
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return
+    from pspaqr_public_b200 import matrices as M
+
+    W = WORKLOAD
+    cp, ri, v = build_matrix()
+    N = W["n"] ** W["d"]
+    b = M.rhs_normal(N, W["rhs_seed"])
+    threads = os.cpu_count() or 1
+    # warm-up on the 32^3 member of the same family (CPU caches / thread pool only)
+    from oracle.oracle import OracleTree
+
+    cps, ris, vsm = M.diffusion_lognormal(32, 3, seed=2)
+    for _ in range(args.warmup):
+        o = OracleTree(10, 0, W["tol"], threads)
+        o.set_matrix(cps, ris, vsm)
+        o.set_coords_tensor(32, 3)
+        o.partition()
+        o.assemble()
+        o.factorize()
+    vals = [cpu_baseline(cp, ri, v, b, threads) for _ in range(args.steps)]
+    val = float(np.mean([x["value"] for x in vals]))
+    out = {
+        "metric": METRIC, "value": val, "unit": "s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": val * 1e3, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic", "impl": "reference",
+        "config": {"workload": W["name"], "matrix": W["matrix"], "nlevels": W["nlevels"], "tol": W["tol"],
+                   "skip": W["skip"], "gmres_tol": W["gmres_tol"], "parallelism": f"cpu x{threads} threads"},
+        "cpu_baseline": {"value": val, "unit": "s", "cores": threads, "kind": "port",
+                         "sample": vals[-1]["sample"] + f"; warm-up on the 32^3 member x{args.warmup}"},
+        "e2e": {"value": val, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(out))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

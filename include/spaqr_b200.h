@@ -109,18 +109,23 @@ int spq_num_edges(spq_tree* t);
 int spq_find_edge(spq_tree* t, int n1, int n2);
 /* Final block A(n2 rows, n1 cols): shape[0..2] = rows, cols, ld; out may be null. */
 int spq_get_block(spq_tree* t, int n1, int n2, double* out, int* shape);
-/* Factors of cluster `order` (which: 0 = diagonal-QR T of an interior,
- * 1 = scaling T, 2 = sparsification reflectors V (n x rank), 3 = their T);
+/* Factors of cluster `order` (which: 0 = block factors T of an interior's
+ * diagonal QR (32 x n, one upper triangle per 32 columns), 1 = scaling block
+ * factors, 2 = sparsification reflectors V (n x rank), 3 = their block factors);
  * shape[0..2] = rows, cols, ld of the stored factor; out receives rows x cols. */
 int spq_get_factor(spq_tree* t, int order, int which, double* out, int* shape);
 /* times[0..4] = partition, assemble, factorize, last solve, last gmres (seconds). */
 int spq_times(spq_tree* t, double* times);
-/* Per level: elim, scale, spars, merge milliseconds (4 * nlevels values). */
+/* Per level, 8 values (milliseconds): geqrt+tsqrt chains, trailing updates,
+ * scaling QR, scaling applies, RRQR, compression applies, merge, level total. */
 int spq_level_times(spq_tree* t, float* ms);
 /* Nominal FP64 flops of the last factorization (LAPACK Working Note 41 counts). */
 double spq_factor_flops(spq_tree* t);
 /* Bytes of device memory held by factor blocks. */
 double spq_pool_bytes(spq_tree* t);
+/* Kernels this library has launched in the process so far (graph nodes counted
+ * per graph launch); no reference counterpart, used to attribute device work. */
+long long spq_kernel_launches(void);
 const char* spq_last_error(spq_tree* t);
 
 #ifdef __cplusplus

@@ -7,6 +7,7 @@
 
 #include "../../include/spaqr_b200.h"
 #include "engine.hpp"
+#include "kernels.hpp"
 
 struct spq_tree {
   spq::Tree* t;
@@ -210,15 +211,21 @@ int spq_level_times(spq_tree* h, float* ms) {
   if (!h || !ms) return -1;
   const auto& lt = h->t->level_timing();
   for (size_t l = 0; l < lt.size(); ++l) {
-    ms[4 * l] = lt[l].elim_ms;
-    ms[4 * l + 1] = lt[l].scale_ms;
-    ms[4 * l + 2] = lt[l].spars_ms;
-    ms[4 * l + 3] = lt[l].merge_ms;
+    float* m = ms + 8 * l;
+    m[0] = lt[l].e1_ms;
+    m[1] = lt[l].e2_ms;
+    m[2] = lt[l].sqr_ms;
+    m[3] = lt[l].sapp_ms;
+    m[4] = lt[l].rrqr_ms;
+    m[5] = lt[l].capp_ms;
+    m[6] = lt[l].merge_ms;
+    m[7] = lt[l].elim_ms + lt[l].scale_ms + lt[l].spars_ms + lt[l].merge_ms;
   }
   return 0;
 }
 double spq_factor_flops(spq_tree* h) { return h ? h->t->factor_flops() : -1.0; }
 double spq_pool_bytes(spq_tree* h) { return h ? (double)h->t->pool_bytes() : -1.0; }
+long long spq_kernel_launches(void) { return spq::kernel_launches(); }
 const char* spq_last_error(spq_tree* h) {
   if (!h) return "null handle";
   return h->err.c_str();

@@ -1,16 +1,17 @@
 // dense.cuh -- CTA-cooperative FP64 Householder building blocks for sm_100a.
 //
-// Every routine is called by all threads of one CTA (kThreads threads) and
-// synchronises internally; matrices are column-major (element (i,j) at
-// p[i + j*ld]) and may live in global or shared memory (generic pointers).
-// Conventions follow LAPACK so results agree with the reference's LAPACK
-// calls up to rounding:
+// Matrices are column-major (element (i,j) at p[i + j*ld]).  Conventions
+// follow LAPACK so results agree with the reference's LAPACK calls up to
+// rounding:
 //   * reflectors H = I - tau v v^T with v(0) = 1, beta = -sign(alpha)*||x||,
 //     tau = (beta - alpha)/beta, v(1:) = x(1:)/(alpha - beta)  (dlarfg);
-//   * a block of k reflectors is I - V T V^T with V unit lower trapezoidal and
-//     T upper triangular (dlarft 'F','C'); the T here always spans all k
-//     reflectors (one block), which is the same operator LAPACK's nb-blocked
-//     T factors represent.
+//   * k reflectors form I - V T V^T with V unit lower trapezoidal; T is kept
+//     in LAPACK's blocked layout with panel width kNB (dgeqrt/dtpqrt with
+//     nb = 32): an kNB x k array, columns [p*kNB, p*kNB+kb) holding the kb x kb
+//     upper-triangular T of panel p.  Q = Q_0 Q_1 ... Q_{P-1} over panels.
+// Apply routines are called by all threads of one CTA and synchronise
+// internally; factorization routines in kernels.cu distribute panels over
+// the CTAs of a thread-block cluster.
 #pragma once
 #include <cuda_runtime.h>
 #include <math.h>
@@ -21,6 +22,7 @@ namespace dev {
 
 constexpr int kThreads = 256;
 constexpr int kWarps = kThreads / 32;
+constexpr int kNB = 32;  // panel width of the blocked reflector storage
 
 __device__ __forceinline__ double warp_sum(double v) {
 #pragma unroll
@@ -45,8 +47,8 @@ __device__ __forceinline__ double cta_sum(double v, double* red) {
   return r;
 }
 
-// dlarfg on (alpha, x[0:len]) given sumsq = ||x||^2.  Returns tau, writes
-// beta; the caller scales x by *scal (0 when tau == 0).
+// dlarfg on (alpha, x) given sumsq = ||x||^2.  Returns tau, writes beta and
+// the scale the caller applies to x (0 when tau == 0).
 __device__ __forceinline__ double house(double alpha, double sumsq, double* beta, double* scal) {
   if (sumsq == 0.0) {
     *beta = alpha;
@@ -59,11 +61,10 @@ __device__ __forceinline__ double house(double alpha, double sumsq, double* beta
   return (b - alpha) / b;
 }
 
-// T factor (k x k, upper) from G(l,j) = v_l^T v_j stored in the strictly upper
-// part of T on entry, and tau[0:k] (shared).  dlarft recurrence:
-//   T(0:j, j) = -tau_j * T(0:j, 0:j) * G(0:j, j),  T(j,j) = tau_j.
-__device__ void larft_from_gram(double* T, int ldt, int k, const double* tau, double* tmp /*smem >= k*/) {
-  for (int j = 0; j < k; ++j) {
+// T (kb x kb, ld ldt) from G(l,j) = v_l^T v_j in its strictly upper part on
+// entry and tau[0:kb].  dlarft recurrence T(0:j,j) = -tau_j T(0:j,0:j) G(0:j,j).
+__device__ void larft_from_gram(double* T, int ldt, int kb, const double* tau, double* tmp /*>= kb*/) {
+  for (int j = 0; j < kb; ++j) {
     for (int i = threadIdx.x; i < j; i += kThreads) tmp[i] = T[i + (size_t)j * ldt];
     __syncthreads();
     const double tj = tau[j];
@@ -75,235 +76,241 @@ __device__ void larft_from_gram(double* T, int ldt, int k, const double* tau, do
     if (threadIdx.x == 0) T[j + (size_t)j * ldt] = tj;
     __syncthreads();
   }
-  // zero the strictly lower part
-  for (int idx = threadIdx.x; idx < k * k; idx += kThreads) {
-    int i = idx % k, j = idx / k;
+  for (int idx = threadIdx.x; idx < kb * kb; idx += kThreads) {
+    const int i = idx % kb, j = idx / kb;
     if (i > j) T[i + (size_t)j * ldt] = 0.0;
   }
   __syncthreads();
 }
 
-// Householder QR (m >= n assumed by callers; handles m < n too) of A (m x n).
-// On exit R in the upper triangle, V below the diagonal, T (n x n) upper.
-// tau: shared scratch >= n; red: shared >= kWarps+1; tmp: shared >= n.
-__device__ void geqrt(double* A, int lda, int m, int n, double* T, int ldt, double* tau, double* red, double* tmp) {
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int kmax = m < n ? m : n;
-  for (int j = 0; j < kmax; ++j) {
-    double* aj = A + (size_t)j * lda;
-    double s = 0.0;
-    for (int i = j + 1 + threadIdx.x; i < m; i += kThreads) s += aj[i] * aj[i];
-    s = cta_sum(s, red);
-    const double alpha = aj[j];
-    double beta, scal;
-    const double tj = house(alpha, s, &beta, &scal);
-    if (tj != 0.0)
-      for (int i = j + 1 + threadIdx.x; i < m; i += kThreads) aj[i] *= scal;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      aj[j] = beta;
-      tau[j] = tj;
-    }
-    if (tj != 0.0) {
-      for (int k = j + 1 + warp; k < n; k += kWarps) {
-        double* ak = A + (size_t)k * lda;
-        double d = lane == 0 ? ak[j] : 0.0;
-        for (int i = j + 1 + lane; i < m; i += 32) d += aj[i] * ak[i];
-        d = warp_sum(d) * tj;
-        if (lane == 0) ak[j] -= d;
-        for (int i = j + 1 + lane; i < m; i += 32) ak[i] -= aj[i] * d;
-      }
-    }
-    __syncthreads();
-  }
-  for (int j = kmax; j < n; ++j)
-    if (threadIdx.x == 0) tau[j] = 0.0;
-  // Gram of the unit lower trapezoidal V: G(l,j) = A(j,l) + sum_{i>j} A(i,l) A(i,j)
-  const int npairs = kmax * (kmax - 1) / 2;
-  for (int p = warp; p < npairs; p += kWarps) {
-    int j = (int)((1.0 + sqrt(1.0 + 8.0 * p)) * 0.5);
-    while (j * (j - 1) / 2 > p) --j;
-    while ((j + 1) * j / 2 <= p) ++j;
-    const int l = p - j * (j - 1) / 2;
-    const double* al = A + (size_t)l * lda;
-    const double* aj = A + (size_t)j * lda;
-    double d = lane == 0 ? al[j] : 0.0;
-    for (int i = j + 1 + lane; i < m; i += 32) d += al[i] * aj[i];
-    d = warp_sum(d);
-    if (lane == 0) T[l + (size_t)j * ldt] = d;
-  }
-  __syncthreads();
-  larft_from_gram(T, ldt, kmax, tau, tmp);
-  for (int idx = threadIdx.x; idx < n * n; idx += kThreads) {
-    int i = idx % n, j = idx / n;
-    if (i >= kmax || j >= kmax) T[i + (size_t)j * ldt] = 0.0;
-  }
-  __syncthreads();
+// Pair index p -> (l, j), l < j, p = j(j-1)/2 + l.
+__device__ __forceinline__ void pair_of(int p, int* l, int* j) {
+  int jj = (int)((1.0 + sqrt(1.0 + 8.0 * p)) * 0.5);
+  while (jj * (jj - 1) / 2 > p) --jj;
+  while ((jj + 1) * jj / 2 <= p) ++jj;
+  *j = jj;
+  *l = p - jj * (jj - 1) / 2;
 }
 
-// Triangular-pentagonal QR with l = 0 (dtpqrt): [R (n x n upper); B (m x n)].
-// R's upper triangle and B are overwritten (B becomes the reflector tails);
-// T (n x n) is the block factor of I - [I; B] T [I; B]^T.
-__device__ void tpqrt(double* R, int ldr, double* B, int ldb, int m, int n, double* T, int ldt, double* tau,
-                      double* red, double* tmp) {
+// Panel T of kb reflectors stored unit-lower-trapezoidal in V (m x kb, rows
+// from the panel's diagonal).  unit = 1: V(i,i) = 1 implied (geqrt / RRQR);
+// unit = 0: full tails of a pentagonal panel (tpqrt, identity on top).
+__device__ void panel_t(const double* V, int ldv, int m, int kb, int unit, const double* tau, double* T, int ldt,
+                        double* tmp) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  for (int j = 0; j < n; ++j) {
-    double* bj = B + (size_t)j * ldb;
-    double s = 0.0;
-    for (int i = threadIdx.x; i < m; i += kThreads) s += bj[i] * bj[i];
-    s = cta_sum(s, red);
-    const double alpha = R[j + (size_t)j * ldr];
-    double beta, scal;
-    const double tj = house(alpha, s, &beta, &scal);
-    if (tj != 0.0)
-      for (int i = threadIdx.x; i < m; i += kThreads) bj[i] *= scal;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      R[j + (size_t)j * ldr] = beta;
-      tau[j] = tj;
-    }
-    if (tj != 0.0) {
-      for (int k = j + 1 + warp; k < n; k += kWarps) {
-        double* bk = B + (size_t)k * ldb;
-        double* rjk = R + j + (size_t)k * ldr;
-        double d = lane == 0 ? *rjk : 0.0;
-        for (int i = lane; i < m; i += 32) d += bj[i] * bk[i];
-        d = warp_sum(d) * tj;
-        if (lane == 0) *rjk -= d;
-        for (int i = lane; i < m; i += 32) bk[i] -= bj[i] * d;
-      }
-    }
-    __syncthreads();
-  }
-  const int npairs = n * (n - 1) / 2;
+  const int npairs = kb * (kb - 1) / 2;
   for (int p = warp; p < npairs; p += kWarps) {
-    int j = (int)((1.0 + sqrt(1.0 + 8.0 * p)) * 0.5);
-    while (j * (j - 1) / 2 > p) --j;
-    while ((j + 1) * j / 2 <= p) ++j;
-    const int l = p - j * (j - 1) / 2;
-    const double* bl = B + (size_t)l * ldb;
-    const double* bj = B + (size_t)j * ldb;
+    int l, j;
+    pair_of(p, &l, &j);
+    const double* vl = V + (size_t)l * ldv;
+    const double* vj = V + (size_t)j * ldv;
     double d = 0.0;
-    for (int i = lane; i < m; i += 32) d += bl[i] * bj[i];
+    if (unit) {
+      d = lane == 0 ? vl[j] : 0.0;
+      for (int i = j + 1 + lane; i < m; i += 32) d += vl[i] * vj[i];
+    } else {
+      for (int i = lane; i < m; i += 32) d += vl[i] * vj[i];
+    }
     d = warp_sum(d);
     if (lane == 0) T[l + (size_t)j * ldt] = d;
   }
   __syncthreads();
-  larft_from_gram(T, ldt, n, tau, tmp);
+  larft_from_gram(T, ldt, kb, tau, tmp);
 }
 
-// C (m x nc) <- (I - V T V^T)^T C, V unit lower trapezoidal (m x k).
-// W: shared scratch of 2*k*chunk doubles; chunk = columns per pass.
-__device__ void apply_qt_left(const double* V, int ldv, const double* T, int ldt, int k, double* C, int ldc, int m,
-                              int nc, double* W, int chunk) {
+// ---------------------------------------------------------------- applies
+// C (m x nc) <- (I - V T V^T)^T C for one block of k <= kNB reflectors,
+// V unit lower trapezoidal (m x k), T (k x k, ld ldt).  W: 2*k*nc doubles.
+__device__ void block_qt(const double* V, int ldv, const double* T, int ldt, int k, double* C, int ldc, int m, int nc,
+                         double* W) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  double* W2 = W + (size_t)k * nc;
+  for (int p = warp; p < k * nc; p += kWarps) {
+    const int i = p % k, c = p / k;
+    const double* v = V + (size_t)i * ldv;
+    const double* x = C + (size_t)c * ldc;
+    double d = (lane == 0 && i < m) ? x[i] : 0.0;
+    for (int r = i + 1 + lane; r < m; r += 32) d += v[r] * x[r];
+    d = warp_sum(d);
+    if (lane == 0) W[i + (size_t)c * k] = d;
+  }
+  __syncthreads();
+  for (int p = threadIdx.x; p < k * nc; p += kThreads) {
+    const int i = p % k, c = p / k;
+    const double* t = T + (size_t)i * ldt;
+    double s = 0.0;
+    for (int l = 0; l <= i; ++l) s += t[l] * W[l + (size_t)c * k];
+    W2[i + (size_t)c * k] = s;
+  }
+  __syncthreads();
+  for (int p = threadIdx.x; p < m * nc; p += kThreads) {
+    const int r = p % m, c = p / m;
+    const int lim = r < k ? r : k;
+    double s = (r < k) ? W2[r + (size_t)c * k] : 0.0;
+    for (int i = 0; i < lim; ++i) s += V[r + (size_t)i * ldv] * W2[i + (size_t)c * k];
+    C[r + (size_t)c * ldc] -= s;
+  }
+  __syncthreads();
+}
+
+// C (m x nc) <- (I - V T V^T) C for one block (no transpose).
+__device__ void block_q(const double* V, int ldv, const double* T, int ldt, int k, double* C, int ldc, int m, int nc,
+                        double* W) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  double* W2 = W + (size_t)k * nc;
+  for (int p = warp; p < k * nc; p += kWarps) {
+    const int i = p % k, c = p / k;
+    const double* v = V + (size_t)i * ldv;
+    const double* x = C + (size_t)c * ldc;
+    double d = (lane == 0 && i < m) ? x[i] : 0.0;
+    for (int r = i + 1 + lane; r < m; r += 32) d += v[r] * x[r];
+    d = warp_sum(d);
+    if (lane == 0) W[i + (size_t)c * k] = d;
+  }
+  __syncthreads();
+  // W2 = T W  (T upper: W2(i) = sum_{l>=i} T(i,l) W(l))
+  for (int p = threadIdx.x; p < k * nc; p += kThreads) {
+    const int i = p % k, c = p / k;
+    double s = 0.0;
+    for (int l = i; l < k; ++l) s += T[i + (size_t)l * ldt] * W[l + (size_t)c * k];
+    W2[i + (size_t)c * k] = s;
+  }
+  __syncthreads();
+  for (int p = threadIdx.x; p < m * nc; p += kThreads) {
+    const int r = p % m, c = p / m;
+    const int lim = r < k ? r : k;
+    double s = (r < k) ? W2[r + (size_t)c * k] : 0.0;
+    for (int i = 0; i < lim; ++i) s += V[r + (size_t)i * ldv] * W2[i + (size_t)c * k];
+    C[r + (size_t)c * ldc] -= s;
+  }
+  __syncthreads();
+}
+
+// [A (k x nc, rows of the panel); B (m x nc)] <- Q^T [A; B] for one pentagonal
+// block, Q = I - [I; V] T [I; V]^T with V full (m x k).
+__device__ void block_tpqt(const double* V, int ldv, const double* T, int ldt, int k, double* A, int lda, double* B,
+                           int ldb, int m, int nc, double* W) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  double* W2 = W + (size_t)k * nc;
+  for (int p = warp; p < k * nc; p += kWarps) {
+    const int i = p % k, c = p / k;
+    const double* v = V + (size_t)i * ldv;
+    const double* x = B + (size_t)c * ldb;
+    double d = lane == 0 ? A[i + (size_t)c * lda] : 0.0;
+    for (int r = lane; r < m; r += 32) d += v[r] * x[r];
+    d = warp_sum(d);
+    if (lane == 0) W[i + (size_t)c * k] = d;
+  }
+  __syncthreads();
+  for (int p = threadIdx.x; p < k * nc; p += kThreads) {
+    const int i = p % k, c = p / k;
+    const double* t = T + (size_t)i * ldt;
+    double s = 0.0;
+    for (int l = 0; l <= i; ++l) s += t[l] * W[l + (size_t)c * k];
+    W2[i + (size_t)c * k] = s;
+  }
+  __syncthreads();
+  for (int p = threadIdx.x; p < k * nc; p += kThreads) {
+    const int i = p % k, c = p / k;
+    A[i + (size_t)c * lda] -= W2[i + (size_t)c * k];
+  }
+  for (int p = threadIdx.x; p < m * nc; p += kThreads) {
+    const int r = p % m, c = p / m;
+    double s = 0.0;
+    for (int i = 0; i < k; ++i) s += V[r + (size_t)i * ldv] * W2[i + (size_t)c * k];
+    B[r + (size_t)c * ldb] -= s;
+  }
+  __syncthreads();
+}
+
+// C (m x n) <- C (I - V T V^T) for one block, V unit lower trapezoidal (n x k).
+// W: 2*k*m doubles.
+__device__ void block_q_right(const double* V, int ldv, const double* T, int ldt, int k, double* C, int ldc, int m,
+                              int n, double* W) {
+  double* W2 = W + (size_t)k * m;
+  for (int p = threadIdx.x; p < k * m; p += kThreads) {
+    const int r = p % m, i = p / m;
+    const double* v = V + (size_t)i * ldv;
+    double s = C[r + (size_t)i * ldc];
+    for (int c = i + 1; c < n; ++c) s += C[r + (size_t)c * ldc] * v[c];
+    W[i + (size_t)r * k] = s;
+  }
+  __syncthreads();
+  for (int p = threadIdx.x; p < k * m; p += kThreads) {
+    const int r = p % m, i = p / m;
+    const double* t = T + (size_t)i * ldt;
+    double s = 0.0;
+    for (int l = 0; l <= i; ++l) s += W[l + (size_t)r * k] * t[l];
+    W2[i + (size_t)r * k] = s;
+  }
+  __syncthreads();
+  for (int p = threadIdx.x; p < m * n; p += kThreads) {
+    const int r = p % m, c = p / m;
+    double s = (c < k) ? W2[c + (size_t)r * k] : 0.0;
+    const int top = (c < k) ? c : k;
+    for (int i = 0; i < top; ++i) s += W2[i + (size_t)r * k] * V[c + (size_t)i * ldv];
+    C[r + (size_t)c * ldc] -= s;
+  }
+  __syncthreads();
+}
+
+// Panel-blocked applies over k reflectors (T in kNB x k layout).
+// Q^T C: panels in order; each acts on rows [j0, m).
+__device__ void apply_qt(const double* V, int ldv, const double* T, int k, double* C, int ldc, int m, int nc,
+                         double* W, int wcap) {
   if (k <= 0 || nc <= 0 || m <= 0) return;
-  double* W2 = W + (size_t)k * chunk;
-  for (int c0 = 0; c0 < nc; c0 += chunk) {
-    const int cn = (nc - c0) < chunk ? (nc - c0) : chunk;
-    for (int p = warp; p < k * cn; p += kWarps) {
-      const int i = p % k, c = p / k;
-      const double* v = V + (size_t)i * ldv;
-      const double* x = C + (size_t)(c0 + c) * ldc;
-      double d = (lane == 0 && i < m) ? x[i] : 0.0;
-      for (int r = i + 1 + lane; r < m; r += 32) d += v[r] * x[r];
-      d = warp_sum(d);
-      if (lane == 0) W[i + (size_t)c * k] = d;
+  const int cmax = (wcap / (2 * kNB)) > 0 ? (wcap / (2 * kNB)) : 1;
+  for (int j0 = 0; j0 < k; j0 += kNB) {
+    const int kb = (k - j0) < kNB ? (k - j0) : kNB;
+    for (int c0 = 0; c0 < nc; c0 += cmax) {
+      const int cn = (nc - c0) < cmax ? (nc - c0) : cmax;
+      block_qt(V + j0 + (size_t)j0 * ldv, ldv, T + (size_t)j0 * kNB, kNB, kb, C + j0 + (size_t)c0 * ldc, ldc, m - j0,
+               cn, W);
     }
-    __syncthreads();
-    for (int p = threadIdx.x; p < k * cn; p += kThreads) {
-      const int i = p % k, c = p / k;
-      const double* t = T + (size_t)i * ldt;
-      double s = 0.0;
-      for (int l = 0; l <= i; ++l) s += t[l] * W[l + (size_t)c * k];
-      W2[i + (size_t)c * k] = s;
-    }
-    __syncthreads();
-    for (int p = threadIdx.x; p < m * cn; p += kThreads) {
-      const int r = p % m, c = p / m;
-      const int lim = r < k ? r : k;
-      double s = (r < k) ? W2[r + (size_t)c * k] : 0.0;
-      for (int i = 0; i < lim; ++i) s += V[r + (size_t)i * ldv] * W2[i + (size_t)c * k];
-      C[r + (size_t)(c0 + c) * ldc] -= s;
-    }
-    __syncthreads();
   }
 }
-
-// [A (k x nc); B (m x nc)] <- Q^T [A; B], Q = I - [I; V] T [I; V]^T, V full (m x k).
-__device__ void apply_tpqt_left(const double* V, int ldv, const double* T, int ldt, int k, double* A, int lda,
-                                double* B, int ldb, int m, int nc, double* W, int chunk) {
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+// Q C: panels in reverse order.
+__device__ void apply_q(const double* V, int ldv, const double* T, int k, double* C, int ldc, int m, int nc, double* W,
+                        int wcap) {
+  if (k <= 0 || nc <= 0 || m <= 0) return;
+  const int cmax = (wcap / (2 * kNB)) > 0 ? (wcap / (2 * kNB)) : 1;
+  const int np = (k + kNB - 1) / kNB;
+  for (int p = np - 1; p >= 0; --p) {
+    const int j0 = p * kNB;
+    const int kb = (k - j0) < kNB ? (k - j0) : kNB;
+    for (int c0 = 0; c0 < nc; c0 += cmax) {
+      const int cn = (nc - c0) < cmax ? (nc - c0) : cmax;
+      block_q(V + j0 + (size_t)j0 * ldv, ldv, T + (size_t)j0 * kNB, kNB, kb, C + j0 + (size_t)c0 * ldc, ldc, m - j0,
+              cn, W);
+    }
+  }
+}
+// [A (k x nc); B (m x nc)] <- Q^T [A; B] for a pentagonal (tpqrt) factor.
+__device__ void apply_tpqt(const double* V, int ldv, const double* T, int k, double* A, int lda, double* B, int ldb,
+                           int m, int nc, double* W, int wcap) {
   if (k <= 0 || nc <= 0) return;
-  double* W2 = W + (size_t)k * chunk;
-  for (int c0 = 0; c0 < nc; c0 += chunk) {
-    const int cn = (nc - c0) < chunk ? (nc - c0) : chunk;
-    for (int p = warp; p < k * cn; p += kWarps) {
-      const int i = p % k, c = p / k;
-      const double* v = V + (size_t)i * ldv;
-      const double* x = B + (size_t)(c0 + c) * ldb;
-      double d = lane == 0 ? A[i + (size_t)(c0 + c) * lda] : 0.0;
-      for (int r = lane; r < m; r += 32) d += v[r] * x[r];
-      d = warp_sum(d);
-      if (lane == 0) W[i + (size_t)c * k] = d;
+  const int cmax = (wcap / (2 * kNB)) > 0 ? (wcap / (2 * kNB)) : 1;
+  for (int j0 = 0; j0 < k; j0 += kNB) {
+    const int kb = (k - j0) < kNB ? (k - j0) : kNB;
+    for (int c0 = 0; c0 < nc; c0 += cmax) {
+      const int cn = (nc - c0) < cmax ? (nc - c0) : cmax;
+      block_tpqt(V + (size_t)j0 * ldv, ldv, T + (size_t)j0 * kNB, kNB, kb, A + j0 + (size_t)c0 * lda, lda,
+                 B + (size_t)c0 * ldb, ldb, m, cn, W);
     }
-    __syncthreads();
-    for (int p = threadIdx.x; p < k * cn; p += kThreads) {
-      const int i = p % k, c = p / k;
-      const double* t = T + (size_t)i * ldt;
-      double s = 0.0;
-      for (int l = 0; l <= i; ++l) s += t[l] * W[l + (size_t)c * k];
-      W2[i + (size_t)c * k] = s;
-    }
-    __syncthreads();
-    for (int p = threadIdx.x; p < k * cn; p += kThreads) {
-      const int i = p % k, c = p / k;
-      A[i + (size_t)(c0 + c) * lda] -= W2[i + (size_t)c * k];
-    }
-    for (int p = threadIdx.x; p < m * cn; p += kThreads) {
-      const int r = p % m, c = p / m;
-      double s = 0.0;
-      for (int i = 0; i < k; ++i) s += V[r + (size_t)i * ldv] * W2[i + (size_t)c * k];
-      B[r + (size_t)(c0 + c) * ldb] -= s;
-    }
-    __syncthreads();
   }
 }
-
-// C (m x n) <- C (I - V T V^T), V unit lower trapezoidal (n x k).
-__device__ void apply_q_right(const double* V, int ldv, const double* T, int ldt, int k, double* C, int ldc, int m,
-                              int n, double* W, int chunk) {
+// C (m x n) <- C Q, panels in order; each acts on columns [j0, n).
+__device__ void apply_q_right(const double* V, int ldv, const double* T, int k, double* C, int ldc, int m, int n,
+                              double* W, int wcap) {
   if (k <= 0 || m <= 0 || n <= 0) return;
-  double* W2 = W + (size_t)k * chunk;
-  for (int r0 = 0; r0 < m; r0 += chunk) {
-    const int rn = (m - r0) < chunk ? (m - r0) : chunk;
-    // W(r,i) = sum_{c>=i} C(r,c) V(c,i), V(i,i) = 1   (stored W[i + r*k])
-    for (int p = threadIdx.x; p < k * rn; p += kThreads) {
-      const int r = p % rn, i = p / rn;
-      const double* v = V + (size_t)i * ldv;
-      double s = C[(r0 + r) + (size_t)i * ldc];
-      for (int c = i + 1; c < n; ++c) s += C[(r0 + r) + (size_t)c * ldc] * v[c];
-      W[i + (size_t)r * k] = s;
+  const int rmax = (wcap / (2 * kNB)) > 0 ? (wcap / (2 * kNB)) : 1;
+  for (int j0 = 0; j0 < k; j0 += kNB) {
+    const int kb = (k - j0) < kNB ? (k - j0) : kNB;
+    for (int r0 = 0; r0 < m; r0 += rmax) {
+      const int rn = (m - r0) < rmax ? (m - r0) : rmax;
+      block_q_right(V + j0 + (size_t)j0 * ldv, ldv, T + (size_t)j0 * kNB, kNB, kb, C + r0 + (size_t)j0 * ldc, ldc, rn,
+                    n - j0, W);
     }
-    __syncthreads();
-    // W2(r,i) = sum_{l<=i} W(r,l) T(l,i)
-    for (int p = threadIdx.x; p < k * rn; p += kThreads) {
-      const int r = p % rn, i = p / rn;
-      const double* t = T + (size_t)i * ldt;
-      double s = 0.0;
-      for (int l = 0; l <= i; ++l) s += W[l + (size_t)r * k] * t[l];
-      W2[i + (size_t)r * k] = s;
-    }
-    __syncthreads();
-    // C(r,c) -= sum_{i <= min(c,k-1)} W2(r,i) V(c,i)
-    for (int p = threadIdx.x; p < rn * n; p += kThreads) {
-      const int r = p % rn, c = p / rn;
-      double s = (c < k) ? W2[c + (size_t)r * k] : 0.0;
-      const int top = (c < k) ? c : k;
-      for (int i = 0; i < top; ++i) s += W2[i + (size_t)r * k] * V[c + (size_t)i * ldv];
-      C[(r0 + r) + (size_t)c * ldc] -= s;
-    }
-    __syncthreads();
   }
 }
 
@@ -316,41 +323,6 @@ __device__ void trsm_right_upper(const double* R, int ldr, double* C, int ldc, i
       for (int i = 0; i < j; ++i) s -= C[r + (size_t)i * ldc] * rj[i];
       C[r + (size_t)j * ldc] = s / rj[j];
     }
-  }
-  __syncthreads();
-}
-
-// ---------------------------------------------------------------- vectors
-// x (m) <- (I - V T V^T)^T x, V unit lower trapezoidal (m x k).  w: shared >= 2k.
-__device__ void apply_qt_vec(const double* V, int ldv, const double* T, int ldt, int k, double* x, int m, double* w) {
-  apply_qt_left(V, ldv, T, ldt, k, x, m, m, 1, w, 1);
-}
-
-// x (m) <- (I - V T V^T) x  (forward product applied without transpose).
-__device__ void apply_q_vec(const double* V, int ldv, const double* T, int ldt, int k, double* x, int m, double* w) {
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  if (k <= 0 || m <= 0) return;
-  double* w2 = w + k;
-  for (int i = warp; i < k; i += kWarps) {
-    const double* v = V + (size_t)i * ldv;
-    double d = (lane == 0 && i < m) ? x[i] : 0.0;
-    for (int r = i + 1 + lane; r < m; r += 32) d += v[r] * x[r];
-    d = warp_sum(d);
-    if (lane == 0) w[i] = d;
-  }
-  __syncthreads();
-  // w2 = T w  (T upper: w2(i) = sum_{l>=i} T(i,l) w(l))
-  for (int i = threadIdx.x; i < k; i += kThreads) {
-    double s = 0.0;
-    for (int l = i; l < k; ++l) s += T[i + (size_t)l * ldt] * w[l];
-    w2[i] = s;
-  }
-  __syncthreads();
-  for (int r = threadIdx.x; r < m; r += kThreads) {
-    const int top = r < k ? r : k;
-    double s = (r < k) ? w2[r] : 0.0;
-    for (int i = 0; i < top; ++i) s += V[r + (size_t)i * ldv] * w2[i];
-    x[r] -= s;
   }
   __syncthreads();
 }

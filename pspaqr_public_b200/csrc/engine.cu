@@ -17,9 +17,12 @@ double wall() {
   return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
 }
 constexpr size_t kAlign = 256;
-constexpr size_t kChunk = size_t(1) << 30;
+constexpr size_t kArenaChunk = size_t(1) << 30;
 // bounded wait of the forward sweep: ~1 s at 2 GHz
 constexpr long long kSpinLimit = 2000000000LL;
+constexpr int kChunk = 64;        // columns (rows) per CTA of the chunked applies
+constexpr int kBigCluster = 8;    // CTAs per task for blocks of >= 8 panels
+inline int dev_nb() { return 32; }  // panel width of the blocked T factors (dense.cuh kNB)
 }  // namespace
 
 // ---------------------------------------------------------------- Arena
@@ -29,7 +32,7 @@ void* Arena::alloc(size_t bytes) {
   bytes = (bytes + kAlign - 1) / kAlign * kAlign;
   if (bytes == 0) bytes = kAlign;
   if (chunks_.empty() || chunks_.back().off + bytes > chunks_.back().size) {
-    size_t sz = std::max(kChunk, bytes);
+    size_t sz = std::max(kArenaChunk, bytes);
     void* p = nullptr;
     if (cudaMalloc(&p, sz) != cudaSuccess) return nullptr;
     chunks_.push_back({static_cast<char*>(p), sz, 0});
@@ -70,7 +73,7 @@ Tree::~Tree() {
 
 int Tree::check_cuda(cudaError_t e, const char* where) {
   if (e == cudaSuccess) return 0;
-  error = std::string(where) + ": " + cudaGetErrorString(e);
+  error = std::string(where) + ": " + cudaGetErrorString(e) + " (last launcher: " + last_launch_name() + ")";
   return -10;
 }
 
@@ -95,8 +98,8 @@ int Tree::device_status() {
 }
 
 void* Tree::upload(const void* host, size_t bytes) {
-  void* d = scratch_.alloc(bytes);
-  if (d && bytes) cudaMemcpyAsync(d, host, bytes, cudaMemcpyHostToDevice, stream_);
+  void* d = scratch_.alloc(std::max<size_t>(bytes, 1));
+  if (d && bytes && host) cudaMemcpyAsync(d, host, bytes, cudaMemcpyHostToDevice, stream_);
   return d;
 }
 
@@ -175,18 +178,12 @@ int Tree::assemble() {
   const Level& L0 = st_.levels[0];
   for (int o = L0.first; o < L0.first + L0.count; ++o) size_[o] = size_org_[o] = st_.clusters[o].size0;
   // level-0 blocks, zeroed, then the nonzeros of App scattered in
-  size_t total = 0;
   for (int e : L0.edges) {
     const Edge& E = st_.edges[e];
     rows_[e] = size_[E.n2];
     cols_[e] = size_[E.n1];
-    ld_[e] = std::max(1, rows_[e]);
-    ptr_[e] = arena_.dalloc((size_t)ld_[e] * cols_[e]);
-    if (!ptr_[e]) return fail(-11, "out of device memory (level-0 blocks)");
-    total += (size_t)ld_[e] * cols_[e];
   }
-  for (int e : L0.edges) cudaMemsetAsync(ptr_[e], 0, sizeof(double) * (size_t)ld_[e] * cols_[e], stream_);
-  (void)total;
+  if (int rc = alloc_level_blocks(L0.edges)) return rc;
   const Csc& P = st_.App;
   std::vector<int> leaf_of(n);
   for (int o = L0.first; o < L0.first + L0.count; ++o)
@@ -238,7 +235,7 @@ int Tree::assemble() {
   double* d_cval = static_cast<double*>(upload(cval.data(), sizeof(double) * nnz));
   double** d_dst = static_cast<double**>(upload(dst.data(), sizeof(double*) * nnz));
   if (!d_cval || !d_dst) return fail(-11, "out of device memory (assembly)");
-  launch_scatter(nnz, d_cval, d_dst, stream_);
+  if (check_cuda(launch_scatter(nnz, d_cval, d_dst, stream_), "scatter")) return -10;
   if (check_cuda(cudaStreamSynchronize(stream_), "assemble")) return -10;
   scratch_.release();
   assembled_ = true;
@@ -248,57 +245,76 @@ int Tree::assemble() {
   return 0;
 }
 
+// Cluster size (CTAs per task) of the distributed factorizations: one CTA
+// for small blocks, a thread-block cluster of kBigCluster CTAs once a block
+// has enough 32-column panels to share.
+static int cluster_for(int ncols) {
+  const int panels = (ncols + dev_nb() - 1) / dev_nb();
+  if (panels >= 8) return kBigCluster;
+  if (panels >= 4) return 4;
+  return 1;
+}
+
 int Tree::factorize() {
   if (!assembled_) return fail(-4, "factorize called before assemble");
   if (factorized_) return fail(-4, "factorize called twice; assemble again first");
   double t0 = wall();
   const int L = st_.nlevels;
+  const int NB = dev_nb();
   lt_.assign(L, LevelTiming());
   flops_ = 0;
-  cudaEvent_t ev[5];
+  cudaEvent_t ev[5], fe[6];
   for (auto& e : ev) cudaEventCreate(&e);
+  for (auto& e : fe) cudaEventCreate(&e);
   std::vector<int> host_rank(st_.clusters.size(), 0);
+  auto ck = [&](cudaError_t e, const char* where) { return check_cuda(e, where); };
   for (int lvl = 0; lvl < L; ++lvl) {
     const Level& Lv = st_.levels[lvl];
     cudaEventRecord(ev[0], stream_);
-    // ---------------- elimination: geqrt + tsqrt chains
-    std::vector<ElimTask> et;
+    // ---------------- elimination: geqrt + tsqrt chains, grouped by cluster size
+    std::vector<ElimTask> et[3];
     std::vector<ElimOut> eo;
-    int nmax = 1;
+    int nmax[3] = {1, 1, 1}, vmax[3] = {1, 1, 1};
+    const int csz[3] = {1, 4, kBigCluster};
     for (size_t ii = 0; ii < Lv.interiors.size(); ++ii) {
       const int c = Lv.interiors[ii];
       const int nc = size_[c];
       const int se = Lv.self_edge_of[c - Lv.first];
-      T_[c] = arena_.dalloc((size_t)nc * nc);
+      T_[c] = arena_.dalloc((size_t)NB * std::max(nc, 1));
       ElimTask t;
       t.S = ptr_[se];
       t.T = T_[c];
+      t.tau = scratch_.dalloc(std::max(nc, 1));
       t.n = nc;
       t.out_begin = (int)eo.size();
       flops_ += 2.0 * nc * nc * (nc - nc / 3.0);
+      int vm = nc;
       for (int q = Lv.out_begin[ii]; q < Lv.out_end[ii]; ++q) {
         const int e = Lv.out_edges[q];
-        tsqrtT_[e] = arena_.dalloc((size_t)nc * nc);
+        tsqrtT_[e] = arena_.dalloc((size_t)NB * std::max(nc, 1));
         ElimOut o;
         o.B = ptr_[e];
         o.T = tsqrtT_[e];
         o.m = rows_[e];
         eo.push_back(o);
+        vm = std::max(vm, o.m);
         flops_ += 2.0 * rows_[e] * nc * nc;
       }
       t.out_end = (int)eo.size();
-      et.push_back(t);
-      nmax = std::max(nmax, nc);
+      if (!t.T || !t.tau) return fail(-11, "out of device memory (elimination)");
+      const int cs = cluster_for(nc);
+      const int g = cs == 1 ? 0 : (cs == 4 ? 1 : 2);
+      et[g].push_back(t);
+      nmax[g] = std::max(nmax[g], nc);
+      vmax[g] = std::max(vmax[g], vm);
     }
-    // trailing updates by column cluster
+    // trailing updates: one task per (column cluster, chunk of kChunk columns)
     std::vector<UpdTask> ut;
     std::vector<UpdOp> uo;
-    int kmax_upd = 1;
     for (size_t ct = 0; ct < Lv.col_m.size(); ++ct) {
       const int m = Lv.col_m[ct];
-      UpdTask t;
-      t.op_begin = (int)uo.size();
-      t.ncols = size_[m];
+      const int op_begin = (int)uo.size();
+      const int ncol = size_[m];
       for (int q = Lv.col_begin[ct]; q < Lv.col_end[ct]; ++q) {
         const int c = Lv.col_c[q];
         const int ecm = Lv.col_ecm[q];
@@ -312,13 +328,11 @@ int Tree::factorize() {
         a.B = nullptr;
         a.k = nc;
         a.m = nc;
-        a.ldv = nc;
+        a.ldv = ld_[se];
         a.lda = ld_[ecm];
         a.ldb = 0;
         uo.push_back(a);
-        kmax_upd = std::max(kmax_upd, nc);
-        flops_ += 4.0 * nc * nc * t.ncols;
-        // interior's out-edges in chain order, aligned with col_emn
+        flops_ += 4.0 * nc * nc * ncol;
         const int ii = (int)(std::lower_bound(Lv.interiors.begin(), Lv.interiors.end(), c) - Lv.interiors.begin());
         int j = Lv.col_emn_begin[q];
         for (int r = Lv.out_begin[ii]; r < Lv.out_end[ii]; ++r, ++j) {
@@ -336,64 +350,87 @@ int Tree::factorize() {
           b.lda = ld_[ecm];
           b.ldb = ld_[emn];
           uo.push_back(b);
-          flops_ += 4.0 * rows_[ecn] * nc * t.ncols;
+          flops_ += 4.0 * rows_[ecn] * nc * ncol;
         }
       }
-      t.op_end = (int)uo.size();
-      ut.push_back(t);
+      const int op_end = (int)uo.size();
+      for (int c0 = 0; c0 < ncol; c0 += kChunk) ut.push_back({op_begin, op_end, c0, std::min(kChunk, ncol - c0)});
     }
-    lt_[lvl].ntasks_elim = (int)et.size();
+    lt_[lvl].ntasks_elim = (int)Lv.interiors.size();
     lt_[lvl].ntasks_upd = (int)ut.size();
     {
-      auto* d_et = static_cast<ElimTask*>(upload(et.data(), sizeof(ElimTask) * et.size()));
-      auto* d_eo = static_cast<ElimOut*>(upload(eo.data(), sizeof(ElimOut) * std::max<size_t>(eo.size(), 1)));
-      auto* d_ut = static_cast<UpdTask*>(upload(ut.data(), sizeof(UpdTask) * std::max<size_t>(ut.size(), 1)));
-      auto* d_uo = static_cast<UpdOp*>(upload(uo.data(), sizeof(UpdOp) * std::max<size_t>(uo.size(), 1)));
-      if (!d_et || !d_eo || !d_ut || !d_uo) return fail(-11, "out of device memory (elimination descriptors)");
-      launch_elim(d_et, d_eo, (int)et.size(), nmax, stream_);
-      launch_update(d_ut, d_uo, (int)ut.size(), kmax_upd, stream_);
+      auto* d_eo = static_cast<ElimOut*>(upload(eo.data(), sizeof(ElimOut) * eo.size()));
+      for (int g = 0; g < 3; ++g) {
+        if (et[g].empty()) continue;
+        auto* d_et = static_cast<ElimTask*>(upload(et[g].data(), sizeof(ElimTask) * et[g].size()));
+        if (!d_et || !d_eo) return fail(-11, "out of device memory (elimination descriptors)");
+        if (ck(launch_elim(d_et, d_eo, (int)et[g].size(), csz[g], nmax[g], vmax[g], stream_), "elimination kernel"))
+          return -10;
+      }
+      cudaEventRecord(fe[0], stream_);
+      auto* d_ut = static_cast<UpdTask*>(upload(ut.data(), sizeof(UpdTask) * ut.size()));
+      auto* d_uo = static_cast<UpdOp*>(upload(uo.data(), sizeof(UpdOp) * uo.size()));
+      if (!d_ut || !d_uo) return fail(-11, "out of device memory (update descriptors)");
+      if (ck(launch_update(d_ut, d_uo, (int)ut.size(), stream_), "update kernel")) return -10;
     }
     cudaEventRecord(ev[1], stream_);
     // ---------------- scaling + sparsification
     const bool spars = !Lv.spars_clusters.empty();
     if (spars) {
-      std::vector<ScaleTask> sc;
-      int smax = 1;
+      std::vector<ScaleTask> sc[3];
+      int smax[3] = {1, 1, 1};
       for (int p : Lv.spars_clusters) {
         const int np = size_[p];
-        Ts_[p] = arena_.dalloc((size_t)np * np);
+        Ts_[p] = arena_.dalloc((size_t)NB * std::max(np, 1));
         ScaleTask t;
         t.S = ptr_[Lv.self_edge_of[p - Lv.first]];
         t.T = Ts_[p];
+        t.tau = scratch_.dalloc(std::max(np, 1));
         t.n = np;
-        sc.push_back(t);
-        smax = std::max(smax, np);
+        if (!t.T || !t.tau) return fail(-11, "out of device memory (scaling)");
+        const int cs = cluster_for(np);
+        const int g = cs == 1 ? 0 : (cs == 4 ? 1 : 2);
+        sc[g].push_back(t);
+        smax[g] = std::max(smax[g], np);
         flops_ += 2.0 * np * np * (np - np / 3.0);
       }
-      std::vector<ScaleEdgeTask> se;
-      int kmax_se = 1, kmax_sp = 1;
+      std::vector<EdgeChunk> rows_scale, cols_scale;
       for (int e : Lv.spars_edges) {
         const Edge& E = st_.edges[e];
         const bool r = st_.clusters[E.n2].sparsify, c = st_.clusters[E.n1].sparsify;
-        if (!r && !c) continue;
-        ScaleEdgeTask t;
+        EdgeChunk t{};
         t.A = ptr_[e];
         t.lda = ld_[e];
         t.m = rows_[e];
         t.nc = cols_[e];
-        t.Qr = r ? ptr_[Lv.self_edge_of[E.n2 - Lv.first]] : nullptr;
-        t.Tr = r ? Ts_[E.n2] : nullptr;
-        t.ldqr = size_[E.n2];
-        t.Qc = c ? ptr_[Lv.self_edge_of[E.n1 - Lv.first]] : nullptr;
-        t.ldqc = size_[E.n1];
-        se.push_back(t);
-        if (r) kmax_se = std::max(kmax_se, t.m);
-        if (r) flops_ += 4.0 * t.m * t.m * t.nc;
-        if (c) flops_ += (double)t.m * t.nc * t.nc;
+        if (r) {
+          t.V = ptr_[Lv.self_edge_of[E.n2 - Lv.first]];
+          t.T = Ts_[E.n2];
+          t.ldv = size_[E.n2];
+          t.k = t.m;
+          for (int c0 = 0; c0 < t.nc; c0 += kChunk) {
+            t.lo = c0;
+            t.cnt = std::min(kChunk, t.nc - c0);
+            rows_scale.push_back(t);
+          }
+          flops_ += 4.0 * t.m * t.m * t.nc;
+        }
+        if (c) {
+          t.V = ptr_[Lv.self_edge_of[E.n1 - Lv.first]];
+          t.T = nullptr;
+          t.ldv = size_[E.n1];
+          for (int r0 = 0; r0 < t.m; r0 += kChunk) {
+            t.lo = r0;
+            t.cnt = std::min(kChunk, t.m - r0);
+            cols_scale.push_back(t);
+          }
+          flops_ += (double)t.m * t.nc * t.nc;
+        }
       }
-      std::vector<RrqrTask> rt;
+      std::vector<RrqrTask> rt[3];
       std::vector<RrqrSrc> rs;
-      int mmax = 1;
+      int mmax[3] = {1, 1, 1}, wloc[3] = {1, 1, 1};
+      std::vector<std::pair<double, double>> rr_dims;
       for (size_t q = 0; q < Lv.spars_clusters.size(); ++q) {
         const int p = Lv.spars_clusters[q];
         const int mp = size_[p];
@@ -413,59 +450,95 @@ int Tree::factorize() {
         }
         t.src_end = (int)rs.size();
         t.w = w;
-        Qsp_[p] = arena_.dalloc((size_t)mp * std::max(w, 1));
-        Tsp_[p] = arena_.dalloc((size_t)mp * mp);
-        t.C = Qsp_[p];
+        Qsp_[p] = arena_.dalloc((size_t)std::max(mp, 1) * std::max(mp, 1));
+        Tsp_[p] = arena_.dalloc((size_t)NB * std::max(mp, 1));
+        t.V = Qsp_[p];
         t.T = Tsp_[p];
+        t.C = scratch_.dalloc((size_t)std::max(mp, 1) * std::max(w, 1));
         t.tau = scratch_.dalloc(std::max(mp, 1));
         t.vn = scratch_.dalloc(2 * (size_t)std::max(w, 1));
-        t.jpvt = static_cast<int*>(scratch_.alloc(sizeof(int) * std::max(w, 1)));
+        t.colat = static_cast<int*>(scratch_.alloc(sizeof(int) * std::max(w, 1)));
+        t.bc = scratch_.dalloc(16);
         t.rank = d_rank_ + p;
-        if (!t.C || !t.T || !t.tau || !t.vn || !t.jpvt) return fail(-11, "out of device memory (rrqr)");
-        rt.push_back(t);
-        mmax = std::max(mmax, mp);
+        if (!t.C || !t.V || !t.T || !t.tau || !t.vn || !t.colat || !t.bc)
+          return fail(-11, "out of device memory (rrqr)");
+        const int cs = cluster_for(w);
+        const int g = cs == 1 ? 0 : (cs == 4 ? 1 : 2);
+        rt[g].push_back(t);
+        mmax[g] = std::max(mmax[g], mp);
+        const int npan = (w + NB - 1) / NB;
+        wloc[g] = std::max(wloc[g], ((npan + cs - 1) / cs) * NB);
+        rr_dims.push_back({(double)mp, (double)w});
       }
-      std::vector<SparsEdgeTask> sp;
+      std::vector<EdgeChunk> right, left;
       for (int e : Lv.spars_edges) {
         const Edge& E = st_.edges[e];
         const bool r = st_.clusters[E.n2].sparsify, c = st_.clusters[E.n1].sparsify;
-        if (!r && !c) continue;
-        SparsEdgeTask t;
+        EdgeChunk t{};
         t.A = ptr_[e];
         t.lda = ld_[e];
         t.m = rows_[e];
         t.nc = cols_[e];
-        t.Vr = r ? Qsp_[E.n2] : nullptr;
-        t.Tr = r ? Tsp_[E.n2] : nullptr;
-        t.rank_r = d_rank_ + E.n2;
-        t.ldvr = size_[E.n2];
-        t.Vc = c ? Qsp_[E.n1] : nullptr;
-        t.Tc = c ? Tsp_[E.n1] : nullptr;
-        t.rank_c = d_rank_ + E.n1;
-        t.ldvc = size_[E.n1];
-        sp.push_back(t);
-        kmax_sp = std::max(kmax_sp, std::max(r ? t.ldvr : 1, c ? t.ldvc : 1));
+        if (c) {
+          t.V = Qsp_[E.n1];
+          t.T = Tsp_[E.n1];
+          t.kdev = d_rank_ + E.n1;
+          t.ldv = size_[E.n1];
+          for (int r0 = 0; r0 < t.m; r0 += kChunk) {
+            t.lo = r0;
+            t.cnt = std::min(kChunk, t.m - r0);
+            right.push_back(t);
+          }
+        }
+        if (r) {
+          t.V = Qsp_[E.n2];
+          t.T = Tsp_[E.n2];
+          t.kdev = d_rank_ + E.n2;
+          t.ldv = size_[E.n2];
+          t.limdev = c ? d_rank_ + E.n1 : nullptr;
+          for (int c0 = 0; c0 < t.nc; c0 += kChunk) {
+            t.lo = c0;
+            t.cnt = std::min(kChunk, t.nc - c0);
+            left.push_back(t);
+          }
+        }
       }
-      auto* d_sc = static_cast<ScaleTask*>(upload(sc.data(), sizeof(ScaleTask) * sc.size()));
-      auto* d_se = static_cast<ScaleEdgeTask*>(upload(se.data(), sizeof(ScaleEdgeTask) * std::max<size_t>(se.size(), 1)));
-      auto* d_rt = static_cast<RrqrTask*>(upload(rt.data(), sizeof(RrqrTask) * rt.size()));
-      auto* d_rs = static_cast<RrqrSrc*>(upload(rs.data(), sizeof(RrqrSrc) * std::max<size_t>(rs.size(), 1)));
-      auto* d_sp = static_cast<SparsEdgeTask*>(upload(sp.data(), sizeof(SparsEdgeTask) * std::max<size_t>(sp.size(), 1)));
-      if (!d_sc || !d_se || !d_rt || !d_rs || !d_sp) return fail(-11, "out of device memory (sparsification)");
-      launch_scale(d_sc, (int)sc.size(), smax, stream_);
-      launch_scale_edge(d_se, (int)se.size(), kmax_se, stream_);
+      auto up_vec = [&](auto& v) { return upload(v.data(), sizeof(v[0]) * v.size()); };
+      auto* d_rs = static_cast<RrqrSrc*>(up_vec(rs));
+      auto* d_rows = static_cast<EdgeChunk*>(up_vec(rows_scale));
+      auto* d_cols = static_cast<EdgeChunk*>(up_vec(cols_scale));
+      auto* d_right = static_cast<EdgeChunk*>(up_vec(right));
+      auto* d_left = static_cast<EdgeChunk*>(up_vec(left));
+      if (!d_rs || !d_rows || !d_cols || !d_right || !d_left) return fail(-11, "out of device memory (sparsification)");
+      for (int g = 0; g < 3; ++g) {
+        if (sc[g].empty()) continue;
+        auto* d = static_cast<ScaleTask*>(up_vec(sc[g]));
+        if (!d || ck(launch_scale(d, (int)sc[g].size(), csz[g], smax[g], stream_), "scaling kernel")) return -10;
+      }
+      cudaEventRecord(fe[1], stream_);
+      if (ck(launch_edge(0, d_rows, (int)rows_scale.size(), stream_), "row scaling") ||
+          ck(launch_edge(1, d_cols, (int)cols_scale.size(), stream_), "column scaling"))
+        return -10;
       cudaEventRecord(ev[2], stream_);
-      launch_rrqr(d_rt, d_rs, (int)rt.size(), mmax, st_.tol, pivot_rtol, stream_);
-      launch_spars_edge(d_sp, (int)sp.size(), kmax_sp, stream_);
+      for (int g = 0; g < 3; ++g) {
+        if (rt[g].empty()) continue;
+        auto* d = static_cast<RrqrTask*>(up_vec(rt[g]));
+        if (!d || ck(launch_rrqr(d, d_rs, (int)rt[g].size(), csz[g], mmax[g], wloc[g], st_.tol, pivot_rtol, stream_),
+                     "rrqr kernel"))
+          return -10;
+      }
+      cudaEventRecord(fe[2], stream_);
+      if (ck(launch_edge(2, d_right, (int)right.size(), stream_), "right compression") ||
+          ck(launch_edge(0, d_left, (int)left.size(), stream_), "left compression"))
+        return -10;
       cudaEventRecord(ev[3], stream_);
-      if (check_cuda(cudaMemcpyAsync(host_rank.data(), d_rank_, sizeof(int) * host_rank.size(), cudaMemcpyDeviceToHost,
-                                     stream_),
-                     "rank readback") ||
-          check_cuda(cudaStreamSynchronize(stream_), "sparsification"))
+      if (ck(cudaMemcpyAsync(host_rank.data(), d_rank_, sizeof(int) * host_rank.size(), cudaMemcpyDeviceToHost, stream_),
+             "rank readback") ||
+          ck(cudaStreamSynchronize(stream_), "sparsification"))
         return -10;
       for (int p : Lv.spars_clusters) size_[p] = host_rank[p];
-      for (size_t q = 0; q < rt.size(); ++q) {
-        const double m = rt[q].m, w = rt[q].w, r = size_[Lv.spars_clusters[q]];
+      for (size_t q = 0; q < Lv.spars_clusters.size(); ++q) {
+        const double m = rr_dims[q].first, w = rr_dims[q].second, r = size_[Lv.spars_clusters[q]];
         flops_ += 4.0 * m * w * r - 2.0 * r * r * (m + w) + 4.0 * r * r * r / 3.0 + m * r * r;
       }
       for (int e : Lv.spars_edges) {
@@ -474,7 +547,9 @@ int Tree::factorize() {
       }
       lt_[lvl].nspars = (int)Lv.spars_clusters.size();
     } else {
+      cudaEventRecord(fe[1], stream_);
       cudaEventRecord(ev[2], stream_);
+      cudaEventRecord(fe[2], stream_);
       cudaEventRecord(ev[3], stream_);
     }
     // ---------------- merge into the next level
@@ -490,18 +565,12 @@ int Tree::factorize() {
         }
         size_[P] = size_org_[P] = off;
       }
-      size_t region = 0;
       for (int e : N.edges) {
         const Edge& E = st_.edges[e];
         rows_[e] = size_[E.n2];
         cols_[e] = size_[E.n1];
-        ld_[e] = std::max(1, rows_[e]);
-        ptr_[e] = arena_.dalloc((size_t)ld_[e] * cols_[e]);
-        if (!ptr_[e]) return fail(-11, "out of device memory (level blocks)");
-        cudaMemsetAsync(ptr_[e], 0, sizeof(double) * (size_t)ld_[e] * cols_[e], stream_);
-        region += (size_t)ld_[e] * cols_[e];
       }
-      (void)region;
+      if (int rc = alloc_level_blocks(N.edges)) return rc;
       std::vector<MergeTask> mt;
       for (size_t q = 0; q < Lv.merge_src.size(); ++q) {
         const int s = Lv.merge_src[q], d = Lv.merge_dst[q];
@@ -518,16 +587,22 @@ int Tree::factorize() {
         t.identity = (E.n1 == E.n2 && st_.clusters[E.n1].sparsify) ? 1 : 0;
         if (t.rows > 0 && t.cols > 0) mt.push_back(t);
       }
-      auto* d_mt = static_cast<MergeTask*>(upload(mt.data(), sizeof(MergeTask) * std::max<size_t>(mt.size(), 1)));
+      auto* d_mt = static_cast<MergeTask*>(upload(mt.data(), sizeof(MergeTask) * mt.size()));
       if (!d_mt) return fail(-11, "out of device memory (merge)");
-      launch_merge(d_mt, (int)mt.size(), stream_);
+      if (ck(launch_merge(d_mt, (int)mt.size(), stream_), "merge kernel")) return -10;
     }
     cudaEventRecord(ev[4], stream_);
-    if (check_cuda(cudaStreamSynchronize(stream_), "factorize level")) return -10;
+    if (ck(cudaStreamSynchronize(stream_), "factorize level")) return -10;
     cudaEventElapsedTime(&lt_[lvl].elim_ms, ev[0], ev[1]);
     cudaEventElapsedTime(&lt_[lvl].scale_ms, ev[1], ev[2]);
     cudaEventElapsedTime(&lt_[lvl].spars_ms, ev[2], ev[3]);
     cudaEventElapsedTime(&lt_[lvl].merge_ms, ev[3], ev[4]);
+    cudaEventElapsedTime(&lt_[lvl].e1_ms, ev[0], fe[0]);
+    cudaEventElapsedTime(&lt_[lvl].e2_ms, fe[0], ev[1]);
+    cudaEventElapsedTime(&lt_[lvl].sqr_ms, ev[1], fe[1]);
+    cudaEventElapsedTime(&lt_[lvl].sapp_ms, fe[1], ev[2]);
+    cudaEventElapsedTime(&lt_[lvl].rrqr_ms, ev[2], fe[2]);
+    cudaEventElapsedTime(&lt_[lvl].capp_ms, fe[2], ev[3]);
     scratch_.release();
     if (verbose)
       printf("%d    elim %.3f ms  scale %.3f ms  spars %.3f ms  merge %.3f ms  (interiors %zu, interfaces %zu)\n", lvl,
@@ -535,6 +610,7 @@ int Tree::factorize() {
              Lv.interfaces.size());
   }
   for (auto& e : ev) cudaEventDestroy(e);
+  for (auto& e : fe) cudaEventDestroy(e);
   factorized_ = true;
   int rc = build_solve_graph();
   if (rc) return rc;
@@ -543,6 +619,24 @@ int Tree::factorize() {
     printf("Tolerance set: %e\n", st_.tol);
     printf("Time to factorize:  %g\n", t_factorize);
   }
+  return 0;
+}
+
+int Tree::alloc_level_blocks(const std::vector<int>& edges) {
+  // blocks padded to 32 doubles (256 B) so every block starts aligned
+  size_t total = 0;
+  for (int e : edges) {
+    ld_[e] = std::max(1, rows_[e]);
+    total += ((size_t)ld_[e] * cols_[e] + 31) / 32 * 32;
+  }
+  double* base = arena_.dalloc(std::max<size_t>(total, 32));
+  if (!base) return fail(-11, "out of device memory (level blocks)");
+  size_t off = 0;
+  for (int e : edges) {
+    ptr_[e] = base + off;
+    off += ((size_t)ld_[e] * cols_[e] + 31) / 32 * 32;
+  }
+  if (check_cuda(cudaMemsetAsync(base, 0, sizeof(double) * std::max<size_t>(total, 32), stream_), "memset")) return -10;
   return 0;
 }
 
@@ -583,7 +677,7 @@ int Tree::build_solve_graph() {
   std::vector<LevelSolve> ls(L);
   auto up = [&](const void* h, size_t bytes) -> void* {
     void* d = arena_.alloc(std::max<size_t>(bytes, 1));
-    if (d && bytes) cudaMemcpyAsync(d, h, bytes, cudaMemcpyHostToDevice, stream_);
+    if (d && bytes && h) cudaMemcpyAsync(d, h, bytes, cudaMemcpyHostToDevice, stream_);
     return d;
   };
   for (int lvl = 0; lvl < L; ++lvl) {
@@ -689,22 +783,26 @@ int Tree::build_solve_graph() {
     solve_exec_ = nullptr;
   }
   if (check_cuda(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal), "capture")) return -10;
+  const long long launches_before = kernel_launches();
+  cudaError_t cerr = cudaSuccess;
   cudaMemsetAsync(d_turn_, 0, sizeof(int) * ncl, stream_);
   cudaMemsetAsync(d_tickets_, 0, sizeof(int) * L, stream_);
   for (int lvl = 0; lvl < L; ++lvl) {
     LevelSolve& S = ls[lvl];
-    launch_fwd_elim(S.fe, S.fo, S.nfe, S.fe_nmax, S.fe_mmax, d_tickets_ + lvl, d_status_, kSpinLimit, stream_);
-    launch_fwd_spars(S.fs, S.nfs, S.fs_nmax, stream_);
-    launch_copy_idx(S.ng, S.gsrc, S.gdst, d_xw_, stream_);
+    cerr = cerr ? cerr : launch_fwd_elim(S.fe, S.fo, S.nfe, S.fe_nmax, S.fe_mmax, d_tickets_ + lvl, d_status_, kSpinLimit, stream_);
+    cerr = cerr ? cerr : launch_fwd_spars(S.fs, S.nfs, S.fs_nmax, stream_);
+    cerr = cerr ? cerr : launch_copy_idx(S.ng, S.gsrc, S.gdst, d_xw_, stream_);
   }
   for (int lvl = L - 1; lvl >= 0; --lvl) {
     LevelSolve& S = ls[lvl];
-    launch_bwd_spars(S.fs, S.nfs, S.fs_nmax, stream_);
-    launch_bwd_elim(S.be, S.bi, S.nbe, S.be_nmax, stream_);
-    if (lvl > 0) launch_copy_idx(ls[lvl - 1].ng, ls[lvl - 1].gdst, ls[lvl - 1].gsrc, d_xw_, stream_);
+    cerr = cerr ? cerr : launch_bwd_spars(S.fs, S.nfs, S.fs_nmax, stream_);
+    cerr = cerr ? cerr : launch_bwd_elim(S.be, S.bi, S.nbe, S.be_nmax, stream_);
+    if (lvl > 0) cerr = cerr ? cerr : launch_copy_idx(ls[lvl - 1].ng, ls[lvl - 1].gdst, ls[lvl - 1].gsrc, d_xw_, stream_);
   }
+  solve_graph_kernels_ = kernel_launches() - launches_before;
+  add_kernel_launches(-solve_graph_kernels_);  // captured, not executed
   cudaError_t ce = cudaStreamEndCapture(stream_, &solve_graph_);
-  if (check_cuda(ce, "end capture")) return -10;
+  if (check_cuda(cerr, "solve kernel launch") || check_cuda(ce, "end capture")) return -10;
   if (check_cuda(cudaGraphInstantiate(&solve_exec_, solve_graph_, 0), "instantiate")) return -10;
   return 0;
 }
@@ -714,6 +812,7 @@ int Tree::solve_device(double* x) {
   const int n = st_.n;
   cudaMemcpyAsync(d_xw_, x, sizeof(double) * n, cudaMemcpyDeviceToDevice, stream_);
   if (check_cuda(cudaGraphLaunch(solve_exec_, stream_), "solve graph")) return -10;
+  add_kernel_launches(solve_graph_kernels_);
   cudaMemcpyAsync(x, d_xw_, sizeof(double) * n, cudaMemcpyDeviceToDevice, stream_);
   return 0;
 }
@@ -744,8 +843,7 @@ int Tree::solve_global(const double* b, double* x) {
 
 int Tree::spmv_device(const double* x, double* y) {
   if (!assembled_) return fail(-4, "spmv called before assemble");
-  launch_spmv(st_.n, d_rowptr_, d_col_, d_val_, x, y, stream_);
-  return 0;
+  return check_cuda(launch_spmv(st_.n, d_rowptr_, d_col_, d_val_, x, y, stream_), "spmv");
 }
 
 int Tree::spmv_host(const double* x, double* y) {
@@ -786,12 +884,24 @@ int Tree::gmres_device(double* b, int maxit, double gtol, int* iters, double* re
   cudaMemsetAsync(done, 0, sizeof(unsigned int), stream_);
   cudaMemcpyAsync(bsave, b, sizeof(double) * n, cudaMemcpyDeviceToDevice, stream_);
   cudaMemcpyAsync(q, b, sizeof(double) * n, cudaMemcpyDeviceToDevice, stream_);
-  solve_device(q);
-  launch_mgs_step(n, q, nullptr, nullptr, nullptr, partial, done, hcol, 1, stream_);  // ||r||
-  launch_scale_copy(n, q, hcol, Q, stream_);
+  if (int src = solve_device(q)) {
+    cudaFree(Q);
+    cudaFree(q);
+    cudaFree(bsave);
+    cudaFree(hcol);
+    cudaFree(partial);
+    cudaFree(done);
+    return src;
+  }
+  cudaError_t ge = cudaSuccess;
+  auto g = [&](cudaError_t e) {
+    if (!ge) ge = e;
+  };
+  g(launch_mgs_step(n, q, nullptr, nullptr, nullptr, partial, done, hcol, 1, stream_));  // ||r||
+  g(launch_scale_copy(n, q, hcol, Q, stream_));
   double r_norm = 0;
   cudaMemcpyAsync(&r_norm, hcol, sizeof(double), cudaMemcpyDeviceToHost, stream_);
-  int rc = check_cuda(cudaStreamSynchronize(stream_), "gmres start");
+  int rc = check_cuda(ge ? ge : cudaStreamSynchronize(stream_), "gmres start");
   std::vector<double> H((size_t)(maxit + 1) * maxit, 0.0), cs(maxit, 0.0), sn(maxit, 0.0), beta(maxit + 1, 0.0);
   auto Hc = [&](int i, int j) -> double& { return H[(size_t)j * (maxit + 1) + i]; };
   beta[0] = r_norm;
@@ -800,15 +910,14 @@ int Tree::gmres_device(double* b, int maxit, double gtol, int* iters, double* re
   int nh = 0;
   if (!rc && (std::isnan(r_norm) || device_status() != 0)) rc = fail(-12, "preconditioner apply failed");
   for (; !rc && k < maxit; ++k) {
-    spmv_device(Q + (size_t)k * ldq, q);
-    solve_device(q);
+    if ((rc = spmv_device(Q + (size_t)k * ldq, q)) || (rc = solve_device(q))) break;
     for (int i = 0; i <= k; ++i)
-      launch_mgs_step(n, q, i ? Q + (size_t)(i - 1) * ldq : nullptr, i ? hcol + (i - 1) : nullptr, Q + (size_t)i * ldq,
-                      partial, done, hcol + i, 0, stream_);
-    launch_mgs_step(n, q, Q + (size_t)k * ldq, hcol + k, nullptr, partial, done, hcol + k + 1, 1, stream_);
-    launch_scale_copy(n, q, hcol + k + 1, Q + (size_t)(k + 1) * ldq, stream_);
+      g(launch_mgs_step(n, q, i ? Q + (size_t)(i - 1) * ldq : nullptr, i ? hcol + (i - 1) : nullptr,
+                        Q + (size_t)i * ldq, partial, done, hcol + i, 0, stream_));
+    g(launch_mgs_step(n, q, Q + (size_t)k * ldq, hcol + k, nullptr, partial, done, hcol + k + 1, 1, stream_));
+    g(launch_scale_copy(n, q, hcol + k + 1, Q + (size_t)(k + 1) * ldq, stream_));
     cudaMemcpyAsync(hk.data(), hcol, sizeof(double) * (k + 2), cudaMemcpyDeviceToHost, stream_);
-    if ((rc = check_cuda(cudaStreamSynchronize(stream_), "gmres iteration"))) break;
+    if ((rc = check_cuda(ge ? ge : cudaStreamSynchronize(stream_), "gmres iteration"))) break;
     for (int i = 0; i <= k + 1; ++i) Hc(i, k) = hk[i];
     for (int i = 0; i < k; ++i) {
       const double temp = cs[i] * Hc(i, k) + sn[i] * Hc(i + 1, k);
@@ -845,14 +954,14 @@ int Tree::gmres_device(double* b, int maxit, double gtol, int* iters, double* re
     }
     double* dy = hcol;
     cudaMemcpyAsync(dy, y.data(), sizeof(double) * (k + 1), cudaMemcpyHostToDevice, stream_);
-    launch_combine(n, k + 1, Q, ldq, dy, b, stream_);
-    spmv_device(b, q);
-    launch_sub(n, bsave, q, q, stream_);
-    launch_mgs_step(n, q, nullptr, nullptr, nullptr, partial, done, hcol, 1, stream_);
-    launch_mgs_step(n, bsave, nullptr, nullptr, nullptr, partial, done, hcol + 1, 1, stream_);
-    double nr[2];
+    g(launch_combine(n, k + 1, Q, ldq, dy, b, stream_));
+    g(spmv_device(b, q) ? cudaErrorUnknown : cudaSuccess);
+    g(launch_sub(n, bsave, q, q, stream_));
+    g(launch_mgs_step(n, q, nullptr, nullptr, nullptr, partial, done, hcol, 1, stream_));
+    g(launch_mgs_step(n, bsave, nullptr, nullptr, nullptr, partial, done, hcol + 1, 1, stream_));
+    double nr[2] = {0, 1};
     cudaMemcpyAsync(nr, hcol, sizeof(double) * 2, cudaMemcpyDeviceToHost, stream_);
-    rc = check_cuda(cudaStreamSynchronize(stream_), "gmres finish");
+    rc = check_cuda(ge ? ge : cudaStreamSynchronize(stream_), "gmres finish");
     *iters = k;
     *relres = nr[0] / nr[1];
     last_gmres_iters = k;
@@ -892,18 +1001,19 @@ int Tree::get_block(int n1, int n2, double* out, int* rows, int* cols, int* ld) 
   return 0;
 }
 
-// which: 0 = T of an interior's diagonal QR (n x n), 1 = scaling T (n x n),
-// 2 = sparsification reflectors V (n x rank), 3 = their T (rank x rank).
+// which: 0 = block factors of an interior's diagonal QR (32 x n), 1 = scaling
+// block factors (32 x n), 2 = sparsification reflectors V (n x rank), 3 = their
+// block factors (32 x rank).
 int Tree::get_factor(int order, int which, double* out, int* shape) const {
   if (!factorized_ || order < 0 || order >= (int)size_.size()) return -4;
   const double* p = nullptr;
   int r = 0, c = 0, ld = 0;
   const int n = size_org_[order];
   switch (which) {
-    case 0: p = T_[order]; r = c = ld = n; break;
-    case 1: p = Ts_[order]; r = c = ld = n; break;
+    case 0: p = T_[order]; r = ld = dev_nb(); c = n; break;
+    case 1: p = Ts_[order]; r = ld = dev_nb(); c = n; break;
     case 2: p = Qsp_[order]; r = ld = n; c = size_[order]; break;
-    case 3: p = Tsp_[order]; r = c = size_[order]; ld = n; break;
+    case 3: p = Tsp_[order]; r = ld = dev_nb(); c = size_[order]; break;
     default: return -1;
   }
   if (!p) return -1;

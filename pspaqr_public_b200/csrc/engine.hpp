@@ -39,6 +39,9 @@ class Arena {
 
 struct LevelTiming {
   float elim_ms = 0, scale_ms = 0, spars_ms = 0, merge_ms = 0;
+  // finer split: geqrt+tsqrt chains, trailing updates, scaling QR, scaling
+  // applies, RRQR, compression applies
+  float e1_ms = 0, e2_ms = 0, sqr_ms = 0, sapp_ms = 0, rrqr_ms = 0, capp_ms = 0;
   int ntasks_elim = 0, ntasks_upd = 0, nspars = 0;
 };
 
@@ -97,6 +100,8 @@ class Tree {
   int check_cuda(cudaError_t e, const char* where);
   void* upload(const void* host, size_t bytes);   // into the per-level scratch arena
   int build_solve_graph();
+  // one zeroed region for the blocks of `edges`; sets ptr_/ld_ (rows_/cols_ must be set)
+  int alloc_level_blocks(const std::vector<int>& edges);
 
   Structure st_;
   Csc A_;
@@ -130,6 +135,7 @@ class Tree {
   int* d_status_ = nullptr;
   cudaGraphExec_t solve_exec_ = nullptr;
   cudaGraph_t solve_graph_ = nullptr;
+  long long solve_graph_kernels_ = 0;
   double* d_tmp_ = nullptr;    // 2 vectors for host-pointer entry points
   std::vector<LevelTiming> lt_;
   double flops_ = 0;

@@ -1,270 +1,414 @@
 // kernels.cu -- grouped FP64 kernels of the factorization, the preconditioner
-// apply and the Krylov loop.  One CTA per task; tasks of a launch touch
-// disjoint blocks except where noted (forward elimination sweep).
+// apply and the Krylov loop for sm_100a.
+//
+// Factorizations whose work is sequential over reflectors (the diagonal QR +
+// tsqrt chain of an interior, the scaling QR, the pivoted QR of the
+// sparsification) run one task per thread-block cluster: the task's 32-column
+// panels are dealt round-robin to the cluster's CTAs, the CTA owning column j
+// builds reflector j, a cluster barrier publishes it, and every CTA applies it
+// to its own panels.  Small tasks use clusters of one CTA.  Block applies that
+// are independent across columns (or rows) are split into chunks, one CTA each.
+#include <cooperative_groups.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cstdint>
 
 #include "dense.cuh"
 #include "kernels.hpp"
 #include "tasks.hpp"
 
+namespace cg = cooperative_groups;
+
 namespace spq {
 namespace {
 
+using dev::kNB;
 using dev::kThreads;
 using dev::kWarps;
 
-constexpr int kRed = 16;        // reduction scratch (doubles)
-constexpr int kWcap = 6144;     // W scratch (doubles) of the blocked reflector applies
+constexpr int kRed = 16;     // reduction scratch (doubles)
+constexpr int kWcap = 4096;  // W scratch (doubles) of the chunked block applies
 
-// W scratch of `wcap` doubles holds W and W2 (k x chunk each); the launcher
-// guarantees wcap >= 2*k for every k of the launch.
-__device__ __forceinline__ int chunk_for(int k, int wcap) {
-  int c = (wcap / 2) / (k > 0 ? k : 1);
-  return c < 1 ? 1 : c;
+__device__ __forceinline__ void csync(int cs) {
+  if (cs > 1) cg::this_cluster().sync();
+  else __syncthreads();
 }
+__device__ __forceinline__ int crank(int cs) { return cs > 1 ? (int)cg::this_cluster().block_rank() : 0; }
+__device__ __forceinline__ bool owns(int col, int rank, int cs) { return ((col / kNB) % cs) == rank; }
 
 // ------------------------------------------------------------ assembly
 __global__ void k_scatter(int nnz, const double* __restrict__ val, double* const* __restrict__ dst) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nnz; i += gridDim.x * blockDim.x) *dst[i] = val[i];
 }
 
-// ------------------------------------------------------------ elimination
-__global__ void __launch_bounds__(kThreads) k_elim(const ElimTask* __restrict__ tasks, const ElimOut* __restrict__ outs) {
+// ------------------------------------------------------------ distributed Householder QR
+// Reflector j of a geqrt (unit = 1: v = [1; S(j+1:m, j)]) or of a tpqrt step
+// (unit = 0: v = [1 (on R(j,j)); B(:, j)]).  The owner of column j computes it;
+// after the cluster barrier every CTA loads the tail into shared `vb` and
+// applies H_j to its own columns k > j.  `lt` holds the owner's tau values for
+// its panels (T factors), `tg` broadcasts tau through global memory.
+__device__ void dist_qr(double* R, int ldr, double* B, int ldb, int m, int n, int unit, double* Tout, double* tg,
+                        double* lt, double* vb, double* red, double* tmp, int cs) {
+  const int rank = crank(cs);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  // unit: reflector tails live in R itself (rows j+1..m-1 of column j), m rows
+  // pentagonal: tails are the m rows of B, the diagonal lives in R
+  for (int j = 0; j < n; ++j) {
+    const int vlen = unit ? (m - j - 1) : m;
+    double* tail = unit ? (R + (j + 1) + (size_t)j * ldr) : (B + (size_t)j * ldb);
+    if (owns(j, rank, cs)) {
+      double s = 0.0;
+      for (int i = threadIdx.x; i < vlen; i += kThreads) s += tail[i] * tail[i];
+      s = dev::cta_sum(s, red);
+      const double alpha = R[j + (size_t)j * ldr];
+      double beta, scal;
+      const double tj = dev::house(alpha, s, &beta, &scal);
+      if (tj != 0.0)
+        for (int i = threadIdx.x; i < vlen; i += kThreads) tail[i] *= scal;
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        R[j + (size_t)j * ldr] = beta;
+        lt[j] = tj;
+        tg[j] = tj;
+      }
+      __threadfence();
+    }
+    csync(cs);
+    const double tj = __ldcg(tg + j);
+    if (tj != 0.0) {
+      for (int i = threadIdx.x; i < vlen; i += kThreads) vb[i] = __ldcg(tail + i);
+      __syncthreads();
+      // apply H_j to own columns k > j
+      for (int k = j + 1 + warp; k < n; k += kWarps) {
+        if (!owns(k, rank, cs)) continue;
+        double* rjk = R + j + (size_t)k * ldr;
+        double* tk = unit ? (R + (j + 1) + (size_t)k * ldr) : (B + (size_t)k * ldb);
+        double d = lane == 0 ? *rjk : 0.0;
+        for (int i = lane; i < vlen; i += 32) d += vb[i] * tk[i];
+        d = dev::warp_sum(d) * tj;
+        if (lane == 0) *rjk -= d;
+        for (int i = lane; i < vlen; i += 32) tk[i] -= vb[i] * d;
+      }
+    }
+    __syncthreads();
+  }
+  // block factors of own panels
+  for (int j0 = rank * kNB; j0 < n; j0 += cs * kNB) {
+    const int kb = (n - j0) < kNB ? (n - j0) : kNB;
+    if (unit)
+      dev::panel_t(R + j0 + (size_t)j0 * ldr, ldr, m - j0, kb, 1, lt + j0, Tout + (size_t)j0 * kNB, kNB, tmp);
+    else
+      dev::panel_t(B + (size_t)j0 * ldb, ldb, m, kb, 0, lt + j0, Tout + (size_t)j0 * kNB, kNB, tmp);
+  }
+  csync(cs);
+}
+
+__global__ void __launch_bounds__(kThreads) k_elim(const ElimTask* __restrict__ tasks, const ElimOut* __restrict__ outs,
+                                                   int cs, int vmax) {
   extern __shared__ double sm[];
-  const ElimTask t = tasks[blockIdx.x];
+  const ElimTask t = tasks[blockIdx.x / cs];
   double* red = sm;
-  double* tau = sm + kRed;
-  double* tmp = tau + t.n;
-  dev::geqrt(t.S, t.n, t.n, t.n, t.T, t.n, tau, red, tmp);
+  double* tmp = red + kRed;
+  double* lt = tmp + kNB;
+  double* vb = lt + t.n;
+  (void)vmax;
+  dist_qr(t.S, t.n, nullptr, 0, t.n, t.n, 1, t.T, t.tau, lt, vb, red, tmp, cs);
   for (int o = t.out_begin; o < t.out_end; ++o) {
     const ElimOut e = outs[o];
-    dev::tpqrt(t.S, t.n, e.B, e.m, e.m, t.n, e.T, t.n, tau, red, tmp);
+    dist_qr(t.S, t.n, e.B, e.m, e.m, t.n, 0, e.T, t.tau, lt, vb, red, tmp, cs);
   }
 }
 
-__global__ void __launch_bounds__(kThreads) k_update(const UpdTask* __restrict__ tasks, const UpdOp* __restrict__ ops,
-                                                     int wcap) {
+__global__ void __launch_bounds__(kThreads) k_scale(const ScaleTask* __restrict__ tasks, int cs) {
+  extern __shared__ double sm[];
+  const ScaleTask t = tasks[blockIdx.x / cs];
+  double* red = sm;
+  double* tmp = red + kRed;
+  double* lt = tmp + kNB;
+  double* vb = lt + t.n;
+  dist_qr(t.S, t.n, nullptr, 0, t.n, t.n, 1, t.T, t.tau, lt, vb, red, tmp, cs);
+}
+
+// ------------------------------------------------------------ chunked applies
+__global__ void __launch_bounds__(kThreads) k_update(const UpdTask* __restrict__ tasks, const UpdOp* __restrict__ ops) {
   extern __shared__ double sm[];
   const UpdTask t = tasks[blockIdx.x];
   for (int o = t.op_begin; o < t.op_end; ++o) {
     const UpdOp op = ops[o];
     if (op.kind == 0)
-      dev::apply_qt_left(op.V, op.ldv, op.T, op.k, op.k, op.A, op.lda, op.m, t.ncols, sm, chunk_for(op.k, wcap));
+      dev::apply_qt(op.V, op.ldv, op.T, op.k, op.A + (size_t)t.col0 * op.lda, op.lda, op.m, t.ncols, sm, kWcap);
     else
-      dev::apply_tpqt_left(op.V, op.ldv, op.T, op.k, op.k, op.A, op.lda, op.B, op.ldb, op.m, t.ncols, sm,
-                           chunk_for(op.k, wcap));
+      dev::apply_tpqt(op.V, op.ldv, op.T, op.k, op.A + (size_t)t.col0 * op.lda, op.lda, op.B + (size_t)t.col0 * op.ldb,
+                      op.ldb, op.m, t.ncols, sm, kWcap);
   }
 }
 
-// ------------------------------------------------------------ scaling
-__global__ void __launch_bounds__(kThreads) k_scale(const ScaleTask* __restrict__ tasks) {
+// row scaling: columns [lo, lo+cnt) of A <- Qs^T A
+__global__ void __launch_bounds__(kThreads) k_edge_left(const EdgeChunk* __restrict__ tasks) {
   extern __shared__ double sm[];
-  const ScaleTask t = tasks[blockIdx.x];
-  double* red = sm;
-  double* tau = sm + kRed;
-  double* tmp = tau + t.n;
-  dev::geqrt(t.S, t.n, t.n, t.n, t.T, t.n, tau, red, tmp);
+  const EdgeChunk t = tasks[blockIdx.x];
+  const int k = t.kdev ? *t.kdev : t.k;
+  int cnt = t.cnt;
+  if (t.limdev) {
+    const int lim = *t.limdev;
+    if (t.lo >= lim) return;
+    cnt = min(cnt, lim - t.lo);
+  }
+  dev::apply_qt(t.V, t.ldv, t.T, k, t.A + (size_t)t.lo * t.lda, t.lda, t.m, cnt, sm, kWcap);
 }
 
-__global__ void __launch_bounds__(kThreads) k_scale_edge(const ScaleEdgeTask* __restrict__ tasks, int wcap) {
+// column scaling: rows [lo, lo+cnt) of A <- A R^{-1}
+__global__ void __launch_bounds__(kThreads) k_edge_trsm(const EdgeChunk* __restrict__ tasks) {
+  const EdgeChunk t = tasks[blockIdx.x];
+  dev::trsm_right_upper(t.V, t.ldv, t.A + t.lo, t.lda, t.cnt, t.nc);
+}
+
+// right compression: rows [lo, lo+cnt) of A <- A Q
+__global__ void __launch_bounds__(kThreads) k_edge_right(const EdgeChunk* __restrict__ tasks) {
   extern __shared__ double sm[];
-  const ScaleEdgeTask t = tasks[blockIdx.x];
-  if (t.Qr) dev::apply_qt_left(t.Qr, t.ldqr, t.Tr, t.ldqr, t.m, t.A, t.lda, t.m, t.nc, sm, chunk_for(t.m, wcap));
-  if (t.Qc) dev::trsm_right_upper(t.Qc, t.ldqc, t.A, t.lda, t.m, t.nc);
+  const EdgeChunk t = tasks[blockIdx.x];
+  const int k = t.kdev ? *t.kdev : t.k;
+  dev::apply_q_right(t.V, t.ldv, t.T, k, t.A + t.lo, t.lda, t.cnt, t.nc, sm, kWcap);
 }
 
 // ------------------------------------------------------------ RRQR
-// Column-pivoted Householder QR of C (m x w), stopped at the first i >= 1 with
+// Column-pivoted Householder QR of C (m x w) stopped at the first i >= 1 with
 // |R(i,i)| / |R(0,0)| < tol (util.cpp:830-851 choose_rank on the dgeqp3
-// diagonal).  Pivoting and norm downdating follow LAPACK dlaqp2.
-__global__ void __launch_bounds__(kThreads) k_rrqr(const RrqrTask* __restrict__ tasks,
-                                                   const RrqrSrc* __restrict__ srcs, double tol,
-                                                   double pivot_rtol) {
+// diagonal).  Pivot and norm downdating follow LAPACK dlaqp2, with the pivot
+// taken as the first POSITION (LAPACK's column order after its swaps) whose
+// partial norm is within pivot_rtol of the largest.  Columns stay in place;
+// pos[] (per CTA, own columns) and colat[] (global) track the swaps.
+__global__ void __launch_bounds__(kThreads) k_rrqr(const RrqrTask* __restrict__ tasks, const RrqrSrc* __restrict__ srcs,
+                                                   double tol, double pivot_rtol, int cs, int wloc_max) {
   extern __shared__ double sm[];
-  __shared__ int s_piv;
-  __shared__ double s_v[kWarps];
-  __shared__ int s_i[kWarps];
-  const RrqrTask t = tasks[blockIdx.x];
+  __shared__ double s_x[2][kWarps];
+  __shared__ int s_k[2][kWarps];
+  __shared__ double s_cmax;   // this CTA's max partial norm (read by the cluster)
+  __shared__ int s_cpos, s_ccol;
+  const RrqrTask t = tasks[blockIdx.x / cs];
+  const int rank = crank(cs);
   const int m = t.m, w = t.w;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   double* C = t.C;
   double* red = sm;
-  double* tau = sm + kRed;
-  double* tmp = tau + (m > 0 ? m : 1);
-  // assemble C
-  int col = 0;
-  for (int s = t.src_begin; s < t.src_end; ++s) {
-    const RrqrSrc src = srcs[s];
-    if (src.transpose) {
-      for (int idx = threadIdx.x; idx < src.rows * m; idx += kThreads) {
-        const int i = idx % src.rows, j = idx / src.rows;
-        C[j + (size_t)(col + i) * m] = src.A[i + (size_t)j * src.lda];
-      }
-      col += src.rows;
-    } else {
-      for (int idx = threadIdx.x; idx < m * src.cols; idx += kThreads) {
-        const int i = idx % m, j = idx / m;
-        C[i + (size_t)(col + j) * m] = src.A[i + (size_t)j * src.lda];
-      }
-      col += src.cols;
-    }
-  }
-  __syncthreads();
+  double* tmp = red + kRed;
+  double* vb = tmp + kNB;
+  double* ltau = vb + (m > 0 ? m : 1);
+  int* pos = reinterpret_cast<int*>(ltau + (m > 0 ? m : 1));  // own columns, by local index
+  (void)wloc_max;
   double* vn1 = t.vn;
   double* vn2 = t.vn + w;
-  for (int j = warp; j < w; j += kWarps) {
-    const double* cj = C + (size_t)j * m;
-    double s = 0.0;
-    for (int i = lane; i < m; i += 32) s += cj[i] * cj[i];
-    s = sqrt(dev::warp_sum(s));
-    if (lane == 0) {
-      vn1[j] = s;
-      vn2[j] = s;
-      t.jpvt[j] = j;
+  // assemble own panels of C
+  {
+    int col = 0;
+    for (int s = t.src_begin; s < t.src_end; ++s) {
+      const RrqrSrc src = srcs[s];
+      const int width = src.transpose ? src.rows : src.cols;
+      for (int idx = threadIdx.x; idx < width * m; idx += kThreads) {
+        const int c = idx / m, r = idx % m;
+        const int gc = col + c;
+        if (!owns(gc, rank, cs)) continue;
+        C[r + (size_t)gc * m] = src.transpose ? src.A[c + (size_t)r * src.lda] : src.A[r + (size_t)c * src.lda];
+      }
+      col += width;
     }
   }
   __syncthreads();
+  // own columns: local index li <-> global column gc
+  const int npan = (w + kNB - 1) / kNB;
+  auto gcol = [&](int li) { return ((li / kNB) * cs + rank) * kNB + (li % kNB); };
+  const int own_pan = (npan - rank + cs - 1) / cs;
+  int nloc = 0;
+  if (own_pan > 0) {
+    const int last_pan = rank + (own_pan - 1) * cs;
+    nloc = (own_pan - 1) * kNB + min(kNB, w - last_pan * kNB);
+  }
+  for (int li = warp; li < nloc; li += kWarps) {
+    const int gc = gcol(li);
+    const double* cj = C + (size_t)gc * m;
+    double s = 0.0;
+    for (int r = lane; r < m; r += 32) s += cj[r] * cj[r];
+    s = sqrt(dev::warp_sum(s));
+    if (lane == 0) {
+      vn1[gc] = s;
+      vn2[gc] = s;
+      pos[li] = gc;
+      t.colat[gc] = gc;
+    }
+  }
+  __syncthreads();
+  csync(cs);
   const int kmin = m < w ? m : w;
   const double tol3z = sqrt(1.1102230246251565e-16);
-  int rank = kmin;
-  double r00 = 0.0;
+  int rk = kmin;
   for (int i = 0; i < kmin; ++i) {
-    // pivot = first column whose partial norm is within pivot_rtol of the
-    // largest remaining one (pivot_rtol = 0: LAPACK idamax, first maximum)
+    // (a) largest partial norm over active columns (position >= i)
     double bv = -1.0;
-    for (int j = i + threadIdx.x; j < w; j += kThreads) bv = fmax(bv, vn1[j]);
-#pragma unroll
+    for (int li = threadIdx.x; li < nloc; li += kThreads)
+      if (pos[li] >= i) bv = fmax(bv, vn1[gcol(li)]);
     for (int o = 16; o > 0; o >>= 1) bv = fmax(bv, __shfl_xor_sync(0xffffffffu, bv, o));
-    if (lane == 0) s_v[warp] = bv;
+    if (lane == 0) s_x[0][warp] = bv;
     __syncthreads();
     if (threadIdx.x == 0) {
-      double v = s_v[0];
-      for (int q = 1; q < kWarps; ++q) v = fmax(v, s_v[q]);
-      s_v[0] = v;
+      double v = s_x[0][0];
+      for (int q = 1; q < kWarps; ++q) v = fmax(v, s_x[0][q]);
+      s_cmax = v;
     }
-    __syncthreads();
-    const double thr = s_v[0] * (1.0 - pivot_rtol);
-    int bi = w;
-    for (int j = i + threadIdx.x; j < w; j += kThreads)
-      if (vn1[j] >= thr) {
-        bi = j;
-        break;
+    csync(cs);
+    double gmax = -1.0;
+    if (cs > 1) {
+      cg::cluster_group cl = cg::this_cluster();
+      for (int q = 0; q < cs; ++q) gmax = fmax(gmax, *cl.map_shared_rank(&s_cmax, q));
+    } else {
+      gmax = s_cmax;
+    }
+    // (b) first position with vn1 >= (1 - pivot_rtol) * max
+    const double thr = gmax * (1.0 - pivot_rtol);
+    int bp = 0x7fffffff, bc = -1;
+    for (int li = threadIdx.x; li < nloc; li += kThreads) {
+      const int p = pos[li];
+      if (p >= i && p < bp && vn1[gcol(li)] >= thr) {
+        bp = p;
+        bc = gcol(li);
       }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) bi = min(bi, __shfl_xor_sync(0xffffffffu, bi, o));
-    __syncthreads();
-    if (lane == 0) s_i[warp] = bi;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      int id = s_i[0];
-      for (int q = 1; q < kWarps; ++q) id = min(id, s_i[q]);
-      s_piv = (id >= i && id < w) ? id : i;  // no finite maximum (NaN norms): keep column i
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+      const int op = __shfl_xor_sync(0xffffffffu, bp, o);
+      const int oc = __shfl_xor_sync(0xffffffffu, bc, o);
+      if (op < bp) {
+        bp = op;
+        bc = oc;
+      }
+    }
+    if (lane == 0) {
+      s_k[0][warp] = bp;
+      s_k[1][warp] = bc;
     }
     __syncthreads();
-    const int pvt = s_piv;
-    if (pvt != i) {
-      double* ci = C + (size_t)i * m;
-      double* cp = C + (size_t)pvt * m;
+    if (threadIdx.x == 0) {
+      int p = s_k[0][0], c = s_k[1][0];
+      for (int q = 1; q < kWarps; ++q)
+        if (s_k[0][q] < p) {
+          p = s_k[0][q];
+          c = s_k[1][q];
+        }
+      s_cpos = p;
+      s_ccol = c;
+    }
+    csync(cs);
+    int ppos = 0x7fffffff, pcol = -1;
+    if (cs > 1) {
+      cg::cluster_group cl = cg::this_cluster();
+      for (int q = 0; q < cs; ++q) {
+        const int p = *cl.map_shared_rank(&s_cpos, q);
+        const int c = *cl.map_shared_rank(&s_ccol, q);
+        if (p < ppos) {
+          ppos = p;
+          pcol = c;
+        }
+      }
+    } else {
+      ppos = s_cpos;
+      pcol = s_ccol;
+    }
+    if (pcol < 0) {  // no finite maximum (NaN norms): take the column at position i
+      ppos = i;
+      pcol = __ldcg(t.colat + i);
+    }
+    // (c) the owner of the pivot column builds reflector i and books the swap
+    const int cur = __ldcg(t.colat + i);  // column now at position i
+    if (owns(pcol, rank, cs)) {
+      double* cp = C + (size_t)pcol * m;
+      double s = 0.0;
+      for (int r = i + 1 + threadIdx.x; r < m; r += kThreads) s += cp[r] * cp[r];
+      s = dev::cta_sum(s, red);
+      const double alpha = cp[i];
+      double beta, scal;
+      const double ti = dev::house(alpha, s, &beta, &scal);
+      double* vo = t.V + (size_t)i * m;
       for (int r = threadIdx.x; r < m; r += kThreads) {
-        const double a = ci[r];
-        ci[r] = cp[r];
-        cp[r] = a;
+        double v = 0.0;
+        if (r == i) v = 1.0;
+        else if (r > i) v = ti != 0.0 ? cp[r] * scal : cp[r];
+        vo[r] = v;
       }
       if (threadIdx.x == 0) {
-        vn1[pvt] = vn1[i];
-        vn2[pvt] = vn2[i];
-        const int ip = t.jpvt[pvt];
-        t.jpvt[pvt] = t.jpvt[i];
-        t.jpvt[i] = ip;
+        t.tau[i] = ti;
+        double stop = 0.0;
+        const double absb = fabs(beta);
+        if (i == 0) t.bc[2] = absb;
+        else if (!(absb / __ldcg(t.bc + 2) >= tol)) stop = 1.0;
+        t.bc[i & 1] = stop;
       }
-      __syncthreads();
+      __threadfence();
     }
-    double* ci = C + (size_t)i * m;
-    double s = 0.0;
-    for (int r = i + 1 + threadIdx.x; r < m; r += kThreads) s += ci[r] * ci[r];
-    s = dev::cta_sum(s, red);
-    const double alpha = ci[i];
-    double beta, scal;
-    const double ti = dev::house(alpha, s, &beta, &scal);
-    const double absb = fabs(beta);
-    if (i == 0) r00 = absb;
-    else if (!(absb / r00 >= tol)) {
-      rank = i;
+    csync(cs);
+    if (__ldcg(t.bc + (i & 1)) != 0.0) {
+      rk = i;
       break;
     }
-    if (ti != 0.0)
-      for (int r = i + 1 + threadIdx.x; r < m; r += kThreads) ci[r] *= scal;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      ci[i] = beta;
-      tau[i] = ti;
-      t.tau[i] = ti;
+    // every CTA has read colat[i] above; book the swap for the next steps
+    if (owns(pcol, rank, cs) && threadIdx.x == 0) {
+      t.colat[ppos] = cur;
+      t.colat[i] = pcol;
+      __threadfence();
     }
-    for (int j = i + 1 + warp; j < w; j += kWarps) {
-      double* cj = C + (size_t)j * m;
-      double d = lane == 0 ? cj[i] : 0.0;
-      for (int r = i + 1 + lane; r < m; r += 32) d += ci[r] * cj[r];
-      d = dev::warp_sum(d) * ti;
-      const double top = __shfl_sync(0xffffffffu, cj[i], 0) - d;
-      __syncwarp();
-      if (lane == 0) cj[i] = top;
-      for (int r = i + 1 + lane; r < m; r += 32) cj[r] -= ci[r] * d;
-      __syncwarp();
-      const double v1 = vn1[j];
+    // (d) position bookkeeping of own columns
+    for (int li = threadIdx.x; li < nloc; li += kThreads) {
+      const int gc = gcol(li);
+      if (gc == pcol) pos[li] = i;
+      else if (gc == cur) pos[li] = ppos;
+    }
+    const double ti = __ldcg(t.tau + i);
+    for (int r = threadIdx.x; r < m - i; r += kThreads) vb[r] = __ldcg(t.V + (size_t)i * m + i + r);
+    __syncthreads();
+    // (e) apply H_i to own active columns and downdate their norms
+    for (int li = warp; li < nloc; li += kWarps) {
+      if (pos[li] <= i) continue;
+      const int gc = gcol(li);
+      double* cj = C + (size_t)gc * m;
+      if (ti != 0.0) {
+        double d = 0.0;
+        for (int r = lane; r < m - i; r += 32) d += vb[r] * cj[i + r];
+        d = dev::warp_sum(d) * ti;
+        __syncwarp();
+        for (int r = lane; r < m - i; r += 32) cj[i + r] -= vb[r] * d;
+        __syncwarp();
+      }
+      const double v1 = vn1[gc];
       if (v1 != 0.0) {
-        double temp = fabs(top) / v1;
+        double temp = fabs(cj[i]) / v1;
         temp = 1.0 - temp * temp;
         temp = temp < 0.0 ? 0.0 : temp;
-        const double q = v1 / vn2[j];
-        const double temp2 = temp * q * q;
-        if (temp2 <= tol3z) {
+        const double q = v1 / vn2[gc];
+        if (temp * q * q <= tol3z) {
           double nn = 0.0;
           for (int r = i + 1 + lane; r < m; r += 32) nn += cj[r] * cj[r];
           nn = (i + 1 < m) ? sqrt(dev::warp_sum(nn)) : 0.0;
           if (lane == 0) {
-            vn1[j] = nn;
-            vn2[j] = nn;
+            vn1[gc] = nn;
+            vn2[gc] = nn;
           }
         } else if (lane == 0) {
-          vn1[j] = v1 * sqrt(temp);
+          vn1[gc] = v1 * sqrt(temp);
         }
       }
       __syncwarp();
     }
     __syncthreads();
   }
-  __syncthreads();
-  // block factor of the kept reflectors
-  const int npairs = rank * (rank - 1) / 2;
-  for (int p = warp; p < npairs; p += kWarps) {
-    int j = (int)((1.0 + sqrt(1.0 + 8.0 * p)) * 0.5);
-    while (j * (j - 1) / 2 > p) --j;
-    while ((j + 1) * j / 2 <= p) ++j;
-    const int l = p - j * (j - 1) / 2;
-    const double* cl = C + (size_t)l * m;
-    const double* cj = C + (size_t)j * m;
-    double d = lane == 0 ? cl[j] : 0.0;
-    for (int r = j + 1 + lane; r < m; r += 32) d += cl[r] * cj[r];
-    d = dev::warp_sum(d);
-    if (lane == 0) t.T[l + (size_t)j * m] = d;
+  csync(cs);
+  // block factors of the kept reflectors, panels dealt over the cluster
+  for (int j0 = rank * kNB; j0 < rk; j0 += cs * kNB) {
+    const int kb = (rk - j0) < kNB ? (rk - j0) : kNB;
+    for (int q = threadIdx.x; q < kb; q += kThreads) ltau[q] = __ldcg(t.tau + j0 + q);
+    __syncthreads();
+    dev::panel_t(t.V + j0 + (size_t)j0 * m, m, m - j0, kb, 1, ltau, t.T + (size_t)j0 * kNB, kNB, tmp);
   }
-  __syncthreads();
-  dev::larft_from_gram(t.T, m, rank, tau, tmp);
-  if (threadIdx.x == 0) *t.rank = rank;
-}
-
-__global__ void __launch_bounds__(kThreads) k_spars_edge(const SparsEdgeTask* __restrict__ tasks, int wcap) {
-  extern __shared__ double sm[];
-  const SparsEdgeTask t = tasks[blockIdx.x];
-  const int rc = t.Vc ? *t.rank_c : t.nc;
-  if (t.Vc) dev::apply_q_right(t.Vc, t.ldvc, t.Tc, t.ldvc, rc, t.A, t.lda, t.m, t.nc, sm, chunk_for(rc, wcap));
-  if (t.Vr) {
-    const int rr = *t.rank_r;
-    dev::apply_qt_left(t.Vr, t.ldvr, t.Tr, t.ldvr, rr, t.A, t.lda, t.m, rc, sm, chunk_for(rr, wcap));
-  }
+  if (rank == 0 && threadIdx.x == 0) *t.rank = rk;
+  csync(cs);
 }
 
 // ------------------------------------------------------------ merge
@@ -296,7 +440,7 @@ __device__ __forceinline__ void st_release(int* p, int v) {
 // cannot deadlock; a wait that exceeds `spin_limit` cycles sets *status = 2.
 __global__ void __launch_bounds__(kThreads) k_fwd_elim(const FwdElimTask* __restrict__ tasks,
                                                        const FwdOut* __restrict__ outs, int ntasks, int* ticket,
-                                                       int* status, long long spin_limit) {
+                                                       int* status, long long spin_limit, int nmax) {
   extern __shared__ double sm[];
   __shared__ int s_task, s_abort;
   if (threadIdx.x == 0) {
@@ -307,12 +451,12 @@ __global__ void __launch_bounds__(kThreads) k_fwd_elim(const FwdElimTask* __rest
   const int ti = s_task;
   if (ti >= ntasks) return;
   const FwdElimTask t = tasks[ti];
-  double* xc = sm;
-  double* w = xc + t.n;
-  double* xn = w + 2 * (t.n > 0 ? t.n : 1);
+  double* w = sm;
+  double* xc = w + 2 * kNB;
+  double* xn = xc + (nmax > 0 ? nmax : 1);
   for (int i = threadIdx.x; i < t.n; i += kThreads) xc[i] = __ldcg(t.x + i);
   __syncthreads();
-  dev::apply_qt_vec(t.S, t.n, t.T, t.n, t.n, xc, t.n, w);
+  dev::apply_qt(t.S, t.n, t.T, t.n, xc, t.n, t.n, 1, w, 2 * kNB);
   for (int o = t.out_begin; o < t.out_end; ++o) {
     const FwdOut e = outs[o];
     if (threadIdx.x == 0) {
@@ -337,7 +481,7 @@ __global__ void __launch_bounds__(kThreads) k_fwd_elim(const FwdElimTask* __rest
     if (s_abort) return;
     for (int i = threadIdx.x; i < e.m; i += kThreads) xn[i] = __ldcg(e.xn + i);
     __syncthreads();
-    dev::apply_tpqt_left(e.V, e.m, e.T, t.n, t.n, xc, t.n, xn, e.m, e.m, 1, w, 1);
+    dev::apply_tpqt(e.V, e.m, e.T, t.n, xc, t.n, xn, e.m, e.m, 1, w, 2 * kNB);
     for (int i = threadIdx.x; i < e.m; i += kThreads) __stcg(e.xn + i, xn[i]);
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -351,24 +495,24 @@ __global__ void __launch_bounds__(kThreads) k_fwd_elim(const FwdElimTask* __rest
 __global__ void __launch_bounds__(kThreads) k_fwd_spars(const FwdSparsTask* __restrict__ tasks) {
   extern __shared__ double sm[];
   const FwdSparsTask t = tasks[blockIdx.x];
-  double* x = sm;
-  double* w = sm + t.n;
+  double* w = sm;
+  double* x = sm + 2 * kNB;
   for (int i = threadIdx.x; i < t.n; i += kThreads) x[i] = t.x[i];
   __syncthreads();
-  dev::apply_qt_vec(t.Qs, t.n, t.Ts, t.n, t.n, x, t.n, w);
-  dev::apply_qt_vec(t.V, t.n, t.T, t.n, *t.rank, x, t.n, w);
+  dev::apply_qt(t.Qs, t.n, t.Ts, t.n, x, t.n, t.n, 1, w, 2 * kNB);
+  dev::apply_qt(t.V, t.n, t.T, *t.rank, x, t.n, t.n, 1, w, 2 * kNB);
   for (int i = threadIdx.x; i < t.n; i += kThreads) t.x[i] = x[i];
 }
 
 __global__ void __launch_bounds__(kThreads) k_bwd_spars(const FwdSparsTask* __restrict__ tasks) {
   extern __shared__ double sm[];
   const FwdSparsTask t = tasks[blockIdx.x];
-  double* x = sm;
-  double* w = sm + t.n;
-  double* xs = w + 2 * t.n;
+  double* w = sm;
+  double* xs = w + 2 * kNB;
+  double* x = xs + 32;
   for (int i = threadIdx.x; i < t.n; i += kThreads) x[i] = t.x[i];
   __syncthreads();
-  dev::apply_q_vec(t.V, t.n, t.T, t.n, *t.rank, x, t.n, w);
+  dev::apply_q(t.V, t.n, t.T, *t.rank, x, t.n, t.n, 1, w, 2 * kNB);
   dev::trsv_upper(t.Qs, t.n, x, t.n, xs);
   for (int i = threadIdx.x; i < t.n; i += kThreads) t.x[i] = x[i];
 }
@@ -377,8 +521,8 @@ __global__ void __launch_bounds__(kThreads) k_bwd_elim(const BwdElimTask* __rest
                                                        const BwdIn* __restrict__ ins) {
   extern __shared__ double sm[];
   const BwdElimTask t = tasks[blockIdx.x];
-  double* x = sm;
-  double* xs = sm + t.n;
+  double* xs = sm;
+  double* x = sm + 32;
   for (int i = threadIdx.x; i < t.n; i += kThreads) x[i] = t.x[i];
   __syncthreads();
   for (int q = t.in_begin; q < t.in_end; ++q) {
@@ -466,6 +610,7 @@ __global__ void k_sub(int n, const double* __restrict__ a, const double* __restr
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) c[i] = a[i] - b[i];
 }
 
+
 inline int grid_for(int n, int per = 256, int cap = 148 * 16) {
   int g = (n + per - 1) / per;
   return g < 1 ? 1 : (g > cap ? cap : g);
@@ -476,104 +621,217 @@ inline size_t smem_bytes(size_t doubles) { return doubles * sizeof(double); }
 }  // namespace
 
 // ---------------------------------------------------------------- launchers
-#define SPQ_SET_SMEM(kern, bytes)                                                              \
-  do {                                                                                         \
-    if ((bytes) > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(bytes)); \
-  } while (0)
+namespace {
+std::atomic<long long> g_launches{0};
+inline void counted() { g_launches.fetch_add(1, std::memory_order_relaxed); }
 
-void launch_scatter(int nnz, const double* val, double* const* dst, cudaStream_t st) {
-  if (nnz > 0) k_scatter<<<grid_for(nnz), 256, 0, st>>>(nnz, val, dst);
-}
-void launch_elim(const ElimTask* t, const ElimOut* o, int ntasks, int nmax, cudaStream_t st) {
-  if (ntasks <= 0) return;
-  size_t b = smem_bytes(kRed + 2 * (size_t)nmax);
-  SPQ_SET_SMEM(k_elim, b);
-  k_elim<<<ntasks, kThreads, b, st>>>(t, o);
-}
-inline int wcap_for(int kmax) { return std::max(kWcap, 2 * std::max(kmax, 1)); }
+constexpr size_t kSmemMax = 227 * 1024;
 
-void launch_update(const UpdTask* t, const UpdOp* o, int ntasks, int kmax, cudaStream_t st) {
-  if (ntasks <= 0) return;
-  const int wcap = wcap_for(kmax);
-  size_t b = smem_bytes(wcap);
-  SPQ_SET_SMEM(k_update, b);
-  k_update<<<ntasks, kThreads, b, st>>>(t, o, wcap);
+template <typename K>
+cudaError_t prep(K kern, size_t bytes) {
+  if (bytes > kSmemMax) return cudaErrorInvalidValue;
+  if (bytes > 48 * 1024) return cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  return cudaSuccess;
 }
-void launch_scale(const ScaleTask* t, int ntasks, int nmax, cudaStream_t st) {
-  if (ntasks <= 0) return;
-  size_t b = smem_bytes(kRed + 2 * (size_t)nmax);
-  SPQ_SET_SMEM(k_scale, b);
-  k_scale<<<ntasks, kThreads, b, st>>>(t);
+
+template <typename... KArgs, typename... Args>
+cudaError_t launch_clustered(void (*kern)(KArgs...), int ntasks, int cs, size_t smem, cudaStream_t st,
+                             Args... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)(ntasks * cs));
+  cfg.blockDim = dim3(kThreads);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = (unsigned)cs;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  counted();
+  return cudaLaunchKernelEx(&cfg, kern, static_cast<KArgs>(args)...);
 }
-void launch_scale_edge(const ScaleEdgeTask* t, int ntasks, int kmax, cudaStream_t st) {
-  if (ntasks <= 0) return;
-  const int wcap = wcap_for(kmax);
-  size_t b = smem_bytes(wcap);
-  SPQ_SET_SMEM(k_scale_edge, b);
-  k_scale_edge<<<ntasks, kThreads, b, st>>>(t, wcap);
+
+inline cudaError_t last() { return cudaGetLastError(); }
+thread_local const char* g_last_launch = "";
+// Clears a stale error left by an earlier runtime call so that the status a
+// launcher returns belongs to its own launch; a stale error is reported as is.
+inline cudaError_t begin(const char* name) {
+  g_last_launch = name;
+  return cudaGetLastError();
 }
-void launch_rrqr(const RrqrTask* t, const RrqrSrc* s, int ntasks, int mmax, double tol, double pivot_rtol,
-                 cudaStream_t st) {
-  if (ntasks <= 0) return;
-  size_t b = smem_bytes(kRed + 2 * (size_t)(mmax > 0 ? mmax : 1));
-  SPQ_SET_SMEM(k_rrqr, b);
-  k_rrqr<<<ntasks, kThreads, b, st>>>(t, s, tol, pivot_rtol);
+}  // namespace
+
+const char* last_launch_name() { return g_last_launch; }
+
+long long kernel_launches() { return g_launches.load(); }
+void add_kernel_launches(long long n) { g_launches.fetch_add(n); }
+
+cudaError_t launch_scatter(int nnz, const double* val, double* const* dst, cudaStream_t st) {
+  if (cudaError_t pre = begin("launch_scatter")) return pre;
+  if (nnz <= 0) return cudaSuccess;
+  counted();
+  k_scatter<<<grid_for(nnz), 256, 0, st>>>(nnz, val, dst);
+  return last();
 }
-void launch_spars_edge(const SparsEdgeTask* t, int ntasks, int kmax, cudaStream_t st) {
-  if (ntasks <= 0) return;
-  const int wcap = wcap_for(kmax);
-  size_t b = smem_bytes(wcap);
-  SPQ_SET_SMEM(k_spars_edge, b);
-  k_spars_edge<<<ntasks, kThreads, b, st>>>(t, wcap);
+
+cudaError_t launch_elim(const ElimTask* t, const ElimOut* o, int ntasks, int cs, int nmax, int vmax,
+                        cudaStream_t st) {
+  if (cudaError_t pre = begin("launch_elim")) return pre;
+  if (ntasks <= 0) return cudaSuccess;
+  const size_t b = smem_bytes(kRed + kNB + (size_t)nmax + (size_t)std::max(vmax, 1));
+  cudaError_t e = prep(k_elim, b);
+  if (e) return e;
+  return launch_clustered(k_elim, ntasks, cs, b, st, t, o, cs, vmax);
 }
-void launch_merge(const MergeTask* t, int ntasks, cudaStream_t st) {
-  if (ntasks > 0) k_merge<<<ntasks, 256, 0, st>>>(t);
+
+cudaError_t launch_scale(const ScaleTask* t, int ntasks, int cs, int nmax, cudaStream_t st) {
+  if (cudaError_t pre = begin("launch_scale")) return pre;
+  if (ntasks <= 0) return cudaSuccess;
+  const size_t b = smem_bytes(kRed + kNB + 2 * (size_t)nmax);
+  cudaError_t e = prep(k_scale, b);
+  if (e) return e;
+  return launch_clustered(k_scale, ntasks, cs, b, st, t, cs);
 }
-void launch_fwd_elim(const FwdElimTask* t, const FwdOut* o, int ntasks, int nmax, int mmax, int* ticket, int* status,
-                     long long spin_limit, cudaStream_t st) {
-  if (ntasks <= 0) return;
-  size_t b = smem_bytes(3 * (size_t)(nmax > 0 ? nmax : 1) + (size_t)(mmax > 0 ? mmax : 1));
-  SPQ_SET_SMEM(k_fwd_elim, b);
-  k_fwd_elim<<<ntasks, kThreads, b, st>>>(t, o, ntasks, ticket, status, spin_limit);
+
+cudaError_t launch_update(const UpdTask* t, const UpdOp* o, int ntasks, cudaStream_t st) {
+  if (cudaError_t pre = begin("launch_update")) return pre;
+  if (ntasks <= 0) return cudaSuccess;
+  const size_t b = smem_bytes(kWcap);
+  cudaError_t e = prep(k_update, b);
+  if (e) return e;
+  counted();
+  k_update<<<ntasks, kThreads, b, st>>>(t, o);
+  return last();
 }
-void launch_fwd_spars(const FwdSparsTask* t, int ntasks, int nmax, cudaStream_t st) {
-  if (ntasks <= 0) return;
-  size_t b = smem_bytes(3 * (size_t)nmax);
-  SPQ_SET_SMEM(k_fwd_spars, b);
+
+cudaError_t launch_edge(int kind, const EdgeChunk* t, int ntasks, cudaStream_t st) {
+  if (cudaError_t pre = begin("launch_edge")) return pre;
+  if (ntasks <= 0) return cudaSuccess;
+  const size_t b = smem_bytes(kWcap);
+  cudaError_t e = cudaSuccess;
+  counted();
+  if (kind == 0) {
+    if ((e = prep(k_edge_left, b))) return e;
+    k_edge_left<<<ntasks, kThreads, b, st>>>(t);
+  } else if (kind == 1) {
+    k_edge_trsm<<<ntasks, kThreads, 0, st>>>(t);
+  } else {
+    if ((e = prep(k_edge_right, b))) return e;
+    k_edge_right<<<ntasks, kThreads, b, st>>>(t);
+  }
+  return last();
+}
+
+cudaError_t launch_rrqr(const RrqrTask* t, const RrqrSrc* s, int ntasks, int cs, int mmax, int wloc_max, double tol,
+                        double pivot_rtol, cudaStream_t st) {
+  if (cudaError_t pre = begin("launch_rrqr")) return pre;
+  if (ntasks <= 0) return cudaSuccess;
+  const size_t b = smem_bytes(kRed + kNB + 2 * (size_t)std::max(mmax, 1)) + sizeof(int) * (size_t)(wloc_max + 1);
+  cudaError_t e = prep(k_rrqr, b);
+  if (e) return e;
+  return launch_clustered(k_rrqr, ntasks, cs, b, st, t, s, tol, pivot_rtol, cs, wloc_max);
+}
+
+cudaError_t launch_merge(const MergeTask* t, int ntasks, cudaStream_t st) {
+  if (cudaError_t pre = begin("launch_merge")) return pre;
+  if (ntasks <= 0) return cudaSuccess;
+  counted();
+  k_merge<<<ntasks, 256, 0, st>>>(t);
+  return last();
+}
+
+cudaError_t launch_fwd_elim(const FwdElimTask* t, const FwdOut* o, int ntasks, int nmax, int mmax, int* ticket,
+                            int* status, long long spin_limit, cudaStream_t st) {
+  if (cudaError_t pre = begin("launch_fwd_elim")) return pre;
+  if (ntasks <= 0) return cudaSuccess;
+  const size_t b = smem_bytes(2 * kNB + (size_t)std::max(nmax, 1) + (size_t)std::max(mmax, 1));
+  cudaError_t e = prep(k_fwd_elim, b);
+  if (e) return e;
+  counted();
+  k_fwd_elim<<<ntasks, kThreads, b, st>>>(t, o, ntasks, ticket, status, spin_limit, nmax);
+  return last();
+}
+
+cudaError_t launch_fwd_spars(const FwdSparsTask* t, int ntasks, int nmax, cudaStream_t st) {
+  if (cudaError_t pre = begin("launch_fwd_spars")) return pre;
+  if (ntasks <= 0) return cudaSuccess;
+  const size_t b = smem_bytes(2 * kNB + (size_t)nmax);
+  cudaError_t e = prep(k_fwd_spars, b);
+  if (e) return e;
+  counted();
   k_fwd_spars<<<ntasks, kThreads, b, st>>>(t);
+  return last();
 }
-void launch_bwd_spars(const FwdSparsTask* t, int ntasks, int nmax, cudaStream_t st) {
-  if (ntasks <= 0) return;
-  size_t b = smem_bytes(3 * (size_t)nmax + 32);
-  SPQ_SET_SMEM(k_bwd_spars, b);
+
+cudaError_t launch_bwd_spars(const FwdSparsTask* t, int ntasks, int nmax, cudaStream_t st) {
+  if (cudaError_t pre = begin("launch_bwd_spars")) return pre;
+  if (ntasks <= 0) return cudaSuccess;
+  const size_t b = smem_bytes(2 * kNB + 32 + (size_t)nmax);
+  cudaError_t e = prep(k_bwd_spars, b);
+  if (e) return e;
+  counted();
   k_bwd_spars<<<ntasks, kThreads, b, st>>>(t);
+  return last();
 }
-void launch_bwd_elim(const BwdElimTask* t, const BwdIn* in, int ntasks, int nmax, cudaStream_t st) {
-  if (ntasks <= 0) return;
-  size_t b = smem_bytes((size_t)nmax + 32);
-  SPQ_SET_SMEM(k_bwd_elim, b);
+
+cudaError_t launch_bwd_elim(const BwdElimTask* t, const BwdIn* in, int ntasks, int nmax, cudaStream_t st) {
+  if (cudaError_t pre = begin("launch_bwd_elim")) return pre;
+  if (ntasks <= 0) return cudaSuccess;
+  const size_t b = smem_bytes(32 + (size_t)nmax);
+  cudaError_t e = prep(k_bwd_elim, b);
+  if (e) return e;
+  counted();
   k_bwd_elim<<<ntasks, kThreads, b, st>>>(t, in);
+  return last();
 }
-void launch_copy_idx(int n, const int* src, const int* dst, double* x, cudaStream_t st) {
-  if (n > 0) k_copy_idx<<<grid_for(n), 256, 0, st>>>(n, src, dst, x);
+
+cudaError_t launch_copy_idx(int n, const int* src, const int* dst, double* x, cudaStream_t st) {
+  if (cudaError_t pre = begin("launch_copy_idx")) return pre;
+  if (n <= 0) return cudaSuccess;
+  counted();
+  k_copy_idx<<<grid_for(n), 256, 0, st>>>(n, src, dst, x);
+  return last();
 }
-void launch_spmv(int n, const int* rowptr, const int* col, const double* val, const double* x, double* y,
-                 cudaStream_t st) {
+
+cudaError_t launch_spmv(int n, const int* rowptr, const int* col, const double* val, const double* x, double* y,
+                        cudaStream_t st) {
+  if (cudaError_t pre = begin("launch_spmv")) return pre;
+  counted();
   k_spmv<<<grid_for(n), 256, 0, st>>>(n, rowptr, col, val, x, y);
+  return last();
 }
+
 int mgs_grid(int n) { return grid_for(n, kThreads * 4, 148 * 4); }
-void launch_mgs_step(int n, double* q, const double* Qprev, const double* hprev, const double* Qi, double* partial,
-                     unsigned int* done, double* out, int take_sqrt, cudaStream_t st) {
+
+cudaError_t launch_mgs_step(int n, double* q, const double* Qprev, const double* hprev, const double* Qi,
+                            double* partial, unsigned int* done, double* out, int take_sqrt, cudaStream_t st) {
+  if (cudaError_t pre = begin("launch_mgs_step")) return pre;
+  counted();
   k_mgs_step<<<mgs_grid(n), kThreads, 0, st>>>(n, q, Qprev, hprev, Qi, partial, done, out, take_sqrt);
+  return last();
 }
-void launch_scale_copy(int n, const double* src, const double* s, double* dst, cudaStream_t st) {
+
+cudaError_t launch_scale_copy(int n, const double* src, const double* s, double* dst, cudaStream_t st) {
+  if (cudaError_t pre = begin("launch_scale_copy")) return pre;
+  counted();
   k_scale_copy<<<grid_for(n), 256, 0, st>>>(n, src, s, dst);
+  return last();
 }
-void launch_combine(int n, int k, const double* Q, size_t ldq, const double* y, double* x, cudaStream_t st) {
+
+cudaError_t launch_combine(int n, int k, const double* Q, size_t ldq, const double* y, double* x, cudaStream_t st) {
+  if (cudaError_t pre = begin("launch_combine")) return pre;
+  counted();
   k_combine<<<grid_for(n), 256, 0, st>>>(n, k, Q, ldq, y, x);
+  return last();
 }
-void launch_sub(int n, const double* a, const double* b, double* c, cudaStream_t st) {
+
+cudaError_t launch_sub(int n, const double* a, const double* b, double* c, cudaStream_t st) {
+  if (cudaError_t pre = begin("launch_sub")) return pre;
+  counted();
   k_sub<<<grid_for(n), 256, 0, st>>>(n, a, b, c);
+  return last();
 }
 
 }  // namespace spq

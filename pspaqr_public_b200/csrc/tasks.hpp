@@ -1,35 +1,39 @@
-// tasks.hpp -- descriptors of the grouped (one CTA per task) kernels.
+// tasks.hpp -- descriptors of the grouped kernels.
 //
 // The host plans each level once the sizes of its clusters are known and
 // uploads arrays of these plain structs; every pointer is a device address
 // inside the block pool.  Blocks are column-major with an explicit leading
 // dimension that never changes after allocation (truncation by the
-// sparsification only shrinks the logical size).
+// sparsification only shrinks the logical size).  Block reflector factors T
+// use the blocked layout of dense.cuh (kNB x k, one triangle per 32 columns).
 #pragma once
 #include <cstdint>
 
 namespace spq {
 
 // Per interior c: geqrt of its diagonal block, then the tsqrt chain over its
-// out-blocks in ascending neighbour order (ptree.cpp:170-214).
+// out-blocks in ascending neighbour order (ptree.cpp:170-214).  Run by one
+// thread-block cluster; 32-column panels are distributed over its CTAs.
 struct ElimTask {
   double* S;      // n x n diagonal block (ld = n)
-  double* T;      // n x n block factor of the diagonal QR
+  double* T;      // kNB x n block factors of the diagonal QR
+  double* tau;    // n doubles of scratch (reflector broadcast)
   int n;
   int out_begin, out_end;  // range in ElimOut
 };
 struct ElimOut {
   double* B;  // m x n block A(n_j, c), ld = m; becomes the reflector tails
-  double* T;  // n x n block factor of this tsqrt step
+  double* T;  // kNB x n block factors of this tsqrt step
   int m;
 };
 
-// Trailing update of one column cluster (ptree.cpp:216-266): a list of ops
-// applied in order; kind 0 = larfb of an interior's diagonal reflectors on
-// A(c, m), kind 1 = tpmqrt of one chain step on [A(c, m); A(n_j, m)].
+// Trailing update of columns [col0, col0+ncols) of one column cluster
+// (ptree.cpp:216-266): the ops of the cluster applied in order; kind 0 =
+// larfb of an interior's diagonal reflectors on A(c, m), kind 1 = tpmqrt of
+// one chain step on [A(c, m); A(n_j, m)].
 struct UpdTask {
   int op_begin, op_end;
-  int ncols;
+  int col0, ncols;
 };
 struct UpdOp {
   const double* V;
@@ -39,31 +43,38 @@ struct UpdOp {
   int kind, k, m, ldv, lda, ldb;
 };
 
-// Scaling of a sparsified interface (ptree.cpp:269-286): QR of its diagonal
-// block in place (the block keeps Qs/Rs), block factor Ts.
+// Distributed geqrt of one diagonal block (scaling QR, ptree.cpp:269-286).
 struct ScaleTask {
   double* S;
   double* T;
+  double* tau;
   int n;
 };
-// Scaling of one block between interfaces (ptree.cpp:1613-1659):
-// rows by Qs^T of the row cluster, columns by Rs^{-1} of the column cluster.
-struct ScaleEdgeTask {
+
+// One chunk of a block apply between interfaces.  Row-scaling / left
+// compression act on columns [lo, lo+cnt) of A; column-scaling / right
+// compression act on rows [lo, lo+cnt).
+struct EdgeChunk {
   double* A;
-  const double* Qr;  // row cluster's Qs (null: not scaled)
-  const double* Tr;
-  const double* Qc;  // column cluster's Qs holding Rs (null: not scaled)
-  int lda, m, nc, ldqr, ldqc;
+  const double* V;     // reflectors (or the upper-triangular R for column scaling)
+  const double* T;     // block factors (kNB x k)
+  const int* kdev;     // number of reflectors read on the device (rank), or null: use k
+  const int* limdev;   // left compression: only columns < *limdev exist, or null
+  int lda, m, nc, ldv, k, lo, cnt;
 };
 
 // Truncated column-pivoted QR of the compression matrix of one interface
-// (ptree.cpp:373-439): C = [A(n,p)^T ... | A(p,m) ...], m = cols of p.
+// (ptree.cpp:373-439): C = [A(n,p)^T ... | A(p,m) ...], m = size of p.
+// Run by one thread-block cluster; C's 32-column panels are distributed over
+// its CTAs and pivot columns are tracked by position (no physical swaps).
 struct RrqrTask {
-  double* C;      // m x w, ld m; keeps V in its first rank columns
-  double* tau;    // >= m
-  double* T;      // m x m region for the rank x rank block factor
-  double* vn;     // 2*w scratch (partial column norms)
-  int* jpvt;      // w scratch
+  double* C;      // m x w scratch (ld m)
+  double* V;      // m x m output: reflector j in column j (ld m)
+  double* T;      // kNB x m output block factors
+  double* tau;    // m
+  double* vn;     // 2*w partial column norms
+  int* colat;     // w: column at each pivot position
+  double* bc;     // 16 doubles: broadcast slots
   int* rank;      // output
   int m, w;
   int src_begin, src_end;  // range in RrqrSrc
@@ -72,19 +83,6 @@ struct RrqrSrc {
   const double* A;
   int lda, rows, cols;
   int transpose;  // 1: out-block A(n,p) (rows x m) enters transposed
-};
-
-// Compression of one block between interfaces (ptree.cpp:1860-1903):
-// A <- Q_r^T A Q_c restricted to rank_r x rank_c.
-struct SparsEdgeTask {
-  double* A;
-  const double* Vr;  // row cluster's sparsification reflectors (m x rank_r), null if none
-  const double* Tr;
-  const int* rank_r;
-  const double* Vc;  // column cluster's reflectors (nc x rank_c), null if none
-  const double* Tc;
-  const int* rank_c;
-  int lda, m, nc, ldvr, ldvc;
 };
 
 // Merge of one child block into its parent block (ptree.cpp:289-340).

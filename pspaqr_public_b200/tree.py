@@ -79,6 +79,7 @@ def lib():
             "spq_factor_flops": (f64, [vp]),
             "spq_pool_bytes": (f64, [vp]),
             "spq_last_error": (C.c_char_p, [vp]),
+            "spq_kernel_launches": (C.c_longlong, []),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -125,6 +126,11 @@ def random_reference(n: int, seed: int) -> np.ndarray:
     out = np.empty(n)
     lib().spq_random_reference(n, seed, _pd(out))
     return out
+
+
+def kernel_launches() -> int:
+    """Kernels launched by libspaqr_b200.so in this process so far."""
+    return int(lib().spq_kernel_launches())
 
 
 INFO_FIELDS = ("lvl", "merge_lvl", "size", "rank", "parent", "cstart", "sep", "l_lvl", "l_sep", "r_lvl", "r_sep",
@@ -302,10 +308,13 @@ class ParTree:
         lib().spq_times(self._h, _pd(t))
         return dict(zip(("partition", "assemble", "factorize", "solve", "gmres"), t.tolist()))
 
+    LEVEL_PHASES = ("chains", "updates", "scale_qr", "scale_apply", "rrqr", "compress_apply", "merge", "total")
+
     def level_times(self) -> np.ndarray:
-        out = np.zeros(4 * self.nlevels, np.float32)
+        """(nlevels, 8) milliseconds per phase, columns as LEVEL_PHASES."""
+        out = np.zeros(8 * self.nlevels, np.float32)
         lib().spq_level_times(self._h, out.ctypes.data_as(C.POINTER(C.c_float)))
-        return out.reshape(self.nlevels, 4)
+        return out.reshape(self.nlevels, 8)
 
     def factor_flops(self) -> float:
         return lib().spq_factor_flops(self._h)
