@@ -46,6 +46,11 @@ int spq_set_square(spq_tree* t, int s);
  * equal-norm ties by rounding noise): the pivot is the first column whose
  * partial norm is within rtol of the largest.  0 = first maximum. Default 1e-6. */
 int spq_set_pivot_rtol(spq_tree* t, double rtol);
+/* Tuning of the pivoted QR (no reference counterpart).  Each interface gets
+ * the smallest thread-block cluster (1..16 CTAs) whose CTAs handle at most
+ * max(elems, level total / (fill * SMs)) elements of the compression matrix
+ * per pivot step.  elems >= 1024 (default 65536), 0 < fill <= 64 (default 2). */
+int spq_set_rrqr_work(spq_tree* t, double elems, double fill);
 
 /* Tree::set_Xcoo(MatrixXd*) (src/tree.cpp:21): coordinates, dim x n
  * column-major (the reference borrows the pointer; this copies it). */
@@ -121,6 +126,11 @@ int spq_times(spq_tree* t, double* times);
 int spq_level_times(spq_tree* t, float* ms);
 /* Nominal FP64 flops of the last factorization (LAPACK Working Note 41 counts). */
 double spq_factor_flops(spq_tree* t);
+/* Bytes of compression-matrix data the pivoted QR of the last factorization
+ * reads: one pass for the column norms and one per pivot step over the
+ * columns still active (the algorithmic traffic of its roofline).  No
+ * reference counterpart. */
+double spq_rrqr_bytes(spq_tree* t);
 /* Bytes of device memory held by factor blocks. */
 double spq_pool_bytes(spq_tree* t);
 /* Kernels this library has launched in the process so far (graph nodes counted

@@ -63,6 +63,13 @@ int spq_set_pivot_rtol(spq_tree* h, double r) {
   return 0;
 }
 
+int spq_set_rrqr_work(spq_tree* h, double elems, double fill) {
+  if (!h || !(elems >= 1024) || !(fill > 0 && fill <= 64)) return -1;
+  h->t->rrqr_work = elems;
+  h->t->rrqr_fill = fill;
+  return 0;
+}
+
 int spq_set_square(spq_tree* h, int s) {
   if (!h) return -1;
   if (!s) {
@@ -224,6 +231,7 @@ int spq_level_times(spq_tree* h, float* ms) {
   return 0;
 }
 double spq_factor_flops(spq_tree* h) { return h ? h->t->factor_flops() : -1.0; }
+double spq_rrqr_bytes(spq_tree* h) { return h ? h->t->rrqr_bytes() : -1.0; }
 double spq_pool_bytes(spq_tree* h) { return h ? (double)h->t->pool_bytes() : -1.0; }
 long long spq_kernel_launches(void) { return spq::kernel_launches(); }
 const char* spq_last_error(spq_tree* h) {

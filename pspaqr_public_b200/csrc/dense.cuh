@@ -314,6 +314,294 @@ __device__ void apply_q_right(const double* V, int ldv, const double* T, int k, 
   }
 }
 
+
+// ---------------------------------------------------------------- tiled matrix applies
+// Register-tiled FP64 block reflector applies on matrices: rows are streamed
+// through shared memory in tiles of kRT, each thread owns a 4 x 2 micro-tile
+// of W = V^T C (kNB x kNC) and of the update C -= V W2.  `sm` holds
+// kTileSmem doubles.
+constexpr int kNC = 64;   // columns (rows for right applies) per pass
+constexpr int kRT = 32;   // rows (columns) per shared-memory tile
+constexpr int kTileSmem = kRT * (kNB + 1) + kNC * (kRT + 1) + kNB * kNC;
+
+// C (m x nc <= kNC) <- Q^T C with one panel: unit = 1: V unit lower trapezoidal
+// (geqrt / RRQR reflectors), A unused; unit = 0: pentagonal tpqrt panel,
+// [A (kb x nc); C] <- Q^T [A; C] with V full (m x kb).
+__device__ void tile_left_qt(const double* V, int ldv, const double* T, int ldt, int kb, int unit, double* A, int lda,
+                             double* C, int ldc, int m, int nc, double* sm) {
+  double* sV = sm;                              // [kRT][kNB+1]
+  double* sC = sV + kRT * (kNB + 1);            // [kRT][kNC+1]; later W2 [kNB][kNC]
+  double* sW = sC + kNC * (kRT + 1);            // [kNB][kNC]
+  const int t = threadIdx.x;
+  const int ti = t & 7, tc = t >> 3;            // rows ti*4..+3, cols tc*2..+1
+  double acc[4][2] = {{0, 0}, {0, 0}, {0, 0}, {0, 0}};
+  for (int r0 = 0; r0 < m; r0 += kRT) {
+    const int rn = (m - r0) < kRT ? (m - r0) : kRT;
+    for (int idx = t; idx < kRT * kNB; idx += kThreads) {
+      const int r = idx % kRT, i = idx / kRT, gr = r0 + r;
+      double v = 0.0;
+      if (r < rn && i < kb) v = unit ? (gr == i ? 1.0 : (gr < i ? 0.0 : V[gr + (size_t)i * ldv])) : V[gr + (size_t)i * ldv];
+      sV[r * (kNB + 1) + i] = v;
+    }
+    for (int idx = t; idx < kRT * kNC; idx += kThreads) {
+      const int r = idx % kRT, c = idx / kRT;
+      sC[r * (kNC + 1) + c] = (r < rn && c < nc) ? C[(r0 + r) + (size_t)c * ldc] : 0.0;
+    }
+    __syncthreads();
+#pragma unroll 4
+    for (int r = 0; r < kRT; ++r) {
+      const double* vr = sV + r * (kNB + 1) + ti * 4;
+      const double* cr = sC + r * (kNC + 1) + tc * 2;
+      const double b0 = cr[0], b1 = cr[1];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const double a = vr[q];
+        acc[q][0] += a * b0;
+        acc[q][1] += a * b1;
+      }
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int q = 0; q < 4; ++q)
+#pragma unroll
+    for (int p = 0; p < 2; ++p) {
+      const int i = ti * 4 + q, c = tc * 2 + p;
+      double w = acc[q][p];
+      if (!unit && i < kb && c < nc) w += A[i + (size_t)c * lda];
+      sW[i * kNC + c] = w;
+    }
+  __syncthreads();
+  // W2 = T^T W  (T upper triangular: W2(i) = sum_{l <= i} T(l, i) W(l))
+  double* sW2 = sC;
+#pragma unroll
+  for (int q = 0; q < 4; ++q)
+#pragma unroll
+    for (int p = 0; p < 2; ++p) {
+      const int i = ti * 4 + q, c = tc * 2 + p;
+      double s = 0.0;
+      if (i < kb)
+        for (int l = 0; l <= i; ++l) s += T[l + (size_t)i * ldt] * sW[l * kNC + c];
+      sW2[i * kNC + c] = s;
+    }
+  __syncthreads();
+  if (!unit)
+    for (int idx = t; idx < kb * nc; idx += kThreads) {
+      const int i = idx % kb, c = idx / kb;
+      A[i + (size_t)c * lda] -= sW2[i * kNC + c];
+    }
+  // C -= V W2
+  const int tr = t & 7, tcc = t >> 3;  // rows tr*4..+3, cols tcc*2..+1
+  for (int r0 = 0; r0 < m; r0 += kRT) {
+    const int rn = (m - r0) < kRT ? (m - r0) : kRT;
+    for (int idx = t; idx < kRT * kNB; idx += kThreads) {
+      const int r = idx % kRT, i = idx / kRT, gr = r0 + r;
+      double v = 0.0;
+      if (r < rn && i < kb) v = unit ? (gr == i ? 1.0 : (gr < i ? 0.0 : V[gr + (size_t)i * ldv])) : V[gr + (size_t)i * ldv];
+      sV[r * (kNB + 1) + i] = v;
+    }
+    __syncthreads();
+    double u[4][2] = {{0, 0}, {0, 0}, {0, 0}, {0, 0}};
+#pragma unroll 4
+    for (int i = 0; i < kNB; ++i) {
+      const double w0 = sW2[i * kNC + tcc * 2], w1 = sW2[i * kNC + tcc * 2 + 1];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const double a = sV[(tr * 4 + q) * (kNB + 1) + i];
+        u[q][0] += a * w0;
+        u[q][1] += a * w1;
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < 4; ++q)
+#pragma unroll
+      for (int p = 0; p < 2; ++p) {
+        const int r = tr * 4 + q, c = tcc * 2 + p;
+        if (r < rn && c < nc) C[(r0 + r) + (size_t)c * ldc] -= u[q][p];
+      }
+    __syncthreads();
+  }
+}
+
+// C (m <= kNC rows x n) <- C (I - V T V^T) with one panel, V unit lower
+// trapezoidal (n x kb).
+__device__ void tile_right_q(const double* V, int ldv, const double* T, int ldt, int kb, double* C, int ldc, int m,
+                             int n, double* sm) {
+  double* sV = sm;                              // [kRT][kNB+1]: V rows c0..c0+31
+  double* sC = sV + kRT * (kNB + 1);            // [kNC][kRT+1]: C(r, c0+c)
+  double* sW = sC + kNC * (kRT + 1);            // [kNC][kNB] W(r, i)
+  const int t = threadIdx.x;
+  const int ti = t & 7, tr = t >> 3;            // i = ti*4..+3, r = tr*2..+1
+  double acc[2][4] = {{0, 0, 0, 0}, {0, 0, 0, 0}};
+  for (int c0 = 0; c0 < n; c0 += kRT) {
+    const int cn = (n - c0) < kRT ? (n - c0) : kRT;
+    for (int idx = t; idx < kRT * kNB; idx += kThreads) {
+      const int c = idx % kRT, i = idx / kRT, gc = c0 + c;
+      double v = 0.0;
+      if (c < cn && i < kb) v = gc == i ? 1.0 : (gc < i ? 0.0 : V[gc + (size_t)i * ldv]);
+      sV[c * (kNB + 1) + i] = v;
+    }
+    for (int idx = t; idx < kNC * kRT; idx += kThreads) {
+      const int r = idx % kNC, c = idx / kNC;
+      sC[r * (kRT + 1) + c] = (r < m && c < cn) ? C[r + (size_t)(c0 + c) * ldc] : 0.0;
+    }
+    __syncthreads();
+#pragma unroll 4
+    for (int c = 0; c < kRT; ++c) {
+      const double a0 = sC[(tr * 2) * (kRT + 1) + c], a1 = sC[(tr * 2 + 1) * (kRT + 1) + c];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const double v = sV[c * (kNB + 1) + ti * 4 + q];
+        acc[0][q] += a0 * v;
+        acc[1][q] += a1 * v;
+      }
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int p = 0; p < 2; ++p)
+#pragma unroll
+    for (int q = 0; q < 4; ++q) sW[(tr * 2 + p) * kNB + ti * 4 + q] = acc[p][q];
+  __syncthreads();
+  // W2 = W T (W2(r,i) = sum_{l <= i} W(r,l) T(l,i))
+  double* sW2 = sC;  // [kNC][kNB]
+#pragma unroll
+  for (int p = 0; p < 2; ++p)
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int r = tr * 2 + p, i = ti * 4 + q;
+      double s = 0.0;
+      if (i < kb)
+        for (int l = 0; l <= i; ++l) s += sW[r * kNB + l] * T[l + (size_t)i * ldt];
+      sW2[r * kNB + i] = s;
+    }
+  __syncthreads();
+  // C(r, c) -= sum_i W2(r, i) V(c, i)
+  const int rr = t & 31, cc = t >> 5;  // rows rr, rr+32; cols cc*4..+3 of the tile
+  for (int c0 = 0; c0 < n; c0 += kRT) {
+    const int cn = (n - c0) < kRT ? (n - c0) : kRT;
+    for (int idx = t; idx < kRT * kNB; idx += kThreads) {
+      const int c = idx % kRT, i = idx / kRT, gc = c0 + c;
+      double v = 0.0;
+      if (c < cn && i < kb) v = gc == i ? 1.0 : (gc < i ? 0.0 : V[gc + (size_t)i * ldv]);
+      sV[c * (kNB + 1) + i] = v;
+    }
+    __syncthreads();
+    double u[2][4] = {{0, 0, 0, 0}, {0, 0, 0, 0}};
+#pragma unroll 4
+    for (int i = 0; i < kNB; ++i) {
+      const double w0 = sW2[rr * kNB + i], w1 = sW2[(rr + 32) * kNB + i];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const double v = sV[(cc * 4 + q) * (kNB + 1) + i];
+        u[0][q] += w0 * v;
+        u[1][q] += w1 * v;
+      }
+    }
+#pragma unroll
+    for (int p = 0; p < 2; ++p)
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const int r = rr + 32 * p, c = cc * 4 + q;
+        if (r < m && c < cn) C[r + (size_t)(c0 + c) * ldc] -= u[p][q];
+      }
+    __syncthreads();
+  }
+}
+
+// Panel loops of the tiled applies over k reflectors (T in kNB x k layout).
+__device__ void mat_apply_qt(const double* V, int ldv, const double* T, int k, double* C, int ldc, int m, int nc,
+                             double* sm) {
+  for (int j0 = 0; j0 < k; j0 += kNB) {
+    const int kb = (k - j0) < kNB ? (k - j0) : kNB;
+    for (int c0 = 0; c0 < nc; c0 += kNC)
+      tile_left_qt(V + j0 + (size_t)j0 * ldv, ldv, T + (size_t)j0 * kNB, kNB, kb, 1, nullptr, 0,
+                   C + j0 + (size_t)c0 * ldc, ldc, m - j0, (nc - c0) < kNC ? (nc - c0) : kNC, sm);
+  }
+}
+__device__ void mat_apply_tpqt(const double* V, int ldv, const double* T, int k, double* A, int lda, double* B,
+                               int ldb, int m, int nc, double* sm) {
+  for (int j0 = 0; j0 < k; j0 += kNB) {
+    const int kb = (k - j0) < kNB ? (k - j0) : kNB;
+    for (int c0 = 0; c0 < nc; c0 += kNC)
+      tile_left_qt(V + (size_t)j0 * ldv, ldv, T + (size_t)j0 * kNB, kNB, kb, 0, A + j0 + (size_t)c0 * lda, lda,
+                   B + (size_t)c0 * ldb, ldb, m, (nc - c0) < kNC ? (nc - c0) : kNC, sm);
+  }
+}
+__device__ void mat_apply_q_right(const double* V, int ldv, const double* T, int k, double* C, int ldc, int m, int n,
+                                  double* sm) {
+  for (int j0 = 0; j0 < k; j0 += kNB) {
+    const int kb = (k - j0) < kNB ? (k - j0) : kNB;
+    for (int r0 = 0; r0 < m; r0 += kNC)
+      tile_right_q(V + j0 + (size_t)j0 * ldv, ldv, T + (size_t)j0 * kNB, kNB, kb, C + r0 + (size_t)j0 * ldc, ldc,
+                   (m - r0) < kNC ? (m - r0) : kNC, n - j0, sm);
+  }
+}
+
+
+// C (m <= kNC rows x n) <- C R^{-1}, R upper triangular (n x n), blocked by 32
+// columns: C(:, J) -= C(:, 0:j0) R(0:j0, J) through shared-memory tiles, then
+// the 32 x 32 diagonal block is solved one row per thread.
+__device__ void tile_trsm_right_upper(const double* R, int ldr, double* C, int ldc, int m, int n, double* sm) {
+  double* sR = sm;                      // [kRT][kNB+1]  R(l0+l, j0+j)
+  double* sC = sR + kRT * (kNB + 1);    // [kNC][kRT+1]  C(r, l0+l), later the solved block
+  const int t = threadIdx.x;
+  const int tj = t & 7, tr = t >> 3;    // cols tj*4..+3, rows tr*2..+1
+  for (int j0 = 0; j0 < n; j0 += kNB) {
+    const int jb = (n - j0) < kNB ? (n - j0) : kNB;
+    double acc[2][4] = {{0, 0, 0, 0}, {0, 0, 0, 0}};
+    for (int l0 = 0; l0 < j0; l0 += kRT) {
+      for (int idx = t; idx < kRT * kNB; idx += kThreads) {
+        const int l = idx % kRT, j = idx / kRT;
+        sR[l * (kNB + 1) + j] = (j < jb) ? R[(l0 + l) + (size_t)(j0 + j) * ldr] : 0.0;
+      }
+      for (int idx = t; idx < kNC * kRT; idx += kThreads) {
+        const int r = idx % kNC, l = idx / kNC;
+        sC[r * (kRT + 1) + l] = (r < m) ? C[r + (size_t)(l0 + l) * ldc] : 0.0;
+      }
+      __syncthreads();
+#pragma unroll 4
+      for (int l = 0; l < kRT; ++l) {
+        const double a0 = sC[(tr * 2) * (kRT + 1) + l], a1 = sC[(tr * 2 + 1) * (kRT + 1) + l];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          const double rv = sR[l * (kNB + 1) + tj * 4 + q];
+          acc[0][q] += a0 * rv;
+          acc[1][q] += a1 * rv;
+        }
+      }
+      __syncthreads();
+    }
+    // subtract into the block, stage it in shared memory with the diagonal R block
+    for (int idx = t; idx < kNB * kNB; idx += kThreads) {
+      const int l = idx % kNB, j = idx / kNB;
+      sR[l * (kNB + 1) + j] = (l < jb && j < jb) ? R[(j0 + l) + (size_t)(j0 + j) * ldr] : 0.0;
+    }
+#pragma unroll
+    for (int p = 0; p < 2; ++p)
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const int r = tr * 2 + p, j = tj * 4 + q;
+        sC[r * (kRT + 1) + j] = (r < m && j < jb) ? C[r + (size_t)(j0 + j) * ldc] - acc[p][q] : 0.0;
+      }
+    __syncthreads();
+    for (int r = t; r < m; r += kThreads) {
+      double* cr = sC + r * (kRT + 1);
+      for (int j = 0; j < jb; ++j) {
+        double s = cr[j];
+        for (int l = 0; l < j; ++l) s -= cr[l] * sR[l * (kNB + 1) + j];
+        cr[j] = s / sR[j * (kNB + 1) + j];
+      }
+    }
+    __syncthreads();
+    for (int idx = t; idx < kNC * kNB; idx += kThreads) {
+      const int r = idx % kNC, j = idx / kNC;
+      if (r < m && j < jb) C[r + (size_t)(j0 + j) * ldc] = sC[r * (kRT + 1) + j];
+    }
+    __syncthreads();
+  }
+}
+
 // C (m x n) <- C R^{-1}, R upper triangular (n x n).  One thread per row.
 __device__ void trsm_right_upper(const double* R, int ldr, double* C, int ldc, int m, int n) {
   for (int r = threadIdx.x; r < m; r += kThreads) {

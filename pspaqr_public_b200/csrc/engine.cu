@@ -22,6 +22,20 @@ constexpr size_t kArenaChunk = size_t(1) << 30;
 constexpr long long kSpinLimit = 2000000000LL;
 constexpr int kChunk = 64;        // columns (rows) per CTA of the chunked applies
 constexpr int kBigCluster = 8;    // CTAs per task for blocks of >= 8 panels
+constexpr int kRrqrMaxCols = 1024;  // own columns of C per CTA (four per thread)
+
+// SMs of the current device (queried once per process)
+int num_sms() {
+  static int n = [] {
+    int dev = 0, v = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) {
+      cudaGetLastError();
+      return 148;
+    }
+    return v > 0 ? v : 148;
+  }();
+  return n;
+}
 inline int dev_nb() { return 32; }  // panel width of the blocked T factors (dense.cuh kNB)
 }  // namespace
 
@@ -31,23 +45,32 @@ Arena::~Arena() { release(); }
 void* Arena::alloc(size_t bytes) {
   bytes = (bytes + kAlign - 1) / kAlign * kAlign;
   if (bytes == 0) bytes = kAlign;
-  if (chunks_.empty() || chunks_.back().off + bytes > chunks_.back().size) {
+  // first chunk from the current one on that still has room
+  while (cur_ < chunks_.size() && chunks_[cur_].off + bytes > chunks_[cur_].size) ++cur_;
+  if (cur_ == chunks_.size()) {
     size_t sz = std::max(kArenaChunk, bytes);
     void* p = nullptr;
     if (cudaMalloc(&p, sz) != cudaSuccess) return nullptr;
     chunks_.push_back({static_cast<char*>(p), sz, 0});
     reserved_ += sz;
   }
-  Chunk& c = chunks_.back();
+  Chunk& c = chunks_[cur_];
   void* r = c.base + c.off;
   c.off += bytes;
   used_ += bytes;
   return r;
 }
 
+void Arena::reset() {
+  for (auto& c : chunks_) c.off = 0;
+  cur_ = 0;
+  used_ = 0;
+}
+
 void Arena::release() {
   for (auto& c : chunks_) cudaFree(c.base);
   chunks_.clear();
+  cur_ = 0;
   used_ = reserved_ = 0;
 }
 
@@ -66,6 +89,7 @@ Tree::~Tree() {
   cudaFree(d_tickets_);
   cudaFree(d_status_);
   cudaFree(d_tmp_);
+  cudaFree(d_krylov_);
   scratch_.release();
   arena_.release();
   if (own_stream_ && stream_) cudaStreamDestroy(stream_);
@@ -174,7 +198,15 @@ int Tree::assemble() {
   rows_.assign(ned, 0);
   cols_.assign(ned, 0);
   tsqrtT_.assign(ned, nullptr);
-  arena_.release();
+  // a re-assembly reuses the device memory of the previous factorization
+  if (check_cuda(cudaStreamSynchronize(stream_), "assemble")) return -10;
+  if (solve_exec_) {
+    cudaGraphExecDestroy(solve_exec_);
+    cudaGraphDestroy(solve_graph_);
+    solve_exec_ = nullptr;
+    solve_graph_ = nullptr;
+  }
+  arena_.reset();
   const Level& L0 = st_.levels[0];
   for (int o = L0.first; o < L0.first + L0.count; ++o) size_[o] = size_org_[o] = st_.clusters[o].size0;
   // level-0 blocks, zeroed, then the nonzeros of App scattered in
@@ -226,6 +258,7 @@ int Tree::assemble() {
       check_cuda(cudaMalloc(&d_status_, sizeof(int)), "malloc") ||
       check_cuda(cudaMalloc(&d_tmp_, sizeof(double) * 2 * n), "malloc"))
     return -10;
+  scratch_.reset();
   cudaMemcpyAsync(d_rowptr_, rowptr.data(), sizeof(int) * (n + 1), cudaMemcpyHostToDevice, stream_);
   cudaMemcpyAsync(d_col_, col.data(), sizeof(int) * nnz, cudaMemcpyHostToDevice, stream_);
   cudaMemcpyAsync(d_val_, val.data(), sizeof(double) * nnz, cudaMemcpyHostToDevice, stream_);
@@ -237,7 +270,7 @@ int Tree::assemble() {
   if (!d_cval || !d_dst) return fail(-11, "out of device memory (assembly)");
   if (check_cuda(launch_scatter(nnz, d_cval, d_dst, stream_), "scatter")) return -10;
   if (check_cuda(cudaStreamSynchronize(stream_), "assemble")) return -10;
-  scratch_.release();
+  scratch_.reset();
   assembled_ = true;
   factorized_ = false;
   t_assemble = wall() - t0;
@@ -263,6 +296,7 @@ int Tree::factorize() {
   const int NB = dev_nb();
   lt_.assign(L, LevelTiming());
   flops_ = 0;
+  rrqr_bytes_ = 0;
   cudaEvent_t ev[5], fe[6];
   for (auto& e : ev) cudaEventCreate(&e);
   for (auto& e : fe) cudaEventCreate(&e);
@@ -427,48 +461,83 @@ int Tree::factorize() {
           flops_ += (double)t.m * t.nc * t.nc;
         }
       }
-      std::vector<RrqrTask> rt[3];
+      // pivoted-QR launch groups by cluster size 1, 2, 4, 8, 16.  The level's
+      // compression matrices are dealt so that about rrqr_fill CTAs per SM
+      // share the work: a task gets the smallest cluster whose CTAs each hold
+      // at most max(rrqr_work, level work / (rrqr_fill * SMs)) elements, and
+      // at most kRrqrMaxCols columns.
+      std::vector<RrqrTask> rt[5];
       std::vector<RrqrSrc> rs;
-      int mmax[3] = {1, 1, 1}, wloc[3] = {1, 1, 1};
+      int gm[5], gk[5], gnl[5], grc[5];
+      for (int g = 0; g < 5; ++g) gm[g] = gk[g] = gnl[g] = grc[g] = 1;
       std::vector<std::pair<double, double>> rr_dims;
+      std::vector<int> rr_cs;
+      int* d_stats = verbose >= 2 ? static_cast<int*>(scratch_.alloc(sizeof(int) * 8 * Lv.spars_clusters.size() + 8))
+                                  : nullptr;
+      std::vector<int> sp_w(Lv.spars_clusters.size());
+      double level_work = 0;
+      for (size_t q = 0; q < Lv.spars_clusters.size(); ++q) {
+        int w = 0;
+        for (int k = Lv.sp_out_begin[q]; k < Lv.sp_out_end[q]; ++k) w += rows_[Lv.sp_out[k]];
+        for (int k = Lv.sp_in_begin[q]; k < Lv.sp_in_end[q]; ++k) w += cols_[Lv.sp_in[k]];
+        sp_w[q] = w;
+        level_work += (double)size_[Lv.spars_clusters[q]] * w;
+      }
+      const double cta_work = std::max(rrqr_work, level_work / (rrqr_fill * num_sms()));
       for (size_t q = 0; q < Lv.spars_clusters.size(); ++q) {
         const int p = Lv.spars_clusters[q];
         const int mp = size_[p];
-        RrqrTask t;
+        const int w = sp_w[q];
+        const double work = (double)mp * w;
+        auto local_cols = [&](int c) { return ((w + c - 1) / c + 31) / 32 * 32; };
+        int g = 0;
+        while (g < 4 && (work > cta_work * (1 << g) || local_cols(1 << g) > kRrqrMaxCols) &&
+               (w + NB - 1) / NB >= (2 << g))
+          ++g;
+        if (g == 4 && !rrqr_cluster_fits(16, rrqr_smem(std::max(gm[4], mp), std::max(gk[4], std::min(mp, w)),
+                                                       std::max(gnl[4], local_cols(16)),
+                                                       std::max(grc[4], (mp + 15) / 16))))
+          g = 3;
+        const int cs = 1 << g;
+        if (local_cols(cs) > kRrqrMaxCols) return fail(-12, "interface too wide for the pivoted QR kernel");
+        RrqrTask t{};
         t.m = mp;
-        t.src_begin = (int)rs.size();
-        int w = 0;
-        for (int k = Lv.sp_out_begin[q]; k < Lv.sp_out_end[q]; ++k) {
-          const int e = Lv.sp_out[k];
-          rs.push_back({ptr_[e], ld_[e], rows_[e], cols_[e], 1});
-          w += rows_[e];
-        }
-        for (int k = Lv.sp_in_begin[q]; k < Lv.sp_in_end[q]; ++k) {
-          const int e = Lv.sp_in[k];
-          rs.push_back({ptr_[e], ld_[e], rows_[e], cols_[e], 0});
-          w += cols_[e];
-        }
-        t.src_end = (int)rs.size();
         t.w = w;
+        t.ldw = (w + 3) / 4 * 4;
+        t.ldq = std::max(1, std::min(mp, w));
+        double* Ct = scratch_.dalloc((size_t)std::max(mp, 1) * std::max(t.ldw, 4));
+        t.C = Ct;
+        t.Q = scratch_.dalloc((size_t)std::max(mp, 1) * t.ldq);
+        t.Qc = scratch_.dalloc((size_t)std::max(mp, 1) * t.ldq);
+        t.F = scratch_.dalloc((size_t)std::max(w, 1) * t.ldq);
         Qsp_[p] = arena_.dalloc((size_t)std::max(mp, 1) * std::max(mp, 1));
         Tsp_[p] = arena_.dalloc((size_t)NB * std::max(mp, 1));
         t.V = Qsp_[p];
         t.T = Tsp_[p];
-        t.C = scratch_.dalloc((size_t)std::max(mp, 1) * std::max(w, 1));
         t.tau = scratch_.dalloc(std::max(mp, 1));
-        t.vn = scratch_.dalloc(2 * (size_t)std::max(w, 1));
         t.colat = static_cast<int*>(scratch_.alloc(sizeof(int) * std::max(w, 1)));
-        t.bc = scratch_.dalloc(16);
         t.rank = d_rank_ + p;
-        if (!t.C || !t.V || !t.T || !t.tau || !t.vn || !t.colat || !t.bc)
+        t.stats = d_stats ? d_stats + 8 * q : nullptr;
+        if (!Ct || !t.Q || !t.Qc || !t.F || !t.V || !t.T || !t.tau || !t.colat)
           return fail(-11, "out of device memory (rrqr)");
-        const int cs = cluster_for(w);
-        const int g = cs == 1 ? 0 : (cs == 4 ? 1 : 2);
+        int c0 = 0;
+        for (int k = Lv.sp_out_begin[q]; k < Lv.sp_out_end[q]; ++k) {
+          const int e = Lv.sp_out[k];
+          if (rows_[e] > 0 && mp > 0) rs.push_back({ptr_[e], ld_[e], rows_[e], cols_[e], 1, Ct, t.ldw, c0});
+          c0 += rows_[e];
+        }
+        for (int k = Lv.sp_in_begin[q]; k < Lv.sp_in_end[q]; ++k) {
+          const int e = Lv.sp_in[k];
+          if (cols_[e] > 0 && mp > 0) rs.push_back({ptr_[e], ld_[e], rows_[e], cols_[e], 0, Ct, t.ldw, c0});
+          c0 += cols_[e];
+        }
         rt[g].push_back(t);
-        mmax[g] = std::max(mmax[g], mp);
-        const int npan = (w + NB - 1) / NB;
-        wloc[g] = std::max(wloc[g], ((npan + cs - 1) / cs) * NB);
+        gm[g] = std::max(gm[g], mp);
+        gk[g] = std::max(gk[g], std::min(mp, w));
+        gnl[g] = std::max(gnl[g], local_cols(cs));
+        grc[g] = std::max(grc[g], (mp + cs - 1) / cs);
         rr_dims.push_back({(double)mp, (double)w});
+        rr_cs.push_back(cs);
       }
       std::vector<EdgeChunk> right, left;
       for (int e : Lv.spars_edges) {
@@ -520,12 +589,19 @@ int Tree::factorize() {
           ck(launch_edge(1, d_cols, (int)cols_scale.size(), stream_), "column scaling"))
         return -10;
       cudaEventRecord(ev[2], stream_);
-      for (int g = 0; g < 3; ++g) {
+      if (ck(launch_rrqr_assemble(d_rs, (int)rs.size(), stream_), "rrqr assembly")) return -10;
+      for (int g = 0; g < 5; ++g) {
         if (rt[g].empty()) continue;
         auto* d = static_cast<RrqrTask*>(up_vec(rt[g]));
-        if (!d || ck(launch_rrqr(d, d_rs, (int)rt[g].size(), csz[g], mmax[g], wloc[g], st_.tol, pivot_rtol, stream_),
-                     "rrqr kernel"))
+        if (!d) return fail(-11, "out of device memory (rrqr tasks)");
+        if (ck(launch_rrqr(d, (int)rt[g].size(), 1 << g, gm[g], gk[g], gnl[g], grc[g], st_.tol, pivot_rtol, stream_),
+               "rrqr kernel")) {
+          error += " [cluster " + std::to_string(1 << g) + ", tasks " + std::to_string(rt[g].size()) + ", rows " +
+                   std::to_string(gm[g]) + ", steps " + std::to_string(gk[g]) + ", columns/CTA " +
+                   std::to_string(gnl[g]) + ", shared " + std::to_string(rrqr_smem(gm[g], gk[g], gnl[g], grc[g])) +
+                   " B]";
           return -10;
+        }
       }
       cudaEventRecord(fe[2], stream_);
       if (ck(launch_edge(2, d_right, (int)right.size(), stream_), "right compression") ||
@@ -537,9 +613,22 @@ int Tree::factorize() {
           ck(cudaStreamSynchronize(stream_), "sparsification"))
         return -10;
       for (int p : Lv.spars_clusters) size_[p] = host_rank[p];
+      std::vector<int> stats;
+      if (d_stats) {
+        stats.resize(8 * Lv.spars_clusters.size());
+        if (ck(cudaMemcpy(stats.data(), d_stats, sizeof(int) * stats.size(), cudaMemcpyDeviceToHost), "rrqr stats"))
+          return -10;
+      }
       for (size_t q = 0; q < Lv.spars_clusters.size(); ++q) {
         const double m = rr_dims[q].first, w = rr_dims[q].second, r = size_[Lv.spars_clusters[q]];
         flops_ += 4.0 * m * w * r - 2.0 * r * r * (m + w) + 4.0 * r * r * r / 3.0 + m * r * r;
+        // C read once for the norms and once per step over the active columns
+        const double steps = std::min(r + 1.0, std::min(m, w));
+        rrqr_bytes_ += 8.0 * m * (w + steps * w - steps * (steps + 1.0) / 2.0);
+        if (verbose >= 2)
+          printf("rrqr level %d m %d w %d rank %d cluster %d recomputed %d kcycles %d %d %d %d %d %d\n", lvl, (int)m,
+                 (int)w, (int)r, rr_cs[q], stats[8 * q], stats[8 * q + 2], stats[8 * q + 3], stats[8 * q + 4],
+                 stats[8 * q + 5], stats[8 * q + 6], stats[8 * q + 7]);
       }
       for (int e : Lv.spars_edges) {
         rows_[e] = size_[st_.edges[e].n2];
@@ -603,7 +692,7 @@ int Tree::factorize() {
     cudaEventElapsedTime(&lt_[lvl].sapp_ms, fe[1], ev[2]);
     cudaEventElapsedTime(&lt_[lvl].rrqr_ms, ev[2], fe[2]);
     cudaEventElapsedTime(&lt_[lvl].capp_ms, fe[2], ev[3]);
-    scratch_.release();
+    scratch_.reset();
     if (verbose)
       printf("%d    elim %.3f ms  scale %.3f ms  spars %.3f ms  merge %.3f ms  (interiors %zu, interfaces %zu)\n", lvl,
              lt_[lvl].elim_ms, lt_[lvl].scale_ms, lt_[lvl].spars_ms, lt_[lvl].merge_ms, Lv.interiors.size(),
@@ -864,35 +953,20 @@ int Tree::gmres_device(double* b, int maxit, double gtol, int* iters, double* re
   double t0 = wall();
   const int n = st_.n;
   const size_t ldq = (size_t)n;
-  double *Q = nullptr, *q = nullptr, *bsave = nullptr, *hcol = nullptr, *partial = nullptr;
-  unsigned int* done = nullptr;
   const int grid = mgs_grid(n);
-  if (check_cuda(cudaMalloc(&Q, sizeof(double) * ldq * (maxit + 1)), "malloc Krylov basis") ||
-      check_cuda(cudaMalloc(&q, sizeof(double) * n), "malloc") ||
-      check_cuda(cudaMalloc(&bsave, sizeof(double) * n), "malloc") ||
-      check_cuda(cudaMalloc(&hcol, sizeof(double) * (maxit + 3)), "malloc") ||
-      check_cuda(cudaMalloc(&partial, sizeof(double) * grid), "malloc") ||
-      check_cuda(cudaMalloc(&done, sizeof(unsigned int)), "malloc")) {
-    cudaFree(Q);
-    cudaFree(q);
-    cudaFree(bsave);
-    cudaFree(hcol);
-    cudaFree(partial);
-    cudaFree(done);
-    return -10;
-  }
+  // workspace: basis (n x maxit+1) | q | b | H column | partial sums | counter
+  const size_t need = ldq * (maxit + 1) + 2 * (size_t)n + (maxit + 3) + grid + 1;
+  if (int erc = ensure_krylov(need)) return erc;
+  double* Q = d_krylov_;
+  double* q = Q + ldq * (maxit + 1);
+  double* bsave = q + n;
+  double* hcol = bsave + n;
+  double* partial = hcol + (maxit + 3);
+  unsigned int* done = reinterpret_cast<unsigned int*>(partial + grid);
   cudaMemsetAsync(done, 0, sizeof(unsigned int), stream_);
   cudaMemcpyAsync(bsave, b, sizeof(double) * n, cudaMemcpyDeviceToDevice, stream_);
   cudaMemcpyAsync(q, b, sizeof(double) * n, cudaMemcpyDeviceToDevice, stream_);
-  if (int src = solve_device(q)) {
-    cudaFree(Q);
-    cudaFree(q);
-    cudaFree(bsave);
-    cudaFree(hcol);
-    cudaFree(partial);
-    cudaFree(done);
-    return src;
-  }
+  if (int src = solve_device(q)) return src;
   cudaError_t ge = cudaSuccess;
   auto g = [&](cudaError_t e) {
     if (!ge) ge = e;
@@ -966,14 +1040,18 @@ int Tree::gmres_device(double* b, int maxit, double gtol, int* iters, double* re
     *relres = nr[0] / nr[1];
     last_gmres_iters = k;
   }
-  cudaFree(Q);
-  cudaFree(q);
-  cudaFree(bsave);
-  cudaFree(hcol);
-  cudaFree(partial);
-  cudaFree(done);
   t_gmres = wall() - t0;
   return rc;
+}
+
+int Tree::ensure_krylov(size_t doubles) {
+  if (doubles <= krylov_doubles_) return 0;
+  cudaFree(d_krylov_);
+  d_krylov_ = nullptr;
+  krylov_doubles_ = 0;
+  if (check_cuda(cudaMalloc(&d_krylov_, sizeof(double) * doubles), "malloc Krylov workspace")) return -11;
+  krylov_doubles_ = doubles;
+  return 0;
 }
 
 int Tree::gmres_host(double* b, int maxit, double gtol, int* iters, double* relres, double* hist, int hist_cap) {

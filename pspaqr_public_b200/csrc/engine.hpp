@@ -24,6 +24,8 @@ class Arena {
   ~Arena();
   void* alloc(size_t bytes);
   double* dalloc(size_t n) { return static_cast<double*>(alloc(n * sizeof(double))); }
+  // forget every allocation but keep the chunks for reuse (no cudaFree)
+  void reset();
   void release();
   size_t used() const { return used_; }
   size_t reserved() const { return reserved_; }
@@ -34,6 +36,7 @@ class Arena {
     size_t size, off;
   };
   std::vector<Chunk> chunks_;
+  size_t cur_ = 0;  // chunk being filled
   size_t used_ = 0, reserved_ = 0;
 };
 
@@ -59,6 +62,11 @@ class Tree {
   // largest (0 = LAPACK's first maximum).  Equal norms in exact arithmetic
   // (symmetric stencils) are otherwise resolved by rounding noise.
   double pivot_rtol = 1e-6;
+  // pivoted QR: elements of the compression matrix each CTA of a cluster
+  // handles per pivot step (sets the cluster size, 1..16 CTAs per interface)
+  double rrqr_work = 65536;
+  // ... and a level's compression work is spread over about rrqr_fill CTAs per SM
+  double rrqr_fill = 2;
 
   int set_coords(int dim, int n, const double* X);
   int set_coords_tensor(int n, int d);
@@ -90,6 +98,9 @@ class Tree {
   std::string error;
   size_t pool_bytes() const { return arena_.used(); }
   double factor_flops() const { return flops_; }
+  // bytes of the compression matrices the pivoted QR reads (one pass for the
+  // norms, one per pivot step over the active columns)
+  double rrqr_bytes() const { return rrqr_bytes_; }
   int device_status();
 
  private:
@@ -137,8 +148,13 @@ class Tree {
   cudaGraph_t solve_graph_ = nullptr;
   long long solve_graph_kernels_ = 0;
   double* d_tmp_ = nullptr;    // 2 vectors for host-pointer entry points
+  // Krylov workspace kept across GMRES calls
+  double* d_krylov_ = nullptr;
+  size_t krylov_doubles_ = 0;
+  int ensure_krylov(size_t doubles);
   std::vector<LevelTiming> lt_;
   double flops_ = 0;
+  double rrqr_bytes_ = 0;
 };
 
 }  // namespace spq

@@ -29,7 +29,7 @@ using dev::kThreads;
 using dev::kWarps;
 
 constexpr int kRed = 16;     // reduction scratch (doubles)
-constexpr int kWcap = 4096;  // W scratch (doubles) of the chunked block applies
+constexpr int kWcap = dev::kTileSmem;  // shared scratch (doubles) of the tiled block applies
 
 __device__ __forceinline__ void csync(int cs) {
   if (cs > 1) cg::this_cluster().sync();
@@ -138,10 +138,10 @@ __global__ void __launch_bounds__(kThreads) k_update(const UpdTask* __restrict__
   for (int o = t.op_begin; o < t.op_end; ++o) {
     const UpdOp op = ops[o];
     if (op.kind == 0)
-      dev::apply_qt(op.V, op.ldv, op.T, op.k, op.A + (size_t)t.col0 * op.lda, op.lda, op.m, t.ncols, sm, kWcap);
+      dev::mat_apply_qt(op.V, op.ldv, op.T, op.k, op.A + (size_t)t.col0 * op.lda, op.lda, op.m, t.ncols, sm);
     else
-      dev::apply_tpqt(op.V, op.ldv, op.T, op.k, op.A + (size_t)t.col0 * op.lda, op.lda, op.B + (size_t)t.col0 * op.ldb,
-                      op.ldb, op.m, t.ncols, sm, kWcap);
+      dev::mat_apply_tpqt(op.V, op.ldv, op.T, op.k, op.A + (size_t)t.col0 * op.lda, op.lda,
+                          op.B + (size_t)t.col0 * op.ldb, op.ldb, op.m, t.ncols, sm);
   }
 }
 
@@ -156,13 +156,14 @@ __global__ void __launch_bounds__(kThreads) k_edge_left(const EdgeChunk* __restr
     if (t.lo >= lim) return;
     cnt = min(cnt, lim - t.lo);
   }
-  dev::apply_qt(t.V, t.ldv, t.T, k, t.A + (size_t)t.lo * t.lda, t.lda, t.m, cnt, sm, kWcap);
+  dev::mat_apply_qt(t.V, t.ldv, t.T, k, t.A + (size_t)t.lo * t.lda, t.lda, t.m, cnt, sm);
 }
 
 // column scaling: rows [lo, lo+cnt) of A <- A R^{-1}
 __global__ void __launch_bounds__(kThreads) k_edge_trsm(const EdgeChunk* __restrict__ tasks) {
+  extern __shared__ double sm[];
   const EdgeChunk t = tasks[blockIdx.x];
-  dev::trsm_right_upper(t.V, t.ldv, t.A + t.lo, t.lda, t.cnt, t.nc);
+  dev::tile_trsm_right_upper(t.V, t.ldv, t.A + t.lo, t.lda, t.cnt, t.nc, sm);
 }
 
 // right compression: rows [lo, lo+cnt) of A <- A Q
@@ -170,245 +171,544 @@ __global__ void __launch_bounds__(kThreads) k_edge_right(const EdgeChunk* __rest
   extern __shared__ double sm[];
   const EdgeChunk t = tasks[blockIdx.x];
   const int k = t.kdev ? *t.kdev : t.k;
-  dev::apply_q_right(t.V, t.ldv, t.T, k, t.A + t.lo, t.lda, t.cnt, t.nc, sm, kWcap);
+  dev::mat_apply_q_right(t.V, t.ldv, t.T, k, t.A + t.lo, t.lda, t.cnt, t.nc, sm);
 }
 
 // ------------------------------------------------------------ RRQR
-// Column-pivoted Householder QR of C (m x w) stopped at the first i >= 1 with
-// |R(i,i)| / |R(0,0)| < tol (util.cpp:830-851 choose_rank on the dgeqp3
-// diagonal).  Pivot and norm downdating follow LAPACK dlaqp2, with the pivot
-// taken as the first POSITION (LAPACK's column order after its swaps) whose
-// partial norm is within pivot_rtol of the largest.  Columns stay in place;
-// pos[] (per CTA, own columns) and colat[] (global) track the swaps.
-__global__ void __launch_bounds__(kThreads) k_rrqr(const RrqrTask* __restrict__ tasks, const RrqrSrc* __restrict__ srcs,
-                                                   double tol, double pivot_rtol, int cs, int wloc_max) {
+// Truncated column-pivoted QR of the compression matrix C (m x w) of one
+// interface: LAPACK geqp3 stopped at the first i >= 1 with
+// |R(i,i)| / |R(0,0)| < tol (ptree.cpp:373-439, util.cpp:830-851).
+//
+// The pivot sequence follows dlaqp2 step by step: the pivot is the first
+// POSITION (column order after dlaqp2's swaps) whose partial norm is within
+// pivot_rtol of the largest, partial norms are downdated with row i of R and
+// recomputed when the downdate loses accuracy (tol3z = sqrt(eps)).  C itself
+// is never rewritten: row i of R is q_i^T C, where q_i is column i of the
+// orthonormal factor, obtained by Gram-Schmidt with reorthogonalisation (CGS2)
+// of the pivot column against q_0..q_{i-1}; |R(i,i)| is the norm left after
+// the projection.  Each step therefore READS C once (one GEMV) instead of
+// reading and rewriting the trailing matrix.  With the pivots known, the
+// Householder reflectors are those of an unpivoted QR of the selected
+// columns in pivot order (the first k steps of a pivoted QR act on exactly
+// those columns), computed by dist_qr into V, tau and the panel factors T.
+//
+// A task runs on one thread-block cluster.  C is stored transposed (Ct, w x m)
+// so the GEMV is coalesced with one column per thread; columns are dealt to
+// the CTAs in contiguous ranges and rows of the basis in contiguous slices.
+// Five cluster barriers per step publish the two pivot reductions, the two
+// Gram-Schmidt projections and the new basis vector; every published value
+// is reduced over the CTAs in rank order, so all CTAs take identical
+// decisions.
+
+// Gathers the compression matrix of every task, transposed: C column c0 + jj
+// is row jj of an out-block A(n,p) or column jj of an in-block A(p,m).
+__global__ void __launch_bounds__(kThreads) k_rrqr_assemble(const RrqrSrc* __restrict__ srcs) {
+  __shared__ double tile[32][33];
+  const RrqrSrc s = srcs[blockIdx.x];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  double* dst = s.Ct + s.c0;
+  if (s.transpose) {
+    for (int r = warp; r < s.cols; r += kWarps)
+      for (int jj = lane; jj < s.rows; jj += 32) dst[(size_t)r * s.w + jj] = s.A[jj + (size_t)r * s.lda];
+    return;
+  }
+  for (int j0 = 0; j0 < s.cols; j0 += 32)
+    for (int r0 = 0; r0 < s.rows; r0 += 32) {
+      for (int q = warp; q < 32; q += kWarps) {
+        const int r = r0 + lane, j = j0 + q;
+        tile[q][lane] = (r < s.rows && j < s.cols) ? s.A[r + (size_t)j * s.lda] : 0.0;
+      }
+      __syncthreads();
+      for (int q = warp; q < 32; q += kWarps) {
+        const int r = r0 + q, j = j0 + lane;
+        if (r < s.rows && j < s.cols) dst[(size_t)r * s.w + j] = tile[lane][q];
+      }
+      __syncthreads();
+    }
+}
+
+// Column dots over the CTA's own columns [ja, ja + nloc) of C:
+// fin(jl, sum_r C(r, ja + jl) * x(r)) (kSq: x = the column itself) for every
+// jl with act(jl).  A lane reads two adjacent columns per 16-byte load, a warp
+// 64 consecutive columns (512 bytes of a row of Ct) per load instruction and
+// four such segments at once; the warps split into RG row groups (rows
+// r = rg mod RG, about 16 rows each) times kWarps / RG column groups.  The
+// loads of kRows rows are issued before their products, so every thread
+// keeps sixteen 16-byte loads in flight (64 KB per CTA).  Partial sums meet in `gp` (8 * kThreads doubles)
+// and are added in row-group order.
+constexpr int kRows = 4;  // rows of loads issued together in col_dots
+
+template <bool kSq, typename Act, typename Fin>
+__device__ __forceinline__ void col_dots(const double* __restrict__ Ct, int ldw, int m, int ja, int nloc,
+                                         const double* x, double* gp, Act act, Fin fin) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  int RG = 1;
+  while (RG < kWarps && RG * 16 < m) RG <<= 1;
+  const int CG = kWarps / RG;
+  const int rg = warp % RG, cgp = warp / RG;
+  for (int base = 0; base < nloc; base += 256 * CG) {
+    const int cb = base + 256 * cgp + 2 * lane;
+    bool a[4][2], l[4];
+    double acc[4][2];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+#pragma unroll
+      for (int e = 0; e < 2; ++e) {
+        const int jl = cb + 64 * u + e;
+        a[u][e] = jl < nloc && act(jl);
+        acc[u][e] = 0.0;
+      }
+      l[u] = a[u][0] || a[u][1];
+    }
+    const double* col = Ct + ja + cb;
+    for (int r0 = rg; r0 < m; r0 += kRows * RG) {
+      double2 v[kRows][4];
+#pragma unroll
+      for (int k = 0; k < kRows; ++k) {
+        const int r = r0 + k * RG;
+        const double2* row = reinterpret_cast<const double2*>(col + (size_t)r * ldw);
+#pragma unroll
+        for (int u = 0; u < 4; ++u) v[k][u] = (r < m && l[u]) ? __ldg(row + 32 * u) : make_double2(0.0, 0.0);
+      }
+#pragma unroll
+      for (int k = 0; k < kRows; ++k) {
+        const int r = r0 + k * RG;
+        const double xr = kSq ? 0.0 : (r < m ? x[r] : 0.0);
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          acc[u][0] += kSq ? v[k][u].x * v[k][u].x : v[k][u].x * xr;
+          acc[u][1] += kSq ? v[k][u].y * v[k][u].y : v[k][u].y * xr;
+        }
+      }
+    }
+    if (RG > 1) {
+#pragma unroll
+      for (int u = 0; u < 4; ++u)
+#pragma unroll
+        for (int e = 0; e < 2; ++e) gp[(size_t)((warp * 4 + u) * 2 + e) * 32 + lane] = acc[u][e];
+      __syncthreads();
+      if (rg == 0) {
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+#pragma unroll
+          for (int e = 0; e < 2; ++e)
+            for (int q = 1; q < RG; ++q) acc[u][e] += gp[(size_t)(((warp + q) * 4 + u) * 2 + e) * 32 + lane];
+      }
+      __syncthreads();
+    }
+    if (rg == 0) {
+#pragma unroll
+      for (int u = 0; u < 4; ++u)
+#pragma unroll
+        for (int e = 0; e < 2; ++e)
+          if (a[u][e]) fin(cb + 64 * u + e, acc[u][e]);
+    }
+  }
+  __syncthreads();
+}
+
+// Sum over the cluster's CTAs, in rank order, of the value at shared address
+// x in each CTA; the remote loads are issued together.
+__device__ __forceinline__ double cluster_sum(double* x, int cs) {
+  if (cs == 1) return *x;
+  cg::cluster_group cl = cg::this_cluster();
+  double v[16];
+#pragma unroll
+  for (int q = 0; q < 16; ++q) v[q] = q < cs ? *cl.map_shared_rank(x, q) : 0.0;
+  double sum = v[0];
+#pragma unroll
+  for (int q = 1; q < 16; ++q)
+    if (q < cs) sum += v[q];
+  return sum;
+}
+
+// (position, column) with the smallest position across the warp
+__device__ __forceinline__ void warp_min_pos(int& bp, int& bc) {
+  for (int o = 16; o > 0; o >>= 1) {
+    const int op = __shfl_xor_sync(0xffffffffu, bp, o);
+    const int oc = __shfl_xor_sync(0xffffffffu, bc, o);
+    if (op < bp || (op == bp && oc < bc)) {
+      bp = op;
+      bc = oc;
+    }
+  }
+}
+
+// Shared-memory carve of k_rrqr (doubles, then ints); rrqr_smem mirrors it.
+struct RrqrSmem {
+  double *red, *tmp, *spa, *spb, *s1, *s2, *sq, *cv, *qf, *vn1, *vn2, *gp;
+  int *pos, *flg;
+  __device__ RrqrSmem(double* sm, int mmax, int kmax, int nlmax, int rcmax) {
+    red = sm;
+    tmp = red + kRed;
+    spa = tmp + kNB;
+    spb = spa + kmax + 1;
+    s1 = spb + kmax + 1;
+    s2 = s1 + kmax + 1;
+    sq = s2 + kmax + 1;
+    cv = sq + rcmax;
+    qf = cv + rcmax;
+    vn1 = qf + mmax;
+    vn2 = vn1 + nlmax;
+    gp = vn2 + nlmax;
+    pos = reinterpret_cast<int*>(gp + 8 * kThreads);
+    flg = pos + nlmax;
+  }
+};
+
+// First own active position (>= i) whose partial norm is >= thr: position,
+// global column and norm in s_k[0][0], s_k[1][0], s_xv[0] (INT_MAX, -1, -1 if none).
+__device__ __forceinline__ void own_first(const RrqrSmem& S, int nloc, int ja, int i, double thr, int (*s_k)[kWarps],
+                                          double* s_xv) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  int bp = 0x7fffffff, bc = -1;
+  double bvn = -1.0;
+  for (int jl = threadIdx.x; jl < nloc; jl += kThreads) {
+    const int p = S.pos[jl];
+    if (p >= i && p < bp && S.vn1[jl] >= thr) {
+      bp = p;
+      bc = ja + jl;
+      bvn = S.vn1[jl];
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    const int op = __shfl_xor_sync(0xffffffffu, bp, o);
+    const int oc = __shfl_xor_sync(0xffffffffu, bc, o);
+    const double ov = __shfl_xor_sync(0xffffffffu, bvn, o);
+    if (op < bp) {
+      bp = op;
+      bc = oc;
+      bvn = ov;
+    }
+  }
+  __syncthreads();  // s_k / s_xv free (an earlier reader may still hold them)
+  if (lane == 0) {
+    s_k[0][warp] = bp;
+    s_k[1][warp] = bc;
+    s_xv[warp] = bvn;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int q = 1; q < kWarps; ++q)
+      if (s_k[0][q] < s_k[0][0]) {
+        s_k[0][0] = s_k[0][q];
+        s_k[1][0] = s_k[1][q];
+        s_xv[0] = s_xv[q];
+      }
+  }
+  __syncthreads();
+}
+
+__global__ void __launch_bounds__(kThreads, 2) k_rrqr(const RrqrTask* __restrict__ tasks, double tol,
+                                                      double pivot_rtol, int cs, int mmax, int kmax, int nlmax,
+                                                      int rcmax) {
   extern __shared__ double sm[];
-  __shared__ double s_x[2][kWarps];
+  __shared__ double s_x[kWarps];
   __shared__ int s_k[2][kWarps];
-  __shared__ double s_cmax;   // this CTA's max partial norm (read by the cluster)
-  __shared__ int s_cpos, s_ccol;
+  __shared__ double s_xv[kWarps];
+  // published by step parity: own largest partial norm M, the first own
+  // position P whose norm is within pivot_rtol of M, its column and norm;
+  // P2/C2 for the exact second round
+  __shared__ double s_pm[2], s_pv[2];
+  __shared__ int s_pp[2], s_pc[2], s_p2[2], s_c2[2];
+  __shared__ int s_piv[3];
+  __shared__ double s_thr;
+  __shared__ int s_nflag;
+  RrqrSmem S(sm, mmax, kmax, nlmax, rcmax);
   const RrqrTask t = tasks[blockIdx.x / cs];
   const int rank = crank(cs);
-  const int m = t.m, w = t.w;
+  const int m = t.m, w = t.w, ldq = t.ldq;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  double* C = t.C;
-  double* red = sm;
-  double* tmp = red + kRed;
-  double* vb = tmp + kNB;
-  double* ltau = vb + (m > 0 ? m : 1);
-  int* pos = reinterpret_cast<int*>(ltau + (m > 0 ? m : 1));  // own columns, by local index
-  (void)wloc_max;
-  double* vn1 = t.vn;
-  double* vn2 = t.vn + w;
-  // assemble own panels of C
-  {
-    int col = 0;
-    for (int s = t.src_begin; s < t.src_end; ++s) {
-      const RrqrSrc src = srcs[s];
-      const int width = src.transpose ? src.rows : src.cols;
-      for (int idx = threadIdx.x; idx < width * m; idx += kThreads) {
-        const int c = idx / m, r = idx % m;
-        const int gc = col + c;
-        if (!owns(gc, rank, cs)) continue;
-        C[r + (size_t)gc * m] = src.transpose ? src.A[c + (size_t)r * src.lda] : src.A[r + (size_t)c * src.lda];
-      }
-      col += width;
-    }
-  }
-  __syncthreads();
-  // own columns: local index li <-> global column gc
-  const int npan = (w + kNB - 1) / kNB;
-  auto gcol = [&](int li) { return ((li / kNB) * cs + rank) * kNB + (li % kNB); };
-  const int own_pan = (npan - rank + cs - 1) / cs;
-  int nloc = 0;
-  if (own_pan > 0) {
-    const int last_pan = rank + (own_pan - 1) * cs;
-    nloc = (own_pan - 1) * kNB + min(kNB, w - last_pan * kNB);
-  }
-  for (int li = warp; li < nloc; li += kWarps) {
-    const int gc = gcol(li);
-    const double* cj = C + (size_t)gc * m;
-    double s = 0.0;
-    for (int r = lane; r < m; r += 32) s += cj[r] * cj[r];
-    s = sqrt(dev::warp_sum(s));
-    if (lane == 0) {
-      vn1[gc] = s;
-      vn2[gc] = s;
-      pos[li] = gc;
-      t.colat[gc] = gc;
-    }
-  }
-  __syncthreads();
+  const double* __restrict__ Ct = t.C;
+  const int ldw = t.ldw;
+  double* Qt = t.Q;
+
+  // own columns [ja, jb) and own rows [ra, rb)
+  const int wc = ((w + cs - 1) / cs + 31) / 32 * 32;
+  const int ja = min(w, rank * wc), jb = min(w, ja + wc), nloc = jb - ja;
+  const int rc = (m + cs - 1) / cs;
+  const int ra = min(m, rank * rc), rb = min(m, ra + rc);
+  const int kmin = min(m, w);
+  // remote shared memory of cluster rank q (the CTA's own for cs == 1)
+  auto remote = [&](double* p, int q) -> double {
+    if (cs == 1) return *p;
+    return *cg::this_cluster().map_shared_rank(p, q);
+  };
+  auto remote_i = [&](int* p, int q) -> int {
+    if (cs == 1) return *p;
+    return *cg::this_cluster().map_shared_rank(p, q);
+  };
+  // initial norms, positions
+  col_dots<true>(Ct, ldw, m, ja, nloc, nullptr, S.gp, [](int) { return true; }, [&](int jl, double ss) {
+    const double v = sqrt(ss);
+    S.vn1[jl] = v;
+    S.vn2[jl] = v;
+    S.pos[jl] = ja + jl;
+    t.colat[ja + jl] = ja + jl;
+  });
+  __threadfence();
   csync(cs);
-  const int kmin = m < w ? m : w;
   const double tol3z = sqrt(1.1102230246251565e-16);
-  int rk = kmin;
+  double r00 = 0.0;
+  int rk = kmin, nrecomp = 0;
+  long long ph[4] = {0, 0, 0, 0};  // cycles: pivot choice, projections, basis vector, row of R
+  long long tc = clock64();
+  auto lap = [&](int k) {
+    const long long now = clock64();
+    ph[k] += now - tc;
+    tc = now;
+  };
   for (int i = 0; i < kmin; ++i) {
-    // (a) largest partial norm over active columns (position >= i)
+    const int par = i & 1;
+    // (a) own largest partial norm M over active columns (position >= i)
     double bv = -1.0;
-    for (int li = threadIdx.x; li < nloc; li += kThreads)
-      if (pos[li] >= i) bv = fmax(bv, vn1[gcol(li)]);
+    for (int jl = threadIdx.x; jl < nloc; jl += kThreads)
+      if (S.pos[jl] >= i) bv = fmax(bv, S.vn1[jl]);
     for (int o = 16; o > 0; o >>= 1) bv = fmax(bv, __shfl_xor_sync(0xffffffffu, bv, o));
-    if (lane == 0) s_x[0][warp] = bv;
+    if (lane == 0) s_x[warp] = bv;
     __syncthreads();
+    double mloc = s_x[0];
+    for (int q = 1; q < kWarps; ++q) mloc = fmax(mloc, s_x[q]);
+    // (b) first own position within pivot_rtol of M, published with M
+    own_first(S, nloc, ja, i, mloc * (1.0 - pivot_rtol), s_k, s_xv);
     if (threadIdx.x == 0) {
-      double v = s_x[0][0];
-      for (int q = 1; q < kWarps; ++q) v = fmax(v, s_x[0][q]);
-      s_cmax = v;
+      s_pm[par] = mloc;
+      s_pp[par] = s_k[0][0];
+      s_pc[par] = s_k[1][0];
+      s_pv[par] = s_xv[0];
     }
     csync(cs);
-    double gmax = -1.0;
-    if (cs > 1) {
-      cg::cluster_group cl = cg::this_cluster();
-      for (int q = 0; q < cs; ++q) gmax = fmax(gmax, *cl.map_shared_rank(&s_cmax, q));
-    } else {
-      gmax = s_cmax;
-    }
-    // (b) first position with vn1 >= (1 - pivot_rtol) * max
-    const double thr = gmax * (1.0 - pivot_rtol);
-    int bp = 0x7fffffff, bc = -1;
-    for (int li = threadIdx.x; li < nloc; li += kThreads) {
-      const int p = pos[li];
-      if (p >= i && p < bp && vn1[gcol(li)] >= thr) {
-        bp = p;
-        bc = gcol(li);
+    // the pivot: the first position within pivot_rtol of the cluster's largest
+    // norm.  A CTA's published position is exact unless its own maximum is
+    // within pivot_rtol of the largest but the published column is not: then
+    // a second round at the cluster's threshold decides.
+    if (warp == 0) {
+      double M = -1.0, V = -1.0;
+      int P = 0x7fffffff, Cc = -1;
+      if (lane < cs) {
+        M = remote(&s_pm[par], lane);
+        V = remote(&s_pv[par], lane);
+        P = remote_i(&s_pp[par], lane);
+        Cc = remote_i(&s_pc[par], lane);
       }
-    }
-    for (int o = 16; o > 0; o >>= 1) {
-      const int op = __shfl_xor_sync(0xffffffffu, bp, o);
-      const int oc = __shfl_xor_sync(0xffffffffu, bc, o);
-      if (op < bp) {
-        bp = op;
-        bc = oc;
+      double gm = M;
+      for (int o = 16; o > 0; o >>= 1) gm = fmax(gm, __shfl_xor_sync(0xffffffffu, gm, o));
+      const double thr = gm * (1.0 - pivot_rtol);
+      const bool amb = lane < cs && M >= thr && !(V >= thr);
+      int bp = (lane < cs && M >= thr && V >= thr) ? P : 0x7fffffff, bc = bp != 0x7fffffff ? Cc : -1;
+      warp_min_pos(bp, bc);
+      const bool any_amb = __any_sync(0xffffffffu, amb);
+      if (lane == 0) {
+        s_piv[0] = bp;
+        s_piv[1] = bc;
+        s_piv[2] = any_amb ? 1 : 0;
+        s_thr = thr;
       }
-    }
-    if (lane == 0) {
-      s_k[0][warp] = bp;
-      s_k[1][warp] = bc;
     }
     __syncthreads();
-    if (threadIdx.x == 0) {
-      int p = s_k[0][0], c = s_k[1][0];
-      for (int q = 1; q < kWarps; ++q)
-        if (s_k[0][q] < p) {
-          p = s_k[0][q];
-          c = s_k[1][q];
-        }
-      s_cpos = p;
-      s_ccol = c;
-    }
-    csync(cs);
-    int ppos = 0x7fffffff, pcol = -1;
-    if (cs > 1) {
-      cg::cluster_group cl = cg::this_cluster();
-      for (int q = 0; q < cs; ++q) {
-        const int p = *cl.map_shared_rank(&s_cpos, q);
-        const int c = *cl.map_shared_rank(&s_ccol, q);
-        if (p < ppos) {
-          ppos = p;
-          pcol = c;
-        }
-      }
-    } else {
-      ppos = s_cpos;
-      pcol = s_ccol;
-    }
-    if (pcol < 0) {  // no finite maximum (NaN norms): take the column at position i
-      ppos = i;
-      pcol = __ldcg(t.colat + i);
-    }
-    // (c) the owner of the pivot column builds reflector i and books the swap
-    const int cur = __ldcg(t.colat + i);  // column now at position i
-    if (owns(pcol, rank, cs)) {
-      double* cp = C + (size_t)pcol * m;
-      double s = 0.0;
-      for (int r = i + 1 + threadIdx.x; r < m; r += kThreads) s += cp[r] * cp[r];
-      s = dev::cta_sum(s, red);
-      const double alpha = cp[i];
-      double beta, scal;
-      const double ti = dev::house(alpha, s, &beta, &scal);
-      double* vo = t.V + (size_t)i * m;
-      for (int r = threadIdx.x; r < m; r += kThreads) {
-        double v = 0.0;
-        if (r == i) v = 1.0;
-        else if (r > i) v = ti != 0.0 ? cp[r] * scal : cp[r];
-        vo[r] = v;
-      }
+    int ppos = s_piv[0], pcol = s_piv[1];
+    if (s_piv[2]) {
+      own_first(S, nloc, ja, i, s_thr, s_k, s_xv);
       if (threadIdx.x == 0) {
-        t.tau[i] = ti;
-        double stop = 0.0;
-        const double absb = fabs(beta);
-        if (i == 0) t.bc[2] = absb;
-        else if (!(absb / __ldcg(t.bc + 2) >= tol)) stop = 1.0;
-        t.bc[i & 1] = stop;
+        s_p2[par] = s_k[0][0];
+        s_c2[par] = s_k[1][0];
       }
-      __threadfence();
+      csync(cs);
+      if (warp == 0) {
+        int bp = 0x7fffffff, bc = -1;
+        if (lane < cs) {
+          bp = remote_i(&s_p2[par], lane);
+          bc = remote_i(&s_c2[par], lane);
+        }
+        warp_min_pos(bp, bc);
+        if (lane == 0) {
+          s_piv[0] = bp;
+          s_piv[1] = bc;
+        }
+      }
+      __syncthreads();
+      ppos = s_piv[0];
+      pcol = s_piv[1];
+    }
+    const int cur = __ldcg(t.colat + i);  // column now at position i
+    if (pcol < 0) {  // no finite maximum (NaN norms): keep the column at position i
+      ppos = i;
+      pcol = cur;
+    }
+    lap(0);
+    // (c) projection s = Q^T c of the pivot column on q_0..q_{i-1} and ||c||^2,
+    // partial sums over own rows published together
+    for (int r = ra + threadIdx.x; r < rb; r += kThreads) S.cv[r - ra] = __ldg(Ct + (size_t)r * ldw + pcol);
+    __syncthreads();
+    for (int l = threadIdx.x; l < i; l += kThreads) {
+      double acc = 0.0;
+      for (int r = ra; r < rb; ++r) acc += Qt[(size_t)r * ldq + l] * S.cv[r - ra];
+      S.spa[l] = acc;
+    }
+    {
+      double cc = 0.0;
+      for (int r = ra + threadIdx.x; r < rb; r += kThreads) cc += S.cv[r - ra] * S.cv[r - ra];
+      cc = dev::cta_sum(cc, S.red);
+      if (threadIdx.x == 0) S.spa[kmax] = cc;
     }
     csync(cs);
-    if (__ldcg(t.bc + (i & 1)) != 0.0) {
+    double ss = 0.0;
+    for (int l = threadIdx.x; l < i; l += kThreads) {
+      const double v = cluster_sum(S.spa + l, cs);
+      S.s1[l] = v;
+      ss += v * v;
+    }
+    ss = dev::cta_sum(ss, S.red);
+    const double cc = cluster_sum(S.spa + kmax, cs);
+    // |R(i,i)|^2 = ||c||^2 - ||s||^2 while that loses at most 1e-10 relative
+    // accuracy; otherwise a second, explicit projection pass (CGS2)
+    double nrm2 = cc - ss;
+    const double* proj = S.s1;
+    __syncthreads();
+    for (int r = ra + warp; r < rb; r += kWarps) {
+      const double* qr = Qt + (size_t)r * ldq;
+      double d = 0.0;
+      for (int l = lane; l < i; l += 32) d += qr[l] * S.s1[l];
+      d = dev::warp_sum(d);
+      if (lane == 0) S.cv[r - ra] -= d;
+    }
+    if (!(nrm2 >= 1e-6 * cc)) {
+      __syncthreads();
+      for (int l = threadIdx.x; l < i; l += kThreads) {
+        double acc = 0.0;
+        for (int r = ra; r < rb; ++r) acc += Qt[(size_t)r * ldq + l] * S.cv[r - ra];
+        S.spb[l] = acc;
+      }
+      {
+        double nn = 0.0;
+        for (int r = ra + threadIdx.x; r < rb; r += kThreads) nn += S.cv[r - ra] * S.cv[r - ra];
+        nn = dev::cta_sum(nn, S.red);
+        if (threadIdx.x == 0) S.spb[kmax] = nn;
+      }
+      csync(cs);
+      double s2s = 0.0;
+      for (int l = threadIdx.x; l < i; l += kThreads) {
+        const double v = cluster_sum(S.spb + l, cs);
+        S.s2[l] = v;
+        s2s += v * v;
+      }
+      s2s = dev::cta_sum(s2s, S.red);
+      nrm2 = cluster_sum(S.spb + kmax, cs) - s2s;
+      proj = S.s2;
+    }
+    const double nrm = sqrt(fmax(nrm2, 0.0));  // |R(i,i)|
+    lap(1);
+    if (i == 0) {
+      r00 = nrm;
+    } else if (!(nrm / r00 >= tol)) {
       rk = i;
       break;
     }
-    // every CTA has read colat[i] above; book the swap for the next steps
-    if (owns(pcol, rank, cs) && threadIdx.x == 0) {
+    // (d) every CTA has read colat[i]; book the swap, update own positions
+    if (pcol >= ja && pcol < jb && threadIdx.x == 0) {
       t.colat[ppos] = cur;
       t.colat[i] = pcol;
       __threadfence();
     }
-    // (d) position bookkeeping of own columns
-    for (int li = threadIdx.x; li < nloc; li += kThreads) {
-      const int gc = gcol(li);
-      if (gc == pcol) pos[li] = i;
-      else if (gc == cur) pos[li] = ppos;
+    for (int jl = threadIdx.x; jl < nloc; jl += kThreads) {
+      const int gc = ja + jl;
+      if (gc == pcol) S.pos[jl] = i;
+      else if (gc == cur) S.pos[jl] = ppos;
     }
-    const double ti = __ldcg(t.tau + i);
-    for (int r = threadIdx.x; r < m - i; r += kThreads) vb[r] = __ldcg(t.V + (size_t)i * m + i + r);
-    __syncthreads();
-    // (e) apply H_i to own active columns and downdate their norms
-    for (int li = warp; li < nloc; li += kWarps) {
-      if (pos[li] <= i) continue;
-      const int gc = gcol(li);
-      double* cj = C + (size_t)gc * m;
-      if (ti != 0.0) {
-        double d = 0.0;
-        for (int r = lane; r < m - i; r += 32) d += vb[r] * cj[i + r];
-        d = dev::warp_sum(d) * ti;
-        __syncwarp();
-        for (int r = lane; r < m - i; r += 32) cj[i + r] -= vb[r] * d;
-        __syncwarp();
+    // q_i = (c - Q s [- Q s2]) / |R(i,i)| on own rows, then gathered whole
+    const double inv = nrm > 0.0 ? 1.0 / nrm : 0.0;
+    const bool second = proj == S.s2;
+    for (int r = ra + warp; r < rb; r += kWarps) {
+      double* qr = Qt + (size_t)r * ldq;
+      double d = 0.0;
+      if (second)
+        for (int l = lane; l < i; l += 32) d += qr[l] * S.s2[l];
+      d = dev::warp_sum(d);
+      if (lane == 0) {
+        const double v = (S.cv[r - ra] - d) * inv;
+        S.sq[r - ra] = v;
+        qr[i] = v;
+        t.Qc[r + (size_t)i * m] = v;
       }
-      const double v1 = vn1[gc];
-      if (v1 != 0.0) {
-        double temp = fabs(cj[i]) / v1;
-        temp = 1.0 - temp * temp;
-        temp = temp < 0.0 ? 0.0 : temp;
-        const double q = v1 / vn2[gc];
-        if (temp * q * q <= tol3z) {
-          double nn = 0.0;
-          for (int r = i + 1 + lane; r < m; r += 32) nn += cj[r] * cj[r];
-          nn = (i + 1 < m) ? sqrt(dev::warp_sum(nn)) : 0.0;
-          if (lane == 0) {
-            vn1[gc] = nn;
-            vn2[gc] = nn;
+    }
+    __threadfence();
+    csync(cs);
+    for (int r = threadIdx.x; r < m; r += kThreads) {
+      const int q = r / rc;
+      S.qf[r] = remote(S.sq + (r - q * rc), q);
+    }
+    if (threadIdx.x == 0) s_nflag = 0;
+    __syncthreads();
+    lap(2);
+    // (e) row i of R over own active columns (kept in F for recomputations);
+    // dlaqp2 downdate of the partial norms
+    double* Fi = t.F + (size_t)i * w + ja;
+    col_dots<false>(Ct, ldw, m, ja, nloc, S.qf, S.gp, [&](int jl) { return S.pos[jl] > i; },
+                    [&](int jl, double rij) {
+                      Fi[jl] = rij;
+                      const double v1 = S.vn1[jl];
+                      if (v1 == 0.0) return;
+                      double temp = fabs(rij) / v1;
+                      temp = 1.0 - temp * temp;
+                      temp = temp < 0.0 ? 0.0 : temp;
+                      const double qq = v1 / S.vn2[jl];
+                      if (temp * qq * qq <= tol3z) S.flg[atomicAdd(&s_nflag, 1)] = jl;
+                      else S.vn1[jl] = v1 * sqrt(temp);
+                    });
+    // recomputed partial norms ||c_j - Q(:, 0:i) R(0:i, j)||, one warp per column
+    const int nf = s_nflag;
+    nrecomp += nf;
+    for (int f = warp; f < nf; f += kWarps) {
+      const int jl = S.flg[f], j = ja + jl;
+      double res = 0.0;
+      if (i + 1 < m) {
+        for (int r = lane; r < m; r += 32) {
+          double x[4] = {0.0, 0.0, 0.0, 0.0};
+          int l = 0;
+          for (; l + 8 <= i + 1; l += 8) {
+            double qv[8], fv[8];
+#pragma unroll
+            for (int u = 0; u < 8; ++u) {
+              qv[u] = __ldcg(t.Qc + (size_t)(l + u) * m + r);
+              fv[u] = t.F[(size_t)(l + u) * w + j];
+            }
+#pragma unroll
+            for (int u = 0; u < 8; ++u) x[u & 3] += qv[u] * fv[u];
           }
-        } else if (lane == 0) {
-          vn1[gc] = v1 * sqrt(temp);
+          for (; l <= i; ++l) x[0] += __ldcg(t.Qc + (size_t)l * m + r) * t.F[(size_t)l * w + j];
+          const double e = __ldg(Ct + (size_t)r * ldw + j) - ((x[0] + x[1]) + (x[2] + x[3]));
+          res += e * e;
         }
+        res = dev::warp_sum(res);
       }
-      __syncwarp();
+      if (lane == 0) {
+        S.vn1[jl] = sqrt(res);
+        S.vn2[jl] = sqrt(res);
+      }
     }
     __syncthreads();
+    lap(3);
   }
-  csync(cs);
-  // block factors of the kept reflectors, panels dealt over the cluster
-  for (int j0 = rank * kNB; j0 < rk; j0 += cs * kNB) {
-    const int kb = (rk - j0) < kNB ? (rk - j0) : kNB;
-    for (int q = threadIdx.x; q < kb; q += kThreads) ltau[q] = __ldcg(t.tau + j0 + q);
-    __syncthreads();
-    dev::panel_t(t.V + j0 + (size_t)j0 * m, m, m - j0, kb, 1, ltau, t.T + (size_t)j0 * kNB, kNB, tmp);
+  csync(cs);  // no CTA reads another's shared memory past this point
+  if (rank == 0 && threadIdx.x == 0 && t.stats) {
+    t.stats[0] = nrecomp;
+    t.stats[1] = rk;
+    for (int k = 0; k < 4; ++k) t.stats[2 + k] = (int)(ph[k] >> 10);
+    t.stats[7] = 0;
   }
-  if (rank == 0 && threadIdx.x == 0) *t.rank = rk;
-  csync(cs);
+  const long long tq = clock64();
+  // Householder QR of the selected columns C(:, colat[0:rk]) into V
+  for (int l = warp; l < rk; l += kWarps) {
+    if (!owns(l, rank, cs)) continue;
+    const int c = __ldcg(t.colat + l);
+    for (int r = lane; r < m; r += 32) t.V[r + (size_t)l * m] = __ldg(Ct + (size_t)r * ldw + c);
+  }
+  __syncthreads();
+  dist_qr(t.V, m, nullptr, 0, m, rk, 1, t.T, t.tau, S.s1, S.qf, S.red, S.tmp, cs);
+  if (rank == 0 && threadIdx.x == 0) {
+    *t.rank = rk;
+    if (t.stats) t.stats[6] = (int)((clock64() - tq) >> 10);
+  }
 }
 
 // ------------------------------------------------------------ merge
@@ -630,7 +930,9 @@ constexpr size_t kSmemMax = 227 * 1024;
 template <typename K>
 cudaError_t prep(K kern, size_t bytes) {
   if (bytes > kSmemMax) return cudaErrorInvalidValue;
-  if (bytes > 48 * 1024) return cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  // above 48 KB of dynamic plus static shared memory the kernel must opt in;
+  // static shared memory of these kernels stays below 8 KB
+  if (bytes > 40 * 1024) return cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
   return cudaSuccess;
 }
 
@@ -716,7 +1018,8 @@ cudaError_t launch_edge(int kind, const EdgeChunk* t, int ntasks, cudaStream_t s
     if ((e = prep(k_edge_left, b))) return e;
     k_edge_left<<<ntasks, kThreads, b, st>>>(t);
   } else if (kind == 1) {
-    k_edge_trsm<<<ntasks, kThreads, 0, st>>>(t);
+    if ((e = prep(k_edge_trsm, b))) return e;
+    k_edge_trsm<<<ntasks, kThreads, b, st>>>(t);
   } else {
     if ((e = prep(k_edge_right, b))) return e;
     k_edge_right<<<ntasks, kThreads, b, st>>>(t);
@@ -724,14 +1027,56 @@ cudaError_t launch_edge(int kind, const EdgeChunk* t, int ntasks, cudaStream_t s
   return last();
 }
 
-cudaError_t launch_rrqr(const RrqrTask* t, const RrqrSrc* s, int ntasks, int cs, int mmax, int wloc_max, double tol,
+size_t rrqr_smem(int mmax, int kmax, int nlmax, int rcmax) {
+  const size_t d = kRed + kNB + 4 * ((size_t)kmax + 1) + 2 * (size_t)rcmax + (size_t)std::max(mmax, 1) +
+                   2 * (size_t)nlmax + 8 * (size_t)kThreads;
+  return smem_bytes(d) + sizeof(int) * 2 * (size_t)nlmax;
+}
+
+bool rrqr_cluster_fits(int cs, size_t smem) {
+  if (smem > kSmemMax) return false;
+  if (cs <= 8) return true;
+  if (prep(k_rrqr, smem)) return false;
+  if (cudaFuncSetAttribute(k_rrqr, cudaFuncAttributeNonPortableClusterSizeAllowed, 1)) {
+    cudaGetLastError();
+    return false;
+  }
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)cs);
+  cfg.blockDim = dim3(kThreads);
+  cfg.dynamicSmemBytes = smem;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = (unsigned)cs;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  int n = 0;
+  if (cudaOccupancyMaxActiveClusters(&n, k_rrqr, &cfg) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return n > 0;
+}
+
+cudaError_t launch_rrqr_assemble(const RrqrSrc* s, int nsrc, cudaStream_t st) {
+  if (cudaError_t pre = begin("launch_rrqr_assemble")) return pre;
+  if (nsrc <= 0) return cudaSuccess;
+  counted();
+  k_rrqr_assemble<<<nsrc, kThreads, 0, st>>>(s);
+  return last();
+}
+
+cudaError_t launch_rrqr(const RrqrTask* t, int ntasks, int cs, int mmax, int kmax, int nlmax, int rcmax, double tol,
                         double pivot_rtol, cudaStream_t st) {
   if (cudaError_t pre = begin("launch_rrqr")) return pre;
   if (ntasks <= 0) return cudaSuccess;
-  const size_t b = smem_bytes(kRed + kNB + 2 * (size_t)std::max(mmax, 1)) + sizeof(int) * (size_t)(wloc_max + 1);
+  const size_t b = rrqr_smem(mmax, kmax, nlmax, rcmax);
   cudaError_t e = prep(k_rrqr, b);
+  if (!e && cs > 8) e = cudaFuncSetAttribute(k_rrqr, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
   if (e) return e;
-  return launch_clustered(k_rrqr, ntasks, cs, b, st, t, s, tol, pivot_rtol, cs, wloc_max);
+  return launch_clustered(k_rrqr, ntasks, cs, b, st, t, tol, pivot_rtol, cs, mmax, kmax, nlmax, rcmax);
 }
 
 cudaError_t launch_merge(const MergeTask* t, int ntasks, cudaStream_t st) {

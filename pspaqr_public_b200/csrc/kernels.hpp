@@ -23,7 +23,14 @@ cudaError_t launch_update(const UpdTask* t, const UpdOp* o, int ntasks, cudaStre
 // kind 0: left apply on column chunks, 1: right triangular solve on row chunks,
 // 2: right apply on row chunks
 cudaError_t launch_edge(int kind, const EdgeChunk* t, int ntasks, cudaStream_t st);
-cudaError_t launch_rrqr(const RrqrTask* t, const RrqrSrc* s, int ntasks, int cs, int mmax, int wloc_max, double tol,
+// Shared memory of one pivoted-QR CTA for tasks of at most mmax rows, kmax
+// steps, nlmax own columns and rcmax own rows.
+size_t rrqr_smem(int mmax, int kmax, int nlmax, int rcmax);
+// a cluster of cs CTAs with smem bytes each of the pivoted QR can be resident
+bool rrqr_cluster_fits(int cs, size_t smem);
+// transposed gather of the compression matrices (one CTA per source block)
+cudaError_t launch_rrqr_assemble(const RrqrSrc* s, int nsrc, cudaStream_t st);
+cudaError_t launch_rrqr(const RrqrTask* t, int ntasks, int cs, int mmax, int kmax, int nlmax, int rcmax, double tol,
                         double pivot_rtol, cudaStream_t st);
 cudaError_t launch_merge(const MergeTask* t, int ntasks, cudaStream_t st);
 

@@ -65,24 +65,29 @@ struct EdgeChunk {
 
 // Truncated column-pivoted QR of the compression matrix of one interface
 // (ptree.cpp:373-439): C = [A(n,p)^T ... | A(p,m) ...], m = size of p.
-// Run by one thread-block cluster; C's 32-column panels are distributed over
-// its CTAs and pivot columns are tracked by position (no physical swaps).
+// C is assembled transposed (w x m, element (j, r) at Ct[r * w + j]) and stays
+// read-only while a thread-block cluster selects the pivots; the reflectors
+// are then computed from the selected columns.
 struct RrqrTask {
-  double* C;      // m x w scratch (ld m)
-  double* V;      // m x m output: reflector j in column j (ld m)
-  double* T;      // kNB x m output block factors
-  double* tau;    // m
-  double* vn;     // 2*w partial column norms
-  int* colat;     // w: column at each pivot position
-  double* bc;     // 16 doubles: broadcast slots
-  int* rank;      // output
-  int m, w;
-  int src_begin, src_end;  // range in RrqrSrc
+  const double* C;  // Ct: element (j, r) at C[r * ldw + j], ldw >= w a multiple of 4
+  double* Q;        // m x ldq scratch: row r of the orthonormal basis at Q[r * ldq]
+  double* Qc;       // the same basis column-major (m x ldq, ld m)
+  double* F;        // ldq x w scratch: row i of R at F[i * w]
+  double* V;        // m x m output: reflector j below the diagonal of column j, R above (ld m)
+  double* T;        // kNB x m output block factors
+  double* tau;      // m
+  int* colat;       // w: column at each pivot position
+  int* rank;        // output
+  int* stats;       // 8 ints or null: recomputations, rank, kilocycles of pivot choice,
+                    // projections, basis vector, row of R, final QR, whole selection
+  int m, w, ldq, ldw;
 };
 struct RrqrSrc {
   const double* A;
   int lda, rows, cols;
   int transpose;  // 1: out-block A(n,p) (rows x m) enters transposed
+  double* Ct;     // destination: columns [c0, c0 + width) of the task's C
+  int w, c0;      // w: leading dimension of Ct
 };
 
 // Merge of one child block into its parent block (ptree.cpp:289-340).

@@ -48,6 +48,7 @@ def lib():
             "spq_set_ttor_log": (i32, [vp, i32]),
             "spq_set_square": (i32, [vp, i32]),
             "spq_set_pivot_rtol": (i32, [vp, f64]),
+            "spq_set_rrqr_work": (i32, [vp, f64, f64]),
             "spq_get_factor": (i32, [vp, i32, i32, pd, pi]),
             "spq_set_coords": (i32, [vp, i32, i32, pd]),
             "spq_set_coords_tensor": (i32, [vp, i32, i32]),
@@ -77,6 +78,7 @@ def lib():
             "spq_times": (i32, [vp, pd]),
             "spq_level_times": (i32, [vp, pf]),
             "spq_factor_flops": (f64, [vp]),
+            "spq_rrqr_bytes": (f64, [vp]),
             "spq_pool_bytes": (f64, [vp]),
             "spq_last_error": (C.c_char_p, [vp]),
             "spq_kernel_launches": (C.c_longlong, []),
@@ -191,6 +193,11 @@ class ParTree:
 
     def set_pivot_rtol(self, r: float):
         self._chk(lib().spq_set_pivot_rtol(self._h, r), "set_pivot_rtol")
+
+    def set_rrqr_work(self, elems: float, fill: float = 2.0):
+        """Cluster sizing of the pivoted QR: elements of the compression matrix
+        per CTA and pivot step, and CTAs per SM a level's work is spread over."""
+        self._chk(lib().spq_set_rrqr_work(self._h, elems, fill), "set_rrqr_work")
 
     def set_Xcoo(self, X: np.ndarray):
         """Coordinates as a dim x n array (tree.cpp:21)."""
@@ -318,6 +325,10 @@ class ParTree:
 
     def factor_flops(self) -> float:
         return lib().spq_factor_flops(self._h)
+
+    def rrqr_bytes(self) -> float:
+        """Compression-matrix bytes the pivoted QR read in the last factorize."""
+        return lib().spq_rrqr_bytes(self._h)
 
     def pool_bytes(self) -> float:
         return lib().spq_pool_bytes(self._h)
