@@ -85,6 +85,23 @@ int spq_gmres(spq_tree* t, double* b, int maxit, double tol, int* iters, double*
 /* Same with a device-resident right-hand side / solution. */
 int spq_gmres_device(spq_tree* t, double* b, int maxit, double tol, int* iters, double* relres, double* hist,
                      int hist_cap);
+/* spq_gmres_device without any device allocation.  No counterpart in the
+ * reference, which always allocates its Krylov vectors per solve.
+ *
+ * For callers that cannot allocate device memory at solve time: a service
+ * that reserves all device memory when it starts, or a process whose device
+ * memory belongs to another framework's pool.  spq_gmres_device grows a cached
+ * workspace with cudaMalloc; this entry point uses instead one fixed device
+ * array of 6,291,456 doubles (48 MiB) built into the library, which bounds
+ * the problem: n * (maxit + 3) + maxit + 1028 <= 6,291,456 (the 64^3 grid,
+ * n = 262,144, allows maxit <= 20), and maxit <= 100.  Larger requests fail
+ * with an error naming the size; nothing is truncated.  The array's device
+ * address is looked up by the first call on each device, so make that call
+ * before any stream capture on the device.  The array is shared by every tree
+ * on a device: calls that overlap in time (several host threads or streams)
+ * race on it and must be serialised.  b, iters and relres as spq_gmres_device;
+ * no residual history. */
+int spq_gmres_device_noalloc(spq_tree* t, double* b, int maxit, double tol, int* iters, double* relres);
 
 /* ParTree::distribute_x / extract_x (src/ptree.cpp:3264-3303), single rank:
  * x_local = x[rperm]  and  x[cperm] = x_local. */

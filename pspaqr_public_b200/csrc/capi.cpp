@@ -8,6 +8,7 @@
 #include "../../include/spaqr_b200.h"
 #include "engine.hpp"
 #include "kernels.hpp"
+#include "noalloc.hpp"
 
 struct spq_tree {
   spq::Tree* t;
@@ -112,6 +113,15 @@ int spq_gmres_device(spq_tree* h, double* b, int maxit, double tol, int* iters, 
                      int hist_cap) {
   if (!h || !b || !iters || !relres) return -1;
   return done(h, h->t->gmres_device(b, maxit, tol, iters, relres, hist, hist_cap));
+}
+int spq_gmres_device_noalloc(spq_tree* h, double* b, int maxit, double tol, int* iters, double* relres) {
+  if (!h || !b || !iters || !relres) return -1;
+  double* ws = nullptr;
+  if (cudaError_t e = spq::noalloc_workspace(&ws)) {
+    h->t->error = std::string("allocation-free GMRES workspace: ") + cudaGetErrorString(e);
+    return -10;
+  }
+  return done(h, h->t->gmres_device_fixed(b, maxit, tol, iters, relres, ws, spq::kNoAllocDoubles));
 }
 int spq_distribute_x(spq_tree* h, const double* x, double* xl) {
   if (!h || !x || !xl) return -1;

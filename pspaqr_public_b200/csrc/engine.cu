@@ -9,6 +9,7 @@
 #include <numeric>
 
 #include "kernels.hpp"
+#include "noalloc.hpp"
 
 namespace spq {
 
@@ -1035,6 +1036,108 @@ int Tree::gmres_device(double* b, int maxit, double gtol, int* iters, double* re
     g(launch_mgs_step(n, bsave, nullptr, nullptr, nullptr, partial, done, hcol + 1, 1, stream_));
     double nr[2] = {0, 1};
     cudaMemcpyAsync(nr, hcol, sizeof(double) * 2, cudaMemcpyDeviceToHost, stream_);
+    rc = check_cuda(ge ? ge : cudaStreamSynchronize(stream_), "gmres finish");
+    *iters = k;
+    *relres = nr[0] / nr[1];
+    last_gmres_iters = k;
+  }
+  t_gmres = wall() - t0;
+  return rc;
+}
+
+// The GMRES loop of gmres_device on a caller-given device workspace and fixed
+// host arrays: nothing is allocated on the device or the heap.  The workspace
+// counter the reductions use is cleared on every call.
+int Tree::gmres_device_fixed(double* b, int maxit, double gtol, int* iters, double* relres, double* ws,
+                             size_t ws_doubles) {
+  if (!factorized_) return fail(-4, "gmres called before factorize");
+  if (maxit < 1 || maxit > kNoAllocMaxit)
+    return fail(-1, "maxit must be in [1, " + std::to_string(kNoAllocMaxit) + "] for the allocation-free GMRES");
+  double t0 = wall();
+  const int n = st_.n;
+  const size_t ldq = (size_t)n;
+  const int grid = mgs_grid(n);
+  const size_t need = ldq * (maxit + 1) + 2 * (size_t)n + (maxit + 3) + grid + 1;
+  if (need > ws_doubles)
+    return fail(-14, "allocation-free GMRES needs " + std::to_string(need) + " doubles of workspace, the fixed array holds " +
+                         std::to_string(ws_doubles) + "; lower maxit or use spq_gmres_device");
+  double* Q = ws;
+  double* q = Q + ldq * (maxit + 1);
+  double* bsave = q + n;
+  double* hcol = bsave + n;
+  double* partial = hcol + (maxit + 3);
+  unsigned int* done = reinterpret_cast<unsigned int*>(partial + grid);
+  cudaError_t ge = cudaSuccess;
+  auto g = [&](cudaError_t e) {
+    if (!ge) ge = e;
+  };
+  g(cudaMemsetAsync(done, 0, sizeof(unsigned int), stream_));
+  g(cudaMemcpyAsync(bsave, b, sizeof(double) * n, cudaMemcpyDeviceToDevice, stream_));
+  g(cudaMemcpyAsync(q, b, sizeof(double) * n, cudaMemcpyDeviceToDevice, stream_));
+  if (ge) return check_cuda(ge, "gmres start");
+  if (int src = solve_device(q)) return src;
+  g(launch_mgs_step(n, q, nullptr, nullptr, nullptr, partial, done, hcol, 1, stream_));  // ||r||
+  g(launch_scale_copy(n, q, hcol, Q, stream_));
+  double r_norm = 0;
+  g(cudaMemcpyAsync(&r_norm, hcol, sizeof(double), cudaMemcpyDeviceToHost, stream_));
+  int rc = check_cuda(ge ? ge : cudaStreamSynchronize(stream_), "gmres start");
+  constexpr int M = kNoAllocMaxit;
+  double H[(M + 1) * M], cs[M], sn[M], beta[M + 1], hk[M + 2], y[M];
+  for (int i = 0; i < (M + 1) * M; ++i) H[i] = 0.0;
+  for (int i = 0; i < M; ++i) cs[i] = sn[i] = beta[i] = 0.0;
+  beta[M] = 0.0;
+  auto Hc = [&](int i, int j) -> double& { return H[(size_t)j * (maxit + 1) + i]; };
+  beta[0] = r_norm;
+  int k = 0;
+  if (!rc && (std::isnan(r_norm) || device_status() != 0)) rc = fail(-12, "preconditioner apply failed");
+  for (; !rc && k < maxit; ++k) {
+    if ((rc = spmv_device(Q + (size_t)k * ldq, q)) || (rc = solve_device(q))) break;
+    for (int i = 0; i <= k; ++i)
+      g(launch_mgs_step(n, q, i ? Q + (size_t)(i - 1) * ldq : nullptr, i ? hcol + (i - 1) : nullptr,
+                        Q + (size_t)i * ldq, partial, done, hcol + i, 0, stream_));
+    g(launch_mgs_step(n, q, Q + (size_t)k * ldq, hcol + k, nullptr, partial, done, hcol + k + 1, 1, stream_));
+    g(launch_scale_copy(n, q, hcol + k + 1, Q + (size_t)(k + 1) * ldq, stream_));
+    g(cudaMemcpyAsync(hk, hcol, sizeof(double) * (k + 2), cudaMemcpyDeviceToHost, stream_));
+    if ((rc = check_cuda(ge ? ge : cudaStreamSynchronize(stream_), "gmres iteration"))) break;
+    for (int i = 0; i <= k + 1; ++i) Hc(i, k) = hk[i];
+    for (int i = 0; i < k; ++i) {
+      const double temp = cs[i] * Hc(i, k) + sn[i] * Hc(i + 1, k);
+      Hc(i + 1, k) = -sn[i] * Hc(i, k) + cs[i] * Hc(i + 1, k);
+      Hc(i, k) = temp;
+    }
+    if (Hc(k, k) == 0) {
+      cs[k] = 0;
+      sn[k] = 1;
+    } else {
+      const double t = std::sqrt(Hc(k, k) * Hc(k, k) + Hc(k + 1, k) * Hc(k + 1, k));
+      cs[k] = std::fabs(Hc(k, k)) / t;
+      sn[k] = cs[k] * Hc(k + 1, k) / Hc(k, k);
+    }
+    Hc(k, k) = cs[k] * Hc(k, k) + sn[k] * Hc(k + 1, k);
+    Hc(k + 1, k) = 0.0;
+    beta[k + 1] = -sn[k] * beta[k];
+    beta[k] = cs[k] * beta[k];
+    const double err = std::fabs(beta[k + 1]) / r_norm;
+    if (verbose) printf("GMRES: error at step %d is %e\n", k, err);
+    if (err <= gtol) break;
+  }
+  if (!rc && device_status() != 0) rc = fail(-12, "forward sweep wait timed out on the device");
+  if (!rc) {
+    k = std::min(k, maxit - 1);
+    for (int i = k; i >= 0; --i) {  // util.cpp:1019-1032 LUSolve
+      y[i] = beta[i];
+      for (int j = i + 1; j < k + 1; ++j) y[i] -= Hc(i, j) * y[j];
+      y[i] /= Hc(i, i);
+    }
+    double* dy = hcol;
+    g(cudaMemcpyAsync(dy, y, sizeof(double) * (k + 1), cudaMemcpyHostToDevice, stream_));
+    g(launch_combine(n, k + 1, Q, ldq, dy, b, stream_));
+    g(spmv_device(b, q) ? cudaErrorUnknown : cudaSuccess);
+    g(launch_sub(n, bsave, q, q, stream_));
+    g(launch_mgs_step(n, q, nullptr, nullptr, nullptr, partial, done, hcol, 1, stream_));
+    g(launch_mgs_step(n, bsave, nullptr, nullptr, nullptr, partial, done, hcol + 1, 1, stream_));
+    double nr[2] = {0, 1};
+    g(cudaMemcpyAsync(nr, hcol, sizeof(double) * 2, cudaMemcpyDeviceToHost, stream_));
     rc = check_cuda(ge ? ge : cudaStreamSynchronize(stream_), "gmres finish");
     *iters = k;
     *relres = nr[0] / nr[1];

@@ -81,6 +81,9 @@ class Tree {
   int spmv_host(const double* x, double* y);
   int gmres_host(double* b, int maxit, double tol, int* iters, double* relres, double* hist, int hist_cap);
   int gmres_device(double* b_dev, int maxit, double tol, int* iters, double* relres, double* hist, int hist_cap);
+  // gmres_device on a caller-given device workspace of ws_doubles doubles,
+  // with fixed host arrays (maxit <= kNoAllocMaxit); allocates nothing
+  int gmres_device_fixed(double* b, int maxit, double gtol, int* iters, double* relres, double* ws, size_t ws_doubles);
 
   int set_stream(cudaStream_t s);
   cudaStream_t stream() const { return stream_; }

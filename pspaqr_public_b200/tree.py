@@ -61,6 +61,7 @@ def lib():
             "spq_spmv": (i32, [vp, pd, pd]),
             "spq_gmres": (i32, [vp, pd, i32, f64, pi, pd, pd, i32]),
             "spq_gmres_device": (i32, [vp, vp, i32, f64, pi, pd, pd, i32]),
+            "spq_gmres_device_noalloc": (i32, [vp, vp, i32, f64, pi, pd]),
             "spq_distribute_x": (i32, [vp, pd, pd]),
             "spq_extract_x": (i32, [vp, pd, pd]),
             "spq_n": (i32, [vp]),
