@@ -41,6 +41,10 @@ WORKLOAD = {
     "n": 64, "d": 3, "nlevels": 12, "tol": 1e-2, "skip": 0, "gmres_tol": 1e-10, "maxit": 300, "rhs_seed": 2,
 }
 METRIC = "time to 1e-10 rel. residual (factor+GMRES), 64^3 diffusion: mixed+learned vs FP64"
+# DRAM bytes per algorithmic byte of the pivoted-QR launches, from an ncu
+# capture of the 48^3 member of the workload family
+# (profiles/k_rrqr_diff3d_48_traffic.md)
+RRQR_DRAM_PER_ALGO_BYTE = 0.78
 
 
 def build_matrix():
@@ -226,13 +230,19 @@ def run_ours(args):
         step, e2e = float(tt[0]), float(tt[1])
     else:
         e2e = float(np.mean(e2e_times))
-    # per-level kernel-phase timing of the last factorization (events inside the library)
+    # per-level kernel-phase timing of the last factorization (CUDA events the
+    # library records on its stream around each phase)
     lt = t.level_times()
     flops = t.factor_flops()
     peaks = measured_peaks()
     fp64_peak = fp64_gemm_peak(torch) if rank == 0 else 0.0
     fact = float(np.mean(ftimes))
-    achieved = flops / fact / 1e12
+    # dominant kernel: the pivoted QR (k_rrqr_assemble + k_rrqr launches of
+    # every level), HBM-bound; algorithmic bytes over its event-timed duration
+    rrqr_s = float(lt[:, ParTree.LEVEL_PHASES.index("rrqr")].sum()) / 1e3
+    rrqr_bytes = t.rrqr_bytes()
+    hbm_peak = peaks.get("hbm_gbs") or 6650.0
+    achieved = rrqr_bytes / rrqr_s / 1e9
     nnz = len(ri)
     h2d = nnz * (8 + 4) + (N + 1) * 4 + 8 * N + 8 * nnz  # matrix (CSC values + indices) + b
     out = {
@@ -259,10 +269,17 @@ def run_ours(args):
         "partition_s": t_part,
         "e2e": {"value": e2e, "unit": "s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": 8 * N},
         "gpu_launches": int(np.median(launches)),
-        "roofline": {"bound": "fp64", "achieved": achieved, "peak": fp64_peak, "unit": "TFLOP/s",
-                     "frac": achieved / fp64_peak if fp64_peak else None, "traffic": None,
-                     "kernel": "factorization (all phases, nominal LAWN 41 flops / factorize time)",
-                     "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (MEASURED_PEAKS.json has no FP64 figure)"},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
+                     "frac": achieved / hbm_peak, "traffic": RRQR_DRAM_PER_ALGO_BYTE * rrqr_bytes if RRQR_DRAM_PER_ALGO_BYTE else None,
+                     "kernel": "pivoted QR (k_rrqr_assemble + k_rrqr, all levels of one factorization)",
+                     "algorithmic_bytes": rrqr_bytes, "duration_s": rrqr_s, "launches": "per factorization",
+                     "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if peaks.get("hbm_gbs")
+                     else "fallback 6650 GB/s (of fallback)",
+                     "traffic_source": "dram__bytes_read.sum + dram__bytes_write.sum per algorithmic byte of the "
+                                       "k_rrqr* launches of the 48^3 member (ncu), scaled to this step"},
+        "factor_fp64": {"achieved_tflops": flops / fact / 1e12, "dgemm_peak_tflops": fp64_peak,
+                        "note": "nominal LAWN 41 flops of the whole factorization / factorize time; "
+                                "peak = cuBLAS DGEMM 8192^3 in this run"},
         "level_ms": {k: lt[:, i].round(3).tolist() for i, k in enumerate(ParTree.LEVEL_PHASES)},
         "clocks": clk.summary(),
         "hbm_peak_gbs": peaks.get("hbm_gbs"),
@@ -343,7 +360,14 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--size", type=int, default=64,
+                    help="grid points per side (64 = the benchmark; smaller members of the family for profiling)")
     args = ap.parse_args()
+    if args.size != 64:
+        WORKLOAD.update(n=args.size, name=f"diff3d_{args.size}",
+                        nlevels=max(4, round(np.log2(args.size ** 3 / 128)) + 1),
+                        matrix=WORKLOAD["matrix"].replace("64^3", f"{args.size}^3").replace(
+                            "n=262144", f"n={args.size ** 3}"))
     if args.impl == "reference":
         run_reference(args)
     else:

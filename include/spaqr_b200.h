@@ -144,9 +144,9 @@ int spq_level_times(spq_tree* t, float* ms);
 /* Nominal FP64 flops of the last factorization (LAPACK Working Note 41 counts). */
 double spq_factor_flops(spq_tree* t);
 /* Bytes of compression-matrix data the pivoted QR of the last factorization
- * reads: one pass for the column norms and one per pivot step over the
- * columns still active (the algorithmic traffic of its roofline).  No
- * reference counterpart. */
+ * moves: the transposed gather (read + write), one pass for the column norms
+ * and one per pivot step over the columns still active (the algorithmic
+ * traffic of its roofline).  No reference counterpart. */
 double spq_rrqr_bytes(spq_tree* t);
 /* Bytes of device memory held by factor blocks. */
 double spq_pool_bytes(spq_tree* t);

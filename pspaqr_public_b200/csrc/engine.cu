@@ -623,9 +623,10 @@ int Tree::factorize() {
       for (size_t q = 0; q < Lv.spars_clusters.size(); ++q) {
         const double m = rr_dims[q].first, w = rr_dims[q].second, r = size_[Lv.spars_clusters[q]];
         flops_ += 4.0 * m * w * r - 2.0 * r * r * (m + w) + 4.0 * r * r * r / 3.0 + m * r * r;
-        // C read once for the norms and once per step over the active columns
+        // C gathered once (read + write), read once for the norms and once per
+        // step over the active columns
         const double steps = std::min(r + 1.0, std::min(m, w));
-        rrqr_bytes_ += 8.0 * m * (w + steps * w - steps * (steps + 1.0) / 2.0);
+        rrqr_bytes_ += 8.0 * m * (3.0 * w + steps * w - steps * (steps + 1.0) / 2.0);
         if (verbose >= 2)
           printf("rrqr level %d m %d w %d rank %d cluster %d recomputed %d kcycles %d %d %d %d %d %d\n", lvl, (int)m,
                  (int)w, (int)r, rr_cs[q], stats[8 * q], stats[8 * q + 2], stats[8 * q + 3], stats[8 * q + 4],

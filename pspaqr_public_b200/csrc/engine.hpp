@@ -101,8 +101,8 @@ class Tree {
   std::string error;
   size_t pool_bytes() const { return arena_.used(); }
   double factor_flops() const { return flops_; }
-  // bytes of the compression matrices the pivoted QR reads (one pass for the
-  // norms, one per pivot step over the active columns)
+  // bytes of the compression matrices the pivoted QR moves (the transposed
+  // gather, one pass for the norms, one per pivot step over the active columns)
   double rrqr_bytes() const { return rrqr_bytes_; }
   int device_status();
 
