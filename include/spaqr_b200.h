@@ -153,6 +153,47 @@ double spq_pool_bytes(spq_tree* t);
 /* Kernels this library has launched in the process so far (graph nodes counted
  * per graph launch); no reference counterpart, used to attribute device work. */
 long long spq_kernel_launches(void);
+/* ---- learned ranks (no reference counterpart) ------------------------------
+ * Instead of the column-pivoted QR of every interface's compression matrix C
+ * (m x w), a 3-layer MLP (width 64) predicts the kept fraction rank/min(m,w)
+ * from 11 features of C.  C is sketched with ell = predicted rank + oversample
+ * Rademacher columns, the sketch gets the pivoted QR (stopped at tol / 10),
+ * and the kept rank is the smallest k whose largest residual column norm
+ * max_j ||c_j - Q_k Q_k^T c_j|| is below tol * max_j ||c_j|| (the pivoted
+ * QR's own stop rule, util.cpp:830-851).  Interfaces where no such k exists
+ * fall back to the plain pivoted QR.  Features: log2(m+1), log2(w+1),
+ * log10(tol), the fractions (of min(m,w)) of columns with norm >= tol, 0.1,
+ * 0.5 x the largest, Frobenius norm^2 / (largest^2 min(m,w)), log10 of the
+ * 2nd-4th over the 1st diagonal entry of R in a QR of a 4-column sketch, and
+ * the level. */
+/* nparams = parameters of the MLP, nfeatures = 11 */
+int spq_rank_model_size(int* nparams, int* nfeatures);
+/* Use the learned ranks with this model (params as spq_mlp_train; mean / std
+ * standardise the features); params = NULL restores the plain pivoted QR.
+ * Resets the counters of spq_learned_counts. */
+int spq_set_rank_model(spq_tree* t, const float* params, const float* mean, const float* stdev, int oversample);
+/* out[0..2] = interfaces whose learned rank was accepted, interfaces that fell
+ * back to the pivoted QR, and the sum of the sketch widths, since the model was set. */
+int spq_learned_counts(spq_tree* t, long long* out);
+/* Log (features, kept rank, min(m,w), level) of every sparsified interface of
+ * later factorizations (the training pairs of the rank model). */
+int spq_set_rank_log(spq_tree* t, int on);
+int spq_rank_log_count(spq_tree* t);
+/* features: count x nfeatures row-major; ranks, kmin, levels: count each */
+int spq_rank_log(spq_tree* t, float* features, int* ranks, int* kmin, int* levels);
+int spq_rank_log_clear(spq_tree* t);
+/* The rank MLP on the GPU, host arrays in and out.  X: n x nfeatures
+ * standardised features (row-major), y in [0,1]; loss = mean (sigmoid(z)-y)^2.
+ * Layout of params: W1 (64 x 11, row-major), b1 (64), W2 (64 x 64), b2 (64),
+ * w3 (64), b3.  Status -10 = CUDA failure (message: spq_mlp_last_error). */
+int spq_mlp_loss_grad(const float* params, const float* X, const float* y, int n, float* loss, float* grad);
+int spq_mlp_predict(const float* params, const float* X, int n, float* out);
+/* Adam (beta 0.9 / 0.999) over `epochs` seeded shuffles in mini-batches;
+ * params updated in place; loss_hist (epochs values, may be NULL). */
+int spq_mlp_train(float* params, const float* X, const float* y, int n, int epochs, int batch, float lr,
+                  unsigned long long seed, float* loss_hist);
+const char* spq_mlp_last_error(void);
+
 const char* spq_last_error(spq_tree* t);
 
 #ifdef __cplusplus

@@ -17,8 +17,9 @@ LIB = os.path.join(HERE, "libspaqr_b200.so")
 DRIVER = os.path.join(HERE, "spaqr")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-SOURCES = ["structure.cpp", "engine.cu", "kernels.cu", "noalloc.cu", "capi.cpp"]
-HEADERS = ["structure.hpp", "engine.hpp", "tasks.hpp", "kernels.hpp", "dense.cuh", "noalloc.hpp"]
+SOURCES = ["structure.cpp", "engine.cu", "kernels.cu", "learned.cu", "noalloc.cu", "capi.cpp", "capi_learned.cpp"]
+HEADERS = ["structure.hpp", "engine.hpp", "tasks.hpp", "kernels.hpp", "dense.cuh", "noalloc.hpp", "learned.hpp",
+           "capi_internal.hpp"]
 
 
 def _stale(target: str, deps) -> bool:

@@ -6,14 +6,11 @@
 #include <vector>
 
 #include "../../include/spaqr_b200.h"
+#include "capi_internal.hpp"
 #include "engine.hpp"
 #include "kernels.hpp"
 #include "noalloc.hpp"
 
-struct spq_tree {
-  spq::Tree* t;
-  std::string err;
-};
 
 namespace {
 int done(spq_tree* h, int rc) {

@@ -2,6 +2,7 @@
 #include "engine.hpp"
 
 #include <algorithm>
+#include <array>
 #include <chrono>
 #include <cmath>
 #include <cstdio>
@@ -9,6 +10,7 @@
 #include <numeric>
 
 #include "kernels.hpp"
+#include "learned.hpp"
 #include "noalloc.hpp"
 
 namespace spq {
@@ -79,6 +81,7 @@ void Arena::release() {
 Tree::Tree(int L, int s) : nlevels(L), skip(s) {}
 
 Tree::~Tree() {
+  cudaFree(d_model_);
   if (solve_exec_) cudaGraphExecDestroy(solve_exec_);
   if (solve_graph_) cudaGraphDestroy(solve_graph_);
   cudaFree(d_rank_);
@@ -462,84 +465,122 @@ int Tree::factorize() {
           flops_ += (double)t.m * t.nc * t.nc;
         }
       }
-      // pivoted-QR launch groups by cluster size 1, 2, 4, 8, 16.  The level's
-      // compression matrices are dealt so that about rrqr_fill CTAs per SM
-      // share the work: a task gets the smallest cluster whose CTAs each hold
-      // at most max(rrqr_work, level work / (rrqr_fill * SMs)) elements, and
-      // at most kRrqrMaxCols columns.
-      std::vector<RrqrTask> rt[5];
+      // compression matrices C (m x w) of the level's interfaces, gathered
+      // transposed into scratch by k_rrqr_assemble
+      const size_t nsp = Lv.spars_clusters.size();
       std::vector<RrqrSrc> rs;
-      int gm[5], gk[5], gnl[5], grc[5];
-      for (int g = 0; g < 5; ++g) gm[g] = gk[g] = gnl[g] = grc[g] = 1;
+      std::vector<int> sp_w(nsp), sp_ldw(nsp);
+      std::vector<double*> sp_C(nsp);
       std::vector<std::pair<double, double>> rr_dims;
-      std::vector<int> rr_cs;
-      int* d_stats = verbose >= 2 ? static_cast<int*>(scratch_.alloc(sizeof(int) * 8 * Lv.spars_clusters.size() + 8))
-                                  : nullptr;
-      std::vector<int> sp_w(Lv.spars_clusters.size());
+      std::vector<int> rr_cs(nsp, 0);
+      std::vector<char> plain_qr(nsp, 1);            // interface ran the plain pivoted QR on C
+      std::vector<std::array<double, 3>> sketch_qr;  // (m, ell, steps) of each sketch's pivoted QR
+      int* d_stats = verbose >= 2 ? static_cast<int*>(scratch_.alloc(sizeof(int) * 8 * nsp + 8)) : nullptr;
       double level_work = 0;
-      for (size_t q = 0; q < Lv.spars_clusters.size(); ++q) {
+      for (size_t q = 0; q < nsp; ++q) {
+        const int p = Lv.spars_clusters[q];
+        const int mp = size_[p];
         int w = 0;
         for (int k = Lv.sp_out_begin[q]; k < Lv.sp_out_end[q]; ++k) w += rows_[Lv.sp_out[k]];
         for (int k = Lv.sp_in_begin[q]; k < Lv.sp_in_end[q]; ++k) w += cols_[Lv.sp_in[k]];
         sp_w[q] = w;
-        level_work += (double)size_[Lv.spars_clusters[q]] * w;
-      }
-      const double cta_work = std::max(rrqr_work, level_work / (rrqr_fill * num_sms()));
-      for (size_t q = 0; q < Lv.spars_clusters.size(); ++q) {
-        const int p = Lv.spars_clusters[q];
-        const int mp = size_[p];
-        const int w = sp_w[q];
-        const double work = (double)mp * w;
-        auto local_cols = [&](int c) { return ((w + c - 1) / c + 31) / 32 * 32; };
-        int g = 0;
-        while (g < 4 && (work > cta_work * (1 << g) || local_cols(1 << g) > kRrqrMaxCols) &&
-               (w + NB - 1) / NB >= (2 << g))
-          ++g;
-        if (g == 4 && !rrqr_cluster_fits(16, rrqr_smem(std::max(gm[4], mp), std::max(gk[4], std::min(mp, w)),
-                                                       std::max(gnl[4], local_cols(16)),
-                                                       std::max(grc[4], (mp + 15) / 16))))
-          g = 3;
-        const int cs = 1 << g;
-        if (local_cols(cs) > kRrqrMaxCols) return fail(-12, "interface too wide for the pivoted QR kernel");
-        RrqrTask t{};
-        t.m = mp;
-        t.w = w;
-        t.ldw = (w + 3) / 4 * 4;
-        t.ldq = std::max(1, std::min(mp, w));
-        double* Ct = scratch_.dalloc((size_t)std::max(mp, 1) * std::max(t.ldw, 4));
-        t.C = Ct;
-        t.Q = scratch_.dalloc((size_t)std::max(mp, 1) * t.ldq);
-        t.Qc = scratch_.dalloc((size_t)std::max(mp, 1) * t.ldq);
-        t.F = scratch_.dalloc((size_t)std::max(w, 1) * t.ldq);
-        Qsp_[p] = arena_.dalloc((size_t)std::max(mp, 1) * std::max(mp, 1));
-        Tsp_[p] = arena_.dalloc((size_t)NB * std::max(mp, 1));
-        t.V = Qsp_[p];
-        t.T = Tsp_[p];
-        t.tau = scratch_.dalloc(std::max(mp, 1));
-        t.colat = static_cast<int*>(scratch_.alloc(sizeof(int) * std::max(w, 1)));
-        t.rank = d_rank_ + p;
-        t.stats = d_stats ? d_stats + 8 * q : nullptr;
-        if (!Ct || !t.Q || !t.Qc || !t.F || !t.V || !t.T || !t.tau || !t.colat)
-          return fail(-11, "out of device memory (rrqr)");
+        sp_ldw[q] = (w + 3) / 4 * 4;
+        level_work += (double)mp * w;
+        double* Ct = scratch_.dalloc((size_t)std::max(mp, 1) * std::max(sp_ldw[q], 4));
+        if (!Ct) return fail(-11, "out of device memory (rrqr)");
+        sp_C[q] = Ct;
         int c0 = 0;
         for (int k = Lv.sp_out_begin[q]; k < Lv.sp_out_end[q]; ++k) {
           const int e = Lv.sp_out[k];
-          if (rows_[e] > 0 && mp > 0) rs.push_back({ptr_[e], ld_[e], rows_[e], cols_[e], 1, Ct, t.ldw, c0});
+          if (rows_[e] > 0 && mp > 0) rs.push_back({ptr_[e], ld_[e], rows_[e], cols_[e], 1, Ct, sp_ldw[q], c0});
           c0 += rows_[e];
         }
         for (int k = Lv.sp_in_begin[q]; k < Lv.sp_in_end[q]; ++k) {
           const int e = Lv.sp_in[k];
-          if (cols_[e] > 0 && mp > 0) rs.push_back({ptr_[e], ld_[e], rows_[e], cols_[e], 0, Ct, t.ldw, c0});
+          if (cols_[e] > 0 && mp > 0) rs.push_back({ptr_[e], ld_[e], rows_[e], cols_[e], 0, Ct, sp_ldw[q], c0});
           c0 += cols_[e];
         }
-        rt[g].push_back(t);
-        gm[g] = std::max(gm[g], mp);
-        gk[g] = std::max(gk[g], std::min(mp, w));
-        gnl[g] = std::max(gnl[g], local_cols(cs));
-        grc[g] = std::max(grc[g], (mp + cs - 1) / cs);
+        Qsp_[p] = arena_.dalloc((size_t)std::max(mp, 1) * std::max(mp, 1));
+        Tsp_[p] = arena_.dalloc((size_t)NB * std::max(mp, 1));
+        if (!Qsp_[p] || !Tsp_[p]) return fail(-11, "out of device memory (rrqr)");
         rr_dims.push_back({(double)mp, (double)w});
-        rr_cs.push_back(cs);
       }
+      // pivoted-QR launch groups by cluster size 1, 2, 4, 8, 16
+      struct RrqrGroups {
+        std::vector<RrqrTask> t[5];
+        int m[5] = {1, 1, 1, 1, 1}, k[5] = {1, 1, 1, 1, 1}, nl[5] = {1, 1, 1, 1, 1}, rc[5] = {1, 1, 1, 1, 1};
+      };
+      // A set of compression matrices of total work W is dealt so that about
+      // rrqr_fill CTAs per SM share it: each CTA holds at most
+      // max(floor, W / (rrqr_fill * SMs)) elements of C.
+      auto work_cap = [&](double W, double floor_elems) {
+        return std::max(floor_elems, W / (rrqr_fill * num_sms()));
+      };
+      // a pivoted QR of the row-major m x w matrix C (ld ldw) into V / T of
+      // interface p; rank to *rank; the orthonormal basis (m x min(m,w)) to Qc
+      // when given.  The cluster is the smallest whose CTAs each hold at most
+      // `cap` elements of C and kRrqrMaxCols columns.  Returns the cluster
+      // size, 0 on failure.
+      auto add_rrqr = [&](RrqrGroups& G, const double* C, int mp, int w, int ldw, int p, int* rank, double* Qc,
+                          int* stats, double cap) -> int {
+        const double work = (double)mp * w;
+        auto local_cols = [&](int c) { return ((w + c - 1) / c + 31) / 32 * 32; };
+        int g = 0;
+        while (g < 4 && (work > cap * (1 << g) || local_cols(1 << g) > kRrqrMaxCols) && (w + NB - 1) / NB >= (2 << g))
+          ++g;
+        if (g == 4 && !rrqr_cluster_fits(16, rrqr_smem(std::max(G.m[4], mp), std::max(G.k[4], std::min(mp, w)),
+                                                       std::max(G.nl[4], local_cols(16)),
+                                                       std::max(G.rc[4], (mp + 15) / 16))))
+          g = 3;
+        const int cs = 1 << g;
+        if (local_cols(cs) > kRrqrMaxCols) {
+          fail(-12, "interface too wide for the pivoted QR kernel");
+          return 0;
+        }
+        RrqrTask t{};
+        t.m = mp;
+        t.w = w;
+        t.ldw = ldw;
+        t.ldq = std::max(1, std::min(mp, w));
+        t.C = C;
+        t.Q = scratch_.dalloc((size_t)std::max(mp, 1) * t.ldq);
+        t.Qc = Qc ? Qc : scratch_.dalloc((size_t)std::max(mp, 1) * t.ldq);
+        t.F = scratch_.dalloc((size_t)std::max(w, 1) * t.ldq);
+        t.V = Qsp_[p];
+        t.T = Tsp_[p];
+        t.tau = scratch_.dalloc(std::max(mp, 1));
+        t.colat = static_cast<int*>(scratch_.alloc(sizeof(int) * std::max(w, 1)));
+        t.rank = rank;
+        t.stats = stats;
+        if (!t.Q || !t.Qc || !t.F || !t.tau || !t.colat) {
+          fail(-11, "out of device memory (rrqr)");
+          return 0;
+        }
+        G.t[g].push_back(t);
+        G.m[g] = std::max(G.m[g], mp);
+        G.k[g] = std::max(G.k[g], std::min(mp, w));
+        G.nl[g] = std::max(G.nl[g], local_cols(cs));
+        G.rc[g] = std::max(G.rc[g], (mp + cs - 1) / cs);
+        return cs;
+      };
+      auto up_any = [&](auto& v) { return upload(v.data(), sizeof(v[0]) * v.size()); };
+      auto run_rrqr = [&](RrqrGroups& G, double tol) -> int {
+        for (int g = 0; g < 5; ++g) {
+          if (G.t[g].empty()) continue;
+          auto* d = static_cast<RrqrTask*>(up_any(G.t[g]));
+          if (!d) return fail(-11, "out of device memory (rrqr tasks)");
+          if (ck(launch_rrqr(d, (int)G.t[g].size(), 1 << g, G.m[g], G.k[g], G.nl[g], G.rc[g], tol, pivot_rtol,
+                             stream_),
+                 "rrqr kernel")) {
+            error += " [cluster " + std::to_string(1 << g) + ", tasks " + std::to_string(G.t[g].size()) + ", rows " +
+                     std::to_string(G.m[g]) + ", steps " + std::to_string(G.k[g]) + ", columns/CTA " +
+                     std::to_string(G.nl[g]) + ", shared " +
+                     std::to_string(rrqr_smem(G.m[g], G.k[g], G.nl[g], G.rc[g])) + " B]";
+            return -10;
+          }
+        }
+        return 0;
+      };
       std::vector<EdgeChunk> right, left;
       for (int e : Lv.spars_edges) {
         const Edge& E = st_.edges[e];
@@ -591,18 +632,156 @@ int Tree::factorize() {
         return -10;
       cudaEventRecord(ev[2], stream_);
       if (ck(launch_rrqr_assemble(d_rs, (int)rs.size(), stream_), "rrqr assembly")) return -10;
-      for (int g = 0; g < 5; ++g) {
-        if (rt[g].empty()) continue;
-        auto* d = static_cast<RrqrTask*>(up_vec(rt[g]));
-        if (!d) return fail(-11, "out of device memory (rrqr tasks)");
-        if (ck(launch_rrqr(d, (int)rt[g].size(), 1 << g, gm[g], gk[g], gnl[g], grc[g], st_.tol, pivot_rtol, stream_),
-               "rrqr kernel")) {
-          error += " [cluster " + std::to_string(1 << g) + ", tasks " + std::to_string(rt[g].size()) + ", rows " +
-                   std::to_string(gm[g]) + ", steps " + std::to_string(gk[g]) + ", columns/CTA " +
-                   std::to_string(gnl[g]) + ", shared " + std::to_string(rrqr_smem(gm[g], gk[g], gnl[g], grc[g])) +
-                   " B]";
-          return -10;
+      // interface features: inputs of the rank model, or logged with the
+      // plain ranks as its training pairs
+      std::vector<SketchTask> sk;
+      float* d_feat = nullptr;
+      int* d_ell = nullptr;
+      int* d_fb = nullptr;
+      if (rank_model_ || rank_log_) {
+        sk.resize(nsp);
+        int mmax = 1, wmax = 1;
+        d_feat = static_cast<float*>(scratch_.alloc(sizeof(float) * kRankFeatures * std::max<size_t>(nsp, 1)));
+        double* d_cmax2 = scratch_.dalloc(std::max<size_t>(nsp, 1));
+        d_ell = static_cast<int*>(scratch_.alloc(sizeof(int) * std::max<size_t>(nsp, 1)));
+        d_fb = static_cast<int*>(scratch_.alloc(sizeof(int) * std::max<size_t>(nsp, 1)));
+        if (!d_feat || !d_cmax2 || !d_ell || !d_fb) return fail(-11, "out of device memory (rank features)");
+        for (size_t q = 0; q < nsp; ++q) {
+          const int p = Lv.spars_clusters[q];
+          SketchTask& t = sk[q];
+          t = SketchTask{};
+          t.C = sp_C[q];
+          t.m = size_[p];
+          t.w = sp_w[q];
+          t.ldw = sp_ldw[q];
+          t.cn2 = scratch_.dalloc(std::max(t.w, 1));
+          t.feat = d_feat + q * kRankFeatures;
+          t.cmax2 = d_cmax2 + q;
+          t.ell = d_ell + q;
+          t.rank = d_rank_ + p;
+          t.fallback = d_fb + q;
+          t.seed = 0x5EEDull ^ ((unsigned long long)lvl << 40) ^ ((unsigned long long)p * 0x9E3779B97F4A7C15ull);
+          t.level = lvl;
+          if (!t.cn2) return fail(-11, "out of device memory (rank features)");
+          mmax = std::max(mmax, t.m);
+          wmax = std::max(wmax, t.w);
         }
+        auto* d_sk = static_cast<SketchTask*>(up_any(sk));
+        if (!d_sk) return fail(-11, "out of device memory (rank features)");
+        if (ck(launch_rank_features(d_sk, (int)nsp, st_.tol, mmax, wmax, stream_), "rank features")) return -10;
+        if (rank_model_) {
+          RankModel model{d_model_, d_model_ + kMlpParams, d_model_ + kMlpParams + kRankFeatures, oversample_};
+          if (ck(launch_rank_predict(d_sk, (int)nsp, model, stream_), "rank prediction")) return -10;
+        }
+      }
+      if (!rank_model_) {
+        RrqrGroups G;
+        for (size_t q = 0; q < nsp; ++q) {
+          const int p = Lv.spars_clusters[q];
+          rr_cs[q] = add_rrqr(G, sp_C[q], size_[p], sp_w[q], sp_ldw[q], p, d_rank_ + p, nullptr,
+                              d_stats ? d_stats + 8 * q : nullptr, work_cap(level_work, rrqr_work));
+          if (!rr_cs[q]) return -12;
+        }
+        if (int rc = run_rrqr(G, st_.tol)) return rc;
+      } else {
+        // learned ranks: sketch widths back on the host to plan the sketch
+        // GEMMs; pivoted QR of the sketches, projections, rank choice; the
+        // plain pivoted QR for the interfaces that fall back
+        cudaEvent_t le[6];
+        for (auto& e : le) cudaEventCreate(&e);
+        cudaEventRecord(le[0], stream_);
+        std::vector<int> ell(nsp);
+        if (ck(cudaMemcpyAsync(ell.data(), d_ell, sizeof(int) * nsp, cudaMemcpyDeviceToHost, stream_), "sketch widths") ||
+            ck(cudaStreamSynchronize(stream_), "rank prediction"))
+          return -10;
+        std::vector<GemmTile> sk_tiles, pj_tiles, scan_blocks;
+        RrqrGroups G;
+        size_t mtot = 0;
+        double sketch_work = 0;
+        for (size_t q = 0; q < nsp; ++q) {
+          mtot += (size_t)ell[q] + 1;
+          sketch_work += (double)sk[q].m * std::max(1, ell[q]);
+        }
+        auto* d_M =
+            static_cast<unsigned long long*>(scratch_.alloc(sizeof(unsigned long long) * std::max<size_t>(mtot, 1)));
+        if (!d_M || ck(cudaMemsetAsync(d_M, 0, sizeof(unsigned long long) * mtot, stream_), "residuals"))
+          return fail(-11, "out of device memory (sketch)");
+        size_t moff = 0;
+        for (size_t q = 0; q < nsp; ++q) {
+          const int p = Lv.spars_clusters[q];
+          SketchTask& t = sk[q];
+          const int l = std::max(1, ell[q]);
+          t.ldy = (l + 3) / 4 * 4;
+          t.Y = scratch_.dalloc((size_t)std::max(t.m, 1) * t.ldy);
+          double* Qc = scratch_.dalloc((size_t)std::max(t.m, 1) * l);
+          t.Qc = Qc;
+          t.B = scratch_.dalloc((size_t)l * std::max(t.w, 1));
+          t.M = d_M + moff;
+          moff += (size_t)ell[q] + 1;
+          if (!t.Y || !Qc || !t.B) return fail(-11, "out of device memory (sketch)");
+          if (t.m <= 0 || t.w <= 0) continue;
+          for (int r0 = 0; r0 < t.m; r0 += 64)
+            for (int c0 = 0; c0 < ell[q]; c0 += 64) sk_tiles.push_back({(int)q, r0, c0});
+          for (int l0 = 0; l0 < ell[q]; l0 += 64)
+            for (int j0 = 0; j0 < t.w; j0 += 64) pj_tiles.push_back({(int)q, l0, j0});
+          for (int j0 = 0; j0 < t.w; j0 += 256) scan_blocks.push_back({(int)q, 0, j0});
+          // the sketch's pivoted QR stops at sketch_tol * tol and writes its
+          // rank over the sketch width: later stages use only those vectors
+          if (!add_rrqr(G, t.Y, t.m, ell[q], t.ldy, p, d_ell + q, Qc, nullptr, work_cap(sketch_work, 4096)))
+            return -12;
+        }
+        auto* d_sk = static_cast<SketchTask*>(up_any(sk));
+        auto* d_skt = static_cast<GemmTile*>(up_any(sk_tiles));
+        auto* d_pjt = static_cast<GemmTile*>(up_any(pj_tiles));
+        auto* d_scb = static_cast<GemmTile*>(up_any(scan_blocks));
+        if (!d_sk || !d_skt || !d_pjt || !d_scb) return fail(-11, "out of device memory (sketch)");
+        cudaEventRecord(le[1], stream_);
+        if (ck(launch_sketch(d_sk, d_skt, (int)sk_tiles.size(), stream_), "sketch")) return -10;
+        cudaEventRecord(le[2], stream_);
+        if (int rc = run_rrqr(G, sketch_tol * st_.tol)) return rc;
+        cudaEventRecord(le[3], stream_);
+        if (ck(launch_project(d_sk, d_pjt, (int)pj_tiles.size(), stream_), "projection") ||
+            ck(launch_residual_scan(d_sk, d_scb, (int)scan_blocks.size(), stream_), "residual scan") ||
+            ck(launch_rank_select(d_sk, (int)nsp, st_.tol, stream_), "rank selection"))
+          return -10;
+        cudaEventRecord(le[4], stream_);
+        std::vector<int> fb(nsp);
+        if (ck(cudaMemcpyAsync(fb.data(), d_fb, sizeof(int) * nsp, cudaMemcpyDeviceToHost, stream_), "fallback flags") ||
+            ck(cudaStreamSynchronize(stream_), "rank selection"))
+          return -10;
+        RrqrGroups Fb;
+        double fb_work = 0;
+        for (size_t q = 0; q < nsp; ++q)
+          if (fb[q]) fb_work += (double)sk[q].m * sk[q].w;
+        for (size_t q = 0; q < nsp; ++q) {
+          const int p = Lv.spars_clusters[q];
+          const SketchTask& t = sk[q];
+          flops_ += 4.0 * t.m * (double)t.w * ell[q];  // sketch + projection GEMMs
+          learned_ell_ += ell[q];
+          if (t.m <= 0 || t.w <= 0) continue;
+          sketch_qr.push_back({(double)t.m, (double)ell[q], (double)ell[q]});
+          plain_qr[q] = fb[q] ? 1 : 0;
+          if (fb[q]) {
+            ++learned_fallbacks_;
+            rr_cs[q] = add_rrqr(Fb, sp_C[q], t.m, t.w, t.ldw, p, d_rank_ + p, nullptr, nullptr,
+                                work_cap(fb_work, 16384));
+            if (!rr_cs[q]) return -12;
+          } else {
+            ++learned_accepted_;
+          }
+        }
+        if (int rc = run_rrqr(Fb, st_.tol)) return rc;
+        cudaEventRecord(le[5], stream_);
+        if (verbose >= 2) {
+          cudaEventSynchronize(le[5]);
+          float ms[5];
+          for (int k = 0; k < 5; ++k) cudaEventElapsedTime(&ms[k], le[k], le[k + 1]);
+          int nfb = 0;
+          for (int f : fb) nfb += f;
+          printf("learned level %d: plan %.2f sketch %.2f qr %.2f project %.2f fallback(%d) %.2f ms\n", lvl, ms[0], ms[1],
+                 ms[2], ms[3], nfb, ms[4]);
+        }
+        for (auto& e : le) cudaEventDestroy(e);
       }
       cudaEventRecord(fe[2], stream_);
       if (ck(launch_edge(2, d_right, (int)right.size(), stream_), "right compression") ||
@@ -614,19 +793,35 @@ int Tree::factorize() {
           ck(cudaStreamSynchronize(stream_), "sparsification"))
         return -10;
       for (int p : Lv.spars_clusters) size_[p] = host_rank[p];
+      if (rank_log_ && nsp) {
+        std::vector<float> f(kRankFeatures * nsp);
+        if (ck(cudaMemcpy(f.data(), d_feat, sizeof(float) * f.size(), cudaMemcpyDeviceToHost), "rank features"))
+          return -10;
+        log_feat_.insert(log_feat_.end(), f.begin(), f.end());
+        for (size_t q = 0; q < nsp; ++q) {
+          const int p = Lv.spars_clusters[q];
+          log_rank_.push_back(host_rank[p]);
+          log_kmin_.push_back(std::min((int)rr_dims[q].first, (int)rr_dims[q].second));
+          log_level_.push_back(lvl);
+        }
+      }
       std::vector<int> stats;
       if (d_stats) {
         stats.resize(8 * Lv.spars_clusters.size());
         if (ck(cudaMemcpy(stats.data(), d_stats, sizeof(int) * stats.size(), cudaMemcpyDeviceToHost), "rrqr stats"))
           return -10;
       }
+      // nominal flops (LAPACK Working Note 41 geqp3 count) and the bytes of C
+      // the pivoted QR moves: the transposed gather (read + write), one pass
+      // for the norms, one per pivot step over the active columns
+      auto account = [&](double m, double w, double steps, double r) {
+        flops_ += 4.0 * m * w * r - 2.0 * r * r * (m + w) + 4.0 * r * r * r / 3.0 + m * r * r;
+        rrqr_bytes_ += 8.0 * m * (3.0 * w + steps * w - steps * (steps + 1.0) / 2.0);
+      };
+      for (const auto& e : sketch_qr) account(e[0], e[1], e[2], e[2]);
       for (size_t q = 0; q < Lv.spars_clusters.size(); ++q) {
         const double m = rr_dims[q].first, w = rr_dims[q].second, r = size_[Lv.spars_clusters[q]];
-        flops_ += 4.0 * m * w * r - 2.0 * r * r * (m + w) + 4.0 * r * r * r / 3.0 + m * r * r;
-        // C gathered once (read + write), read once for the norms and once per
-        // step over the active columns
-        const double steps = std::min(r + 1.0, std::min(m, w));
-        rrqr_bytes_ += 8.0 * m * (3.0 * w + steps * w - steps * (steps + 1.0) / 2.0);
+        if (plain_qr[q]) account(m, w, std::min(r + 1.0, std::min(m, w)), r);
         if (verbose >= 2)
           printf("rrqr level %d m %d w %d rank %d cluster %d recomputed %d kcycles %d %d %d %d %d %d\n", lvl, (int)m,
                  (int)w, (int)r, rr_cs[q], stats[8 * q], stats[8 * q + 2], stats[8 * q + 3], stats[8 * q + 4],
@@ -1146,6 +1341,28 @@ int Tree::gmres_device_fixed(double* b, int maxit, double gtol, int* iters, doub
   }
   t_gmres = wall() - t0;
   return rc;
+}
+
+int Tree::set_rank_model(const float* params, const float* mean, const float* stdev, int oversample) {
+  learned_accepted_ = learned_fallbacks_ = learned_ell_ = 0;
+  if (!params) {
+    rank_model_ = false;
+    return 0;
+  }
+  if (!mean || !stdev || oversample < 0) return fail(-1, "rank model: mean, std and oversample >= 0 required");
+  for (int f = 0; f < kRankFeatures; ++f)
+    if (!(stdev[f] > 0)) return fail(-1, "rank model: feature std must be positive");
+  const size_t n = (size_t)kMlpParams + 2 * kRankFeatures;
+  if (!d_model_ && check_cuda(cudaMalloc(&d_model_, sizeof(float) * n), "malloc rank model")) return -11;
+  std::vector<float> h(n);
+  std::copy(params, params + kMlpParams, h.begin());
+  std::copy(mean, mean + kRankFeatures, h.begin() + kMlpParams);
+  std::copy(stdev, stdev + kRankFeatures, h.begin() + kMlpParams + kRankFeatures);
+  if (check_cuda(cudaMemcpy(d_model_, h.data(), sizeof(float) * n, cudaMemcpyHostToDevice), "upload rank model"))
+    return -10;
+  rank_model_ = true;
+  oversample_ = oversample;
+  return 0;
 }
 
 int Tree::ensure_krylov(size_t doubles) {

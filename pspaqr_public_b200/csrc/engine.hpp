@@ -67,6 +67,9 @@ class Tree {
   double rrqr_work = 65536;
   // ... and a level's compression work is spread over about rrqr_fill CTAs per SM
   double rrqr_fill = 2;
+  // learned ranks: the sketch's pivoted QR stops at sketch_tol * tol (the
+  // kept rank is then chosen on C itself)
+  double sketch_tol = 0.1;
 
   int set_coords(int dim, int n, const double* X);
   int set_coords_tensor(int n, int d);
@@ -104,6 +107,26 @@ class Tree {
   // bytes of the compression matrices the pivoted QR moves (the transposed
   // gather, one pass for the norms, one per pivot step over the active columns)
   double rrqr_bytes() const { return rrqr_bytes_; }
+
+  // learned ranks: params (kMlpParams), feature mean / std (kRankFeatures
+  // each); null params switch the plain pivoted QR back on
+  int set_rank_model(const float* params, const float* mean, const float* stdev, int oversample);
+  void set_rank_log(bool on) { rank_log_ = on; }
+  void clear_rank_log() {
+    log_feat_.clear();
+    log_rank_.clear();
+    log_kmin_.clear();
+    log_level_.clear();
+  }
+  const std::vector<float>& log_features() const { return log_feat_; }
+  const std::vector<int>& log_ranks() const { return log_rank_; }
+  const std::vector<int>& log_kmin() const { return log_kmin_; }
+  const std::vector<int>& log_levels() const { return log_level_; }
+  void learned_counts(long long* accepted, long long* fallbacks, long long* ell) const {
+    *accepted = learned_accepted_;
+    *fallbacks = learned_fallbacks_;
+    *ell = learned_ell_;
+  }
   int device_status();
 
  private:
@@ -158,6 +181,16 @@ class Tree {
   std::vector<LevelTiming> lt_;
   double flops_ = 0;
   double rrqr_bytes_ = 0;
+
+  // learned ranks (learned.hpp): model on the device (params | mean | std),
+  // logged training pairs, counters since the last set_rank_model
+  float* d_model_ = nullptr;
+  bool rank_model_ = false;
+  int oversample_ = 10;
+  bool rank_log_ = false;
+  std::vector<float> log_feat_;
+  std::vector<int> log_rank_, log_kmin_, log_level_;
+  long long learned_accepted_ = 0, learned_fallbacks_ = 0, learned_ell_ = 0;
 };
 
 }  // namespace spq

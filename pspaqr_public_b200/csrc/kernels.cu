@@ -966,6 +966,7 @@ inline cudaError_t begin(const char* name) {
 }  // namespace
 
 const char* last_launch_name() { return g_last_launch; }
+void set_last_launch(const char* name) { g_last_launch = name; }
 
 long long kernel_launches() { return g_launches.load(); }
 void add_kernel_launches(long long n) { g_launches.fetch_add(n); }

@@ -13,6 +13,8 @@ namespace spq {
 long long kernel_launches();
 // Name of the launcher called last on this thread (error reports).
 const char* last_launch_name();
+// name reported with the next launch error (launchers outside kernels.cu)
+void set_last_launch(const char* name);
 void add_kernel_launches(long long n);
 
 cudaError_t launch_scatter(int nnz, const double* val, double* const* dst, cudaStream_t st);

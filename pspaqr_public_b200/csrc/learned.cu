@@ -1,0 +1,572 @@
+// learned.cu -- kernels of the learned-rank sparsification and of the rank
+// MLP's training (see learned.hpp for the method).
+//
+// Random test matrices Omega are Rademacher (+-1) from a counter-based hash
+// (splitmix64 finaliser, Steele, Lea & Flood 2014) of (seed, row, column
+// block): one 64-bit hash gives the signs of 64 consecutive columns, so the
+// sketch never stores Omega.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdint>
+
+#include "kernels.hpp"
+#include "learned.hpp"
+
+namespace spq {
+namespace {
+
+constexpr int kT = 256;  // threads of the per-task and GEMM kernels
+constexpr int kTile = 64;
+constexpr int kKStep = 32;
+
+__device__ __forceinline__ unsigned long long mix64(unsigned long long z) {
+  z += 0x9E3779B97F4A7C15ull;
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  return z ^ (z >> 31);
+}
+// signs of Omega(j, 64 b .. 64 b + 63), bit t set = +1
+__device__ __forceinline__ unsigned long long omega_bits(unsigned long long seed, int j, int b) {
+  return mix64(seed ^ mix64(((unsigned long long)j << 16) | (unsigned long long)b));
+}
+
+__device__ __forceinline__ double warp_max(double v) {
+  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+__device__ __forceinline__ double warp_sumd(double v) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// Deterministic block sum / max over kT threads through `red` (kT / 32 doubles).
+__device__ double block_sum(double v, double* red) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  v = warp_sumd(v);
+  if (lane == 0) red[warp] = v;
+  __syncthreads();
+  double s = 0.0;
+  for (int q = 0; q < kT / 32; ++q) s += red[q];
+  __syncthreads();
+  return s;
+}
+__device__ double block_max(double v, double* red) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  v = warp_max(v);
+  if (lane == 0) red[warp] = v;
+  __syncthreads();
+  double s = red[0];
+  for (int q = 1; q < kT / 32; ++q) s = fmax(s, red[q]);
+  __syncthreads();
+  return s;
+}
+
+// ---------------------------------------------------------------- features
+// One CTA per interface.  Dynamic shared memory: 4 * mmax doubles (the
+// 4-column sketch) + wmax bytes (its signs).
+__global__ void __launch_bounds__(kT) k_rank_features(const SketchTask* __restrict__ tasks, double tol) {
+  extern __shared__ double sm[];
+  __shared__ double red[kT / 32];
+  const SketchTask t = tasks[blockIdx.x];
+  const int m = t.m, w = t.w;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  double* y4 = sm;
+  unsigned char* sg = reinterpret_cast<unsigned char*>(sm + 4 * (size_t)(m > 0 ? m : 1));
+  // squared column norms
+  double cmax = 0.0, fro = 0.0;
+  for (int j = threadIdx.x; j < w; j += kT) {
+    double s = 0.0;
+#pragma unroll 4
+    for (int r = 0; r < m; ++r) {
+      const double v = __ldg(t.C + (size_t)r * t.ldw + j);
+      s += v * v;
+    }
+    t.cn2[j] = s;
+    cmax = fmax(cmax, s);
+    fro += s;
+    sg[j] = (unsigned char)(omega_bits(t.seed ^ 0x5DEECE66Dull, j, 0) & 15u);
+  }
+  cmax = block_max(cmax, red);
+  fro = block_sum(fro, red);
+  // counts of columns above fractions of the largest norm
+  const double thr[3] = {tol * tol * cmax, 0.01 * cmax, 0.25 * cmax};
+  int cnt[3] = {0, 0, 0};
+  for (int j = threadIdx.x; j < w; j += kT) {
+    const double c = t.cn2[j];
+#pragma unroll
+    for (int q = 0; q < 3; ++q) cnt[q] += c >= thr[q] ? 1 : 0;
+  }
+  double cq[3];
+#pragma unroll
+  for (int q = 0; q < 3; ++q) cq[q] = block_sum((double)cnt[q], red);
+  // 4-column Rademacher sketch, one warp per row
+  for (int r = warp; r < m; r += kT / 32) {
+    double a0 = 0, a1 = 0, a2 = 0, a3 = 0;
+    const double* row = t.C + (size_t)r * t.ldw;
+    for (int j = lane; j < w; j += 32) {
+      const double v = __ldg(row + j);
+      const unsigned s = sg[j];
+      a0 += (s & 1u) ? v : -v;
+      a1 += (s & 2u) ? v : -v;
+      a2 += (s & 4u) ? v : -v;
+      a3 += (s & 8u) ? v : -v;
+    }
+    a0 = warp_sumd(a0);
+    a1 = warp_sumd(a1);
+    a2 = warp_sumd(a2);
+    a3 = warp_sumd(a3);
+    if (lane == 0) {
+      y4[r] = a0;
+      y4[m + r] = a1;
+      y4[2 * m + r] = a2;
+      y4[3 * m + r] = a3;
+    }
+  }
+  __syncthreads();
+  // diagonal of R in a QR of the sketch (modified Gram-Schmidt, warp 0)
+  double d[4] = {0, 0, 0, 0};
+  if (warp == 0) {
+    for (int c = 0; c < 4; ++c) {
+      double* yc = y4 + (size_t)c * m;
+      for (int p = 0; p < c; ++p) {
+        const double* yp = y4 + (size_t)p * m;
+        double s = 0.0;
+        for (int r = lane; r < m; r += 32) s += yp[r] * yc[r];
+        s = warp_sumd(s);
+        for (int r = lane; r < m; r += 32) yc[r] -= s * yp[r];
+        __syncwarp();
+      }
+      double s = 0.0;
+      for (int r = lane; r < m; r += 32) s += yc[r] * yc[r];
+      s = sqrt(warp_sumd(s));
+      d[c] = s;
+      const double inv = s > 0.0 ? 1.0 / s : 0.0;
+      for (int r = lane; r < m; r += 32) yc[r] *= inv;
+      __syncwarp();
+    }
+  }
+  if (threadIdx.x == 0) {
+    const int kmin = m < w ? m : w;
+    const double km = kmin > 0 ? (double)kmin : 1.0;
+    float* f = t.feat;
+    f[0] = (float)log2((double)m + 1.0);
+    f[1] = (float)log2((double)w + 1.0);
+    f[2] = (float)log10(tol);
+    f[3] = (float)fmin(1.0, cq[0] / km);
+    f[4] = (float)fmin(1.0, cq[1] / km);
+    f[5] = (float)fmin(1.0, cq[2] / km);
+    f[6] = (float)fmin(10.0, cmax > 0.0 ? fro / (cmax * km) : 0.0);
+    for (int c = 1; c < 4; ++c) f[6 + c] = (float)(d[0] > 0.0 ? log10(fmax(d[c] / d[0], 1e-12)) : -12.0);
+    f[10] = (float)t.level;
+    *t.cmax2 = cmax;
+  }
+}
+
+// ---------------------------------------------------------------- MLP
+__device__ __forceinline__ float sigmoidf(float z) { return 1.0f / (1.0f + expf(-z)); }
+
+constexpr int kOffB1 = kMlpHidden * kRankFeatures;
+constexpr int kOffW2 = kOffB1 + kMlpHidden;
+constexpr int kOffB2 = kOffW2 + kMlpHidden * kMlpHidden;
+constexpr int kOffW3 = kOffB2 + kMlpHidden;
+constexpr int kOffB3 = kOffW3 + kMlpHidden;
+
+// forward pass of one standardised feature vector
+__device__ float mlp_forward(const float* __restrict__ P, const float* x) {
+  float h1[kMlpHidden];
+#pragma unroll 4
+  for (int i = 0; i < kMlpHidden; ++i) {
+    float s = P[kOffB1 + i];
+#pragma unroll
+    for (int f = 0; f < kRankFeatures; ++f) s += P[i * kRankFeatures + f] * x[f];
+    h1[i] = s > 0.0f ? s : 0.0f;
+  }
+  float z = P[kOffB3];
+  for (int i = 0; i < kMlpHidden; ++i) {
+    float s = P[kOffB2 + i];
+#pragma unroll 8
+    for (int j = 0; j < kMlpHidden; ++j) s += P[kOffW2 + i * kMlpHidden + j] * h1[j];
+    z += P[kOffW3 + i] * (s > 0.0f ? s : 0.0f);
+  }
+  return sigmoidf(z);
+}
+
+__global__ void k_rank_predict(const SketchTask* __restrict__ tasks, int ntasks, RankModel model) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= ntasks) return;
+  const SketchTask t = tasks[q];
+  const int kmin = t.m < t.w ? t.m : t.w;
+  float x[kRankFeatures];
+  for (int f = 0; f < kRankFeatures; ++f) x[f] = (t.feat[f] - model.mean[f]) / model.stdev[f];
+  const float p = mlp_forward(model.params, x);
+  int ell = (int)ceilf(p * (float)kmin) + model.oversample;
+  ell = ell < 1 ? 1 : ell;
+  *t.ell = kmin < ell ? kmin : ell;
+}
+
+__global__ void k_mlp_predict(const float* __restrict__ P, const float* __restrict__ X, int n, float* out) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= n) return;
+  float x[kRankFeatures];
+  for (int f = 0; f < kRankFeatures; ++f) x[f] = X[(size_t)s * kRankFeatures + f];
+  out[s] = mlp_forward(P, x);
+}
+
+// Loss and gradient partials of 64 samples per block (128 threads):
+// loss = sum_s (sigmoid(z_s) - y_s)^2 / n.  Activations stay in shared
+// memory; every parameter's partial is a sum over the block's samples in
+// sample order, written to part[block * (kMlpParams + 1) + p] (loss last).
+constexpr int kMlpBatch = 64;
+constexpr int kMlpThreads = 128;
+constexpr size_t kMlpSmem =
+    sizeof(float) * ((size_t)kMlpBatch * kRankFeatures + 3 * (size_t)kMlpBatch * kMlpHidden + kMlpBatch +
+                     (size_t)kMlpHidden * kMlpHidden);
+
+__global__ void __launch_bounds__(kMlpThreads) k_mlp_grad(const float* __restrict__ P, const float* __restrict__ X,
+                                                          const float* __restrict__ y, int n, float* part) {
+  extern __shared__ float fs[];
+  float* Xs = fs;                                  // 64 x F
+  float* H1 = Xs + kMlpBatch * kRankFeatures;      // 64 x 64
+  float* H2 = H1 + kMlpBatch * kMlpHidden;         // 64 x 64, then dL/dpre2
+  float* D1 = H2 + kMlpBatch * kMlpHidden;         // 64 x 64: dL/dpre1
+  float* dz = D1 + kMlpBatch * kMlpHidden;         // 64
+  float* W2 = dz + kMlpBatch;                      // 64 x 64
+  const int s0 = blockIdx.x * kMlpBatch;
+  for (int i = threadIdx.x; i < kMlpHidden * kMlpHidden; i += kMlpThreads) W2[i] = P[kOffW2 + i];
+  for (int i = threadIdx.x; i < kMlpBatch * kRankFeatures; i += kMlpThreads) {
+    const int s = s0 + i / kRankFeatures;
+    Xs[i] = s < n ? X[(size_t)s0 * kRankFeatures + i] : 0.0f;
+  }
+  __syncthreads();
+  for (int idx = threadIdx.x; idx < kMlpBatch * kMlpHidden; idx += kMlpThreads) {
+    const int s = idx / kMlpHidden, i = idx % kMlpHidden;
+    float a = P[kOffB1 + i];
+    for (int f = 0; f < kRankFeatures; ++f) a += P[i * kRankFeatures + f] * Xs[s * kRankFeatures + f];
+    H1[idx] = a > 0.0f ? a : 0.0f;
+  }
+  __syncthreads();
+  for (int idx = threadIdx.x; idx < kMlpBatch * kMlpHidden; idx += kMlpThreads) {
+    const int s = idx / kMlpHidden, i = idx % kMlpHidden;
+    float a = P[kOffB2 + i];
+    for (int j = 0; j < kMlpHidden; ++j) a += W2[i * kMlpHidden + j] * H1[s * kMlpHidden + j];
+    H2[idx] = a > 0.0f ? a : 0.0f;
+  }
+  __syncthreads();
+  float* out = part + (size_t)blockIdx.x * (kMlpParams + 1);
+  if (threadIdx.x < kMlpBatch) {
+    const int s = threadIdx.x;
+    float z = P[kOffB3];
+    for (int i = 0; i < kMlpHidden; ++i) z += P[kOffW3 + i] * H2[s * kMlpHidden + i];
+    const float p = sigmoidf(z);
+    const bool valid = s0 + s < n;
+    const float diff = valid ? p - y[s0 + s] : 0.0f;
+    dz[s] = valid ? 2.0f * diff * p * (1.0f - p) / (float)n : 0.0f;
+    D1[s] = diff * diff;  // per-sample loss; D1 is rewritten by the backward pass
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    float l = 0.0f;
+    for (int s = 0; s < kMlpBatch; ++s) l += D1[s];
+    out[kMlpParams] = l / (float)n;
+  }
+  // layer 3
+  for (int i = threadIdx.x; i <= kMlpHidden; i += kMlpThreads) {
+    float g = 0.0f;
+    for (int s = 0; s < kMlpBatch; ++s) g += dz[s] * (i < kMlpHidden ? H2[s * kMlpHidden + i] : 1.0f);
+    out[i < kMlpHidden ? kOffW3 + i : kOffB3] = g;
+  }
+  __syncthreads();
+  // dL/dpre2 in place of H2
+  for (int idx = threadIdx.x; idx < kMlpBatch * kMlpHidden; idx += kMlpThreads) {
+    const int s = idx / kMlpHidden, i = idx % kMlpHidden;
+    H2[idx] = H2[idx] > 0.0f ? dz[s] * P[kOffW3 + i] : 0.0f;
+  }
+  __syncthreads();
+  // dL/dpre1
+  for (int idx = threadIdx.x; idx < kMlpBatch * kMlpHidden; idx += kMlpThreads) {
+    const int s = idx / kMlpHidden, j = idx % kMlpHidden;
+    float a = 0.0f;
+    if (H1[idx] > 0.0f)
+      for (int i = 0; i < kMlpHidden; ++i) a += W2[i * kMlpHidden + j] * H2[s * kMlpHidden + i];
+    D1[idx] = a;
+  }
+  __syncthreads();
+  // layer 2 and layer 1
+  for (int p = threadIdx.x; p < kMlpHidden * kMlpHidden + kMlpHidden; p += kMlpThreads) {
+    float g = 0.0f;
+    if (p < kMlpHidden * kMlpHidden) {
+      const int i = p / kMlpHidden, j = p % kMlpHidden;
+      for (int s = 0; s < kMlpBatch; ++s) g += H2[s * kMlpHidden + i] * H1[s * kMlpHidden + j];
+      out[kOffW2 + p] = g;
+    } else {
+      const int i = p - kMlpHidden * kMlpHidden;
+      for (int s = 0; s < kMlpBatch; ++s) g += H2[s * kMlpHidden + i];
+      out[kOffB2 + i] = g;
+    }
+  }
+  for (int p = threadIdx.x; p < kMlpHidden * kRankFeatures + kMlpHidden; p += kMlpThreads) {
+    float g = 0.0f;
+    if (p < kMlpHidden * kRankFeatures) {
+      const int i = p / kRankFeatures, f = p % kRankFeatures;
+      for (int s = 0; s < kMlpBatch; ++s) g += D1[s * kMlpHidden + i] * Xs[s * kRankFeatures + f];
+      out[p] = g;
+    } else {
+      const int i = p - kMlpHidden * kRankFeatures;
+      for (int s = 0; s < kMlpBatch; ++s) g += D1[s * kMlpHidden + i];
+      out[kOffB1 + i] = g;
+    }
+  }
+}
+
+// grad[p] = sum over blocks (in block order) of the partials; loss likewise
+__global__ void k_mlp_reduce(const float* __restrict__ part, int nblocks, float* grad, float* loss) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p > kMlpParams) return;
+  float s = 0.0f;
+  for (int b = 0; b < nblocks; ++b) s += part[(size_t)b * (kMlpParams + 1) + p];
+  if (p < kMlpParams) grad[p] = s;
+  else *loss = s;
+}
+
+__global__ void k_mlp_adam(float* P, const float* __restrict__ g, float* m1, float* m2, float lr, float c1, float c2) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= kMlpParams) return;
+  const float b1 = 0.9f, b2 = 0.999f;
+  const float a = b1 * m1[p] + (1.0f - b1) * g[p];
+  const float v = b2 * m2[p] + (1.0f - b2) * g[p] * g[p];
+  m1[p] = a;
+  m2[p] = v;
+  P[p] -= lr * (a / c1) / (sqrtf(v / c2) + 1e-8f);
+}
+
+// ---------------------------------------------------------------- sketch / projection GEMMs
+// 64 x 64 output tile per CTA, k-steps of 32, each thread a 4 x 4 block of
+// outputs at rows ty + 16 a, columns tx + 16 b.
+__global__ void __launch_bounds__(kT) k_sketch(const SketchTask* __restrict__ tasks,
+                                               const GemmTile* __restrict__ tiles) {
+  __shared__ double As[kKStep][kTile + 1];  // C(r0 + rr, j0 + jj) at As[jj][rr]
+  __shared__ double Bs[kKStep][kTile + 1];  // Omega(j0 + jj, c0 + cc) at Bs[jj][cc]
+  const GemmTile g = tiles[blockIdx.x];
+  const SketchTask t = tasks[g.task];
+  const int ell = *t.ell;
+  if (g.c0 >= ell) return;
+  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+  double acc[4][4] = {};
+  for (int j0 = 0; j0 < t.w; j0 += kKStep) {
+    for (int e = threadIdx.x; e < kTile * kKStep; e += kT) {
+      const int rr = e / kKStep, jj = e % kKStep;
+      const int r = g.r0 + rr, j = j0 + jj;
+      As[jj][rr] = (r < t.m && j < t.w) ? __ldg(t.C + (size_t)r * t.ldw + j) : 0.0;
+    }
+    for (int e = threadIdx.x; e < kKStep * 8; e += kT) {
+      const int jj = e >> 3, part = e & 7;
+      const unsigned long long bits = omega_bits(t.seed, j0 + jj, g.c0 >> 6) >> (8 * part);
+#pragma unroll
+      for (int q = 0; q < 8; ++q) Bs[jj][8 * part + q] = ((bits >> q) & 1ull) ? 1.0 : -1.0;
+    }
+    __syncthreads();
+#pragma unroll 8
+    for (int jj = 0; jj < kKStep; ++jj) {
+      double a[4], b[4];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        a[q] = As[jj][ty + 16 * q];
+        b[q] = Bs[jj][tx + 16 * q];
+      }
+#pragma unroll
+      for (int p = 0; p < 4; ++p)
+#pragma unroll
+        for (int q = 0; q < 4; ++q) acc[p][q] += a[p] * b[q];
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int p = 0; p < 4; ++p) {
+    const int r = g.r0 + ty + 16 * p;
+    if (r >= t.m) continue;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int c = g.c0 + tx + 16 * q;
+      if (c < ell) t.Y[(size_t)r * t.ldy + c] = acc[p][q];
+    }
+  }
+}
+
+// B(l, j) = sum_r Q(r, l) C(r, j); tile rows l (basis vectors), columns j
+__global__ void __launch_bounds__(kT) k_project(const SketchTask* __restrict__ tasks,
+                                                const GemmTile* __restrict__ tiles) {
+  __shared__ double As[kKStep][kTile + 1];  // Q(r0 + rr, l0 + ll) at As[rr][ll]
+  __shared__ double Bs[kKStep][kTile + 1];  // C(r0 + rr, j0 + jj) at Bs[rr][jj]
+  const GemmTile g = tiles[blockIdx.x];
+  const SketchTask t = tasks[g.task];
+  const int ell = *t.ell;
+  if (g.r0 >= ell) return;
+  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+  double acc[4][4] = {};
+  for (int k0 = 0; k0 < t.m; k0 += kKStep) {
+    for (int e = threadIdx.x; e < kTile * kKStep; e += kT) {
+      const int ll = e / kKStep, rr = e % kKStep;
+      const int l = g.r0 + ll, r = k0 + rr;
+      As[rr][ll] = (l < ell && r < t.m) ? __ldg(t.Qc + (size_t)l * t.m + r) : 0.0;
+    }
+    for (int e = threadIdx.x; e < kTile * kKStep; e += kT) {
+      const int rr = e / kTile, jj = e % kTile;
+      const int r = k0 + rr, j = g.c0 + jj;
+      Bs[rr][jj] = (r < t.m && j < t.w) ? __ldg(t.C + (size_t)r * t.ldw + j) : 0.0;
+    }
+    __syncthreads();
+#pragma unroll 8
+    for (int rr = 0; rr < kKStep; ++rr) {
+      double a[4], b[4];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        a[q] = As[rr][ty + 16 * q];
+        b[q] = Bs[rr][tx + 16 * q];
+      }
+#pragma unroll
+      for (int p = 0; p < 4; ++p)
+#pragma unroll
+        for (int q = 0; q < 4; ++q) acc[p][q] += a[p] * b[q];
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int p = 0; p < 4; ++p) {
+    const int l = g.r0 + ty + 16 * p;
+    if (l >= ell) continue;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int j = g.c0 + tx + 16 * q;
+      if (j < t.w) t.B[(size_t)l * t.w + j] = acc[p][q];
+    }
+  }
+}
+
+// Residual scan over a block of 256 columns: res_j(k) = ||c_j||^2 -
+// sum_{l<k} B(l,j)^2, and M[k] = max_j res_j(k) by atomicMax on the bit
+// patterns of non-negative doubles (their order equals the values' order).
+__global__ void __launch_bounds__(kT) k_residual_scan(const SketchTask* __restrict__ tasks,
+                                                      const GemmTile* __restrict__ blocks) {
+  const GemmTile g = blocks[blockIdx.x];
+  const SketchTask t = tasks[g.task];
+  const int ell = *t.ell;
+  const int j = g.c0 + threadIdx.x;
+  const bool ok = j < t.w;
+  double res = ok ? t.cn2[j] : 0.0;
+  const int lane = threadIdx.x & 31;
+  for (int l = 0; l < ell; ++l) {
+    if (ok) {
+      const double b = t.B[(size_t)l * t.w + j];
+      res -= b * b;
+    }
+    const double mx = warp_max(ok ? fmax(res, 0.0) : 0.0);
+    if (lane == 0) atomicMax(t.M + l + 1, (unsigned long long)__double_as_longlong(mx));
+  }
+}
+
+__global__ void k_rank_select(const SketchTask* __restrict__ tasks, int ntasks, double tol) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= ntasks) return;
+  const SketchTask t = tasks[q];
+  const int ell = *t.ell;
+  const double thr = tol * tol * *t.cmax2;
+  int rank = 0;
+  for (int k = 1; k <= ell; ++k)
+    if (__longlong_as_double((long long)t.M[k]) < thr) {
+      rank = k;
+      break;
+    }
+  *t.fallback = rank == 0 ? 1 : 0;
+  if (rank > 0) *t.rank = rank;
+}
+
+cudaError_t done_launch(const char* name) {
+  set_last_launch(name);
+  add_kernel_launches(1);
+  return cudaGetLastError();
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------- launchers
+size_t rank_features_smem(int mmax, int wmax) {
+  return sizeof(double) * (4 * (size_t)std::max(mmax, 1) + ((size_t)std::max(wmax, 1) + 7) / 8);
+}
+
+cudaError_t launch_rank_features(const SketchTask* t, int ntasks, double tol, int mmax, int wmax, cudaStream_t st) {
+  if (cudaError_t e = cudaGetLastError()) return e;
+  if (ntasks <= 0) return cudaSuccess;
+  const size_t smem = rank_features_smem(mmax, wmax);
+  if (smem > 227 * 1024) return cudaErrorInvalidValue;
+  cudaError_t e = cudaFuncSetAttribute(k_rank_features, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e) return e;
+  k_rank_features<<<ntasks, kT, smem, st>>>(t, tol);
+  return done_launch("launch_rank_features");
+}
+
+cudaError_t launch_rank_predict(const SketchTask* t, int ntasks, RankModel model, cudaStream_t st) {
+  if (cudaError_t e = cudaGetLastError()) return e;
+  if (ntasks <= 0) return cudaSuccess;
+  k_rank_predict<<<(ntasks + 127) / 128, 128, 0, st>>>(t, ntasks, model);
+  return done_launch("launch_rank_predict");
+}
+
+cudaError_t launch_sketch(const SketchTask* t, const GemmTile* tiles, int ntiles, cudaStream_t st) {
+  if (cudaError_t e = cudaGetLastError()) return e;
+  if (ntiles <= 0) return cudaSuccess;
+  k_sketch<<<ntiles, kT, 0, st>>>(t, tiles);
+  return done_launch("launch_sketch");
+}
+
+cudaError_t launch_project(const SketchTask* t, const GemmTile* tiles, int ntiles, cudaStream_t st) {
+  if (cudaError_t e = cudaGetLastError()) return e;
+  if (ntiles <= 0) return cudaSuccess;
+  k_project<<<ntiles, kT, 0, st>>>(t, tiles);
+  return done_launch("launch_project");
+}
+
+cudaError_t launch_residual_scan(const SketchTask* t, const GemmTile* blocks, int nblocks, cudaStream_t st) {
+  if (cudaError_t e = cudaGetLastError()) return e;
+  if (nblocks <= 0) return cudaSuccess;
+  k_residual_scan<<<nblocks, kT, 0, st>>>(t, blocks);
+  return done_launch("launch_residual_scan");
+}
+
+cudaError_t launch_rank_select(const SketchTask* t, int ntasks, double tol, cudaStream_t st) {
+  if (cudaError_t e = cudaGetLastError()) return e;
+  if (ntasks <= 0) return cudaSuccess;
+  k_rank_select<<<(ntasks + 127) / 128, 128, 0, st>>>(t, ntasks, tol);
+  return done_launch("launch_rank_select");
+}
+
+size_t mlp_work_floats(int n) { return (size_t)((n + kMlpBatch - 1) / kMlpBatch) * (kMlpParams + 1); }
+
+cudaError_t mlp_loss_grad(const float* params, const float* X, const float* y, int n, float* loss, float* grad,
+                          float* work, cudaStream_t st) {
+  if (cudaError_t e = cudaGetLastError()) return e;
+  if (n <= 0) return cudaErrorInvalidValue;
+  const int nb = (n + kMlpBatch - 1) / kMlpBatch;
+  cudaError_t e = cudaFuncSetAttribute(k_mlp_grad, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMlpSmem);
+  if (e) return e;
+  k_mlp_grad<<<nb, kMlpThreads, kMlpSmem, st>>>(params, X, y, n, work);
+  if ((e = done_launch("mlp_grad"))) return e;
+  k_mlp_reduce<<<(kMlpParams + 1 + 255) / 256, 256, 0, st>>>(work, nb, grad, loss);
+  return done_launch("mlp_reduce");
+}
+
+cudaError_t mlp_predict(const float* params, const float* X, int n, float* out, cudaStream_t st) {
+  if (cudaError_t e = cudaGetLastError()) return e;
+  if (n <= 0) return cudaSuccess;
+  k_mlp_predict<<<(n + 127) / 128, 128, 0, st>>>(params, X, n, out);
+  return done_launch("mlp_predict");
+}
+
+cudaError_t mlp_adam(float* params, const float* grad, float* m1, float* m2, float lr, int step, cudaStream_t st) {
+  if (cudaError_t e = cudaGetLastError()) return e;
+  const float c1 = 1.0f - powf(0.9f, (float)step), c2 = 1.0f - powf(0.999f, (float)step);
+  k_mlp_adam<<<(kMlpParams + 255) / 256, 256, 0, st>>>(params, grad, m1, m2, lr, c1, c2);
+  return done_launch("mlp_adam");
+}
+
+}  // namespace spq

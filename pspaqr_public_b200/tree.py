@@ -62,6 +62,17 @@ def lib():
             "spq_gmres": (i32, [vp, pd, i32, f64, pi, pd, pd, i32]),
             "spq_gmres_device": (i32, [vp, vp, i32, f64, pi, pd, pd, i32]),
             "spq_gmres_device_noalloc": (i32, [vp, vp, i32, f64, pi, pd]),
+            "spq_rank_model_size": (i32, [pi, pi]),
+            "spq_set_rank_model": (i32, [vp, pf, pf, pf, i32]),
+            "spq_learned_counts": (i32, [vp, C.POINTER(C.c_longlong)]),
+            "spq_set_rank_log": (i32, [vp, i32]),
+            "spq_rank_log_count": (i32, [vp]),
+            "spq_rank_log": (i32, [vp, pf, pi, pi, pi]),
+            "spq_rank_log_clear": (i32, [vp]),
+            "spq_mlp_loss_grad": (i32, [pf, pf, pf, i32, pf, pf]),
+            "spq_mlp_predict": (i32, [pf, pf, i32, pf]),
+            "spq_mlp_train": (i32, [pf, pf, pf, i32, i32, i32, f32, C.c_ulonglong, pf]),
+            "spq_mlp_last_error": (C.c_char_p, []),
             "spq_distribute_x": (i32, [vp, pd, pd]),
             "spq_extract_x": (i32, [vp, pd, pd]),
             "spq_n": (i32, [vp]),
@@ -94,6 +105,10 @@ def lib():
 
 def _pi(a):
     return a.ctypes.data_as(C.POINTER(C.c_int))
+
+
+def _pf(a):
+    return a.ctypes.data_as(C.POINTER(C.c_float))
 
 
 def _pd(a):
@@ -199,6 +214,40 @@ class ParTree:
         """Cluster sizing of the pivoted QR: elements of the compression matrix
         per CTA and pivot step, and CTAs per SM a level's work is spread over."""
         self._chk(lib().spq_set_rrqr_work(self._h, elems, fill), "set_rrqr_work")
+
+    def set_rank_model(self, model: Optional[dict], oversample: int = 32):
+        """Learned ranks from ``model`` (``params``, ``mean``, ``std`` float32
+        arrays, e.g. :func:`load_rank_model`); ``None`` restores the plain
+        pivoted QR of every interface."""
+        if model is None:
+            self._chk(lib().spq_set_rank_model(self._h, None, None, None, 0), "set_rank_model")
+            return
+        self._model = {k: np.ascontiguousarray(model[k], dtype=np.float32) for k in ("params", "mean", "std")}
+        m = self._model
+        self._chk(lib().spq_set_rank_model(self._h, _pf(m["params"]), _pf(m["mean"]), _pf(m["std"]), oversample),
+                  "set_rank_model")
+
+    def learned_counts(self) -> dict:
+        out = (C.c_longlong * 3)()
+        self._chk(lib().spq_learned_counts(self._h, out), "learned_counts")
+        return {"accepted": out[0], "fallback": out[1], "sketch_columns": out[2]}
+
+    def set_rank_log(self, on: bool = True):
+        self._chk(lib().spq_set_rank_log(self._h, int(on)), "set_rank_log")
+
+    def rank_log(self) -> dict:
+        """Logged (features, kept rank, min(m, w), level) of the sparsified interfaces."""
+        n = lib().spq_rank_log_count(self._h)
+        _, nf = rank_model_size()
+        out = {"features": np.zeros((n, nf), np.float32), "rank": np.zeros(n, np.int32),
+               "kmin": np.zeros(n, np.int32), "level": np.zeros(n, np.int32)}
+        if n:
+            self._chk(lib().spq_rank_log(self._h, _pf(out["features"]), _pi(out["rank"]), _pi(out["kmin"]),
+                                         _pi(out["level"])), "rank_log")
+        return out
+
+    def clear_rank_log(self):
+        self._chk(lib().spq_rank_log_clear(self._h), "rank_log_clear")
 
     def set_Xcoo(self, X: np.ndarray):
         """Coordinates as a dim x n array (tree.cpp:21)."""
@@ -351,3 +400,71 @@ def dist_gmres(A, b: np.ndarray, M: ParTree, iters: int = 300, tol: float = 1e-1
     if hist is not None:
         hist.extend(h[: k.value + 1].tolist())
     return k.value, rr.value
+
+
+# ---------------------------------------------------------------- rank MLP
+def rank_model_size():
+    """(number of MLP parameters, number of interface features)."""
+    a, b = C.c_int(), C.c_int()
+    lib().spq_rank_model_size(C.byref(a), C.byref(b))
+    return a.value, b.value
+
+
+def _mlp_check(rc, what):
+    if rc != 0:
+        raise SpqError(what, rc, (lib().spq_mlp_last_error() or b"").decode())
+
+
+def _f32(a, shape=None):
+    a = np.ascontiguousarray(a, dtype=np.float32)
+    if shape is not None and a.shape != shape:
+        raise ValueError(f"expected shape {shape}, got {a.shape}")
+    return a
+
+
+def mlp_loss_grad(params, X, y):
+    """Loss mean((sigmoid(z) - y)^2) and its gradient, on the GPU."""
+    P, F = rank_model_size()
+    params, X, y = _f32(params, (P,)), _f32(X), _f32(y)
+    loss, grad = np.zeros(1, np.float32), np.zeros(P, np.float32)
+    _mlp_check(lib().spq_mlp_loss_grad(_pf(params), _pf(X), _pf(y), len(y), _pf(loss), _pf(grad)), "mlp_loss_grad")
+    return float(loss[0]), grad
+
+
+def mlp_predict(params, X):
+    P, F = rank_model_size()
+    params, X = _f32(params, (P,)), _f32(X)
+    out = np.zeros(len(X), np.float32)
+    _mlp_check(lib().spq_mlp_predict(_pf(params), _pf(X), len(X), _pf(out)), "mlp_predict")
+    return out
+
+
+def mlp_train(params, X, y, epochs: int, batch: int = 4096, lr: float = 1e-3, seed: int = 0):
+    """Adam training on the GPU; returns (params, per-epoch loss)."""
+    P, F = rank_model_size()
+    params = _f32(params, (P,)).copy()
+    X, y = _f32(X), _f32(y)
+    hist = np.zeros(max(epochs, 1), np.float32)
+    _mlp_check(lib().spq_mlp_train(_pf(params), _pf(X), _pf(y), len(y), epochs, batch, lr, seed, _pf(hist)),
+               "mlp_train")
+    return params, hist[:epochs]
+
+
+def mlp_init(seed: int = 0):
+    """He-initialised parameters in the library's layout."""
+    P, F = rank_model_size()
+    H = 64
+    rng = np.random.default_rng(seed)
+    W1 = rng.normal(0, np.sqrt(2.0 / F), (H, F))
+    W2 = rng.normal(0, np.sqrt(2.0 / H), (H, H))
+    w3 = rng.normal(0, np.sqrt(1.0 / H), H)
+    p = np.concatenate([W1.ravel(), np.zeros(H), W2.ravel(), np.zeros(H), w3, [0.0]]).astype(np.float32)
+    assert p.size == P
+    return p
+
+
+def load_rank_model(path: Optional[str] = None) -> dict:
+    """The trained rank model shipped with the package (rank_model/rank_mlp.npz)."""
+    path = path or os.path.join(_HERE, "rank_model", "rank_mlp.npz")
+    z = np.load(path)
+    return {k: z[k].astype(np.float32) for k in ("params", "mean", "std")}
