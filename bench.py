@@ -4,13 +4,17 @@
 A step is one full time-to-solution run on an assembled tree: ``factorize()``
 followed by left-preconditioned GMRES until the preconditioned residual is
 <= 1e-10 (is.cpp:447-527), with the true ||b - A x|| / ||b|| checked after it.
+Two variants run on the same tree in the same process: the plain FP64 method
+(column-pivoted QR of every interface) and the learned-rank method (the
+headline, ``value``); ``ratio_vs_fp64`` is their ratio.
 
-  value : device time of the step, inputs resident in HBM (CUDA events on the
-          handle's stream, max over ranks), seconds -- lower is better.
+  value : device time of the learned-rank step, inputs resident in HBM (CUDA
+          events on the handle's stream, max over ranks), seconds -- lower is
+          better.
   e2e   : the same step through the C ABI with host buffers: assemble (matrix
           upload) + factorize + spq_gmres(host b -> host x).
-  roofline : the dominant kernel of the step (from the per-kernel event
-          timing below) against the measured peak it is bound by.
+  roofline : the dominant kernel of the plain factorization (the pivoted QR)
+          against the measured HBM peak.
   cpu_baseline : the CPU oracle (LAPACK restatement of the reference path,
           OpenMP over independent tasks on all host cores) on the same workload.
 
@@ -45,6 +49,8 @@ METRIC = "time to 1e-10 rel. residual (factor+GMRES), 64^3 diffusion: mixed+lear
 # capture of the 48^3 member of the workload family
 # (profiles/k_rrqr_diff3d_48_traffic.md)
 RRQR_DRAM_PER_ALGO_BYTE = 0.78
+# sketch columns beyond the predicted rank in the learned-rank variant
+LEARNED_OVERSAMPLE = 32
 
 
 def build_matrix():
@@ -211,40 +217,65 @@ def run_ours(args):
         wall = time.perf_counter() - s0
         return max(wall, e0.elapsed_time(e1) / 1e3), it.value, rr.value
 
-    for _ in range(args.warmup):
-        device_step()
-    times, ftimes, iters, rels, launches = [], [], [], [], []
+    from pspaqr_public_b200.tree import load_rank_model
+
+    model = load_rank_model()
+
+    def set_variant(name):
+        t.set_rank_model(model if name == "learned" else None, LEARNED_OVERSAMPLE)
+
+    def ranks():
+        cl = t.clusters()
+        return np.array([c["rank"] for c in cl if c["sparsify"]])
+
+    # both variants on the same tree: plain FP64 (the comparison) and learned
+    # ranks (the headline); warm-up of each, then the timed steps of each
+    res = {}
     with ClockSampler(local) as clk:
-        for _ in range(args.steps):
-            dt, ft, it, rr, nl = device_step()
-            times.append(dt)
-            ftimes.append(ft)
-            iters.append(it)
-            rels.append(rr)
-            launches.append(nl)
+        for name in ("fp64", "learned"):
+            set_variant(name)
+            for _ in range(args.warmup):
+                device_step()
+            r = {"times": [], "ftimes": [], "iters": [], "rels": [], "launches": []}
+            for _ in range(args.steps):
+                dt, ft, it, rr, nl = device_step()
+                r["times"].append(dt)
+                r["ftimes"].append(ft)
+                r["iters"].append(it)
+                r["rels"].append(rr)
+                r["launches"].append(nl)
+            r["level_ms"] = t.level_times()
+            r["ranks"] = ranks()
+            r["counts"] = t.learned_counts()
+            r["flops"] = t.factor_flops()
+            r["rrqr_bytes"] = t.rrqr_bytes()
+            res[name] = r
+    head = res["learned"]
     e2e_times = [e2e_step()[0] for _ in range(max(1, min(args.steps, 3)))]
-    step = float(np.mean(times))
+    step = float(np.mean(head["times"]))
+    fp64_step = float(np.mean(res["fp64"]["times"]))
     if dist:
-        tt = torch.tensor([step, float(np.mean(e2e_times))], dtype=torch.float64, device="cuda")
+        tt = torch.tensor([step, float(np.mean(e2e_times)), fp64_step], dtype=torch.float64, device="cuda")
         dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        step, e2e = float(tt[0]), float(tt[1])
+        step, e2e, fp64_step = float(tt[0]), float(tt[1]), float(tt[2])
     else:
         e2e = float(np.mean(e2e_times))
-    # per-level kernel-phase timing of the last factorization (CUDA events the
-    # library records on its stream around each phase)
-    lt = t.level_times()
-    flops = t.factor_flops()
     peaks = measured_peaks()
     fp64_peak = fp64_gemm_peak(torch) if rank == 0 else 0.0
-    fact = float(np.mean(ftimes))
-    # dominant kernel: the pivoted QR (k_rrqr_assemble + k_rrqr launches of
-    # every level), HBM-bound; algorithmic bytes over its event-timed duration
-    rrqr_s = float(lt[:, ParTree.LEVEL_PHASES.index("rrqr")].sum()) / 1e3
-    rrqr_bytes = t.rrqr_bytes()
+    fact = float(np.mean(head["ftimes"]))
+    # dominant kernel of the plain factorization: the pivoted QR
+    # (k_rrqr_assemble + k_rrqr launches of every level), HBM-bound;
+    # algorithmic bytes over its event-timed duration
+    plt = res["fp64"]["level_ms"]
+    rrqr_s = float(plt[:, ParTree.LEVEL_PHASES.index("rrqr")].sum()) / 1e3
+    rrqr_bytes = res["fp64"]["rrqr_bytes"]
     hbm_peak = peaks.get("hbm_gbs") or 6650.0
     achieved = rrqr_bytes / rrqr_s / 1e9
     nnz = len(ri)
     h2d = nnz * (8 + 4) + (N + 1) * 4 + 8 * N + 8 * nnz  # matrix (CSC values + indices) + b
+    cnt = head["counts"]
+    nint = max(cnt["accepted"] + cnt["fallback"], 1)
+    dr = head["ranks"] - res["fp64"]["ranks"]
     out = {
         "metric": METRIC,
         "value": step,
@@ -258,29 +289,41 @@ def run_ours(args):
         "vs_baseline": None,
         "dtype": "f64",
         "data": "synthetic (seeded Gaussian random field coefficients, N(0,1) right-hand side)",
-        "variant": "fp64 (plain spaQR: FP64 tile QR, RRQR sparsification, FP64 GMRES)",
+        "variant": "learned ranks (MLP-sized randomized range finder + residual rank rule, pivoted-QR fallback); "
+                   "FP64 factorization and GMRES -- the FP32 factorization is not built yet",
         "config": {"workload": W["name"], "matrix": W["matrix"], "nlevels": W["nlevels"], "tol": W["tol"],
                    "skip": W["skip"], "gmres_tol": W["gmres_tol"], "parallelism": f"replicas x{world}",
                    "l2": "factor pool (GBs) > L2; 256 MB buffer written before every timed step"},
         "factorize_s": fact,
         "gmres_s": step - fact,
-        "gmres_iters": int(np.median(iters)),
-        "true_relres": float(max(rels)),
+        "gmres_iters": int(np.median(head["iters"])),
+        "true_relres": float(max(head["rels"])),
         "partition_s": t_part,
+        "fp64_plain": {"value": fp64_step, "factorize_s": float(np.mean(res["fp64"]["ftimes"])),
+                       "gmres_iters": int(np.median(res["fp64"]["iters"])),
+                       "true_relres": float(max(res["fp64"]["rels"]))},
+        "ratio_vs_fp64": step / fp64_step,
+        "learned": {"interfaces": int(nint), "fallback_rate": cnt["fallback"] / nint,
+                    "ranks_within_2": float(np.mean(np.abs(dr) <= 2)) if len(dr) else None,
+                    "sketch_columns_per_interface": cnt["sketch_columns"] / nint,
+                    "oversample": LEARNED_OVERSAMPLE},
         "e2e": {"value": e2e, "unit": "s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": 8 * N},
-        "gpu_launches": int(np.median(launches)),
+        "gpu_launches": int(np.median(head["launches"])),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
-                     "frac": achieved / hbm_peak, "traffic": RRQR_DRAM_PER_ALGO_BYTE * rrqr_bytes if RRQR_DRAM_PER_ALGO_BYTE else None,
-                     "kernel": "pivoted QR (k_rrqr_assemble + k_rrqr, all levels of one factorization)",
+                     "frac": achieved / hbm_peak,
+                     "traffic": RRQR_DRAM_PER_ALGO_BYTE * rrqr_bytes if RRQR_DRAM_PER_ALGO_BYTE else None,
+                     "kernel": "pivoted QR (k_rrqr_assemble + k_rrqr, all levels of one plain FP64 factorization)",
                      "algorithmic_bytes": rrqr_bytes, "duration_s": rrqr_s, "launches": "per factorization",
                      "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if peaks.get("hbm_gbs")
                      else "fallback 6650 GB/s (of fallback)",
                      "traffic_source": "dram__bytes_read.sum + dram__bytes_write.sum per algorithmic byte of the "
                                        "k_rrqr* launches of the 48^3 member (ncu), scaled to this step"},
-        "factor_fp64": {"achieved_tflops": flops / fact / 1e12, "dgemm_peak_tflops": fp64_peak,
-                        "note": "nominal LAWN 41 flops of the whole factorization / factorize time; "
+        "factor_fp64": {"achieved_tflops": res["fp64"]["flops"] / float(np.mean(res["fp64"]["ftimes"])) / 1e12,
+                        "dgemm_peak_tflops": fp64_peak,
+                        "note": "nominal LAWN 41 flops of the plain factorization / its time; "
                                 "peak = cuBLAS DGEMM 8192^3 in this run"},
-        "level_ms": {k: lt[:, i].round(3).tolist() for i, k in enumerate(ParTree.LEVEL_PHASES)},
+        "level_ms": {k: head["level_ms"][:, i].round(3).tolist() for i, k in enumerate(ParTree.LEVEL_PHASES)},
+        "level_ms_fp64": {k: plt[:, i].round(3).tolist() for i, k in enumerate(ParTree.LEVEL_PHASES)},
         "clocks": clk.summary(),
         "hbm_peak_gbs": peaks.get("hbm_gbs"),
     }

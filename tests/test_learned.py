@@ -1,0 +1,192 @@
+"""Learned-rank sparsification and the rank MLP.
+
+CPU: the numpy oracle of the MLP against finite differences.  GPU: the MLP's
+own CUDA kernels (loss, gradient, prediction, Adam training) against that
+oracle, and the learned-rank factorization against the plain one: ranks within
++-2, the fallback to the pivoted QR, GMRES convergence, and the gain of the
+trained network over a constant predictor (the method without it).
+"""
+import json
+import os
+
+import numpy as np
+import pytest
+
+from oracle import mlp_oracle as MO
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+MODEL = os.path.join(os.path.dirname(HERE), "pspaqr_public_b200", "rank_model", "rank_mlp.npz")
+
+
+def _params(seed):
+    rng = np.random.default_rng(seed)
+    F, H = MO.F, MO.H
+    W1 = rng.normal(0, np.sqrt(2.0 / F), (H, F))
+    W2 = rng.normal(0, np.sqrt(2.0 / H), (H, H))
+    w3 = rng.normal(0, np.sqrt(1.0 / H), H)
+    b = rng.normal(0, 0.1, 2 * H + 1)
+    return np.concatenate([W1.ravel(), b[:H], W2.ravel(), b[H:2 * H], w3, b[2 * H:]])
+
+
+def test_mlp_oracle_gradient_matches_finite_differences():
+    p = _params(3)
+    rng = np.random.default_rng(0)
+    X, y = rng.normal(size=(50, MO.F)), rng.uniform(size=50)
+    _, g = MO.loss_grad(p, X, y)
+    eps = 1e-6
+    for idx in (0, 100, 704, 800, 4000, 4900, MO.NPARAMS - 1):
+        pp, pm = p.copy(), p.copy()
+        pp[idx] += eps
+        pm[idx] -= eps
+        fd = (MO.loss_grad(pp, X, y)[0] - MO.loss_grad(pm, X, y)[0]) / (2 * eps)
+        assert abs(fd - g[idx]) <= 1e-6 * max(1.0, abs(g[idx])) + 1e-9
+
+
+def _gpu():
+    torch = pytest.importorskip("torch")
+    if not torch.cuda.is_available():
+        pytest.skip("needs a GPU")
+    from pspaqr_public_b200 import tree as T
+
+    return T
+
+
+@pytest.mark.gpu
+def test_mlp_gradient_and_prediction_match_oracle():
+    T = _gpu()
+    assert T.rank_model_size() == (MO.NPARAMS, MO.F)
+    p = _params(5).astype(np.float32)
+    rng = np.random.default_rng(1)
+    X = rng.normal(size=(300, MO.F)).astype(np.float32)  # not a multiple of the 64-sample block
+    y = rng.uniform(size=300).astype(np.float32)
+    loss, g = T.mlp_loss_grad(p, X, y)
+    lo, go = MO.loss_grad(p, X, y)
+    assert abs(loss - lo) <= 1e-5 * lo
+    assert np.abs(g - go).max() <= 1e-4 * np.abs(go).max()
+    out = T.mlp_predict(p, X)
+    ref, _ = MO.forward(p, X)
+    np.testing.assert_allclose(out, ref, rtol=0, atol=1e-5)
+
+
+@pytest.mark.gpu
+def test_mlp_training_reduces_loss():
+    T = _gpu()
+    rng = np.random.default_rng(2)
+    X = rng.normal(size=(5000, MO.F)).astype(np.float32)
+    w = rng.normal(size=MO.F)
+    y = (1.0 / (1.0 + np.exp(-(X @ w) / 2.0))).astype(np.float32)
+    p0 = T.mlp_init(0)
+    l0, _ = T.mlp_loss_grad(p0, X, y)
+    p1, hist = T.mlp_train(p0, X, y, epochs=30, batch=512, lr=3e-3, seed=4)
+    l1, _ = T.mlp_loss_grad(p1, X, y)
+    assert len(hist) == 30 and l1 < 0.1 * l0
+    assert abs(l1 - MO.loss_grad(p1, X, y)[0]) <= 1e-4 * max(l1, 1e-6)
+
+
+def _tree(n, seed, tol):
+    from pspaqr_public_b200 import ParTree, scale_columns
+    from pspaqr_public_b200 import matrices as M
+
+    cp, ri, v = M.diffusion_binary(n, 3, seed=seed)
+    t = ParTree(9, 0)
+    t.set_tol(tol)
+    t.set_coords_tensor(n, 3)
+    t.partition((cp, ri, scale_columns(cp, v)))
+    return t
+
+
+def _ranks(t):
+    cl = t.clusters()
+    sp = np.array([c["sparsify"] for c in cl]) > 0
+    return np.array([c["rank"] for c in cl])[sp]
+
+
+def _solve(t, n):
+    from pspaqr_public_b200 import dist_gmres, random_reference
+
+    return dist_gmres(None, random_reference(n ** 3, 7), t, 100, 1e-10)
+
+
+@pytest.fixture(scope="module")
+def model():
+    _gpu()
+    if not os.path.exists(MODEL):
+        pytest.skip("rank_mlp.npz not trained")
+    from pspaqr_public_b200.tree import load_rank_model
+
+    z = np.load(MODEL)
+    return load_rank_model(MODEL), json.loads(str(z["meta"]))
+
+
+@pytest.mark.gpu
+def test_learned_ranks_track_plain_ranks(model):
+    m, meta = model
+    n = 32
+    t = _tree(n, 55, 1e-2)  # held-out seed
+    t.assemble()
+    t.factorize()
+    plain = _ranks(t)
+    k0, r0 = _solve(t, n)
+    t.set_rank_model(m, meta["oversample"])
+    t.assemble()
+    t.factorize()
+    learned = _ranks(t)
+    cnt = t.learned_counts()
+    k1, r1 = _solve(t, n)
+    assert cnt["accepted"] + cnt["fallback"] == len(plain)
+    assert cnt["fallback"] <= 0.1 * len(plain)
+    # ranks come from the residual rule on the sketch's basis, not from the
+    # network, so they may differ from the greedy pivoted QR by a few
+    assert np.mean(np.abs(learned - plain) <= 2) >= 0.85
+    assert r1 <= 1e-10 and k1 <= k0 + 3
+
+
+@pytest.mark.gpu
+def test_fallback_is_the_plain_pivoted_qr():
+    """A network that predicts rank 0 with no oversampling sketches one column:
+    interfaces needing more fall back to the plain pivoted QR, and the solve is
+    as good as the plain one."""
+    T = _gpu()
+    n = 32
+    t = _tree(n, 51, 1e-2)
+    t.assemble()
+    t.factorize()
+    plain = _ranks(t)
+    k0, _ = _solve(t, n)
+    P, F = T.rank_model_size()
+    p = np.zeros(P, np.float32)
+    p[-1] = -30.0
+    t.set_rank_model({"params": p, "mean": np.zeros(F, np.float32), "std": np.ones(F, np.float32)}, 0)
+    t.assemble()
+    t.factorize()
+    cnt = t.learned_counts()
+    learned = _ranks(t)
+    fb = cnt["fallback"]
+    assert fb >= 0.5 * len(plain)
+    # fallen-back interfaces ran the plain pivoted QR: their ranks are the plain ranks
+    assert np.sum(learned == plain) >= fb
+    k1, r1 = _solve(t, n)
+    assert r1 <= 1e-10 and abs(k1 - k0) <= 1
+
+
+@pytest.mark.gpu
+def test_trained_network_gains_over_constant_prediction(model):
+    """The method without the trained network predicts the training mean for
+    every interface: it falls back more often and/or sketches more columns."""
+    T = _gpu()
+    m, meta = model
+    P, F = T.rank_model_size()
+    mu = meta["mean_target"]
+    pc = np.zeros(P, np.float32)
+    pc[-1] = np.log(mu / (1.0 - mu))
+    const = {"params": pc, "mean": np.zeros(F, np.float32), "std": np.ones(F, np.float32)}
+    res = {}
+    for name, mod in (("trained", m), ("constant", const)):
+        t = _tree(32, 52, 1e-2)
+        t.set_rank_model(mod, meta["oversample"])
+        t.assemble()
+        t.factorize()
+        res[name] = t.learned_counts()
+    tr, co = res["trained"], res["constant"]
+    assert tr["fallback"] <= co["fallback"] and tr["sketch_columns"] <= co["sketch_columns"]
+    assert tr["fallback"] < co["fallback"] or tr["sketch_columns"] < co["sketch_columns"]
