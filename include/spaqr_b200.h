@@ -32,7 +32,9 @@ int spq_destroy(spq_tree* t);
  * (src/ptree.cpp:21-23).  order, hsl, nthreads and ttor_log are accepted and
  * recorded like the reference (ParTree never reads order; the rest steer its
  * CPU runtime, which this path replaces).  set_skip follows the driver rule
- * skip = nlevels-1 when tol == 0 (pspaQR.cpp:150) at partition time. */
+ * skip = nlevels-1 when tol == 0 (pspaQR.cpp:150) at partition time.
+ * The tolerance of the sparsification is read at each factorize; whether it
+ * is zero (no sparsification at all) is fixed by partition. */
 int spq_set_tol(spq_tree* t, double tol);
 int spq_set_skip(spq_tree* t, int skip);
 int spq_set_scale(spq_tree* t, int scale);
@@ -51,6 +53,18 @@ int spq_set_pivot_rtol(spq_tree* t, double rtol);
  * max(elems, level total / (fill * SMs)) elements of the compression matrix
  * per pivot step.  elems >= 1024 (default 65536), 0 < fill <= 64 (default 2). */
 int spq_set_rrqr_work(spq_tree* t, double elems, double fill);
+/* Mixed precision (no reference counterpart; the reference is FP64 only):
+ * bits = 32 stores the factor blocks and applies the preconditioner in float
+ * while the SpMV on the original matrix, the GMRES orthogonalisation and the
+ * pivoted QR of the compression matrices stay in double; bits = 64 (default)
+ * is the plain FP64 method.  Takes effect at the next assemble. */
+int spq_set_precision(spq_tree* t, int bits);
+/* Krylov method of spq_gmres / spq_gmres_device (no reference counterpart):
+ * 0 = left-preconditioned GMRES of is.cpp:447-527; 1 = flexible
+ * right-preconditioned GMRES, whose residual is the true ||b - A x|| however
+ * inexact the preconditioner; -1 (default) = flexible exactly when the
+ * factors are float (spq_set_precision(t, 32)). */
+int spq_set_krylov(spq_tree* t, int method);
 
 /* Tree::set_Xcoo(MatrixXd*) (src/tree.cpp:21): coordinates, dim x n
  * column-major (the reference borrows the pointer; this copies it). */

@@ -68,6 +68,18 @@ int spq_set_rrqr_work(spq_tree* h, double elems, double fill) {
   return 0;
 }
 
+int spq_set_precision(spq_tree* h, int bits) {
+  if (!h || (bits != 32 && bits != 64)) return -1;
+  h->t->precision = bits;
+  return 0;
+}
+
+int spq_set_krylov(spq_tree* h, int method) {
+  if (!h || method < -1 || method > 1) return -1;
+  h->t->krylov = method;
+  return 0;
+}
+
 int spq_set_square(spq_tree* h, int s) {
   if (!h) return -1;
   if (!s) {

@@ -24,38 +24,41 @@ constexpr int kThreads = 256;
 constexpr int kWarps = kThreads / 32;
 constexpr int kNB = 32;  // panel width of the blocked reflector storage
 
-__device__ __forceinline__ double warp_sum(double v) {
+template <typename T>
+__device__ __forceinline__ T warp_sum(T v) {
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
   return v;
 }
 
 // Deterministic CTA-wide sum; `red` is a shared scratch of >= kWarps+1 doubles.
-__device__ __forceinline__ double cta_sum(double v, double* red) {
+template <typename T>
+__device__ __forceinline__ T cta_sum(T v, T* red) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   v = warp_sum(v);
   if (lane == 0) red[warp] = v;
   __syncthreads();
   if (warp == 0) {
-    double t = lane < kWarps ? red[lane] : 0.0;
+    T t = lane < kWarps ? red[lane] : 0.0;
     t = warp_sum(t);
     if (lane == 0) red[kWarps] = t;
   }
   __syncthreads();
-  double r = red[kWarps];
+  T r = red[kWarps];
   __syncthreads();
   return r;
 }
 
 // dlarfg on (alpha, x) given sumsq = ||x||^2.  Returns tau, writes beta and
 // the scale the caller applies to x (0 when tau == 0).
-__device__ __forceinline__ double house(double alpha, double sumsq, double* beta, double* scal) {
+template <typename T>
+__device__ __forceinline__ T house(T alpha, T sumsq, T* beta, T* scal) {
   if (sumsq == 0.0) {
     *beta = alpha;
     *scal = 0.0;
     return 0.0;
   }
-  double b = -copysign(hypot(alpha, sqrt(sumsq)), alpha);
+  T b = -copysign(hypot(alpha, sqrt(sumsq)), alpha);
   *beta = b;
   *scal = 1.0 / (alpha - b);
   return (b - alpha) / b;
@@ -63,22 +66,23 @@ __device__ __forceinline__ double house(double alpha, double sumsq, double* beta
 
 // T (kb x kb, ld ldt) from G(l,j) = v_l^T v_j in its strictly upper part on
 // entry and tau[0:kb].  dlarft recurrence T(0:j,j) = -tau_j T(0:j,0:j) G(0:j,j).
-__device__ void larft_from_gram(double* T, int ldt, int kb, const double* tau, double* tmp /*>= kb*/) {
+template <typename T>
+__device__ void larft_from_gram(T* Tm, int ldt, int kb, const T* tau, T* tmp /*>= kb*/) {
   for (int j = 0; j < kb; ++j) {
-    for (int i = threadIdx.x; i < j; i += kThreads) tmp[i] = T[i + (size_t)j * ldt];
+    for (int i = threadIdx.x; i < j; i += kThreads) tmp[i] = Tm[i + (size_t)j * ldt];
     __syncthreads();
-    const double tj = tau[j];
+    const T tj = tau[j];
     for (int i = threadIdx.x; i < j; i += kThreads) {
-      double s = 0.0;
-      for (int l = i; l < j; ++l) s += T[i + (size_t)l * ldt] * tmp[l];
-      T[i + (size_t)j * ldt] = -tj * s;
+      T s = 0.0;
+      for (int l = i; l < j; ++l) s += Tm[i + (size_t)l * ldt] * tmp[l];
+      Tm[i + (size_t)j * ldt] = -tj * s;
     }
-    if (threadIdx.x == 0) T[j + (size_t)j * ldt] = tj;
+    if (threadIdx.x == 0) Tm[j + (size_t)j * ldt] = tj;
     __syncthreads();
   }
   for (int idx = threadIdx.x; idx < kb * kb; idx += kThreads) {
     const int i = idx % kb, j = idx / kb;
-    if (i > j) T[i + (size_t)j * ldt] = 0.0;
+    if (i > j) Tm[i + (size_t)j * ldt] = 0.0;
   }
   __syncthreads();
 }
@@ -95,16 +99,17 @@ __device__ __forceinline__ void pair_of(int p, int* l, int* j) {
 // Panel T of kb reflectors stored unit-lower-trapezoidal in V (m x kb, rows
 // from the panel's diagonal).  unit = 1: V(i,i) = 1 implied (geqrt / RRQR);
 // unit = 0: full tails of a pentagonal panel (tpqrt, identity on top).
-__device__ void panel_t(const double* V, int ldv, int m, int kb, int unit, const double* tau, double* T, int ldt,
-                        double* tmp) {
+template <typename T>
+__device__ void panel_t(const T* V, int ldv, int m, int kb, int unit, const T* tau, T* Tm, int ldt,
+                        T* tmp) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int npairs = kb * (kb - 1) / 2;
   for (int p = warp; p < npairs; p += kWarps) {
     int l, j;
     pair_of(p, &l, &j);
-    const double* vl = V + (size_t)l * ldv;
-    const double* vj = V + (size_t)j * ldv;
-    double d = 0.0;
+    const T* vl = V + (size_t)l * ldv;
+    const T* vj = V + (size_t)j * ldv;
+    T d = 0.0;
     if (unit) {
       d = lane == 0 ? vl[j] : 0.0;
       for (int i = j + 1 + lane; i < m; i += 32) d += vl[i] * vj[i];
@@ -112,24 +117,25 @@ __device__ void panel_t(const double* V, int ldv, int m, int kb, int unit, const
       for (int i = lane; i < m; i += 32) d += vl[i] * vj[i];
     }
     d = warp_sum(d);
-    if (lane == 0) T[l + (size_t)j * ldt] = d;
+    if (lane == 0) Tm[l + (size_t)j * ldt] = d;
   }
   __syncthreads();
-  larft_from_gram(T, ldt, kb, tau, tmp);
+  larft_from_gram(Tm, ldt, kb, tau, tmp);
 }
 
 // ---------------------------------------------------------------- applies
 // C (m x nc) <- (I - V T V^T)^T C for one block of k <= kNB reflectors,
 // V unit lower trapezoidal (m x k), T (k x k, ld ldt).  W: 2*k*nc doubles.
-__device__ void block_qt(const double* V, int ldv, const double* T, int ldt, int k, double* C, int ldc, int m, int nc,
-                         double* W) {
+template <typename T>
+__device__ void block_qt(const T* V, int ldv, const T* Tm, int ldt, int k, T* C, int ldc, int m, int nc,
+                         T* W) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  double* W2 = W + (size_t)k * nc;
+  T* W2 = W + (size_t)k * nc;
   for (int p = warp; p < k * nc; p += kWarps) {
     const int i = p % k, c = p / k;
-    const double* v = V + (size_t)i * ldv;
-    const double* x = C + (size_t)c * ldc;
-    double d = (lane == 0 && i < m) ? x[i] : 0.0;
+    const T* v = V + (size_t)i * ldv;
+    const T* x = C + (size_t)c * ldc;
+    T d = (lane == 0 && i < m) ? x[i] : 0.0;
     for (int r = i + 1 + lane; r < m; r += 32) d += v[r] * x[r];
     d = warp_sum(d);
     if (lane == 0) W[i + (size_t)c * k] = d;
@@ -137,8 +143,8 @@ __device__ void block_qt(const double* V, int ldv, const double* T, int ldt, int
   __syncthreads();
   for (int p = threadIdx.x; p < k * nc; p += kThreads) {
     const int i = p % k, c = p / k;
-    const double* t = T + (size_t)i * ldt;
-    double s = 0.0;
+    const T* t = Tm + (size_t)i * ldt;
+    T s = 0.0;
     for (int l = 0; l <= i; ++l) s += t[l] * W[l + (size_t)c * k];
     W2[i + (size_t)c * k] = s;
   }
@@ -146,7 +152,7 @@ __device__ void block_qt(const double* V, int ldv, const double* T, int ldt, int
   for (int p = threadIdx.x; p < m * nc; p += kThreads) {
     const int r = p % m, c = p / m;
     const int lim = r < k ? r : k;
-    double s = (r < k) ? W2[r + (size_t)c * k] : 0.0;
+    T s = (r < k) ? W2[r + (size_t)c * k] : 0.0;
     for (int i = 0; i < lim; ++i) s += V[r + (size_t)i * ldv] * W2[i + (size_t)c * k];
     C[r + (size_t)c * ldc] -= s;
   }
@@ -154,15 +160,16 @@ __device__ void block_qt(const double* V, int ldv, const double* T, int ldt, int
 }
 
 // C (m x nc) <- (I - V T V^T) C for one block (no transpose).
-__device__ void block_q(const double* V, int ldv, const double* T, int ldt, int k, double* C, int ldc, int m, int nc,
-                        double* W) {
+template <typename T>
+__device__ void block_q(const T* V, int ldv, const T* Tm, int ldt, int k, T* C, int ldc, int m, int nc,
+                        T* W) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  double* W2 = W + (size_t)k * nc;
+  T* W2 = W + (size_t)k * nc;
   for (int p = warp; p < k * nc; p += kWarps) {
     const int i = p % k, c = p / k;
-    const double* v = V + (size_t)i * ldv;
-    const double* x = C + (size_t)c * ldc;
-    double d = (lane == 0 && i < m) ? x[i] : 0.0;
+    const T* v = V + (size_t)i * ldv;
+    const T* x = C + (size_t)c * ldc;
+    T d = (lane == 0 && i < m) ? x[i] : 0.0;
     for (int r = i + 1 + lane; r < m; r += 32) d += v[r] * x[r];
     d = warp_sum(d);
     if (lane == 0) W[i + (size_t)c * k] = d;
@@ -171,15 +178,15 @@ __device__ void block_q(const double* V, int ldv, const double* T, int ldt, int 
   // W2 = T W  (T upper: W2(i) = sum_{l>=i} T(i,l) W(l))
   for (int p = threadIdx.x; p < k * nc; p += kThreads) {
     const int i = p % k, c = p / k;
-    double s = 0.0;
-    for (int l = i; l < k; ++l) s += T[i + (size_t)l * ldt] * W[l + (size_t)c * k];
+    T s = 0.0;
+    for (int l = i; l < k; ++l) s += Tm[i + (size_t)l * ldt] * W[l + (size_t)c * k];
     W2[i + (size_t)c * k] = s;
   }
   __syncthreads();
   for (int p = threadIdx.x; p < m * nc; p += kThreads) {
     const int r = p % m, c = p / m;
     const int lim = r < k ? r : k;
-    double s = (r < k) ? W2[r + (size_t)c * k] : 0.0;
+    T s = (r < k) ? W2[r + (size_t)c * k] : 0.0;
     for (int i = 0; i < lim; ++i) s += V[r + (size_t)i * ldv] * W2[i + (size_t)c * k];
     C[r + (size_t)c * ldc] -= s;
   }
@@ -188,15 +195,16 @@ __device__ void block_q(const double* V, int ldv, const double* T, int ldt, int 
 
 // [A (k x nc, rows of the panel); B (m x nc)] <- Q^T [A; B] for one pentagonal
 // block, Q = I - [I; V] T [I; V]^T with V full (m x k).
-__device__ void block_tpqt(const double* V, int ldv, const double* T, int ldt, int k, double* A, int lda, double* B,
-                           int ldb, int m, int nc, double* W) {
+template <typename T>
+__device__ void block_tpqt(const T* V, int ldv, const T* Tm, int ldt, int k, T* A, int lda, T* B,
+                           int ldb, int m, int nc, T* W) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  double* W2 = W + (size_t)k * nc;
+  T* W2 = W + (size_t)k * nc;
   for (int p = warp; p < k * nc; p += kWarps) {
     const int i = p % k, c = p / k;
-    const double* v = V + (size_t)i * ldv;
-    const double* x = B + (size_t)c * ldb;
-    double d = lane == 0 ? A[i + (size_t)c * lda] : 0.0;
+    const T* v = V + (size_t)i * ldv;
+    const T* x = B + (size_t)c * ldb;
+    T d = lane == 0 ? A[i + (size_t)c * lda] : 0.0;
     for (int r = lane; r < m; r += 32) d += v[r] * x[r];
     d = warp_sum(d);
     if (lane == 0) W[i + (size_t)c * k] = d;
@@ -204,8 +212,8 @@ __device__ void block_tpqt(const double* V, int ldv, const double* T, int ldt, i
   __syncthreads();
   for (int p = threadIdx.x; p < k * nc; p += kThreads) {
     const int i = p % k, c = p / k;
-    const double* t = T + (size_t)i * ldt;
-    double s = 0.0;
+    const T* t = Tm + (size_t)i * ldt;
+    T s = 0.0;
     for (int l = 0; l <= i; ++l) s += t[l] * W[l + (size_t)c * k];
     W2[i + (size_t)c * k] = s;
   }
@@ -216,7 +224,7 @@ __device__ void block_tpqt(const double* V, int ldv, const double* T, int ldt, i
   }
   for (int p = threadIdx.x; p < m * nc; p += kThreads) {
     const int r = p % m, c = p / m;
-    double s = 0.0;
+    T s = 0.0;
     for (int i = 0; i < k; ++i) s += V[r + (size_t)i * ldv] * W2[i + (size_t)c * k];
     B[r + (size_t)c * ldb] -= s;
   }
@@ -225,28 +233,29 @@ __device__ void block_tpqt(const double* V, int ldv, const double* T, int ldt, i
 
 // C (m x n) <- C (I - V T V^T) for one block, V unit lower trapezoidal (n x k).
 // W: 2*k*m doubles.
-__device__ void block_q_right(const double* V, int ldv, const double* T, int ldt, int k, double* C, int ldc, int m,
-                              int n, double* W) {
-  double* W2 = W + (size_t)k * m;
+template <typename T>
+__device__ void block_q_right(const T* V, int ldv, const T* Tm, int ldt, int k, T* C, int ldc, int m,
+                              int n, T* W) {
+  T* W2 = W + (size_t)k * m;
   for (int p = threadIdx.x; p < k * m; p += kThreads) {
     const int r = p % m, i = p / m;
-    const double* v = V + (size_t)i * ldv;
-    double s = C[r + (size_t)i * ldc];
+    const T* v = V + (size_t)i * ldv;
+    T s = C[r + (size_t)i * ldc];
     for (int c = i + 1; c < n; ++c) s += C[r + (size_t)c * ldc] * v[c];
     W[i + (size_t)r * k] = s;
   }
   __syncthreads();
   for (int p = threadIdx.x; p < k * m; p += kThreads) {
     const int r = p % m, i = p / m;
-    const double* t = T + (size_t)i * ldt;
-    double s = 0.0;
+    const T* t = Tm + (size_t)i * ldt;
+    T s = 0.0;
     for (int l = 0; l <= i; ++l) s += W[l + (size_t)r * k] * t[l];
     W2[i + (size_t)r * k] = s;
   }
   __syncthreads();
   for (int p = threadIdx.x; p < m * n; p += kThreads) {
     const int r = p % m, c = p / m;
-    double s = (c < k) ? W2[c + (size_t)r * k] : 0.0;
+    T s = (c < k) ? W2[c + (size_t)r * k] : 0.0;
     const int top = (c < k) ? c : k;
     for (int i = 0; i < top; ++i) s += W2[i + (size_t)r * k] * V[c + (size_t)i * ldv];
     C[r + (size_t)c * ldc] -= s;
@@ -256,21 +265,23 @@ __device__ void block_q_right(const double* V, int ldv, const double* T, int ldt
 
 // Panel-blocked applies over k reflectors (T in kNB x k layout).
 // Q^T C: panels in order; each acts on rows [j0, m).
-__device__ void apply_qt(const double* V, int ldv, const double* T, int k, double* C, int ldc, int m, int nc,
-                         double* W, int wcap) {
+template <typename T>
+__device__ void apply_qt(const T* V, int ldv, const T* Tm, int k, T* C, int ldc, int m, int nc,
+                         T* W, int wcap) {
   if (k <= 0 || nc <= 0 || m <= 0) return;
   const int cmax = (wcap / (2 * kNB)) > 0 ? (wcap / (2 * kNB)) : 1;
   for (int j0 = 0; j0 < k; j0 += kNB) {
     const int kb = (k - j0) < kNB ? (k - j0) : kNB;
     for (int c0 = 0; c0 < nc; c0 += cmax) {
       const int cn = (nc - c0) < cmax ? (nc - c0) : cmax;
-      block_qt(V + j0 + (size_t)j0 * ldv, ldv, T + (size_t)j0 * kNB, kNB, kb, C + j0 + (size_t)c0 * ldc, ldc, m - j0,
+      block_qt(V + j0 + (size_t)j0 * ldv, ldv, Tm + (size_t)j0 * kNB, kNB, kb, C + j0 + (size_t)c0 * ldc, ldc, m - j0,
                cn, W);
     }
   }
 }
 // Q C: panels in reverse order.
-__device__ void apply_q(const double* V, int ldv, const double* T, int k, double* C, int ldc, int m, int nc, double* W,
+template <typename T>
+__device__ void apply_q(const T* V, int ldv, const T* Tm, int k, T* C, int ldc, int m, int nc, T* W,
                         int wcap) {
   if (k <= 0 || nc <= 0 || m <= 0) return;
   const int cmax = (wcap / (2 * kNB)) > 0 ? (wcap / (2 * kNB)) : 1;
@@ -280,35 +291,37 @@ __device__ void apply_q(const double* V, int ldv, const double* T, int k, double
     const int kb = (k - j0) < kNB ? (k - j0) : kNB;
     for (int c0 = 0; c0 < nc; c0 += cmax) {
       const int cn = (nc - c0) < cmax ? (nc - c0) : cmax;
-      block_q(V + j0 + (size_t)j0 * ldv, ldv, T + (size_t)j0 * kNB, kNB, kb, C + j0 + (size_t)c0 * ldc, ldc, m - j0,
+      block_q(V + j0 + (size_t)j0 * ldv, ldv, Tm + (size_t)j0 * kNB, kNB, kb, C + j0 + (size_t)c0 * ldc, ldc, m - j0,
               cn, W);
     }
   }
 }
 // [A (k x nc); B (m x nc)] <- Q^T [A; B] for a pentagonal (tpqrt) factor.
-__device__ void apply_tpqt(const double* V, int ldv, const double* T, int k, double* A, int lda, double* B, int ldb,
-                           int m, int nc, double* W, int wcap) {
+template <typename T>
+__device__ void apply_tpqt(const T* V, int ldv, const T* Tm, int k, T* A, int lda, T* B, int ldb,
+                           int m, int nc, T* W, int wcap) {
   if (k <= 0 || nc <= 0) return;
   const int cmax = (wcap / (2 * kNB)) > 0 ? (wcap / (2 * kNB)) : 1;
   for (int j0 = 0; j0 < k; j0 += kNB) {
     const int kb = (k - j0) < kNB ? (k - j0) : kNB;
     for (int c0 = 0; c0 < nc; c0 += cmax) {
       const int cn = (nc - c0) < cmax ? (nc - c0) : cmax;
-      block_tpqt(V + (size_t)j0 * ldv, ldv, T + (size_t)j0 * kNB, kNB, kb, A + j0 + (size_t)c0 * lda, lda,
+      block_tpqt(V + (size_t)j0 * ldv, ldv, Tm + (size_t)j0 * kNB, kNB, kb, A + j0 + (size_t)c0 * lda, lda,
                  B + (size_t)c0 * ldb, ldb, m, cn, W);
     }
   }
 }
 // C (m x n) <- C Q, panels in order; each acts on columns [j0, n).
-__device__ void apply_q_right(const double* V, int ldv, const double* T, int k, double* C, int ldc, int m, int n,
-                              double* W, int wcap) {
+template <typename T>
+__device__ void apply_q_right(const T* V, int ldv, const T* Tm, int k, T* C, int ldc, int m, int n,
+                              T* W, int wcap) {
   if (k <= 0 || m <= 0 || n <= 0) return;
   const int rmax = (wcap / (2 * kNB)) > 0 ? (wcap / (2 * kNB)) : 1;
   for (int j0 = 0; j0 < k; j0 += kNB) {
     const int kb = (k - j0) < kNB ? (k - j0) : kNB;
     for (int r0 = 0; r0 < m; r0 += rmax) {
       const int rn = (m - r0) < rmax ? (m - r0) : rmax;
-      block_q_right(V + j0 + (size_t)j0 * ldv, ldv, T + (size_t)j0 * kNB, kNB, kb, C + r0 + (size_t)j0 * ldc, ldc, rn,
+      block_q_right(V + j0 + (size_t)j0 * ldv, ldv, Tm + (size_t)j0 * kNB, kNB, kb, C + r0 + (size_t)j0 * ldc, ldc, rn,
                     n - j0, W);
     }
   }
@@ -327,19 +340,20 @@ constexpr int kTileSmem = kRT * (kNB + 1) + kNC * (kRT + 1) + kNB * kNC;
 // C (m x nc <= kNC) <- Q^T C with one panel: unit = 1: V unit lower trapezoidal
 // (geqrt / RRQR reflectors), A unused; unit = 0: pentagonal tpqrt panel,
 // [A (kb x nc); C] <- Q^T [A; C] with V full (m x kb).
-__device__ void tile_left_qt(const double* V, int ldv, const double* T, int ldt, int kb, int unit, double* A, int lda,
-                             double* C, int ldc, int m, int nc, double* sm) {
-  double* sV = sm;                              // [kRT][kNB+1]
-  double* sC = sV + kRT * (kNB + 1);            // [kRT][kNC+1]; later W2 [kNB][kNC]
-  double* sW = sC + kNC * (kRT + 1);            // [kNB][kNC]
+template <typename T>
+__device__ void tile_left_qt(const T* V, int ldv, const T* Tm, int ldt, int kb, int unit, T* A, int lda,
+                             T* C, int ldc, int m, int nc, T* sm) {
+  T* sV = sm;                              // [kRT][kNB+1]
+  T* sC = sV + kRT * (kNB + 1);            // [kRT][kNC+1]; later W2 [kNB][kNC]
+  T* sW = sC + kNC * (kRT + 1);            // [kNB][kNC]
   const int t = threadIdx.x;
   const int ti = t & 7, tc = t >> 3;            // rows ti*4..+3, cols tc*2..+1
-  double acc[4][2] = {{0, 0}, {0, 0}, {0, 0}, {0, 0}};
+  T acc[4][2] = {{0, 0}, {0, 0}, {0, 0}, {0, 0}};
   for (int r0 = 0; r0 < m; r0 += kRT) {
     const int rn = (m - r0) < kRT ? (m - r0) : kRT;
     for (int idx = t; idx < kRT * kNB; idx += kThreads) {
       const int r = idx % kRT, i = idx / kRT, gr = r0 + r;
-      double v = 0.0;
+      T v = 0.0;
       if (r < rn && i < kb) v = unit ? (gr == i ? 1.0 : (gr < i ? 0.0 : V[gr + (size_t)i * ldv])) : V[gr + (size_t)i * ldv];
       sV[r * (kNB + 1) + i] = v;
     }
@@ -350,12 +364,12 @@ __device__ void tile_left_qt(const double* V, int ldv, const double* T, int ldt,
     __syncthreads();
 #pragma unroll 4
     for (int r = 0; r < kRT; ++r) {
-      const double* vr = sV + r * (kNB + 1) + ti * 4;
-      const double* cr = sC + r * (kNC + 1) + tc * 2;
-      const double b0 = cr[0], b1 = cr[1];
+      const T* vr = sV + r * (kNB + 1) + ti * 4;
+      const T* cr = sC + r * (kNC + 1) + tc * 2;
+      const T b0 = cr[0], b1 = cr[1];
 #pragma unroll
       for (int q = 0; q < 4; ++q) {
-        const double a = vr[q];
+        const T a = vr[q];
         acc[q][0] += a * b0;
         acc[q][1] += a * b1;
       }
@@ -367,21 +381,21 @@ __device__ void tile_left_qt(const double* V, int ldv, const double* T, int ldt,
 #pragma unroll
     for (int p = 0; p < 2; ++p) {
       const int i = ti * 4 + q, c = tc * 2 + p;
-      double w = acc[q][p];
+      T w = acc[q][p];
       if (!unit && i < kb && c < nc) w += A[i + (size_t)c * lda];
       sW[i * kNC + c] = w;
     }
   __syncthreads();
   // W2 = T^T W  (T upper triangular: W2(i) = sum_{l <= i} T(l, i) W(l))
-  double* sW2 = sC;
+  T* sW2 = sC;
 #pragma unroll
   for (int q = 0; q < 4; ++q)
 #pragma unroll
     for (int p = 0; p < 2; ++p) {
       const int i = ti * 4 + q, c = tc * 2 + p;
-      double s = 0.0;
+      T s = 0.0;
       if (i < kb)
-        for (int l = 0; l <= i; ++l) s += T[l + (size_t)i * ldt] * sW[l * kNC + c];
+        for (int l = 0; l <= i; ++l) s += Tm[l + (size_t)i * ldt] * sW[l * kNC + c];
       sW2[i * kNC + c] = s;
     }
   __syncthreads();
@@ -396,18 +410,18 @@ __device__ void tile_left_qt(const double* V, int ldv, const double* T, int ldt,
     const int rn = (m - r0) < kRT ? (m - r0) : kRT;
     for (int idx = t; idx < kRT * kNB; idx += kThreads) {
       const int r = idx % kRT, i = idx / kRT, gr = r0 + r;
-      double v = 0.0;
+      T v = 0.0;
       if (r < rn && i < kb) v = unit ? (gr == i ? 1.0 : (gr < i ? 0.0 : V[gr + (size_t)i * ldv])) : V[gr + (size_t)i * ldv];
       sV[r * (kNB + 1) + i] = v;
     }
     __syncthreads();
-    double u[4][2] = {{0, 0}, {0, 0}, {0, 0}, {0, 0}};
+    T u[4][2] = {{0, 0}, {0, 0}, {0, 0}, {0, 0}};
 #pragma unroll 4
     for (int i = 0; i < kNB; ++i) {
-      const double w0 = sW2[i * kNC + tcc * 2], w1 = sW2[i * kNC + tcc * 2 + 1];
+      const T w0 = sW2[i * kNC + tcc * 2], w1 = sW2[i * kNC + tcc * 2 + 1];
 #pragma unroll
       for (int q = 0; q < 4; ++q) {
-        const double a = sV[(tr * 4 + q) * (kNB + 1) + i];
+        const T a = sV[(tr * 4 + q) * (kNB + 1) + i];
         u[q][0] += a * w0;
         u[q][1] += a * w1;
       }
@@ -425,19 +439,20 @@ __device__ void tile_left_qt(const double* V, int ldv, const double* T, int ldt,
 
 // C (m <= kNC rows x n) <- C (I - V T V^T) with one panel, V unit lower
 // trapezoidal (n x kb).
-__device__ void tile_right_q(const double* V, int ldv, const double* T, int ldt, int kb, double* C, int ldc, int m,
-                             int n, double* sm) {
-  double* sV = sm;                              // [kRT][kNB+1]: V rows c0..c0+31
-  double* sC = sV + kRT * (kNB + 1);            // [kNC][kRT+1]: C(r, c0+c)
-  double* sW = sC + kNC * (kRT + 1);            // [kNC][kNB] W(r, i)
+template <typename T>
+__device__ void tile_right_q(const T* V, int ldv, const T* Tm, int ldt, int kb, T* C, int ldc, int m,
+                             int n, T* sm) {
+  T* sV = sm;                              // [kRT][kNB+1]: V rows c0..c0+31
+  T* sC = sV + kRT * (kNB + 1);            // [kNC][kRT+1]: C(r, c0+c)
+  T* sW = sC + kNC * (kRT + 1);            // [kNC][kNB] W(r, i)
   const int t = threadIdx.x;
   const int ti = t & 7, tr = t >> 3;            // i = ti*4..+3, r = tr*2..+1
-  double acc[2][4] = {{0, 0, 0, 0}, {0, 0, 0, 0}};
+  T acc[2][4] = {{0, 0, 0, 0}, {0, 0, 0, 0}};
   for (int c0 = 0; c0 < n; c0 += kRT) {
     const int cn = (n - c0) < kRT ? (n - c0) : kRT;
     for (int idx = t; idx < kRT * kNB; idx += kThreads) {
       const int c = idx % kRT, i = idx / kRT, gc = c0 + c;
-      double v = 0.0;
+      T v = 0.0;
       if (c < cn && i < kb) v = gc == i ? 1.0 : (gc < i ? 0.0 : V[gc + (size_t)i * ldv]);
       sV[c * (kNB + 1) + i] = v;
     }
@@ -448,10 +463,10 @@ __device__ void tile_right_q(const double* V, int ldv, const double* T, int ldt,
     __syncthreads();
 #pragma unroll 4
     for (int c = 0; c < kRT; ++c) {
-      const double a0 = sC[(tr * 2) * (kRT + 1) + c], a1 = sC[(tr * 2 + 1) * (kRT + 1) + c];
+      const T a0 = sC[(tr * 2) * (kRT + 1) + c], a1 = sC[(tr * 2 + 1) * (kRT + 1) + c];
 #pragma unroll
       for (int q = 0; q < 4; ++q) {
-        const double v = sV[c * (kNB + 1) + ti * 4 + q];
+        const T v = sV[c * (kNB + 1) + ti * 4 + q];
         acc[0][q] += a0 * v;
         acc[1][q] += a1 * v;
       }
@@ -464,15 +479,15 @@ __device__ void tile_right_q(const double* V, int ldv, const double* T, int ldt,
     for (int q = 0; q < 4; ++q) sW[(tr * 2 + p) * kNB + ti * 4 + q] = acc[p][q];
   __syncthreads();
   // W2 = W T (W2(r,i) = sum_{l <= i} W(r,l) T(l,i))
-  double* sW2 = sC;  // [kNC][kNB]
+  T* sW2 = sC;  // [kNC][kNB]
 #pragma unroll
   for (int p = 0; p < 2; ++p)
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
       const int r = tr * 2 + p, i = ti * 4 + q;
-      double s = 0.0;
+      T s = 0.0;
       if (i < kb)
-        for (int l = 0; l <= i; ++l) s += sW[r * kNB + l] * T[l + (size_t)i * ldt];
+        for (int l = 0; l <= i; ++l) s += sW[r * kNB + l] * Tm[l + (size_t)i * ldt];
       sW2[r * kNB + i] = s;
     }
   __syncthreads();
@@ -482,18 +497,18 @@ __device__ void tile_right_q(const double* V, int ldv, const double* T, int ldt,
     const int cn = (n - c0) < kRT ? (n - c0) : kRT;
     for (int idx = t; idx < kRT * kNB; idx += kThreads) {
       const int c = idx % kRT, i = idx / kRT, gc = c0 + c;
-      double v = 0.0;
+      T v = 0.0;
       if (c < cn && i < kb) v = gc == i ? 1.0 : (gc < i ? 0.0 : V[gc + (size_t)i * ldv]);
       sV[c * (kNB + 1) + i] = v;
     }
     __syncthreads();
-    double u[2][4] = {{0, 0, 0, 0}, {0, 0, 0, 0}};
+    T u[2][4] = {{0, 0, 0, 0}, {0, 0, 0, 0}};
 #pragma unroll 4
     for (int i = 0; i < kNB; ++i) {
-      const double w0 = sW2[rr * kNB + i], w1 = sW2[(rr + 32) * kNB + i];
+      const T w0 = sW2[rr * kNB + i], w1 = sW2[(rr + 32) * kNB + i];
 #pragma unroll
       for (int q = 0; q < 4; ++q) {
-        const double v = sV[(cc * 4 + q) * (kNB + 1) + i];
+        const T v = sV[(cc * 4 + q) * (kNB + 1) + i];
         u[0][q] += w0 * v;
         u[1][q] += w1 * v;
       }
@@ -510,30 +525,33 @@ __device__ void tile_right_q(const double* V, int ldv, const double* T, int ldt,
 }
 
 // Panel loops of the tiled applies over k reflectors (T in kNB x k layout).
-__device__ void mat_apply_qt(const double* V, int ldv, const double* T, int k, double* C, int ldc, int m, int nc,
-                             double* sm) {
+template <typename T>
+__device__ void mat_apply_qt(const T* V, int ldv, const T* Tm, int k, T* C, int ldc, int m, int nc,
+                             T* sm) {
   for (int j0 = 0; j0 < k; j0 += kNB) {
     const int kb = (k - j0) < kNB ? (k - j0) : kNB;
     for (int c0 = 0; c0 < nc; c0 += kNC)
-      tile_left_qt(V + j0 + (size_t)j0 * ldv, ldv, T + (size_t)j0 * kNB, kNB, kb, 1, nullptr, 0,
+      tile_left_qt<T>(V + j0 + (size_t)j0 * ldv, ldv, Tm + (size_t)j0 * kNB, kNB, kb, 1, nullptr, 0,
                    C + j0 + (size_t)c0 * ldc, ldc, m - j0, (nc - c0) < kNC ? (nc - c0) : kNC, sm);
   }
 }
-__device__ void mat_apply_tpqt(const double* V, int ldv, const double* T, int k, double* A, int lda, double* B,
-                               int ldb, int m, int nc, double* sm) {
+template <typename T>
+__device__ void mat_apply_tpqt(const T* V, int ldv, const T* Tm, int k, T* A, int lda, T* B,
+                               int ldb, int m, int nc, T* sm) {
   for (int j0 = 0; j0 < k; j0 += kNB) {
     const int kb = (k - j0) < kNB ? (k - j0) : kNB;
     for (int c0 = 0; c0 < nc; c0 += kNC)
-      tile_left_qt(V + (size_t)j0 * ldv, ldv, T + (size_t)j0 * kNB, kNB, kb, 0, A + j0 + (size_t)c0 * lda, lda,
+      tile_left_qt(V + (size_t)j0 * ldv, ldv, Tm + (size_t)j0 * kNB, kNB, kb, 0, A + j0 + (size_t)c0 * lda, lda,
                    B + (size_t)c0 * ldb, ldb, m, (nc - c0) < kNC ? (nc - c0) : kNC, sm);
   }
 }
-__device__ void mat_apply_q_right(const double* V, int ldv, const double* T, int k, double* C, int ldc, int m, int n,
-                                  double* sm) {
+template <typename T>
+__device__ void mat_apply_q_right(const T* V, int ldv, const T* Tm, int k, T* C, int ldc, int m, int n,
+                                  T* sm) {
   for (int j0 = 0; j0 < k; j0 += kNB) {
     const int kb = (k - j0) < kNB ? (k - j0) : kNB;
     for (int r0 = 0; r0 < m; r0 += kNC)
-      tile_right_q(V + j0 + (size_t)j0 * ldv, ldv, T + (size_t)j0 * kNB, kNB, kb, C + r0 + (size_t)j0 * ldc, ldc,
+      tile_right_q(V + j0 + (size_t)j0 * ldv, ldv, Tm + (size_t)j0 * kNB, kNB, kb, C + r0 + (size_t)j0 * ldc, ldc,
                    (m - r0) < kNC ? (m - r0) : kNC, n - j0, sm);
   }
 }
@@ -542,14 +560,15 @@ __device__ void mat_apply_q_right(const double* V, int ldv, const double* T, int
 // C (m <= kNC rows x n) <- C R^{-1}, R upper triangular (n x n), blocked by 32
 // columns: C(:, J) -= C(:, 0:j0) R(0:j0, J) through shared-memory tiles, then
 // the 32 x 32 diagonal block is solved one row per thread.
-__device__ void tile_trsm_right_upper(const double* R, int ldr, double* C, int ldc, int m, int n, double* sm) {
-  double* sR = sm;                      // [kRT][kNB+1]  R(l0+l, j0+j)
-  double* sC = sR + kRT * (kNB + 1);    // [kNC][kRT+1]  C(r, l0+l), later the solved block
+template <typename T>
+__device__ void tile_trsm_right_upper(const T* R, int ldr, T* C, int ldc, int m, int n, T* sm) {
+  T* sR = sm;                      // [kRT][kNB+1]  R(l0+l, j0+j)
+  T* sC = sR + kRT * (kNB + 1);    // [kNC][kRT+1]  C(r, l0+l), later the solved block
   const int t = threadIdx.x;
   const int tj = t & 7, tr = t >> 3;    // cols tj*4..+3, rows tr*2..+1
   for (int j0 = 0; j0 < n; j0 += kNB) {
     const int jb = (n - j0) < kNB ? (n - j0) : kNB;
-    double acc[2][4] = {{0, 0, 0, 0}, {0, 0, 0, 0}};
+    T acc[2][4] = {{0, 0, 0, 0}, {0, 0, 0, 0}};
     for (int l0 = 0; l0 < j0; l0 += kRT) {
       for (int idx = t; idx < kRT * kNB; idx += kThreads) {
         const int l = idx % kRT, j = idx / kRT;
@@ -562,10 +581,10 @@ __device__ void tile_trsm_right_upper(const double* R, int ldr, double* C, int l
       __syncthreads();
 #pragma unroll 4
       for (int l = 0; l < kRT; ++l) {
-        const double a0 = sC[(tr * 2) * (kRT + 1) + l], a1 = sC[(tr * 2 + 1) * (kRT + 1) + l];
+        const T a0 = sC[(tr * 2) * (kRT + 1) + l], a1 = sC[(tr * 2 + 1) * (kRT + 1) + l];
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
-          const double rv = sR[l * (kNB + 1) + tj * 4 + q];
+          const T rv = sR[l * (kNB + 1) + tj * 4 + q];
           acc[0][q] += a0 * rv;
           acc[1][q] += a1 * rv;
         }
@@ -586,9 +605,9 @@ __device__ void tile_trsm_right_upper(const double* R, int ldr, double* C, int l
       }
     __syncthreads();
     for (int r = t; r < m; r += kThreads) {
-      double* cr = sC + r * (kRT + 1);
+      T* cr = sC + r * (kRT + 1);
       for (int j = 0; j < jb; ++j) {
-        double s = cr[j];
+        T s = cr[j];
         for (int l = 0; l < j; ++l) s -= cr[l] * sR[l * (kNB + 1) + j];
         cr[j] = s / sR[j * (kNB + 1) + j];
       }
@@ -603,11 +622,12 @@ __device__ void tile_trsm_right_upper(const double* R, int ldr, double* C, int l
 }
 
 // C (m x n) <- C R^{-1}, R upper triangular (n x n).  One thread per row.
-__device__ void trsm_right_upper(const double* R, int ldr, double* C, int ldc, int m, int n) {
+template <typename T>
+__device__ void trsm_right_upper(const T* R, int ldr, T* C, int ldc, int m, int n) {
   for (int r = threadIdx.x; r < m; r += kThreads) {
     for (int j = 0; j < n; ++j) {
-      double s = C[r + (size_t)j * ldc];
-      const double* rj = R + (size_t)j * ldr;
+      T s = C[r + (size_t)j * ldc];
+      const T* rj = R + (size_t)j * ldr;
       for (int i = 0; i < j; ++i) s -= C[r + (size_t)i * ldc] * rj[i];
       C[r + (size_t)j * ldc] = s / rj[j];
     }
@@ -617,16 +637,17 @@ __device__ void trsm_right_upper(const double* R, int ldr, double* C, int ldc, i
 
 // Upper triangular solve x <- R^{-1} x (n x n), blocked by 32: one warp solves
 // each diagonal block with shuffles, the CTA updates the rows above.
-__device__ void trsv_upper(const double* R, int ldr, double* x, int n, double* xs /*shared >= 32*/) {
+template <typename T>
+__device__ void trsv_upper(const T* R, int ldr, T* x, int n, T* xs /*shared >= 32*/) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   for (int hi = n; hi > 0; hi -= 32) {
     const int lo = hi > 32 ? hi - 32 : 0;
     const int bs = hi - lo;
     if (warp == 0) {
-      double xv = lane < bs ? x[lo + lane] : 0.0;
+      T xv = lane < bs ? x[lo + lane] : 0.0;
       for (int j = bs - 1; j >= 0; --j) {
         if (lane == j) xv = xv / R[(lo + j) + (size_t)(lo + j) * ldr];
-        const double xj = __shfl_sync(0xffffffffu, xv, j);
+        const T xj = __shfl_sync(0xffffffffu, xv, j);
         if (lane < j) xv -= R[(lo + lane) + (size_t)(lo + j) * ldr] * xj;
       }
       if (lane < bs) {
@@ -636,7 +657,7 @@ __device__ void trsv_upper(const double* R, int ldr, double* x, int n, double* x
     }
     __syncthreads();
     for (int r = threadIdx.x; r < lo; r += kThreads) {
-      double s = 0.0;
+      T s = 0.0;
       for (int j = 0; j < bs; ++j) s += R[r + (size_t)(lo + j) * ldr] * xs[j];
       x[r] -= s;
     }

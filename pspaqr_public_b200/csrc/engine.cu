@@ -190,6 +190,9 @@ int Tree::assemble() {
   const int n = st_.n;
   const int ncl = (int)st_.clusters.size();
   const int ned = (int)st_.edges.size();
+  // factor storage is fixed here: float for the mixed-precision factorization
+  fp32_ = precision == 32;
+  set_factor_fp32(fp32_);
   size_.assign(ncl, 0);
   size_org_.assign(ncl, 0);
   rpos_.assign(ncl, 0);
@@ -232,7 +235,7 @@ int Tree::assemble() {
       const int i = P.rowidx[k];
       const int ri = leaf_of[i];
       const int e = st_.find_edge(cj, ri);
-      dst[k] = ptr_[e] + (i - st_.clusters[ri].cstart) + (size_t)(j - st_.clusters[cj].cstart) * ld_[e];
+      dst[k] = elem(ptr_[e], (i - st_.clusters[ri].cstart) + (size_t)(j - st_.clusters[cj].cstart) * ld_[e]);
     }
   }
   // CSR of App for the SpMV (y = App x)
@@ -294,6 +297,7 @@ static int cluster_for(int ncols) {
 
 int Tree::factorize() {
   if (!assembled_) return fail(-4, "factorize called before assemble");
+  set_factor_fp32(fp32_);
   if (factorized_) return fail(-4, "factorize called twice; assemble again first");
   double t0 = wall();
   const int L = st_.nlevels;
@@ -470,7 +474,9 @@ int Tree::factorize() {
       const size_t nsp = Lv.spars_clusters.size();
       std::vector<RrqrSrc> rs;
       std::vector<int> sp_w(nsp), sp_ldw(nsp);
-      std::vector<double*> sp_C(nsp);
+      std::vector<double*> sp_C(nsp), spV(nsp), spT(nsp);
+      std::vector<int> sp_q(st_.clusters.size(), -1);  // interface -> index in this level's list
+      for (size_t q = 0; q < nsp; ++q) sp_q[Lv.spars_clusters[q]] = (int)q;
       std::vector<std::pair<double, double>> rr_dims;
       std::vector<int> rr_cs(nsp, 0);
       std::vector<char> plain_qr(nsp, 1);            // interface ran the plain pivoted QR on C
@@ -503,6 +509,10 @@ int Tree::factorize() {
         Qsp_[p] = arena_.dalloc((size_t)std::max(mp, 1) * std::max(mp, 1));
         Tsp_[p] = arena_.dalloc((size_t)NB * std::max(mp, 1));
         if (!Qsp_[p] || !Tsp_[p]) return fail(-11, "out of device memory (rrqr)");
+        // the pivoted QR writes double; float factors get a converted copy
+        spV[q] = fp32_ ? scratch_.dalloc((size_t)std::max(mp, 1) * std::max(mp, 1)) : Qsp_[p];
+        spT[q] = fp32_ ? scratch_.dalloc((size_t)NB * std::max(mp, 1)) : Tsp_[p];
+        if (!spV[q] || !spT[q]) return fail(-11, "out of device memory (rrqr)");
         rr_dims.push_back({(double)mp, (double)w});
       }
       // pivoted-QR launch groups by cluster size 1, 2, 4, 8, 16
@@ -546,8 +556,8 @@ int Tree::factorize() {
         t.Q = scratch_.dalloc((size_t)std::max(mp, 1) * t.ldq);
         t.Qc = Qc ? Qc : scratch_.dalloc((size_t)std::max(mp, 1) * t.ldq);
         t.F = scratch_.dalloc((size_t)std::max(w, 1) * t.ldq);
-        t.V = Qsp_[p];
-        t.T = Tsp_[p];
+        t.V = spV[sp_q[p]];
+        t.T = spT[sp_q[p]];
         t.tau = scratch_.dalloc(std::max(mp, 1));
         t.colat = static_cast<int*>(scratch_.alloc(sizeof(int) * std::max(w, 1)));
         t.rank = rank;
@@ -668,7 +678,7 @@ int Tree::factorize() {
         }
         auto* d_sk = static_cast<SketchTask*>(up_any(sk));
         if (!d_sk) return fail(-11, "out of device memory (rank features)");
-        if (ck(launch_rank_features(d_sk, (int)nsp, st_.tol, mmax, wmax, stream_), "rank features")) return -10;
+        if (ck(launch_rank_features(d_sk, (int)nsp, tol, mmax, wmax, stream_), "rank features")) return -10;
         if (rank_model_) {
           RankModel model{d_model_, d_model_ + kMlpParams, d_model_ + kMlpParams + kRankFeatures, oversample_};
           if (ck(launch_rank_predict(d_sk, (int)nsp, model, stream_), "rank prediction")) return -10;
@@ -682,7 +692,7 @@ int Tree::factorize() {
                               d_stats ? d_stats + 8 * q : nullptr, work_cap(level_work, rrqr_work));
           if (!rr_cs[q]) return -12;
         }
-        if (int rc = run_rrqr(G, st_.tol)) return rc;
+        if (int rc = run_rrqr(G, tol)) return rc;
       } else {
         // learned ranks: sketch widths back on the host to plan the sketch
         // GEMMs; pivoted QR of the sketches, projections, rank choice; the
@@ -738,11 +748,11 @@ int Tree::factorize() {
         cudaEventRecord(le[1], stream_);
         if (ck(launch_sketch(d_sk, d_skt, (int)sk_tiles.size(), stream_), "sketch")) return -10;
         cudaEventRecord(le[2], stream_);
-        if (int rc = run_rrqr(G, sketch_tol * st_.tol)) return rc;
+        if (int rc = run_rrqr(G, sketch_tol * tol)) return rc;
         cudaEventRecord(le[3], stream_);
         if (ck(launch_project(d_sk, d_pjt, (int)pj_tiles.size(), stream_), "projection") ||
             ck(launch_residual_scan(d_sk, d_scb, (int)scan_blocks.size(), stream_), "residual scan") ||
-            ck(launch_rank_select(d_sk, (int)nsp, st_.tol, stream_), "rank selection"))
+            ck(launch_rank_select(d_sk, (int)nsp, tol, stream_), "rank selection"))
           return -10;
         cudaEventRecord(le[4], stream_);
         std::vector<int> fb(nsp);
@@ -770,7 +780,7 @@ int Tree::factorize() {
             ++learned_accepted_;
           }
         }
-        if (int rc = run_rrqr(Fb, st_.tol)) return rc;
+        if (int rc = run_rrqr(Fb, tol)) return rc;
         cudaEventRecord(le[5], stream_);
         if (verbose >= 2) {
           cudaEventSynchronize(le[5]);
@@ -782,6 +792,17 @@ int Tree::factorize() {
                  ms[2], ms[3], nfb, ms[4]);
         }
         for (auto& e : le) cudaEventDestroy(e);
+      }
+      if (fp32_ && nsp) {
+        std::vector<ConvTask> cv;
+        for (size_t q = 0; q < nsp; ++q) {
+          const int p = Lv.spars_clusters[q];
+          const long long mp = std::max(size_[p], 1);
+          cv.push_back({spV[q], Qsp_[p], mp * mp});
+          cv.push_back({spT[q], Tsp_[p], (long long)NB * mp});
+        }
+        auto* d_cv = static_cast<ConvTask*>(up_any(cv));
+        if (!d_cv || ck(launch_to_f32_batch(d_cv, (int)cv.size(), stream_), "factor conversion")) return -10;
       }
       cudaEventRecord(fe[2], stream_);
       if (ck(launch_edge(2, d_right, (int)right.size(), stream_), "right compression") ||
@@ -902,7 +923,7 @@ int Tree::factorize() {
   if (rc) return rc;
   t_factorize = wall() - t0;
   if (verbose) {
-    printf("Tolerance set: %e\n", st_.tol);
+    printf("Tolerance set: %e\n", tol);
     printf("Time to factorize:  %g\n", t_factorize);
   }
   return 0;
@@ -929,6 +950,7 @@ int Tree::alloc_level_blocks(const std::vector<int>& edges) {
 // Cluster vectors: level-0 clusters at their permuted columns [0, n); every
 // later cluster gets its own segment of its level size.
 int Tree::build_solve_graph() {
+  set_factor_fp32(fp32_);
   const int L = st_.nlevels;
   const int ncl = (int)st_.clusters.size();
   xoff_.assign(ncl, 0);
@@ -978,7 +1000,7 @@ int Tree::build_solve_graph() {
       FwdElimTask t;
       t.S = ptr_[Lv.self_edge_of[c - Lv.first]];
       t.T = T_[c];
-      t.x = d_xw_ + xoff_[c];
+      t.x = elem(d_xw_, xoff_[c]);
       t.n = size_[c];
       t.out_begin = (int)fo.size();
       for (int q = Lv.out_begin[ii]; q < Lv.out_end[ii]; ++q) {
@@ -987,7 +1009,7 @@ int Tree::build_solve_graph() {
         FwdOut o;
         o.V = ptr_[e];
         o.T = tsqrtT_[e];
-        o.xn = d_xw_ + xoff_[nb];
+        o.xn = elem(d_xw_, xoff_[nb]);
         o.turn = d_turn_ + nb;
         o.m = rows_[e];
         o.my_turn = seen[nb - Lv.first]++;
@@ -1006,7 +1028,7 @@ int Tree::build_solve_graph() {
       t.V = Qsp_[p];
       t.T = Tsp_[p];
       t.rank = d_rank_ + p;
-      t.x = d_xw_ + xoff_[p];
+      t.x = elem(d_xw_, xoff_[p]);
       t.n = size_org_[p];
       fs.push_back(t);
       S.fs_nmax = std::max(S.fs_nmax, t.n);
@@ -1017,7 +1039,7 @@ int Tree::build_solve_graph() {
       const int c = Lv.interiors[ii];
       BwdElimTask t;
       t.S = ptr_[Lv.self_edge_of[c - Lv.first]];
-      t.x = d_xw_ + xoff_[c];
+      t.x = elem(d_xw_, xoff_[c]);
       t.n = size_[c];
       t.in_begin = (int)bi.size();
       for (int q = Lv.in_begin[ii]; q < Lv.in_end[ii]; ++q) {
@@ -1026,7 +1048,7 @@ int Tree::build_solve_graph() {
         b.R = ptr_[e];
         b.ldr = ld_[e];
         b.s = cols_[e];
-        b.xm = d_xw_ + xoff_[st_.edges[e].n1];
+        b.xm = elem(d_xw_, xoff_[st_.edges[e].n1]);
         bi.push_back(b);
       }
       t.in_end = (int)bi.size();
@@ -1096,10 +1118,20 @@ int Tree::build_solve_graph() {
 int Tree::solve_device(double* x) {
   if (!factorized_) return fail(-4, "solve called before factorize");
   const int n = st_.n;
-  cudaMemcpyAsync(d_xw_, x, sizeof(double) * n, cudaMemcpyDeviceToDevice, stream_);
+  set_factor_fp32(fp32_);
+  if (fp32_) {
+    // the preconditioner applies in the factors' precision
+    if (check_cuda(launch_to_f32(n, x, d_xw_, stream_), "solve input")) return -10;
+  } else {
+    cudaMemcpyAsync(d_xw_, x, sizeof(double) * n, cudaMemcpyDeviceToDevice, stream_);
+  }
   if (check_cuda(cudaGraphLaunch(solve_exec_, stream_), "solve graph")) return -10;
   add_kernel_launches(solve_graph_kernels_);
-  cudaMemcpyAsync(x, d_xw_, sizeof(double) * n, cudaMemcpyDeviceToDevice, stream_);
+  if (fp32_) {
+    if (check_cuda(launch_to_f64(n, d_xw_, x, stream_), "solve output")) return -10;
+  } else {
+    cudaMemcpyAsync(x, d_xw_, sizeof(double) * n, cudaMemcpyDeviceToDevice, stream_);
+  }
   return 0;
 }
 
@@ -1146,6 +1178,7 @@ int Tree::spmv_host(const double* x, double* y) {
 // On exit b holds the solution; relres is the true ||b - A x|| / ||b||.
 int Tree::gmres_device(double* b, int maxit, double gtol, int* iters, double* relres, double* hist, int hist_cap) {
   if (!factorized_) return fail(-4, "gmres called before factorize");
+  if (krylov == 1 || (krylov < 0 && fp32_)) return fgmres_device(b, maxit, gtol, iters, relres, hist, hist_cap);
   if (maxit < 1) return fail(-1, "maxit must be >= 1");
   double t0 = wall();
   const int n = st_.n;
@@ -1365,6 +1398,108 @@ int Tree::set_rank_model(const float* params, const float* mean, const float* st
   return 0;
 }
 
+// Flexible (right-preconditioned) GMRES: z_k = M^-1 v_k is kept, the Arnoldi
+// relation is built on A z_k and x = Z y, so the Givens residual is the true
+// residual ||b - A x|| (in exact arithmetic) whatever the accuracy of the
+// preconditioner.  Used with the float factorization, whose preconditioner
+// apply would contaminate the left-preconditioned residual below ~1e-7.
+// No reference counterpart (the reference's is.cpp:447-527 is left GMRES).
+int Tree::fgmres_device(double* b, int maxit, double gtol, int* iters, double* relres, double* hist, int hist_cap) {
+  if (!factorized_) return fail(-4, "gmres called before factorize");
+  if (maxit < 1) return fail(-1, "maxit must be >= 1");
+  double t0 = wall();
+  const int n = st_.n;
+  const size_t ldq = (size_t)n;
+  const int grid = mgs_grid(n);
+  // workspace: V (n x maxit+1) | Z (n x maxit) | q | b | H column | partial sums | counter
+  const size_t need = ldq * (2 * (size_t)maxit + 1) + 2 * (size_t)n + (maxit + 3) + grid + 1;
+  if (int erc = ensure_krylov(need)) return erc;
+  double* Q = d_krylov_;
+  double* Z = Q + ldq * (maxit + 1);
+  double* q = Z + ldq * maxit;
+  double* bsave = q + n;
+  double* hcol = bsave + n;
+  double* partial = hcol + (maxit + 3);
+  unsigned int* done = reinterpret_cast<unsigned int*>(partial + grid);
+  cudaError_t ge = cudaSuccess;
+  auto g = [&](cudaError_t e) {
+    if (!ge) ge = e;
+  };
+  g(cudaMemsetAsync(done, 0, sizeof(unsigned int), stream_));
+  g(cudaMemcpyAsync(bsave, b, sizeof(double) * n, cudaMemcpyDeviceToDevice, stream_));
+  g(cudaMemcpyAsync(q, b, sizeof(double) * n, cudaMemcpyDeviceToDevice, stream_));
+  g(launch_mgs_step(n, q, nullptr, nullptr, nullptr, partial, done, hcol, 1, stream_));  // ||b||
+  g(launch_scale_copy(n, q, hcol, Q, stream_));
+  double r_norm = 0;
+  g(cudaMemcpyAsync(&r_norm, hcol, sizeof(double), cudaMemcpyDeviceToHost, stream_));
+  int rc = check_cuda(ge ? ge : cudaStreamSynchronize(stream_), "gmres start");
+  std::vector<double> H((size_t)(maxit + 1) * maxit, 0.0), cs(maxit, 0.0), sn(maxit, 0.0), beta(maxit + 1, 0.0);
+  auto Hc = [&](int i, int j) -> double& { return H[(size_t)j * (maxit + 1) + i]; };
+  beta[0] = r_norm;
+  int k = 0, nh = 0;
+  std::vector<double> hk(maxit + 2);
+  if (!rc && !(r_norm > 0)) rc = fail(-1, "zero or invalid right-hand side");
+  for (; !rc && k < maxit; ++k) {
+    double* zk = Z + (size_t)k * ldq;
+    g(cudaMemcpyAsync(zk, Q + (size_t)k * ldq, sizeof(double) * n, cudaMemcpyDeviceToDevice, stream_));
+    if ((rc = solve_device(zk)) || (rc = spmv_device(zk, q))) break;
+    for (int i = 0; i <= k; ++i)
+      g(launch_mgs_step(n, q, i ? Q + (size_t)(i - 1) * ldq : nullptr, i ? hcol + (i - 1) : nullptr,
+                        Q + (size_t)i * ldq, partial, done, hcol + i, 0, stream_));
+    g(launch_mgs_step(n, q, Q + (size_t)k * ldq, hcol + k, nullptr, partial, done, hcol + k + 1, 1, stream_));
+    g(launch_scale_copy(n, q, hcol + k + 1, Q + (size_t)(k + 1) * ldq, stream_));
+    g(cudaMemcpyAsync(hk.data(), hcol, sizeof(double) * (k + 2), cudaMemcpyDeviceToHost, stream_));
+    if ((rc = check_cuda(ge ? ge : cudaStreamSynchronize(stream_), "gmres iteration"))) break;
+    for (int i = 0; i <= k + 1; ++i) Hc(i, k) = hk[i];
+    for (int i = 0; i < k; ++i) {
+      const double temp = cs[i] * Hc(i, k) + sn[i] * Hc(i + 1, k);
+      Hc(i + 1, k) = -sn[i] * Hc(i, k) + cs[i] * Hc(i + 1, k);
+      Hc(i, k) = temp;
+    }
+    if (Hc(k, k) == 0) {
+      cs[k] = 0;
+      sn[k] = 1;
+    } else {
+      const double t = std::sqrt(Hc(k, k) * Hc(k, k) + Hc(k + 1, k) * Hc(k + 1, k));
+      cs[k] = std::fabs(Hc(k, k)) / t;
+      sn[k] = cs[k] * Hc(k + 1, k) / Hc(k, k);
+    }
+    Hc(k, k) = cs[k] * Hc(k, k) + sn[k] * Hc(k + 1, k);
+    Hc(k + 1, k) = 0.0;
+    beta[k + 1] = -sn[k] * beta[k];
+    beta[k] = cs[k] * beta[k];
+    const double err = std::fabs(beta[k + 1]) / r_norm;
+    if (hist && nh < hist_cap) hist[nh++] = err;
+    if (verbose) printf("FGMRES: error at step %d is %e\n", k, err);
+    if (err <= gtol) break;
+  }
+  if (!rc && device_status() != 0) rc = fail(-12, "forward sweep wait timed out on the device");
+  if (!rc) {
+    k = std::min(k, maxit - 1);
+    std::vector<double> y(k + 1, 0.0);
+    for (int i = k; i >= 0; --i) {
+      y[i] = beta[i];
+      for (int j = i + 1; j < k + 1; ++j) y[i] -= Hc(i, j) * y[j];
+      y[i] /= Hc(i, i);
+    }
+    double* dy = hcol;
+    g(cudaMemcpyAsync(dy, y.data(), sizeof(double) * (k + 1), cudaMemcpyHostToDevice, stream_));
+    g(launch_combine(n, k + 1, Z, ldq, dy, b, stream_));
+    g(spmv_device(b, q) ? cudaErrorUnknown : cudaSuccess);
+    g(launch_sub(n, bsave, q, q, stream_));
+    g(launch_mgs_step(n, q, nullptr, nullptr, nullptr, partial, done, hcol, 1, stream_));
+    g(launch_mgs_step(n, bsave, nullptr, nullptr, nullptr, partial, done, hcol + 1, 1, stream_));
+    double nr[2] = {0, 1};
+    g(cudaMemcpyAsync(nr, hcol, sizeof(double) * 2, cudaMemcpyDeviceToHost, stream_));
+    rc = check_cuda(ge ? ge : cudaStreamSynchronize(stream_), "gmres finish");
+    *iters = k;
+    *relres = nr[0] / nr[1];
+    last_gmres_iters = k;
+  }
+  t_gmres = wall() - t0;
+  return rc;
+}
+
 int Tree::ensure_krylov(size_t doubles) {
   if (doubles <= krylov_doubles_) return 0;
   cudaFree(d_krylov_);
@@ -1390,13 +1525,28 @@ int Tree::gmres_host(double* b, int maxit, double gtol, int* iters, double* relr
   return rc;
 }
 
+double* Tree::elem(double* p, size_t off) const {
+  return fp32_ ? reinterpret_cast<double*>(reinterpret_cast<float*>(p) + off) : p + off;
+}
+
+// n elements of a factor array at element offset off, widened to double
+void Tree::read_elems(const double* p, size_t off, size_t n, double* out) const {
+  if (!fp32_) {
+    cudaMemcpy(out, p + off, sizeof(double) * n, cudaMemcpyDeviceToHost);
+    return;
+  }
+  std::vector<float> f(n);
+  cudaMemcpy(f.data(), reinterpret_cast<const float*>(p) + off, sizeof(float) * n, cudaMemcpyDeviceToHost);
+  for (size_t i = 0; i < n; ++i) out[i] = f[i];
+}
+
 int Tree::get_block(int n1, int n2, double* out, int* rows, int* cols, int* ld) const {
   const int e = st_.find_edge(n1, n2);
   if (e < 0 || e >= (int)ptr_.size() || !ptr_[e]) return -1;
   *rows = rows_[e];
   *cols = cols_[e];
   *ld = ld_[e];
-  if (out) cudaMemcpy(out, ptr_[e], sizeof(double) * (size_t)ld_[e] * cols_[e], cudaMemcpyDeviceToHost);
+  if (out) read_elems(ptr_[e], 0, (size_t)ld_[e] * cols_[e], out);
   return 0;
 }
 
@@ -1420,7 +1570,7 @@ int Tree::get_factor(int order, int which, double* out, int* shape) const {
   shape[1] = c;
   shape[2] = ld;
   if (out)
-    for (int j = 0; j < c; ++j) cudaMemcpy(out + (size_t)j * r, p + (size_t)j * ld, sizeof(double) * r, cudaMemcpyDeviceToHost);
+    for (int j = 0; j < c; ++j) read_elems(p, (size_t)j * ld, r, out + (size_t)j * r);
   return 0;
 }
 

@@ -67,6 +67,14 @@ class Tree {
   double rrqr_work = 65536;
   // ... and a level's compression work is spread over about rrqr_fill CTAs per SM
   double rrqr_fill = 2;
+  // factor storage and preconditioner arithmetic: 64 (plain) or 32 (mixed
+  // precision: float blocks and solve, double SpMV, Krylov loop and pivoted
+  // QR of the compression matrices); takes effect at the next assemble
+  int precision = 64;
+  // Krylov method of gmres: 0 = left-preconditioned GMRES (is.cpp:447-527),
+  // 1 = flexible right-preconditioned GMRES, -1 (default) = flexible exactly
+  // when the factors are float
+  int krylov = -1;
   // learned ranks: the sketch's pivoted QR stops at sketch_tol * tol (the
   // kept rank is then chosen on C itself)
   double sketch_tol = 0.1;
@@ -84,6 +92,7 @@ class Tree {
   int spmv_host(const double* x, double* y);
   int gmres_host(double* b, int maxit, double tol, int* iters, double* relres, double* hist, int hist_cap);
   int gmres_device(double* b_dev, int maxit, double tol, int* iters, double* relres, double* hist, int hist_cap);
+  int fgmres_device(double* b, int maxit, double gtol, int* iters, double* relres, double* hist, int hist_cap);
   // gmres_device on a caller-given device workspace of ws_doubles doubles,
   // with fixed host arrays (maxit <= kNoAllocMaxit); allocates nothing
   int gmres_device_fixed(double* b, int maxit, double gtol, int* iters, double* relres, double* ws, size_t ws_doubles);
@@ -181,6 +190,10 @@ class Tree {
   std::vector<LevelTiming> lt_;
   double flops_ = 0;
   double rrqr_bytes_ = 0;
+  bool fp32_ = false;  // factor blocks hold float (set by assemble)
+  // address of element off of a factor array (element size by precision)
+  double* elem(double* p, size_t off) const;
+  void read_elems(const double* p, size_t off, size_t n, double* out) const;
 
   // learned ranks (learned.hpp): model on the device (params | mean | std),
   // logged training pairs, counters since the last set_rank_model

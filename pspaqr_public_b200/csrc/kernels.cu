@@ -39,8 +39,21 @@ __device__ __forceinline__ int crank(int cs) { return cs > 1 ? (int)cg::this_clu
 __device__ __forceinline__ bool owns(int col, int rank, int cs) { return ((col / kNB) % cs) == rank; }
 
 // ------------------------------------------------------------ assembly
+// Factor blocks hold T (double, or float in the mixed-precision
+// factorization); descriptors carry their addresses as double*.
+template <typename T>
+__device__ __forceinline__ T* as(double* p) {
+  return reinterpret_cast<T*>(p);
+}
+template <typename T>
+__device__ __forceinline__ const T* as(const double* p) {
+  return reinterpret_cast<const T*>(p);
+}
+
+template <typename T>
 __global__ void k_scatter(int nnz, const double* __restrict__ val, double* const* __restrict__ dst) {
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nnz; i += gridDim.x * blockDim.x) *dst[i] = val[i];
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nnz; i += gridDim.x * blockDim.x)
+    *as<T>(dst[i]) = (T)val[i];
 }
 
 // ------------------------------------------------------------ distributed Householder QR
@@ -49,22 +62,23 @@ __global__ void k_scatter(int nnz, const double* __restrict__ val, double* const
 // after the cluster barrier every CTA loads the tail into shared `vb` and
 // applies H_j to its own columns k > j.  `lt` holds the owner's tau values for
 // its panels (T factors), `tg` broadcasts tau through global memory.
-__device__ void dist_qr(double* R, int ldr, double* B, int ldb, int m, int n, int unit, double* Tout, double* tg,
-                        double* lt, double* vb, double* red, double* tmp, int cs) {
+template <typename T>
+__device__ void dist_qr(T* R, int ldr, T* B, int ldb, int m, int n, int unit, T* Tout, T* tg,
+                        T* lt, T* vb, T* red, T* tmp, int cs) {
   const int rank = crank(cs);
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   // unit: reflector tails live in R itself (rows j+1..m-1 of column j), m rows
   // pentagonal: tails are the m rows of B, the diagonal lives in R
   for (int j = 0; j < n; ++j) {
     const int vlen = unit ? (m - j - 1) : m;
-    double* tail = unit ? (R + (j + 1) + (size_t)j * ldr) : (B + (size_t)j * ldb);
+    T* tail = unit ? (R + (j + 1) + (size_t)j * ldr) : (B + (size_t)j * ldb);
     if (owns(j, rank, cs)) {
-      double s = 0.0;
+      T s = 0.0;
       for (int i = threadIdx.x; i < vlen; i += kThreads) s += tail[i] * tail[i];
       s = dev::cta_sum(s, red);
-      const double alpha = R[j + (size_t)j * ldr];
-      double beta, scal;
-      const double tj = dev::house(alpha, s, &beta, &scal);
+      const T alpha = R[j + (size_t)j * ldr];
+      T beta, scal;
+      const T tj = dev::house(alpha, s, &beta, &scal);
       if (tj != 0.0)
         for (int i = threadIdx.x; i < vlen; i += kThreads) tail[i] *= scal;
       __syncthreads();
@@ -76,16 +90,16 @@ __device__ void dist_qr(double* R, int ldr, double* B, int ldb, int m, int n, in
       __threadfence();
     }
     csync(cs);
-    const double tj = __ldcg(tg + j);
+    const T tj = __ldcg(tg + j);
     if (tj != 0.0) {
       for (int i = threadIdx.x; i < vlen; i += kThreads) vb[i] = __ldcg(tail + i);
       __syncthreads();
       // apply H_j to own columns k > j
       for (int k = j + 1 + warp; k < n; k += kWarps) {
         if (!owns(k, rank, cs)) continue;
-        double* rjk = R + j + (size_t)k * ldr;
-        double* tk = unit ? (R + (j + 1) + (size_t)k * ldr) : (B + (size_t)k * ldb);
-        double d = lane == 0 ? *rjk : 0.0;
+        T* rjk = R + j + (size_t)k * ldr;
+        T* tk = unit ? (R + (j + 1) + (size_t)k * ldr) : (B + (size_t)k * ldb);
+        T d = lane == 0 ? *rjk : 0.0;
         for (int i = lane; i < vlen; i += 32) d += vb[i] * tk[i];
         d = dev::warp_sum(d) * tj;
         if (lane == 0) *rjk -= d;
@@ -105,49 +119,58 @@ __device__ void dist_qr(double* R, int ldr, double* B, int ldb, int m, int n, in
   csync(cs);
 }
 
+template <typename T>
 __global__ void __launch_bounds__(kThreads) k_elim(const ElimTask* __restrict__ tasks, const ElimOut* __restrict__ outs,
                                                    int cs, int vmax) {
-  extern __shared__ double sm[];
+  extern __shared__ __align__(16) unsigned char smraw[];
+  T* sm = reinterpret_cast<T*>(smraw);
   const ElimTask t = tasks[blockIdx.x / cs];
-  double* red = sm;
-  double* tmp = red + kRed;
-  double* lt = tmp + kNB;
-  double* vb = lt + t.n;
+  T* red = sm;
+  T* tmp = red + kRed;
+  T* lt = tmp + kNB;
+  T* vb = lt + t.n;
   (void)vmax;
-  dist_qr(t.S, t.n, nullptr, 0, t.n, t.n, 1, t.T, t.tau, lt, vb, red, tmp, cs);
+  dist_qr<T>(as<T>(t.S), t.n, nullptr, 0, t.n, t.n, 1, as<T>(t.T), as<T>(t.tau), lt, vb, red, tmp, cs);
   for (int o = t.out_begin; o < t.out_end; ++o) {
     const ElimOut e = outs[o];
-    dist_qr(t.S, t.n, e.B, e.m, e.m, t.n, 0, e.T, t.tau, lt, vb, red, tmp, cs);
+    dist_qr<T>(as<T>(t.S), t.n, as<T>(e.B), e.m, e.m, t.n, 0, as<T>(e.T), as<T>(t.tau), lt, vb, red, tmp, cs);
   }
 }
 
+template <typename T>
 __global__ void __launch_bounds__(kThreads) k_scale(const ScaleTask* __restrict__ tasks, int cs) {
-  extern __shared__ double sm[];
+  extern __shared__ __align__(16) unsigned char smraw[];
+  T* sm = reinterpret_cast<T*>(smraw);
   const ScaleTask t = tasks[blockIdx.x / cs];
-  double* red = sm;
-  double* tmp = red + kRed;
-  double* lt = tmp + kNB;
-  double* vb = lt + t.n;
-  dist_qr(t.S, t.n, nullptr, 0, t.n, t.n, 1, t.T, t.tau, lt, vb, red, tmp, cs);
+  T* red = sm;
+  T* tmp = red + kRed;
+  T* lt = tmp + kNB;
+  T* vb = lt + t.n;
+  dist_qr<T>(as<T>(t.S), t.n, nullptr, 0, t.n, t.n, 1, as<T>(t.T), as<T>(t.tau), lt, vb, red, tmp, cs);
 }
 
 // ------------------------------------------------------------ chunked applies
+template <typename T>
 __global__ void __launch_bounds__(kThreads) k_update(const UpdTask* __restrict__ tasks, const UpdOp* __restrict__ ops) {
-  extern __shared__ double sm[];
+  extern __shared__ __align__(16) unsigned char smraw[];
+  T* sm = reinterpret_cast<T*>(smraw);
   const UpdTask t = tasks[blockIdx.x];
   for (int o = t.op_begin; o < t.op_end; ++o) {
     const UpdOp op = ops[o];
     if (op.kind == 0)
-      dev::mat_apply_qt(op.V, op.ldv, op.T, op.k, op.A + (size_t)t.col0 * op.lda, op.lda, op.m, t.ncols, sm);
+      dev::mat_apply_qt<T>(as<T>(op.V), op.ldv, as<T>(op.T), op.k, as<T>(op.A) + (size_t)t.col0 * op.lda, op.lda, op.m,
+                           t.ncols, sm);
     else
-      dev::mat_apply_tpqt(op.V, op.ldv, op.T, op.k, op.A + (size_t)t.col0 * op.lda, op.lda,
-                          op.B + (size_t)t.col0 * op.ldb, op.ldb, op.m, t.ncols, sm);
+      dev::mat_apply_tpqt<T>(as<T>(op.V), op.ldv, as<T>(op.T), op.k, as<T>(op.A) + (size_t)t.col0 * op.lda, op.lda,
+                             as<T>(op.B) + (size_t)t.col0 * op.ldb, op.ldb, op.m, t.ncols, sm);
   }
 }
 
 // row scaling: columns [lo, lo+cnt) of A <- Qs^T A
+template <typename T>
 __global__ void __launch_bounds__(kThreads) k_edge_left(const EdgeChunk* __restrict__ tasks) {
-  extern __shared__ double sm[];
+  extern __shared__ __align__(16) unsigned char smraw[];
+  T* sm = reinterpret_cast<T*>(smraw);
   const EdgeChunk t = tasks[blockIdx.x];
   const int k = t.kdev ? *t.kdev : t.k;
   int cnt = t.cnt;
@@ -156,22 +179,26 @@ __global__ void __launch_bounds__(kThreads) k_edge_left(const EdgeChunk* __restr
     if (t.lo >= lim) return;
     cnt = min(cnt, lim - t.lo);
   }
-  dev::mat_apply_qt(t.V, t.ldv, t.T, k, t.A + (size_t)t.lo * t.lda, t.lda, t.m, cnt, sm);
+  dev::mat_apply_qt<T>(as<T>(t.V), t.ldv, as<T>(t.T), k, as<T>(t.A) + (size_t)t.lo * t.lda, t.lda, t.m, cnt, sm);
 }
 
 // column scaling: rows [lo, lo+cnt) of A <- A R^{-1}
+template <typename T>
 __global__ void __launch_bounds__(kThreads) k_edge_trsm(const EdgeChunk* __restrict__ tasks) {
-  extern __shared__ double sm[];
+  extern __shared__ __align__(16) unsigned char smraw[];
+  T* sm = reinterpret_cast<T*>(smraw);
   const EdgeChunk t = tasks[blockIdx.x];
-  dev::tile_trsm_right_upper(t.V, t.ldv, t.A + t.lo, t.lda, t.cnt, t.nc, sm);
+  dev::tile_trsm_right_upper<T>(as<T>(t.V), t.ldv, as<T>(t.A) + t.lo, t.lda, t.cnt, t.nc, sm);
 }
 
 // right compression: rows [lo, lo+cnt) of A <- A Q
+template <typename T>
 __global__ void __launch_bounds__(kThreads) k_edge_right(const EdgeChunk* __restrict__ tasks) {
-  extern __shared__ double sm[];
+  extern __shared__ __align__(16) unsigned char smraw[];
+  T* sm = reinterpret_cast<T*>(smraw);
   const EdgeChunk t = tasks[blockIdx.x];
   const int k = t.kdev ? *t.kdev : t.k;
-  dev::mat_apply_q_right(t.V, t.ldv, t.T, k, t.A + t.lo, t.lda, t.cnt, t.nc, sm);
+  dev::mat_apply_q_right<T>(as<T>(t.V), t.ldv, as<T>(t.T), k, as<T>(t.A) + t.lo, t.lda, t.cnt, t.nc, sm);
 }
 
 // ------------------------------------------------------------ RRQR
@@ -202,21 +229,23 @@ __global__ void __launch_bounds__(kThreads) k_edge_right(const EdgeChunk* __rest
 
 // Gathers the compression matrix of every task, transposed: C column c0 + jj
 // is row jj of an out-block A(n,p) or column jj of an in-block A(p,m).
+template <typename T>
 __global__ void __launch_bounds__(kThreads) k_rrqr_assemble(const RrqrSrc* __restrict__ srcs) {
   __shared__ double tile[32][33];
   const RrqrSrc s = srcs[blockIdx.x];
+  const T* SA = as<T>(s.A);
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   double* dst = s.Ct + s.c0;
   if (s.transpose) {
     for (int r = warp; r < s.cols; r += kWarps)
-      for (int jj = lane; jj < s.rows; jj += 32) dst[(size_t)r * s.w + jj] = s.A[jj + (size_t)r * s.lda];
+      for (int jj = lane; jj < s.rows; jj += 32) dst[(size_t)r * s.w + jj] = (double)SA[jj + (size_t)r * s.lda];
     return;
   }
   for (int j0 = 0; j0 < s.cols; j0 += 32)
     for (int r0 = 0; r0 < s.rows; r0 += 32) {
       for (int q = warp; q < 32; q += kWarps) {
         const int r = r0 + lane, j = j0 + q;
-        tile[q][lane] = (r < s.rows && j < s.cols) ? s.A[r + (size_t)j * s.lda] : 0.0;
+        tile[q][lane] = (r < s.rows && j < s.cols) ? (double)SA[r + (size_t)j * s.lda] : 0.0;
       }
       __syncthreads();
       for (int q = warp; q < 32; q += kWarps) {
@@ -704,7 +733,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_rrqr(const RrqrTask* __restrict
     for (int r = lane; r < m; r += 32) t.V[r + (size_t)l * m] = __ldg(Ct + (size_t)r * ldw + c);
   }
   __syncthreads();
-  dist_qr(t.V, m, nullptr, 0, m, rk, 1, t.T, t.tau, S.s1, S.qf, S.red, S.tmp, cs);
+  dist_qr<double>(t.V, m, nullptr, 0, m, rk, 1, t.T, t.tau, S.s1, S.qf, S.red, S.tmp, cs);
   if (rank == 0 && threadIdx.x == 0) {
     *t.rank = rk;
     if (t.stats) t.stats[6] = (int)((clock64() - tq) >> 10);
@@ -712,13 +741,16 @@ __global__ void __launch_bounds__(kThreads, 2) k_rrqr(const RrqrTask* __restrict
 }
 
 // ------------------------------------------------------------ merge
+template <typename T>
 __global__ void k_merge(const MergeTask* __restrict__ tasks) {
   const MergeTask t = tasks[blockIdx.x];
   const int total = t.rows * t.cols;
+  const T* src = as<T>(t.src);
+  T* dst = as<T>(t.dst);
   for (int idx = threadIdx.x; idx < total; idx += blockDim.x) {
     const int i = idx % t.rows, j = idx / t.rows;
-    const double v = t.identity ? (i == j ? 1.0 : 0.0) : t.src[i + (size_t)j * t.ld_src];
-    t.dst[(t.roff + i) + (size_t)(t.coff + j) * t.ld_dst] = v;
+    const T v = t.identity ? (i == j ? (T)1 : (T)0) : src[i + (size_t)j * t.ld_src];
+    dst[(t.roff + i) + (size_t)(t.coff + j) * t.ld_dst] = v;
   }
 }
 
@@ -738,10 +770,12 @@ __device__ __forceinline__ void st_release(int* p, int v) {
 // its step, so the order matches the factorization (order_of_trans).  Waits
 // only target lower tickets, which are held by running CTAs, so the sweep
 // cannot deadlock; a wait that exceeds `spin_limit` cycles sets *status = 2.
+template <typename T>
 __global__ void __launch_bounds__(kThreads) k_fwd_elim(const FwdElimTask* __restrict__ tasks,
                                                        const FwdOut* __restrict__ outs, int ntasks, int* ticket,
                                                        int* status, long long spin_limit, int nmax) {
-  extern __shared__ double sm[];
+  extern __shared__ __align__(16) unsigned char smraw[];
+  T* sm = reinterpret_cast<T*>(smraw);
   __shared__ int s_task, s_abort;
   if (threadIdx.x == 0) {
     s_task = atomicAdd(ticket, 1);
@@ -751,12 +785,12 @@ __global__ void __launch_bounds__(kThreads) k_fwd_elim(const FwdElimTask* __rest
   const int ti = s_task;
   if (ti >= ntasks) return;
   const FwdElimTask t = tasks[ti];
-  double* w = sm;
-  double* xc = w + 2 * kNB;
-  double* xn = xc + (nmax > 0 ? nmax : 1);
-  for (int i = threadIdx.x; i < t.n; i += kThreads) xc[i] = __ldcg(t.x + i);
+  T* w = sm;
+  T* xc = w + 2 * kNB;
+  T* xn = xc + (nmax > 0 ? nmax : 1);
+  for (int i = threadIdx.x; i < t.n; i += kThreads) xc[i] = __ldcg(as<T>(t.x) + i);
   __syncthreads();
-  dev::apply_qt(t.S, t.n, t.T, t.n, xc, t.n, t.n, 1, w, 2 * kNB);
+  dev::apply_qt<T>(as<T>(t.S), t.n, as<T>(t.T), t.n, xc, t.n, t.n, 1, w, 2 * kNB);
   for (int o = t.out_begin; o < t.out_end; ++o) {
     const FwdOut e = outs[o];
     if (threadIdx.x == 0) {
@@ -779,66 +813,74 @@ __global__ void __launch_bounds__(kThreads) k_fwd_elim(const FwdElimTask* __rest
     }
     __syncthreads();
     if (s_abort) return;
-    for (int i = threadIdx.x; i < e.m; i += kThreads) xn[i] = __ldcg(e.xn + i);
+    for (int i = threadIdx.x; i < e.m; i += kThreads) xn[i] = __ldcg(as<T>(e.xn) + i);
     __syncthreads();
-    dev::apply_tpqt(e.V, e.m, e.T, t.n, xc, t.n, xn, e.m, e.m, 1, w, 2 * kNB);
-    for (int i = threadIdx.x; i < e.m; i += kThreads) __stcg(e.xn + i, xn[i]);
+    dev::apply_tpqt<T>(as<T>(e.V), e.m, as<T>(e.T), t.n, xc, t.n, xn, e.m, e.m, 1, w, 2 * kNB);
+    for (int i = threadIdx.x; i < e.m; i += kThreads) __stcg(as<T>(e.xn) + i, xn[i]);
     __syncthreads();
     if (threadIdx.x == 0) {
       __threadfence();
       st_release(e.turn, e.my_turn + 1);
     }
   }
-  for (int i = threadIdx.x; i < t.n; i += kThreads) __stcg(t.x + i, xc[i]);
+  for (int i = threadIdx.x; i < t.n; i += kThreads) __stcg(as<T>(t.x) + i, xc[i]);
 }
 
+template <typename T>
 __global__ void __launch_bounds__(kThreads) k_fwd_spars(const FwdSparsTask* __restrict__ tasks) {
-  extern __shared__ double sm[];
+  extern __shared__ __align__(16) unsigned char smraw[];
+  T* sm = reinterpret_cast<T*>(smraw);
   const FwdSparsTask t = tasks[blockIdx.x];
-  double* w = sm;
-  double* x = sm + 2 * kNB;
-  for (int i = threadIdx.x; i < t.n; i += kThreads) x[i] = t.x[i];
+  T* w = sm;
+  T* x = sm + 2 * kNB;
+  for (int i = threadIdx.x; i < t.n; i += kThreads) x[i] = as<T>(t.x)[i];
   __syncthreads();
-  dev::apply_qt(t.Qs, t.n, t.Ts, t.n, x, t.n, t.n, 1, w, 2 * kNB);
-  dev::apply_qt(t.V, t.n, t.T, *t.rank, x, t.n, t.n, 1, w, 2 * kNB);
-  for (int i = threadIdx.x; i < t.n; i += kThreads) t.x[i] = x[i];
+  dev::apply_qt<T>(as<T>(t.Qs), t.n, as<T>(t.Ts), t.n, x, t.n, t.n, 1, w, 2 * kNB);
+  dev::apply_qt<T>(as<T>(t.V), t.n, as<T>(t.T), *t.rank, x, t.n, t.n, 1, w, 2 * kNB);
+  for (int i = threadIdx.x; i < t.n; i += kThreads) as<T>(t.x)[i] = x[i];
 }
 
+template <typename T>
 __global__ void __launch_bounds__(kThreads) k_bwd_spars(const FwdSparsTask* __restrict__ tasks) {
-  extern __shared__ double sm[];
+  extern __shared__ __align__(16) unsigned char smraw[];
+  T* sm = reinterpret_cast<T*>(smraw);
   const FwdSparsTask t = tasks[blockIdx.x];
-  double* w = sm;
-  double* xs = w + 2 * kNB;
-  double* x = xs + 32;
-  for (int i = threadIdx.x; i < t.n; i += kThreads) x[i] = t.x[i];
+  T* w = sm;
+  T* xs = w + 2 * kNB;
+  T* x = xs + 32;
+  for (int i = threadIdx.x; i < t.n; i += kThreads) x[i] = as<T>(t.x)[i];
   __syncthreads();
-  dev::apply_q(t.V, t.n, t.T, *t.rank, x, t.n, t.n, 1, w, 2 * kNB);
-  dev::trsv_upper(t.Qs, t.n, x, t.n, xs);
-  for (int i = threadIdx.x; i < t.n; i += kThreads) t.x[i] = x[i];
+  dev::apply_q<T>(as<T>(t.V), t.n, as<T>(t.T), *t.rank, x, t.n, t.n, 1, w, 2 * kNB);
+  dev::trsv_upper<T>(as<T>(t.Qs), t.n, x, t.n, xs);
+  for (int i = threadIdx.x; i < t.n; i += kThreads) as<T>(t.x)[i] = x[i];
 }
 
+template <typename T>
 __global__ void __launch_bounds__(kThreads) k_bwd_elim(const BwdElimTask* __restrict__ tasks,
                                                        const BwdIn* __restrict__ ins) {
-  extern __shared__ double sm[];
+  extern __shared__ __align__(16) unsigned char smraw[];
+  T* sm = reinterpret_cast<T*>(smraw);
   const BwdElimTask t = tasks[blockIdx.x];
-  double* xs = sm;
-  double* x = sm + 32;
-  for (int i = threadIdx.x; i < t.n; i += kThreads) x[i] = t.x[i];
+  T* xs = sm;
+  T* x = sm + 32;
+  for (int i = threadIdx.x; i < t.n; i += kThreads) x[i] = as<T>(t.x)[i];
   __syncthreads();
   for (int q = t.in_begin; q < t.in_end; ++q) {
     const BwdIn e = ins[q];
     for (int i = threadIdx.x; i < t.n; i += kThreads) {
-      double s = 0.0;
-      for (int j = 0; j < e.s; ++j) s += e.R[i + (size_t)j * e.ldr] * e.xm[j];
+      T s = 0.0;
+      for (int j = 0; j < e.s; ++j) s += as<T>(e.R)[i + (size_t)j * e.ldr] * as<T>(e.xm)[j];
       x[i] -= s;
     }
   }
   __syncthreads();
-  dev::trsv_upper(t.S, t.n, x, t.n, xs);
-  for (int i = threadIdx.x; i < t.n; i += kThreads) t.x[i] = x[i];
+  dev::trsv_upper<T>(as<T>(t.S), t.n, x, t.n, xs);
+  for (int i = threadIdx.x; i < t.n; i += kThreads) as<T>(t.x)[i] = x[i];
 }
 
-__global__ void k_copy_idx(int n, const int* __restrict__ src, const int* __restrict__ dst, double* x) {
+template <typename T>
+__global__ void k_copy_idx(int n, const int* __restrict__ src, const int* __restrict__ dst, double* xd) {
+  T* x = as<T>(xd);
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) x[dst[i]] = x[src[i]];
 }
 
@@ -920,9 +962,27 @@ inline size_t smem_bytes(size_t doubles) { return doubles * sizeof(double); }
 
 }  // namespace
 
+// ------------------------------------------------------------ precision conversion
+// dst (float) <- src (double), n elements
+__global__ void k_to_f32(long long n, const double* __restrict__ src, float* __restrict__ dst) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    dst[i] = (float)src[i];
+}
+__global__ void k_to_f64(long long n, const float* __restrict__ src, double* __restrict__ dst) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    dst[i] = (double)src[i];
+}
+// batched: one CTA per array
+__global__ void k_to_f32_batch(const ConvTask* __restrict__ tasks) {
+  const ConvTask t = tasks[blockIdx.x];
+  float* dst = reinterpret_cast<float*>(t.dst);
+  for (long long i = threadIdx.x; i < t.n; i += blockDim.x) dst[i] = (float)t.src[i];
+}
+
 // ---------------------------------------------------------------- launchers
 namespace {
 std::atomic<long long> g_launches{0};
+thread_local bool g_fp32 = false;  // factor storage of the next launches
 inline void counted() { g_launches.fetch_add(1, std::memory_order_relaxed); }
 
 constexpr size_t kSmemMax = 227 * 1024;
@@ -966,6 +1026,8 @@ inline cudaError_t begin(const char* name) {
 }  // namespace
 
 const char* last_launch_name() { return g_last_launch; }
+void set_factor_fp32(bool on) { g_fp32 = on; }
+bool factor_fp32() { return g_fp32; }
 void set_last_launch(const char* name) { g_last_launch = name; }
 
 long long kernel_launches() { return g_launches.load(); }
@@ -975,7 +1037,8 @@ cudaError_t launch_scatter(int nnz, const double* val, double* const* dst, cudaS
   if (cudaError_t pre = begin("launch_scatter")) return pre;
   if (nnz <= 0) return cudaSuccess;
   counted();
-  k_scatter<<<grid_for(nnz), 256, 0, st>>>(nnz, val, dst);
+  if (g_fp32) k_scatter<float><<<grid_for(nnz), 256, 0, st>>>(nnz, val, dst);
+  else k_scatter<double><<<grid_for(nnz), 256, 0, st>>>(nnz, val, dst);
   return last();
 }
 
@@ -984,28 +1047,38 @@ cudaError_t launch_elim(const ElimTask* t, const ElimOut* o, int ntasks, int cs,
   if (cudaError_t pre = begin("launch_elim")) return pre;
   if (ntasks <= 0) return cudaSuccess;
   const size_t b = smem_bytes(kRed + kNB + (size_t)nmax + (size_t)std::max(vmax, 1));
-  cudaError_t e = prep(k_elim, b);
-  if (e) return e;
-  return launch_clustered(k_elim, ntasks, cs, b, st, t, o, cs, vmax);
+  if (g_fp32) {
+    if (cudaError_t e = prep(k_elim<float>, b)) return e;
+    return launch_clustered(k_elim<float>, ntasks, cs, b, st, t, o, cs, vmax);
+  }
+  if (cudaError_t e = prep(k_elim<double>, b)) return e;
+  return launch_clustered(k_elim<double>, ntasks, cs, b, st, t, o, cs, vmax);
 }
 
 cudaError_t launch_scale(const ScaleTask* t, int ntasks, int cs, int nmax, cudaStream_t st) {
   if (cudaError_t pre = begin("launch_scale")) return pre;
   if (ntasks <= 0) return cudaSuccess;
   const size_t b = smem_bytes(kRed + kNB + 2 * (size_t)nmax);
-  cudaError_t e = prep(k_scale, b);
-  if (e) return e;
-  return launch_clustered(k_scale, ntasks, cs, b, st, t, cs);
+  if (g_fp32) {
+    if (cudaError_t e = prep(k_scale<float>, b)) return e;
+    return launch_clustered(k_scale<float>, ntasks, cs, b, st, t, cs);
+  }
+  if (cudaError_t e = prep(k_scale<double>, b)) return e;
+  return launch_clustered(k_scale<double>, ntasks, cs, b, st, t, cs);
 }
 
 cudaError_t launch_update(const UpdTask* t, const UpdOp* o, int ntasks, cudaStream_t st) {
   if (cudaError_t pre = begin("launch_update")) return pre;
   if (ntasks <= 0) return cudaSuccess;
   const size_t b = smem_bytes(kWcap);
-  cudaError_t e = prep(k_update, b);
-  if (e) return e;
   counted();
-  k_update<<<ntasks, kThreads, b, st>>>(t, o);
+  if (g_fp32) {
+    if (cudaError_t e = prep(k_update<float>, b)) return e;
+    k_update<float><<<ntasks, kThreads, b, st>>>(t, o);
+  } else {
+    if (cudaError_t e = prep(k_update<double>, b)) return e;
+    k_update<double><<<ntasks, kThreads, b, st>>>(t, o);
+  }
   return last();
 }
 
@@ -1015,17 +1088,21 @@ cudaError_t launch_edge(int kind, const EdgeChunk* t, int ntasks, cudaStream_t s
   const size_t b = smem_bytes(kWcap);
   cudaError_t e = cudaSuccess;
   counted();
-  if (kind == 0) {
-    if ((e = prep(k_edge_left, b))) return e;
-    k_edge_left<<<ntasks, kThreads, b, st>>>(t);
-  } else if (kind == 1) {
-    if ((e = prep(k_edge_trsm, b))) return e;
-    k_edge_trsm<<<ntasks, kThreads, b, st>>>(t);
-  } else {
-    if ((e = prep(k_edge_right, b))) return e;
-    k_edge_right<<<ntasks, kThreads, b, st>>>(t);
-  }
-  return last();
+  auto go = [&](auto* left, auto* trsm, auto* right) -> cudaError_t {
+    if (kind == 0) {
+      if ((e = prep(left, b))) return e;
+      left<<<ntasks, kThreads, b, st>>>(t);
+    } else if (kind == 1) {
+      if ((e = prep(trsm, b))) return e;
+      trsm<<<ntasks, kThreads, b, st>>>(t);
+    } else {
+      if ((e = prep(right, b))) return e;
+      right<<<ntasks, kThreads, b, st>>>(t);
+    }
+    return last();
+  };
+  return g_fp32 ? go(k_edge_left<float>, k_edge_trsm<float>, k_edge_right<float>)
+                : go(k_edge_left<double>, k_edge_trsm<double>, k_edge_right<double>);
 }
 
 size_t rrqr_smem(int mmax, int kmax, int nlmax, int rcmax) {
@@ -1065,7 +1142,8 @@ cudaError_t launch_rrqr_assemble(const RrqrSrc* s, int nsrc, cudaStream_t st) {
   if (cudaError_t pre = begin("launch_rrqr_assemble")) return pre;
   if (nsrc <= 0) return cudaSuccess;
   counted();
-  k_rrqr_assemble<<<nsrc, kThreads, 0, st>>>(s);
+  if (g_fp32) k_rrqr_assemble<float><<<nsrc, kThreads, 0, st>>>(s);
+  else k_rrqr_assemble<double><<<nsrc, kThreads, 0, st>>>(s);
   return last();
 }
 
@@ -1084,7 +1162,8 @@ cudaError_t launch_merge(const MergeTask* t, int ntasks, cudaStream_t st) {
   if (cudaError_t pre = begin("launch_merge")) return pre;
   if (ntasks <= 0) return cudaSuccess;
   counted();
-  k_merge<<<ntasks, 256, 0, st>>>(t);
+  if (g_fp32) k_merge<float><<<ntasks, 256, 0, st>>>(t);
+  else k_merge<double><<<ntasks, 256, 0, st>>>(t);
   return last();
 }
 
@@ -1093,10 +1172,14 @@ cudaError_t launch_fwd_elim(const FwdElimTask* t, const FwdOut* o, int ntasks, i
   if (cudaError_t pre = begin("launch_fwd_elim")) return pre;
   if (ntasks <= 0) return cudaSuccess;
   const size_t b = smem_bytes(2 * kNB + (size_t)std::max(nmax, 1) + (size_t)std::max(mmax, 1));
-  cudaError_t e = prep(k_fwd_elim, b);
-  if (e) return e;
   counted();
-  k_fwd_elim<<<ntasks, kThreads, b, st>>>(t, o, ntasks, ticket, status, spin_limit, nmax);
+  if (g_fp32) {
+    if (cudaError_t e = prep(k_fwd_elim<float>, b)) return e;
+    k_fwd_elim<float><<<ntasks, kThreads, b, st>>>(t, o, ntasks, ticket, status, spin_limit, nmax);
+  } else {
+    if (cudaError_t e = prep(k_fwd_elim<double>, b)) return e;
+    k_fwd_elim<double><<<ntasks, kThreads, b, st>>>(t, o, ntasks, ticket, status, spin_limit, nmax);
+  }
   return last();
 }
 
@@ -1104,10 +1187,14 @@ cudaError_t launch_fwd_spars(const FwdSparsTask* t, int ntasks, int nmax, cudaSt
   if (cudaError_t pre = begin("launch_fwd_spars")) return pre;
   if (ntasks <= 0) return cudaSuccess;
   const size_t b = smem_bytes(2 * kNB + (size_t)nmax);
-  cudaError_t e = prep(k_fwd_spars, b);
-  if (e) return e;
   counted();
-  k_fwd_spars<<<ntasks, kThreads, b, st>>>(t);
+  if (g_fp32) {
+    if (cudaError_t e = prep(k_fwd_spars<float>, b)) return e;
+    k_fwd_spars<float><<<ntasks, kThreads, b, st>>>(t);
+  } else {
+    if (cudaError_t e = prep(k_fwd_spars<double>, b)) return e;
+    k_fwd_spars<double><<<ntasks, kThreads, b, st>>>(t);
+  }
   return last();
 }
 
@@ -1115,10 +1202,14 @@ cudaError_t launch_bwd_spars(const FwdSparsTask* t, int ntasks, int nmax, cudaSt
   if (cudaError_t pre = begin("launch_bwd_spars")) return pre;
   if (ntasks <= 0) return cudaSuccess;
   const size_t b = smem_bytes(2 * kNB + 32 + (size_t)nmax);
-  cudaError_t e = prep(k_bwd_spars, b);
-  if (e) return e;
   counted();
-  k_bwd_spars<<<ntasks, kThreads, b, st>>>(t);
+  if (g_fp32) {
+    if (cudaError_t e = prep(k_bwd_spars<float>, b)) return e;
+    k_bwd_spars<float><<<ntasks, kThreads, b, st>>>(t);
+  } else {
+    if (cudaError_t e = prep(k_bwd_spars<double>, b)) return e;
+    k_bwd_spars<double><<<ntasks, kThreads, b, st>>>(t);
+  }
   return last();
 }
 
@@ -1126,10 +1217,14 @@ cudaError_t launch_bwd_elim(const BwdElimTask* t, const BwdIn* in, int ntasks, i
   if (cudaError_t pre = begin("launch_bwd_elim")) return pre;
   if (ntasks <= 0) return cudaSuccess;
   const size_t b = smem_bytes(32 + (size_t)nmax);
-  cudaError_t e = prep(k_bwd_elim, b);
-  if (e) return e;
   counted();
-  k_bwd_elim<<<ntasks, kThreads, b, st>>>(t, in);
+  if (g_fp32) {
+    if (cudaError_t e = prep(k_bwd_elim<float>, b)) return e;
+    k_bwd_elim<float><<<ntasks, kThreads, b, st>>>(t, in);
+  } else {
+    if (cudaError_t e = prep(k_bwd_elim<double>, b)) return e;
+    k_bwd_elim<double><<<ntasks, kThreads, b, st>>>(t, in);
+  }
   return last();
 }
 
@@ -1137,7 +1232,33 @@ cudaError_t launch_copy_idx(int n, const int* src, const int* dst, double* x, cu
   if (cudaError_t pre = begin("launch_copy_idx")) return pre;
   if (n <= 0) return cudaSuccess;
   counted();
-  k_copy_idx<<<grid_for(n), 256, 0, st>>>(n, src, dst, x);
+  if (g_fp32) k_copy_idx<float><<<grid_for(n), 256, 0, st>>>(n, src, dst, x);
+  else k_copy_idx<double><<<grid_for(n), 256, 0, st>>>(n, src, dst, x);
+  return last();
+}
+
+cudaError_t launch_to_f32(long long n, const double* src, double* dst, cudaStream_t st) {
+  if (cudaError_t pre = begin("launch_to_f32")) return pre;
+  if (n <= 0) return cudaSuccess;
+  counted();
+  k_to_f32<<<grid_for((int)std::min<long long>(n, 1 << 30)), 256, 0, st>>>(n, src, reinterpret_cast<float*>(dst));
+  return last();
+}
+
+cudaError_t launch_to_f64(long long n, const double* src, double* dst, cudaStream_t st) {
+  if (cudaError_t pre = begin("launch_to_f64")) return pre;
+  if (n <= 0) return cudaSuccess;
+  counted();
+  k_to_f64<<<grid_for((int)std::min<long long>(n, 1 << 30)), 256, 0, st>>>(n, reinterpret_cast<const float*>(src),
+                                                                           dst);
+  return last();
+}
+
+cudaError_t launch_to_f32_batch(const ConvTask* t, int ntasks, cudaStream_t st) {
+  if (cudaError_t pre = begin("launch_to_f32_batch")) return pre;
+  if (ntasks <= 0) return cudaSuccess;
+  counted();
+  k_to_f32_batch<<<ntasks, 256, 0, st>>>(t);
   return last();
 }
 

@@ -15,6 +15,15 @@ long long kernel_launches();
 const char* last_launch_name();
 // name reported with the next launch error (launchers outside kernels.cu)
 void set_last_launch(const char* name);
+// Storage of factor blocks for the launchers of this thread that follow:
+// float (mixed-precision factorization and preconditioner apply) or double.
+// Descriptors carry block addresses as double* either way.
+void set_factor_fp32(bool on);
+bool factor_fp32();
+// n doubles -> n floats stored at dst, and back (vectors, factors)
+cudaError_t launch_to_f32(long long n, const double* src, double* dst, cudaStream_t st);
+cudaError_t launch_to_f64(long long n, const double* src, double* dst, cudaStream_t st);
+cudaError_t launch_to_f32_batch(const ConvTask* t, int ntasks, cudaStream_t st);
 void add_kernel_launches(long long n);
 
 cudaError_t launch_scatter(int nnz, const double* val, double* const* dst, cudaStream_t st);

@@ -138,4 +138,11 @@ struct BwdIn {
   int ldr, s;
 };
 
+// Conversion of one double array to float (mixed-precision factorization).
+struct ConvTask {
+  const double* src;
+  double* dst;  // holds floats
+  long long n;
+};
+
 }  // namespace spq

@@ -49,6 +49,8 @@ def lib():
             "spq_set_square": (i32, [vp, i32]),
             "spq_set_pivot_rtol": (i32, [vp, f64]),
             "spq_set_rrqr_work": (i32, [vp, f64, f64]),
+            "spq_set_precision": (i32, [vp, i32]),
+            "spq_set_krylov": (i32, [vp, i32]),
             "spq_get_factor": (i32, [vp, i32, i32, pd, pi]),
             "spq_set_coords": (i32, [vp, i32, i32, pd]),
             "spq_set_coords_tensor": (i32, [vp, i32, i32]),
@@ -214,6 +216,16 @@ class ParTree:
         """Cluster sizing of the pivoted QR: elements of the compression matrix
         per CTA and pivot step, and CTAs per SM a level's work is spread over."""
         self._chk(lib().spq_set_rrqr_work(self._h, elems, fill), "set_rrqr_work")
+
+    def set_precision(self, bits: int):
+        """32: float factors and preconditioner apply (FP64 SpMV, Krylov loop and
+        pivoted QR); 64: plain FP64.  Takes effect at the next assemble."""
+        self._chk(lib().spq_set_precision(self._h, bits), "set_precision")
+
+    def set_krylov(self, method: int):
+        """0: left GMRES (reference); 1: flexible right-preconditioned GMRES;
+        -1: flexible exactly with float factors (default)."""
+        self._chk(lib().spq_set_krylov(self._h, method), "set_krylov")
 
     def set_rank_model(self, model: Optional[dict], oversample: int = 32):
         """Learned ranks from ``model`` (``params``, ``mean``, ``std`` float32
