@@ -5,10 +5,12 @@ A step is one full time-to-solution run on an assembled tree: ``factorize()``
 followed by left-preconditioned GMRES until the preconditioned residual is
 <= 1e-10 (is.cpp:447-527), with the true ||b - A x|| / ||b|| checked after it.
 Two variants run on the same tree in the same process: the plain FP64 method
-(column-pivoted QR of every interface) and the learned-rank method (the
-headline, ``value``); ``ratio_vs_fp64`` is their ratio.
+(column-pivoted QR of every interface, left-preconditioned GMRES) and the
+mixed-precision learned-rank method (float factors and preconditioner, learned
+ranks, flexible GMRES in FP64: the headline, ``value``); ``ratio_vs_fp64`` is
+their ratio.
 
-  value : device time of the learned-rank step, inputs resident in HBM (CUDA
+  value : device time of the mixed+learned step, inputs resident in HBM (CUDA
           events on the handle's stream, max over ranks), seconds -- lower is
           better.
   e2e   : the same step through the C ABI with host buffers: assemble (matrix
@@ -222,7 +224,9 @@ def run_ours(args):
     model = load_rank_model()
 
     def set_variant(name):
-        t.set_rank_model(model if name == "learned" else None, LEARNED_OVERSAMPLE)
+        # takes effect at the next assemble (every step assembles)
+        t.set_precision(32 if name == "mixed+learned" else 64)
+        t.set_rank_model(model if name == "mixed+learned" else None, LEARNED_OVERSAMPLE)
 
     def ranks():
         cl = t.clusters()
@@ -232,7 +236,7 @@ def run_ours(args):
     # ranks (the headline); warm-up of each, then the timed steps of each
     res = {}
     with ClockSampler(local) as clk:
-        for name in ("fp64", "learned"):
+        for name in ("fp64", "mixed+learned"):
             set_variant(name)
             for _ in range(args.warmup):
                 device_step()
@@ -250,7 +254,7 @@ def run_ours(args):
             r["flops"] = t.factor_flops()
             r["rrqr_bytes"] = t.rrqr_bytes()
             res[name] = r
-    head = res["learned"]
+    head = res["mixed+learned"]
     e2e_times = [e2e_step()[0] for _ in range(max(1, min(args.steps, 3)))]
     step = float(np.mean(head["times"]))
     fp64_step = float(np.mean(res["fp64"]["times"]))
@@ -287,10 +291,11 @@ def run_ours(args):
         "higher_is_better": False,
         "scaling": "weak",
         "vs_baseline": None,
-        "dtype": "f64",
+        "dtype": "f32 factors and preconditioner / f64 SpMV, Krylov and pivoted QR",
         "data": "synthetic (seeded Gaussian random field coefficients, N(0,1) right-hand side)",
-        "variant": "learned ranks (MLP-sized randomized range finder + residual rank rule, pivoted-QR fallback); "
-                   "FP64 factorization and GMRES -- the FP32 factorization is not built yet",
+        "variant": "mixed precision + learned ranks: float factor blocks and preconditioner apply, ranks from an "
+                   "MLP-sized randomized range finder with the pivoted QR's residual rule (pivoted-QR fallback), "
+                   "flexible right-preconditioned GMRES in FP64; fp64_plain = the reference method on the GPU",
         "config": {"workload": W["name"], "matrix": W["matrix"], "nlevels": W["nlevels"], "tol": W["tol"],
                    "skip": W["skip"], "gmres_tol": W["gmres_tol"], "parallelism": f"replicas x{world}",
                    "l2": "factor pool (GBs) > L2; 256 MB buffer written before every timed step"},
@@ -386,7 +391,7 @@ def run_reference(args):
     out = {
         "metric": METRIC, "value": val, "unit": "s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": val * 1e3, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f64", "data": "synthetic", "impl": "reference",
+        "dtype": "f32 factors and preconditioner / f64 SpMV, Krylov and pivoted QR", "data": "synthetic", "impl": "reference",
         "config": {"workload": W["name"], "matrix": W["matrix"], "nlevels": W["nlevels"], "tol": W["tol"],
                    "skip": W["skip"], "gmres_tol": W["gmres_tol"], "parallelism": f"cpu x{threads} threads"},
         "cpu_baseline": {"value": val, "unit": "s", "cores": threads, "kind": "port",

@@ -186,6 +186,10 @@ int spq_rank_model_size(int* nparams, int* nfeatures);
  * standardise the features); params = NULL restores the plain pivoted QR.
  * Resets the counters of spq_learned_counts. */
 int spq_set_rank_model(spq_tree* t, const float* params, const float* mean, const float* stdev, int oversample);
+/* Tuning of the learned path: the sketch's pivoted QR stops at
+ * sketch_tol * tol (default 0.1); smem = 1 (default) holds each CTA's block of
+ * the sketch in shared memory when it fits. */
+int spq_set_sketch_tuning(spq_tree* t, double sketch_tol, int smem);
 /* out[0..2] = interfaces whose learned rank was accepted, interfaces that fell
  * back to the pivoted QR, and the sum of the sketch widths, since the model was set. */
 int spq_learned_counts(spq_tree* t, long long* out);

@@ -56,6 +56,13 @@ int spq_set_rank_model(spq_tree* h, const float* params, const float* mean, cons
   return rc;
 }
 
+int spq_set_sketch_tuning(spq_tree* h, double sketch_tol, int smem) {
+  if (!h || !(sketch_tol > 0 && sketch_tol <= 1)) return -1;
+  h->t->sketch_tol = sketch_tol;
+  h->t->sketch_smem = smem != 0;
+  return 0;
+}
+
 int spq_learned_counts(spq_tree* h, long long* out) {
   if (!h || !out) return -1;
   h->t->learned_counts(out, out + 1, out + 2);

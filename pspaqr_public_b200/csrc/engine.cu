@@ -26,6 +26,12 @@ constexpr long long kSpinLimit = 2000000000LL;
 constexpr int kChunk = 64;        // columns (rows) per CTA of the chunked applies
 constexpr int kBigCluster = 8;    // CTAs per task for blocks of >= 8 panels
 constexpr int kRrqrMaxCols = 1024;  // own columns of C per CTA (four per thread)
+// shared memory of a CTA holding its block of C (the sketches of the learned
+// path): the block itself, the CTA's whole allotment, and the growth a
+// launch group's arrays may add when sized by its largest task
+constexpr size_t kRrqrSmemBlock = 120 * 1024;
+constexpr size_t kRrqrSmemBudget = 176 * 1024;
+constexpr size_t kRrqrSmemSlack = 48 * 1024;
 
 // SMs of the current device (queried once per process)
 int num_sms() {
@@ -515,10 +521,18 @@ int Tree::factorize() {
         if (!spV[q] || !spT[q]) return fail(-11, "out of device memory (rrqr)");
         rr_dims.push_back({(double)mp, (double)w});
       }
-      // pivoted-QR launch groups by cluster size 1, 2, 4, 8, 16
+      // pivoted-QR launch groups: index 2 * log2(cluster size) + (the CTAs'
+      // blocks of C held in shared memory)
       struct RrqrGroups {
-        std::vector<RrqrTask> t[5];
-        int m[5] = {1, 1, 1, 1, 1}, k[5] = {1, 1, 1, 1, 1}, nl[5] = {1, 1, 1, 1, 1}, rc[5] = {1, 1, 1, 1, 1};
+        std::vector<RrqrTask> t[10];
+        int m[10], k[10], nl[10], rc[10];
+        size_t cd[10];  // largest block of C in shared memory (doubles)
+        RrqrGroups() {
+          for (int g = 0; g < 10; ++g) {
+            m[g] = k[g] = nl[g] = rc[g] = 1;
+            cd[g] = 0;
+          }
+        }
       };
       // A set of compression matrices of total work W is dealt so that about
       // rrqr_fill CTAs per SM share it: each CTA holds at most
@@ -529,24 +543,44 @@ int Tree::factorize() {
       // a pivoted QR of the row-major m x w matrix C (ld ldw) into V / T of
       // interface p; rank to *rank; the orthonormal basis (m x min(m,w)) to Qc
       // when given.  The cluster is the smallest whose CTAs each hold at most
-      // `cap` elements of C and kRrqrMaxCols columns.  Returns the cluster
-      // size, 0 on failure.
+      // `cap` elements of C and kRrqrMaxCols columns.  With `smem` the
+      // smallest cluster whose CTAs' blocks of C fit in kRrqrSmemBlock bytes
+      // of shared memory keeps them there (when one exists).  Returns the
+      // cluster size, 0 on failure.
       auto add_rrqr = [&](RrqrGroups& G, const double* C, int mp, int w, int ldw, int p, int* rank, double* Qc,
-                          int* stats, double cap) -> int {
+                          int* stats, double cap, bool smem) -> int {
         const double work = (double)mp * w;
-        auto local_cols = [&](int c) { return ((w + c - 1) / c + 31) / 32 * 32; };
-        int g = 0;
-        while (g < 4 && (work > cap * (1 << g) || local_cols(1 << g) > kRrqrMaxCols) && (w + NB - 1) / NB >= (2 << g))
-          ++g;
-        if (g == 4 && !rrqr_cluster_fits(16, rrqr_smem(std::max(G.m[4], mp), std::max(G.k[4], std::min(mp, w)),
-                                                       std::max(G.nl[4], local_cols(16)),
-                                                       std::max(G.rc[4], (mp + 15) / 16))))
-          g = 3;
-        const int cs = 1 << g;
-        if (local_cols(cs) > kRrqrMaxCols) {
+        const int npan = (w + NB - 1) / NB;
+        int lg = 0;
+        bool in_smem = false;
+        if (smem) {
+          for (int l2 = 0; l2 <= 4 && !in_smem; ++l2) {
+            const int c = 1 << l2;
+            if (c > 1 && (w + 1) / 2 < c) break;
+            const int nl = rrqr_cols_per_cta(w, c, true);
+            const size_t cdb = (size_t)mp * ((nl + 1) & ~1);
+            const size_t b = rrqr_smem(mp, std::min(mp, w), nl, (mp + c - 1) / c, cdb);
+            if (sizeof(double) * cdb <= kRrqrSmemBlock && b <= kRrqrSmemBudget &&
+                (c <= 8 || rrqr_cluster_fits(c, b + kRrqrSmemSlack, true))) {
+              lg = l2;
+              in_smem = true;
+            }
+          }
+        }
+        if (!in_smem) {
+          auto lc = [&](int c) { return rrqr_cols_per_cta(w, c, false); };
+          while (lg < 4 && (work > cap * (1 << lg) || lc(1 << lg) > kRrqrMaxCols) && npan >= (2 << lg)) ++lg;
+          if (lg == 4 && !rrqr_cluster_fits(16, rrqr_smem(std::max(G.m[8], mp), std::max(G.k[8], std::min(mp, w)),
+                                                          std::max(G.nl[8], lc(16)), std::max(G.rc[8], (mp + 15) / 16))))
+            lg = 3;
+        }
+        const int cs = 1 << lg;
+        const int nlc = rrqr_cols_per_cta(w, cs, in_smem);
+        if (nlc > kRrqrMaxCols) {
           fail(-12, "interface too wide for the pivoted QR kernel");
           return 0;
         }
+        const int g = 2 * lg + (in_smem ? 1 : 0);
         RrqrTask t{};
         t.m = mp;
         t.w = w;
@@ -569,23 +603,25 @@ int Tree::factorize() {
         G.t[g].push_back(t);
         G.m[g] = std::max(G.m[g], mp);
         G.k[g] = std::max(G.k[g], std::min(mp, w));
-        G.nl[g] = std::max(G.nl[g], local_cols(cs));
+        G.nl[g] = std::max(G.nl[g], nlc);
         G.rc[g] = std::max(G.rc[g], (mp + cs - 1) / cs);
+        if (in_smem) G.cd[g] = std::max(G.cd[g], (size_t)mp * ((nlc + 1) & ~1));
         return cs;
       };
       auto up_any = [&](auto& v) { return upload(v.data(), sizeof(v[0]) * v.size()); };
       auto run_rrqr = [&](RrqrGroups& G, double tol) -> int {
-        for (int g = 0; g < 5; ++g) {
+        for (int g = 0; g < 10; ++g) {
           if (G.t[g].empty()) continue;
           auto* d = static_cast<RrqrTask*>(up_any(G.t[g]));
           if (!d) return fail(-11, "out of device memory (rrqr tasks)");
-          if (ck(launch_rrqr(d, (int)G.t[g].size(), 1 << g, G.m[g], G.k[g], G.nl[g], G.rc[g], tol, pivot_rtol,
+          const int cs = 1 << (g / 2);
+          if (ck(launch_rrqr(d, (int)G.t[g].size(), cs, G.m[g], G.k[g], G.nl[g], G.rc[g], G.cd[g], tol, pivot_rtol,
                              stream_),
                  "rrqr kernel")) {
-            error += " [cluster " + std::to_string(1 << g) + ", tasks " + std::to_string(G.t[g].size()) + ", rows " +
-                     std::to_string(G.m[g]) + ", steps " + std::to_string(G.k[g]) + ", columns/CTA " +
-                     std::to_string(G.nl[g]) + ", shared " +
-                     std::to_string(rrqr_smem(G.m[g], G.k[g], G.nl[g], G.rc[g])) + " B]";
+            error += " [cluster " + std::to_string(cs) + ((g & 1) ? " (C in shared memory)" : "") + ", tasks " +
+                     std::to_string(G.t[g].size()) + ", rows " + std::to_string(G.m[g]) + ", steps " +
+                     std::to_string(G.k[g]) + ", columns/CTA " + std::to_string(G.nl[g]) + ", shared " +
+                     std::to_string(rrqr_smem(G.m[g], G.k[g], G.nl[g], G.rc[g], G.cd[g])) + " B]";
             return -10;
           }
         }
@@ -689,7 +725,7 @@ int Tree::factorize() {
         for (size_t q = 0; q < nsp; ++q) {
           const int p = Lv.spars_clusters[q];
           rr_cs[q] = add_rrqr(G, sp_C[q], size_[p], sp_w[q], sp_ldw[q], p, d_rank_ + p, nullptr,
-                              d_stats ? d_stats + 8 * q : nullptr, work_cap(level_work, rrqr_work));
+                              d_stats ? d_stats + 8 * q : nullptr, work_cap(level_work, rrqr_work), false);
           if (!rr_cs[q]) return -12;
         }
         if (int rc = run_rrqr(G, tol)) return rc;
@@ -737,7 +773,7 @@ int Tree::factorize() {
           for (int j0 = 0; j0 < t.w; j0 += 256) scan_blocks.push_back({(int)q, 0, j0});
           // the sketch's pivoted QR stops at sketch_tol * tol and writes its
           // rank over the sketch width: later stages use only those vectors
-          if (!add_rrqr(G, t.Y, t.m, ell[q], t.ldy, p, d_ell + q, Qc, nullptr, work_cap(sketch_work, 4096)))
+          if (!add_rrqr(G, t.Y, t.m, ell[q], t.ldy, p, d_ell + q, Qc, nullptr, work_cap(sketch_work, 4096), sketch_smem))
             return -12;
         }
         auto* d_sk = static_cast<SketchTask*>(up_any(sk));
@@ -774,7 +810,7 @@ int Tree::factorize() {
           if (fb[q]) {
             ++learned_fallbacks_;
             rr_cs[q] = add_rrqr(Fb, sp_C[q], t.m, t.w, t.ldw, p, d_rank_ + p, nullptr, nullptr,
-                                work_cap(fb_work, 16384));
+                                work_cap(fb_work, 16384), false);
             if (!rr_cs[q]) return -12;
           } else {
             ++learned_accepted_;

@@ -78,6 +78,9 @@ class Tree {
   // learned ranks: the sketch's pivoted QR stops at sketch_tol * tol (the
   // kept rank is then chosen on C itself)
   double sketch_tol = 0.1;
+  // the sketch's pivoted QR holds each CTA's block of the sketch in shared
+  // memory when it fits
+  bool sketch_smem = true;
 
   int set_coords(int dim, int n, const double* X);
   int set_coords_tensor(int n, int d);

@@ -267,7 +267,7 @@ __global__ void __launch_bounds__(kThreads) k_rrqr_assemble(const RrqrSrc* __res
 // and are added in row-group order.
 constexpr int kRows = 4;  // rows of loads issued together in col_dots
 
-template <bool kSq, typename Act, typename Fin>
+template <bool kSq, bool kShared, typename Act, typename Fin>
 __device__ __forceinline__ void col_dots(const double* __restrict__ Ct, int ldw, int m, int ja, int nloc,
                                          const double* x, double* gp, Act act, Fin fin) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -297,7 +297,8 @@ __device__ __forceinline__ void col_dots(const double* __restrict__ Ct, int ldw,
         const int r = r0 + k * RG;
         const double2* row = reinterpret_cast<const double2*>(col + (size_t)r * ldw);
 #pragma unroll
-        for (int u = 0; u < 4; ++u) v[k][u] = (r < m && l[u]) ? __ldg(row + 32 * u) : make_double2(0.0, 0.0);
+        for (int u = 0; u < 4; ++u)
+          v[k][u] = (r < m && l[u]) ? (kShared ? row[32 * u] : __ldg(row + 32 * u)) : make_double2(0.0, 0.0);
       }
 #pragma unroll
       for (int k = 0; k < kRows; ++k) {
@@ -428,6 +429,7 @@ __device__ __forceinline__ void own_first(const RrqrSmem& S, int nloc, int ja, i
   __syncthreads();
 }
 
+template <bool kSmemC>
 __global__ void __launch_bounds__(kThreads, 2) k_rrqr(const RrqrTask* __restrict__ tasks, double tol,
                                                       double pivot_rtol, int cs, int mmax, int kmax, int nlmax,
                                                       int rcmax) {
@@ -453,7 +455,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_rrqr(const RrqrTask* __restrict
   double* Qt = t.Q;
 
   // own columns [ja, jb) and own rows [ra, rb)
-  const int wc = ((w + cs - 1) / cs + 31) / 32 * 32;
+  const int wc = rrqr_cols_per_cta(w, cs, kSmemC);
   const int ja = min(w, rank * wc), jb = min(w, ja + wc), nloc = jb - ja;
   const int rc = (m + cs - 1) / cs;
   const int ra = min(m, rank * rc), rb = min(m, ra + rc);
@@ -468,7 +470,21 @@ __global__ void __launch_bounds__(kThreads, 2) k_rrqr(const RrqrTask* __restrict
     return *cg::this_cluster().map_shared_rank(p, q);
   };
   // initial norms, positions
-  col_dots<true>(Ct, ldw, m, ja, nloc, nullptr, S.gp, [](int) { return true; }, [&](int jl, double ss) {
+  // kSmemC: the CTA's column block of C (m x nlp, nlp = nloc rounded up to
+  // even, the pad column zero) is held in shared memory after S's arrays and
+  // every pivot step reads it there
+  const int nlp = (nloc + 1) & ~1;
+  double* sC = reinterpret_cast<double*>((reinterpret_cast<uintptr_t>(S.flg + nlmax) + 15) & ~(uintptr_t)15);
+  if (kSmemC) {
+    for (size_t e = threadIdx.x; e < (size_t)m * nlp; e += kThreads) {
+      const int r = (int)(e / nlp), jl = (int)(e % nlp);
+      sC[e] = jl < nloc ? __ldg(Ct + (size_t)r * ldw + ja + jl) : 0.0;
+    }
+    __syncthreads();
+  }
+  const double* Cb = kSmemC ? sC : Ct + ja;
+  const int ldb = kSmemC ? nlp : ldw;
+  col_dots<true, kSmemC>(Cb, ldb, m, 0, nloc, nullptr, S.gp, [](int) { return true; }, [&](int jl, double ss) {
     const double v = sqrt(ss);
     S.vn1[jl] = v;
     S.vn2[jl] = v;
@@ -672,7 +688,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_rrqr(const RrqrTask* __restrict
     // (e) row i of R over own active columns (kept in F for recomputations);
     // dlaqp2 downdate of the partial norms
     double* Fi = t.F + (size_t)i * w + ja;
-    col_dots<false>(Ct, ldw, m, ja, nloc, S.qf, S.gp, [&](int jl) { return S.pos[jl] > i; },
+    col_dots<false, kSmemC>(Cb, ldb, m, 0, nloc, S.qf, S.gp, [&](int jl) { return S.pos[jl] > i; },
                     [&](int jl, double rij) {
                       Fi[jl] = rij;
                       const double v1 = S.vn1[jl];
@@ -1105,17 +1121,20 @@ cudaError_t launch_edge(int kind, const EdgeChunk* t, int ntasks, cudaStream_t s
                 : go(k_edge_left<double>, k_edge_trsm<double>, k_edge_right<double>);
 }
 
-size_t rrqr_smem(int mmax, int kmax, int nlmax, int rcmax) {
+size_t rrqr_smem(int mmax, int kmax, int nlmax, int rcmax, size_t c_doubles) {
   const size_t d = kRed + kNB + 4 * ((size_t)kmax + 1) + 2 * (size_t)rcmax + (size_t)std::max(mmax, 1) +
                    2 * (size_t)nlmax + 8 * (size_t)kThreads;
-  return smem_bytes(d) + sizeof(int) * 2 * (size_t)nlmax;
+  size_t b = smem_bytes(d) + sizeof(int) * 2 * (size_t)nlmax;
+  if (c_doubles) b += 16 + smem_bytes(c_doubles);
+  return b;
 }
 
-bool rrqr_cluster_fits(int cs, size_t smem) {
+template <bool kSmemC>
+bool rrqr_fits(int cs, size_t smem) {
   if (smem > kSmemMax) return false;
   if (cs <= 8) return true;
-  if (prep(k_rrqr, smem)) return false;
-  if (cudaFuncSetAttribute(k_rrqr, cudaFuncAttributeNonPortableClusterSizeAllowed, 1)) {
+  if (prep(k_rrqr<kSmemC>, smem)) return false;
+  if (cudaFuncSetAttribute(k_rrqr<kSmemC>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1)) {
     cudaGetLastError();
     return false;
   }
@@ -1131,11 +1150,15 @@ bool rrqr_cluster_fits(int cs, size_t smem) {
   cfg.attrs = attr;
   cfg.numAttrs = 1;
   int n = 0;
-  if (cudaOccupancyMaxActiveClusters(&n, k_rrqr, &cfg) != cudaSuccess) {
+  if (cudaOccupancyMaxActiveClusters(&n, k_rrqr<kSmemC>, &cfg) != cudaSuccess) {
     cudaGetLastError();
     return false;
   }
   return n > 0;
+}
+
+bool rrqr_cluster_fits(int cs, size_t smem, bool smem_c) {
+  return smem_c ? rrqr_fits<true>(cs, smem) : rrqr_fits<false>(cs, smem);
 }
 
 cudaError_t launch_rrqr_assemble(const RrqrSrc* s, int nsrc, cudaStream_t st) {
@@ -1147,15 +1170,22 @@ cudaError_t launch_rrqr_assemble(const RrqrSrc* s, int nsrc, cudaStream_t st) {
   return last();
 }
 
-cudaError_t launch_rrqr(const RrqrTask* t, int ntasks, int cs, int mmax, int kmax, int nlmax, int rcmax, double tol,
-                        double pivot_rtol, cudaStream_t st) {
+template <bool kSmemC>
+cudaError_t launch_rrqr_t(const RrqrTask* t, int ntasks, int cs, int mmax, int kmax, int nlmax, int rcmax,
+                          size_t c_doubles, double tol, double pivot_rtol, cudaStream_t st) {
+  const size_t b = rrqr_smem(mmax, kmax, nlmax, rcmax, kSmemC ? c_doubles : 0);
+  cudaError_t e = prep(k_rrqr<kSmemC>, b);
+  if (!e && cs > 8) e = cudaFuncSetAttribute(k_rrqr<kSmemC>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+  if (e) return e;
+  return launch_clustered(k_rrqr<kSmemC>, ntasks, cs, b, st, t, tol, pivot_rtol, cs, mmax, kmax, nlmax, rcmax);
+}
+
+cudaError_t launch_rrqr(const RrqrTask* t, int ntasks, int cs, int mmax, int kmax, int nlmax, int rcmax,
+                        size_t c_doubles, double tol, double pivot_rtol, cudaStream_t st) {
   if (cudaError_t pre = begin("launch_rrqr")) return pre;
   if (ntasks <= 0) return cudaSuccess;
-  const size_t b = rrqr_smem(mmax, kmax, nlmax, rcmax);
-  cudaError_t e = prep(k_rrqr, b);
-  if (!e && cs > 8) e = cudaFuncSetAttribute(k_rrqr, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
-  if (e) return e;
-  return launch_clustered(k_rrqr, ntasks, cs, b, st, t, tol, pivot_rtol, cs, mmax, kmax, nlmax, rcmax);
+  return c_doubles ? launch_rrqr_t<true>(t, ntasks, cs, mmax, kmax, nlmax, rcmax, c_doubles, tol, pivot_rtol, st)
+                   : launch_rrqr_t<false>(t, ntasks, cs, mmax, kmax, nlmax, rcmax, 0, tol, pivot_rtol, st);
 }
 
 cudaError_t launch_merge(const MergeTask* t, int ntasks, cudaStream_t st) {

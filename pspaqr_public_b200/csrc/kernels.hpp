@@ -34,15 +34,28 @@ cudaError_t launch_update(const UpdTask* t, const UpdOp* o, int ntasks, cudaStre
 // kind 0: left apply on column chunks, 1: right triangular solve on row chunks,
 // 2: right apply on row chunks
 cudaError_t launch_edge(int kind, const EdgeChunk* t, int ntasks, cudaStream_t st);
+// Columns of C one CTA of a cs-CTA cluster owns in the pivoted QR: a
+// contiguous range, a multiple of 32 columns when C streams from global
+// memory (whole 256-byte row segments), of 2 when the CTA's block is held in
+// shared memory (16-byte loads).
+#if defined(__CUDACC__)
+__host__ __device__
+#endif
+inline int rrqr_cols_per_cta(int w, int cs, bool smem_c) {
+  const int a = smem_c ? 2 : 32;
+  return ((w + cs - 1) / cs + a - 1) / a * a;
+}
 // Shared memory of one pivoted-QR CTA for tasks of at most mmax rows, kmax
-// steps, nlmax own columns and rcmax own rows.
-size_t rrqr_smem(int mmax, int kmax, int nlmax, int rcmax);
+// steps, nlmax own columns and rcmax own rows; c_doubles = the largest
+// m x (own columns rounded to even) of a task whose block of C is held in
+// shared memory (0: C streams from global memory).
+size_t rrqr_smem(int mmax, int kmax, int nlmax, int rcmax, size_t c_doubles = 0);
 // a cluster of cs CTAs with smem bytes each of the pivoted QR can be resident
-bool rrqr_cluster_fits(int cs, size_t smem);
+bool rrqr_cluster_fits(int cs, size_t smem, bool smem_c = false);
 // transposed gather of the compression matrices (one CTA per source block)
 cudaError_t launch_rrqr_assemble(const RrqrSrc* s, int nsrc, cudaStream_t st);
-cudaError_t launch_rrqr(const RrqrTask* t, int ntasks, int cs, int mmax, int kmax, int nlmax, int rcmax, double tol,
-                        double pivot_rtol, cudaStream_t st);
+cudaError_t launch_rrqr(const RrqrTask* t, int ntasks, int cs, int mmax, int kmax, int nlmax, int rcmax,
+                        size_t c_doubles, double tol, double pivot_rtol, cudaStream_t st);
 cudaError_t launch_merge(const MergeTask* t, int ntasks, cudaStream_t st);
 
 cudaError_t launch_fwd_elim(const FwdElimTask* t, const FwdOut* o, int ntasks, int nmax, int mmax, int* ticket,

@@ -67,6 +67,7 @@ def lib():
             "spq_rank_model_size": (i32, [pi, pi]),
             "spq_set_rank_model": (i32, [vp, pf, pf, pf, i32]),
             "spq_learned_counts": (i32, [vp, C.POINTER(C.c_longlong)]),
+            "spq_set_sketch_tuning": (i32, [vp, f64, i32]),
             "spq_set_rank_log": (i32, [vp, i32]),
             "spq_rank_log_count": (i32, [vp]),
             "spq_rank_log": (i32, [vp, pf, pi, pi, pi]),
@@ -238,6 +239,10 @@ class ParTree:
         m = self._model
         self._chk(lib().spq_set_rank_model(self._h, _pf(m["params"]), _pf(m["mean"]), _pf(m["std"]), oversample),
                   "set_rank_model")
+
+    def set_sketch_tuning(self, sketch_tol: float = 0.1, smem: bool = True):
+        """Stop of the sketch's pivoted QR (x tol) and its shared-memory mode."""
+        self._chk(lib().spq_set_sketch_tuning(self._h, sketch_tol, int(smem)), "set_sketch_tuning")
 
     def learned_counts(self) -> dict:
         out = (C.c_longlong * 3)()

@@ -172,7 +172,9 @@ def test_fallback_is_the_plain_pivoted_qr():
 @pytest.mark.gpu
 def test_trained_network_gains_over_constant_prediction(model):
     """The method without the trained network predicts the training mean for
-    every interface: it falls back more often and/or sketches more columns."""
+    every interface.  The trained network sizes the sketches closer to the
+    ranks needed: fewer sketch columns at no more fallbacks (within 1 % of the
+    interfaces)."""
     T = _gpu()
     m, meta = model
     P, F = T.rank_model_size()
@@ -188,5 +190,6 @@ def test_trained_network_gains_over_constant_prediction(model):
         t.factorize()
         res[name] = t.learned_counts()
     tr, co = res["trained"], res["constant"]
-    assert tr["fallback"] <= co["fallback"] and tr["sketch_columns"] <= co["sketch_columns"]
-    assert tr["fallback"] < co["fallback"] or tr["sketch_columns"] < co["sketch_columns"]
+    n = tr["accepted"] + tr["fallback"]
+    assert tr["sketch_columns"] < co["sketch_columns"]
+    assert tr["fallback"] <= co["fallback"] + 0.01 * n
