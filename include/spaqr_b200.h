@@ -187,8 +187,9 @@ int spq_rank_model_size(int* nparams, int* nfeatures);
  * Resets the counters of spq_learned_counts. */
 int spq_set_rank_model(spq_tree* t, const float* params, const float* mean, const float* stdev, int oversample);
 /* Tuning of the learned path: the sketch's pivoted QR stops at
- * sketch_tol * tol (default 0.1); smem = 1 (default) holds each CTA's block of
- * the sketch in shared memory when it fits. */
+ * sketch_tol * tol (default 0.1); smem = 1 holds each CTA's block of the
+ * sketch in shared memory when it fits (default 0: reads it from global memory,
+ * measured faster on the 64^3 diffusion problem). */
 int spq_set_sketch_tuning(spq_tree* t, double sketch_tol, int smem);
 /* out[0..2] = interfaces whose learned rank was accepted, interfaces that fell
  * back to the pivoted QR, and the sum of the sketch widths, since the model was set. */

@@ -773,7 +773,8 @@ int Tree::factorize() {
           for (int j0 = 0; j0 < t.w; j0 += 256) scan_blocks.push_back({(int)q, 0, j0});
           // the sketch's pivoted QR stops at sketch_tol * tol and writes its
           // rank over the sketch width: later stages use only those vectors
-          if (!add_rrqr(G, t.Y, t.m, ell[q], t.ldy, p, d_ell + q, Qc, nullptr, work_cap(sketch_work, 4096), sketch_smem))
+          if (!add_rrqr(G, t.Y, t.m, ell[q], t.ldy, p, d_ell + q, Qc, d_stats ? d_stats + 8 * q : nullptr,
+                        work_cap(sketch_work, 4096), sketch_smem))
             return -12;
         }
         auto* d_sk = static_cast<SketchTask*>(up_any(sk));
@@ -826,6 +827,21 @@ int Tree::factorize() {
           for (int f : fb) nfb += f;
           printf("learned level %d: plan %.2f sketch %.2f qr %.2f project %.2f fallback(%d) %.2f ms\n", lvl, ms[0], ms[1],
                  ms[2], ms[3], nfb, ms[4]);
+          if (d_stats) {
+            std::vector<int> st(8 * nsp);
+            cudaMemcpy(st.data(), d_stats, sizeof(int) * st.size(), cudaMemcpyDeviceToHost);
+            double steps = 0, recomp = 0, kc[6] = {0, 0, 0, 0, 0, 0}, ellsum = 0;
+            for (size_t q = 0; q < nsp; ++q) {
+              recomp += st[8 * q];
+              steps += st[8 * q + 1];
+              for (int k = 0; k < 5; ++k) kc[k] += st[8 * q + 2 + k];
+              ellsum += ell[q];
+            }
+            printf("  sketch QR: tasks %zu mean ell %.0f mean steps %.0f recomputes/task %.0f  kcycles/task pivot %.0f "
+                   "proj %.0f basis %.0f rowR %.0f finalQR %.0f\n",
+                   nsp, ellsum / nsp, steps / nsp, recomp / nsp, kc[0] / nsp, kc[1] / nsp, kc[2] / nsp, kc[3] / nsp,
+                   kc[4] / nsp);
+          }
         }
         for (auto& e : le) cudaEventDestroy(e);
       }

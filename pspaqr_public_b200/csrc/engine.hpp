@@ -80,7 +80,7 @@ class Tree {
   double sketch_tol = 0.1;
   // the sketch's pivoted QR holds each CTA's block of the sketch in shared
   // memory when it fits
-  bool sketch_smem = true;
+  bool sketch_smem = false;
 
   int set_coords(int dim, int n, const double* X);
   int set_coords_tensor(int n, int d);

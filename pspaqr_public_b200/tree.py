@@ -240,7 +240,7 @@ class ParTree:
         self._chk(lib().spq_set_rank_model(self._h, _pf(m["params"]), _pf(m["mean"]), _pf(m["std"]), oversample),
                   "set_rank_model")
 
-    def set_sketch_tuning(self, sketch_tol: float = 0.1, smem: bool = True):
+    def set_sketch_tuning(self, sketch_tol: float = 0.1, smem: bool = False):
         """Stop of the sketch's pivoted QR (x tol) and its shared-memory mode."""
         self._chk(lib().spq_set_sketch_tuning(self._h, sketch_tol, int(smem)), "set_sketch_tuning")
 
