@@ -406,6 +406,16 @@ int Tree::factorize() {
     }
     lt_[lvl].ntasks_elim = (int)Lv.interiors.size();
     lt_[lvl].ntasks_upd = (int)ut.size();
+    if (verbose >= 2) {
+      double n3 = 0, mn2 = 0;
+      for (int g = 0; g < 3; ++g)
+        for (const ElimTask& t : et[g]) {
+          n3 += (double)t.n * t.n * t.n;
+          for (int o = t.out_begin; o < t.out_end; ++o) mn2 += (double)eo[o].m * t.n * t.n;
+        }
+      printf("level %d elim groups (cs 1/4/%d): %zu/%zu/%zu tasks, nmax %d/%d/%d, outs %zu, sum n^3 %.3g, sum m n^2 %.3g\n",
+             lvl, kBigCluster, et[0].size(), et[1].size(), et[2].size(), nmax[0], nmax[1], nmax[2], eo.size(), n3, mn2);
+    }
     {
       auto* d_eo = static_cast<ElimOut*>(upload(eo.data(), sizeof(ElimOut) * eo.size()));
       for (int g = 0; g < 3; ++g) {
@@ -441,6 +451,13 @@ int Tree::factorize() {
         sc[g].push_back(t);
         smax[g] = std::max(smax[g], np);
         flops_ += 2.0 * np * np * (np - np / 3.0);
+      }
+      if (verbose >= 2) {
+        double n3 = 0;
+        for (int g = 0; g < 3; ++g)
+          for (const ScaleTask& t : sc[g]) n3 += (double)t.n * t.n * t.n;
+        printf("level %d scale groups: %zu/%zu/%zu tasks, nmax %d/%d/%d, sum n^3 %.3g\n", lvl, sc[0].size(),
+               sc[1].size(), sc[2].size(), smax[0], smax[1], smax[2], n3);
       }
       std::vector<EdgeChunk> rows_scale, cols_scale;
       for (int e : Lv.spars_edges) {
@@ -740,8 +757,15 @@ int Tree::factorize() {
         if (ck(cudaMemcpyAsync(ell.data(), d_ell, sizeof(int) * nsp, cudaMemcpyDeviceToHost, stream_), "sketch widths") ||
             ck(cudaStreamSynchronize(stream_), "rank prediction"))
           return -10;
-        std::vector<GemmTile> sk_tiles, pj_tiles, scan_blocks;
+        std::vector<GemmTile> sk_tiles, pj_tiles, scan_blocks, gram_tiles;
         RrqrGroups G;
+        // the sketch's pivots from the pivoted Cholesky of its Gram matrix
+        // where the stop tolerance allows, else the pivoted-QR kernel on Y
+        const double stol = sketch_tol * tol;
+        const bool gram = stol >= kGramMinTol;
+        std::vector<RrqrTask> sel[3];
+        int sel_m[3] = {1, 1, 1}, sel_n[3] = {1, 1, 1}, ellmax = 1;
+        const int sel_cs[3] = {1, 4, kBigCluster};
         size_t mtot = 0;
         double sketch_work = 0;
         for (size_t q = 0; q < nsp; ++q) {
@@ -773,9 +797,34 @@ int Tree::factorize() {
           for (int j0 = 0; j0 < t.w; j0 += 256) scan_blocks.push_back({(int)q, 0, j0});
           // the sketch's pivoted QR stops at sketch_tol * tol and writes its
           // rank over the sketch width: later stages use only those vectors
-          if (!add_rrqr(G, t.Y, t.m, ell[q], t.ldy, p, d_ell + q, Qc, d_stats ? d_stats + 8 * q : nullptr,
-                        work_cap(sketch_work, 4096), sketch_smem))
+          if (gram) {
+            t.G = scratch_.dalloc((size_t)l * t.ldy);
+            t.Lt = scratch_.dalloc((size_t)l * t.ldy);
+            t.colat = static_cast<int*>(scratch_.alloc(sizeof(int) * l));
+            RrqrTask r{};
+            r.C = t.Y;
+            r.ldw = t.ldy;
+            r.m = t.m;
+            r.w = ell[q];
+            r.Qc = Qc;
+            r.V = spV[q];
+            r.T = spT[q];
+            r.tau = scratch_.dalloc(std::max(t.m, 1));
+            r.colat = t.colat;
+            r.rank = d_ell + q;
+            if (!t.G || !t.Lt || !t.colat || !r.tau) return fail(-11, "out of device memory (sketch)");
+            for (int r0 = 0; r0 < ell[q]; r0 += 64)
+              for (int c0 = r0; c0 < ell[q]; c0 += 64) gram_tiles.push_back({(int)q, r0, c0});
+            const int cs = cluster_for(ell[q]);
+            const int g = cs == 1 ? 0 : (cs == 4 ? 1 : 2);
+            sel[g].push_back(r);
+            sel_m[g] = std::max(sel_m[g], t.m);
+            sel_n[g] = std::max(sel_n[g], ell[q]);
+            ellmax = std::max(ellmax, ell[q]);
+          } else if (!add_rrqr(G, t.Y, t.m, ell[q], t.ldy, p, d_ell + q, Qc, d_stats ? d_stats + 8 * q : nullptr,
+                               work_cap(sketch_work, 4096), sketch_smem)) {
             return -12;
+          }
         }
         auto* d_sk = static_cast<SketchTask*>(up_any(sk));
         auto* d_skt = static_cast<GemmTile*>(up_any(sk_tiles));
@@ -785,7 +834,23 @@ int Tree::factorize() {
         cudaEventRecord(le[1], stream_);
         if (ck(launch_sketch(d_sk, d_skt, (int)sk_tiles.size(), stream_), "sketch")) return -10;
         cudaEventRecord(le[2], stream_);
-        if (int rc = run_rrqr(G, sketch_tol * tol)) return rc;
+        if (gram) {
+          auto* d_gt = static_cast<GemmTile*>(up_any(gram_tiles));
+          if (!d_gt) return fail(-11, "out of device memory (sketch)");
+          if (ck(launch_gram(d_sk, d_gt, (int)gram_tiles.size(), stream_), "sketch Gram matrix") ||
+              ck(launch_pchol(d_sk, (int)nsp, ellmax, stol, pivot_rtol, stream_), "sketch pivots"))
+            return -10;
+          for (int g = 0; g < 3; ++g) {
+            if (sel[g].empty()) continue;
+            auto* d_sel = static_cast<RrqrTask*>(up_any(sel[g]));
+            if (!d_sel) return fail(-11, "out of device memory (sketch)");
+            if (ck(launch_selected_qr(d_sel, (int)sel[g].size(), sel_cs[g], sel_m[g], sel_n[g], stream_),
+                   "sketch QR"))
+              return -10;
+          }
+        } else if (int rc = run_rrqr(G, stol)) {
+          return rc;
+        }
         cudaEventRecord(le[3], stream_);
         if (ck(launch_project(d_sk, d_pjt, (int)pj_tiles.size(), stream_), "projection") ||
             ck(launch_residual_scan(d_sk, d_scb, (int)scan_blocks.size(), stream_), "residual scan") ||
@@ -827,7 +892,7 @@ int Tree::factorize() {
           for (int f : fb) nfb += f;
           printf("learned level %d: plan %.2f sketch %.2f qr %.2f project %.2f fallback(%d) %.2f ms\n", lvl, ms[0], ms[1],
                  ms[2], ms[3], nfb, ms[4]);
-          if (d_stats) {
+          if (d_stats && !gram) {
             std::vector<int> st(8 * nsp);
             cudaMemcpy(st.data(), d_stats, sizeof(int) * st.size(), cudaMemcpyDeviceToHost);
             double steps = 0, recomp = 0, kc[6] = {0, 0, 0, 0, 0, 0}, ellsum = 0;

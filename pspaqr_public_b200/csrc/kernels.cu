@@ -756,6 +756,98 @@ __global__ void __launch_bounds__(kThreads, 2) k_rrqr(const RrqrTask* __restrict
   }
 }
 
+// Householder QR of the selected columns C(:, colat[0:rank]) of a row-major C
+// (the pivot order fixed beforehand) into V / T / tau, then the orthonormal
+// basis Qc = C_sel R^{-1} (column-major, ld m) over the cluster's row blocks:
+// tiles of rt rows, 32-column blocks of R, a blocked update from the solved
+// columns and a triangular solve on the diagonal block.
+__global__ void __launch_bounds__(kThreads) k_selected_qr(const RrqrTask* __restrict__ tasks, int cs, int mmax,
+                                                          int nmax, int rt) {
+  extern __shared__ double sm[];
+  const RrqrTask t = tasks[blockIdx.x / cs];
+  const int rank = crank(cs);
+  const int m = t.m, ldw = t.ldw;
+  const int rk = __ldcg(t.rank);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  double* red = sm;
+  double* tmp = red + kRed;
+  double* lt = tmp + kNB;
+  double* vb = lt + nmax;
+  const int ldq = nmax + 1;
+  double* Qt = vb + mmax;      // rt x ldq: rows of the basis being solved
+  double* Rb = Qt + (size_t)rt * ldq;  // 32 x 33 block of R
+  const double* __restrict__ C = t.C;
+  for (int l = warp; l < rk; l += kWarps) {
+    if (!owns(l, rank, cs)) continue;
+    const int c = __ldg(t.colat + l);
+    for (int r = lane; r < m; r += 32) t.V[r + (size_t)l * m] = __ldg(C + (size_t)r * ldw + c);
+  }
+  __syncthreads();
+  dist_qr<double>(t.V, m, nullptr, 0, m, rk, 1, t.T, t.tau, lt, vb, red, tmp, cs);
+  // R(l, j) = V[l + j m] for l <= j, written by the owners of column j
+  auto R = [&](int l, int j) { return __ldcg(t.V + l + (size_t)j * m); };
+  const int rc = (m + cs - 1) / cs;
+  const int ra = min(m, rank * rc), rb = min(m, ra + rc);
+  for (int r0 = ra; r0 < rb; r0 += rt) {
+    const int nr = min(rt, rb - r0);
+    for (int e = threadIdx.x; e < nr * rk; e += kThreads) {
+      const int rr = e / rk, l = e % rk;
+      Qt[rr * ldq + l] = __ldg(C + (size_t)(r0 + rr) * ldw + __ldg(t.colat + l));
+    }
+    __syncthreads();
+    for (int j0 = 0; j0 < rk; j0 += 32) {
+      const int jb = min(32, rk - j0);
+      // Q(:, j0:j0+jb) = X - Q(:, 0:j0) R(0:j0, j0:j0+jb), outputs (o / 32, o % 32)
+      double acc[(32 * 32 + kThreads - 1) / kThreads] = {};
+      for (int l0 = 0; l0 < j0; l0 += 32) {
+        for (int e = threadIdx.x; e < 32 * 32; e += kThreads) {
+          const int jj = e >> 5, ll = e & 31;
+          Rb[ll * 33 + jj] = jj < jb ? R(l0 + ll, j0 + jj) : 0.0;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int u = 0; u < (32 * 32 + kThreads - 1) / kThreads; ++u) {
+          const int o = threadIdx.x + u * kThreads, rr = o >> 5, jj = o & 31;
+          if (rr < nr) {
+            const double* q = Qt + rr * ldq + l0;
+            double a = 0.0;
+#pragma unroll 8
+            for (int ll = 0; ll < 32; ++ll) a += q[ll] * Rb[ll * 33 + jj];
+            acc[u] += a;
+          }
+        }
+        __syncthreads();
+      }
+#pragma unroll
+      for (int u = 0; u < (32 * 32 + kThreads - 1) / kThreads; ++u) {
+        const int o = threadIdx.x + u * kThreads, rr = o >> 5, jj = o & 31;
+        if (rr < nr && jj < jb) Qt[rr * ldq + j0 + jj] -= acc[u];
+      }
+      for (int e = threadIdx.x; e < 32 * 32; e += kThreads) {
+        const int jj = e >> 5, ll = e & 31;
+        Rb[ll * 33 + jj] = (jj < jb && ll <= jj) ? R(j0 + ll, j0 + jj) : 0.0;
+      }
+      __syncthreads();
+      // triangular solve on the diagonal block, one thread per row
+      for (int rr = threadIdx.x; rr < nr; rr += kThreads) {
+        double* q = Qt + rr * ldq + j0;
+        for (int jj = 0; jj < jb; ++jj) {
+          double x = q[jj];
+          for (int ll = 0; ll < jj; ++ll) x -= q[ll] * Rb[ll * 33 + jj];
+          const double dgn = Rb[jj * 33 + jj];
+          q[jj] = dgn != 0.0 ? x / dgn : 0.0;
+        }
+      }
+      __syncthreads();
+    }
+    for (int e = threadIdx.x; e < nr * rk; e += kThreads) {
+      const int l = e / nr, rr = e % nr;
+      t.Qc[(r0 + rr) + (size_t)l * m] = Qt[rr * ldq + l];
+    }
+    __syncthreads();
+  }
+}
+
 // ------------------------------------------------------------ merge
 template <typename T>
 __global__ void k_merge(const MergeTask* __restrict__ tasks) {
@@ -1186,6 +1278,23 @@ cudaError_t launch_rrqr(const RrqrTask* t, int ntasks, int cs, int mmax, int kma
   if (ntasks <= 0) return cudaSuccess;
   return c_doubles ? launch_rrqr_t<true>(t, ntasks, cs, mmax, kmax, nlmax, rcmax, c_doubles, tol, pivot_rtol, st)
                    : launch_rrqr_t<false>(t, ntasks, cs, mmax, kmax, nlmax, rcmax, 0, tol, pivot_rtol, st);
+}
+
+int selected_qr_rows(int nmax) { return std::max(1, std::min(32, 12288 / (std::max(nmax, 1) + 1))); }
+
+size_t selected_qr_smem(int mmax, int nmax) {
+  const int rt = selected_qr_rows(nmax);
+  return smem_bytes(kRed + kNB + (size_t)std::max(nmax, 1) + (size_t)std::max(mmax, 1) +
+                    (size_t)rt * (std::max(nmax, 1) + 1) + 32 * 33);
+}
+
+cudaError_t launch_selected_qr(const RrqrTask* t, int ntasks, int cs, int mmax, int nmax, cudaStream_t st) {
+  if (cudaError_t pre = begin("launch_selected_qr")) return pre;
+  if (ntasks <= 0) return cudaSuccess;
+  const size_t b = selected_qr_smem(mmax, nmax);
+  if (cudaError_t e = prep(k_selected_qr, b)) return e;
+  return launch_clustered(k_selected_qr, ntasks, cs, b, st, t, cs, std::max(mmax, 1), std::max(nmax, 1),
+                          selected_qr_rows(nmax));
 }
 
 cudaError_t launch_merge(const MergeTask* t, int ntasks, cudaStream_t st) {

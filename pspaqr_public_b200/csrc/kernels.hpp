@@ -56,6 +56,12 @@ bool rrqr_cluster_fits(int cs, size_t smem, bool smem_c = false);
 cudaError_t launch_rrqr_assemble(const RrqrSrc* s, int nsrc, cudaStream_t st);
 cudaError_t launch_rrqr(const RrqrTask* t, int ntasks, int cs, int mmax, int kmax, int nlmax, int rcmax,
                         size_t c_doubles, double tol, double pivot_rtol, cudaStream_t st);
+// Householder QR of the columns C(:, colat[0:*rank]) (pivot order given) into
+// V / T / tau and the orthonormal basis Qc = C_sel R^{-1}; cs-CTA clusters,
+// tasks of at most mmax rows and nmax selected columns.  Uses C, Qc, V, T,
+// tau, colat, rank, m, ldw of the task.
+size_t selected_qr_smem(int mmax, int nmax);
+cudaError_t launch_selected_qr(const RrqrTask* t, int ntasks, int cs, int mmax, int nmax, cudaStream_t st);
 cudaError_t launch_merge(const MergeTask* t, int ntasks, cudaStream_t st);
 
 cudaError_t launch_fwd_elim(const FwdElimTask* t, const FwdOut* o, int ntasks, int nmax, int mmax, int* ticket,

@@ -443,6 +443,199 @@ __global__ void __launch_bounds__(kT) k_project(const SketchTask* __restrict__ t
   }
 }
 
+// G(i, j) = sum_r Y(r, i) Y(r, j) on tiles with r0 <= c0; an off-diagonal
+// tile is stored twice (G and its transpose) so that rows of G are whole.
+__global__ void __launch_bounds__(kT) k_gram(const SketchTask* __restrict__ tasks, const GemmTile* __restrict__ tiles) {
+  __shared__ double As[kKStep][kTile + 1];  // Y(k0 + kk, r0 + ii) at As[kk][ii]
+  __shared__ double Bs[kKStep][kTile + 1];  // Y(k0 + kk, c0 + jj) at Bs[kk][jj]
+  const GemmTile g = tiles[blockIdx.x];
+  const SketchTask t = tasks[g.task];
+  const int ell = *t.ell;
+  if (g.r0 >= ell || g.c0 >= ell) return;
+  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+  double acc[4][4] = {};
+  for (int k0 = 0; k0 < t.m; k0 += kKStep) {
+    for (int e = threadIdx.x; e < kTile * kKStep; e += kT) {
+      const int kk = e / kTile, ii = e % kTile;
+      const int r = k0 + kk;
+      const double* row = t.Y + (size_t)r * t.ldy;
+      As[kk][ii] = (r < t.m && g.r0 + ii < ell) ? row[g.r0 + ii] : 0.0;
+      Bs[kk][ii] = (r < t.m && g.c0 + ii < ell) ? row[g.c0 + ii] : 0.0;
+    }
+    __syncthreads();
+#pragma unroll 8
+    for (int kk = 0; kk < kKStep; ++kk) {
+      double a[4], b[4];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        a[q] = As[kk][ty + 16 * q];
+        b[q] = Bs[kk][tx + 16 * q];
+      }
+#pragma unroll
+      for (int p = 0; p < 4; ++p)
+#pragma unroll
+        for (int q = 0; q < 4; ++q) acc[p][q] += a[p] * b[q];
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int p = 0; p < 4; ++p) {
+    const int i = g.r0 + ty + 16 * p;
+    if (i >= ell) continue;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int j = g.c0 + tx + 16 * q;
+      if (j >= ell) continue;
+      t.G[(size_t)i * t.ldy + j] = acc[p][q];
+      if (g.r0 != g.c0) t.G[(size_t)j * t.ldy + i] = acc[p][q];
+    }
+  }
+}
+
+constexpr int kPT = 1024;  // threads of the pivoted Cholesky
+
+// (position, column) with the smallest position across the warp
+__device__ __forceinline__ void warp_min_pos(int& bp, int& bc) {
+  for (int o = 16; o > 0; o >>= 1) {
+    const int op = __shfl_xor_sync(0xffffffffu, bp, o);
+    const int oc = __shfl_xor_sync(0xffffffffu, bc, o);
+    if (op < bp || (op == bp && oc < bc)) {
+      bp = op;
+      bc = oc;
+    }
+  }
+}
+
+// Left-looking pivoted Cholesky of G = Y^T Y, one CTA per task.  d holds the
+// diagonal of the Schur complement (the squared partial column norms of the
+// pivoted QR of Y); step i picks the pivot as the pivoted QR does (the first
+// position within pivot_rtol of the largest norm, LAPACK-style position
+// swaps), stops at |L(i,i)| < stol |L(0,0)|, and computes column i of L over
+// the active columns from the rows of Lt kept in global memory:
+//   L(c, i) = (G(c, p) - sum_{k<i} L(c, k) L(p, k)) / L(i, i).
+// Threads are (k-group, column) pairs so that short columns still keep the
+// CTA's loads in flight.
+__global__ void __launch_bounds__(kPT) k_pchol(const SketchTask* __restrict__ tasks, double stol, double pivot_rtol) {
+  extern __shared__ double psm[];
+  __shared__ double s_v[kPT / 32];
+  __shared__ int s_p[kPT / 32], s_c[kPT / 32];
+  __shared__ int s_piv[2];
+  const SketchTask t = tasks[blockIdx.x];
+  const int n = *t.ell, ld = t.ldy;
+  if (n <= 0 || t.m <= 0 || t.w <= 0 || !t.G) return;
+  const int kmin = min(t.m, n);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  double* d = psm;
+  double* lp = d + n;
+  double* part = lp + n;
+  int* pos = reinterpret_cast<int*>(part + kPT);
+  int* at = pos + n;
+  const int cw = n < kPT ? (n + 31) / 32 * 32 : kPT;  // column slots
+  const int ng = kPT / cw;                            // k-groups
+  const int grp = threadIdx.x / cw, slot = threadIdx.x % cw;
+  for (int c = threadIdx.x; c < n; c += kPT) {
+    d[c] = t.G[(size_t)c * ld + c];
+    pos[c] = c;
+    at[c] = c;
+  }
+  __syncthreads();
+  double r00 = 0.0;
+  int rk = kmin;
+  for (int i = 0; i < kmin; ++i) {
+    // the largest partial norm over the active columns
+    double bv = -1.0;
+    for (int c = threadIdx.x; c < n; c += kPT)
+      if (pos[c] >= i) bv = fmax(bv, sqrt(fmax(d[c], 0.0)));
+    bv = warp_max(bv);
+    if (lane == 0) s_v[warp] = bv;
+    __syncthreads();
+    double M = s_v[0];
+    for (int q = 1; q < kPT / 32; ++q) M = fmax(M, s_v[q]);
+    // the first position within pivot_rtol of it
+    const double thr = M * (1.0 - pivot_rtol);
+    int bp = 0x7fffffff, bc = -1;
+    for (int c = threadIdx.x; c < n; c += kPT) {
+      const int p = pos[c];
+      if (p >= i && p < bp && sqrt(fmax(d[c], 0.0)) >= thr) {
+        bp = p;
+        bc = c;
+      }
+    }
+    warp_min_pos(bp, bc);
+    if (lane == 0) {
+      s_p[warp] = bp;
+      s_c[warp] = bc;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      int P = s_p[0], Cc = s_c[0];
+      for (int q = 1; q < kPT / 32; ++q)
+        if (s_p[q] < P) {
+          P = s_p[q];
+          Cc = s_c[q];
+        }
+      s_piv[0] = P;
+      s_piv[1] = Cc;
+    }
+    __syncthreads();
+    int ppos = s_piv[0], pcol = s_piv[1];
+    const int cur = at[i];
+    if (pcol < 0) {  // no finite maximum (NaN norms): keep the column at position i
+      ppos = i;
+      pcol = cur;
+    }
+    const double nrm = sqrt(fmax(d[pcol], 0.0));  // |R(i,i)|
+    if (i == 0) {
+      r00 = nrm;
+    } else if (!(nrm / r00 >= stol)) {
+      rk = i;
+      break;
+    }
+    __syncthreads();  // every thread has read at[i] and d[pcol]
+    if (threadIdx.x == 0) {
+      at[ppos] = cur;
+      pos[cur] = ppos;
+      at[i] = pcol;
+      pos[pcol] = i;
+      t.Lt[(size_t)i * ld + pcol] = nrm;
+    }
+    for (int k = threadIdx.x; k < i; k += kPT) lp[k] = t.Lt[(size_t)k * ld + pcol];
+    __syncthreads();
+    const double inv = nrm > 0.0 ? 1.0 / nrm : 0.0;
+    for (int c0 = 0; c0 < n; c0 += cw) {
+      const int c = c0 + slot;
+      const bool act = grp < ng && c < n && pos[c] > i;
+      double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
+      if (act) {
+        const double* col = t.Lt + c;
+        int k = grp;
+        for (; k + 3 * ng < i; k += 4 * ng) {
+          a0 += col[(size_t)k * ld] * lp[k];
+          a1 += col[(size_t)(k + ng) * ld] * lp[k + ng];
+          a2 += col[(size_t)(k + 2 * ng) * ld] * lp[k + 2 * ng];
+          a3 += col[(size_t)(k + 3 * ng) * ld] * lp[k + 3 * ng];
+        }
+        for (; k < i; k += ng) a0 += col[(size_t)k * ld] * lp[k];
+      }
+      const double acc = (a0 + a1) + (a2 + a3);
+      if (ng > 1) {
+        part[threadIdx.x] = acc;
+        __syncthreads();
+      }
+      if (grp == 0 && c < n && pos[c] > i) {
+        double sum = acc;
+        for (int q = 1; q < ng; ++q) sum += part[q * cw + slot];
+        const double l = (t.G[(size_t)c * ld + pcol] - sum) * inv;
+        t.Lt[(size_t)i * ld + c] = l;
+        d[c] -= l * l;
+      }
+      __syncthreads();
+    }
+  }
+  for (int k = threadIdx.x; k < n; k += kPT) t.colat[k] = at[k];
+  if (threadIdx.x == 0) *t.ell = rk;
+}
+
 // Residual scan over a block of 256 columns: res_j(k) = ||c_j||^2 -
 // sum_{l<k} B(l,j)^2, and M[k] = max_j res_j(k) by atomicMax on the bit
 // patterns of non-negative doubles (their order equals the values' order).
@@ -524,6 +717,29 @@ cudaError_t launch_project(const SketchTask* t, const GemmTile* tiles, int ntile
   if (ntiles <= 0) return cudaSuccess;
   k_project<<<ntiles, kT, 0, st>>>(t, tiles);
   return done_launch("launch_project");
+}
+
+cudaError_t launch_gram(const SketchTask* t, const GemmTile* tiles, int ntiles, cudaStream_t st) {
+  if (cudaError_t e = cudaGetLastError()) return e;
+  if (ntiles <= 0) return cudaSuccess;
+  k_gram<<<ntiles, kT, 0, st>>>(t, tiles);
+  return done_launch("launch_gram");
+}
+
+size_t pchol_smem(int nmax) {
+  const size_t n = (size_t)std::max(nmax, 1);
+  return sizeof(double) * (2 * n + kPT) + sizeof(int) * 2 * n;
+}
+
+cudaError_t launch_pchol(const SketchTask* t, int ntasks, int nmax, double stol, double pivot_rtol, cudaStream_t st) {
+  if (cudaError_t e = cudaGetLastError()) return e;
+  if (ntasks <= 0) return cudaSuccess;
+  const size_t smem = pchol_smem(nmax);
+  if (smem > 227 * 1024) return cudaErrorInvalidValue;
+  cudaError_t e = cudaFuncSetAttribute(k_pchol, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e) return e;
+  k_pchol<<<ntasks, kPT, smem, st>>>(t, stol, pivot_rtol);
+  return done_launch("launch_pchol");
 }
 
 cudaError_t launch_residual_scan(const SketchTask* t, const GemmTile* blocks, int nblocks, cudaStream_t st) {

@@ -10,9 +10,16 @@
 //   2. predicts the kept fraction rank / min(m, w) with a 3-layer MLP and
 //      sets the sketch width ell = min(min(m,w), ceil(pred * min(m,w)) + p);
 //   3. forms Y = C Omega (m x ell, Omega Rademacher) -- k_sketch;
-//   4. runs the pivoted QR of Y (the plain kernel, stopped at a tolerance ten
-//      times below tol), giving Householder reflectors and an orthonormal
-//      basis q_0..q_{k_Y-1} of the dominant part of range(Y);
+//   4. runs the pivoted QR of Y, stopped at a tolerance ten times below tol,
+//      giving Householder reflectors and an orthonormal basis q_0..q_{k_Y-1}
+//      of the dominant part of range(Y).  The pivots come from a pivoted
+//      Cholesky of the Gram matrix G = Y^T Y (k_gram, k_pchol): the pivot's
+//      Schur-complement diagonal is |R(i,i)|^2 of the pivoted QR of Y, so the
+//      pivot order and the stop rule are those of the pivoted QR; the
+//      Householder QR of the chosen columns and Qc = Y_sel R^{-1} follow
+//      (k_selected_qr).  Below a stop tolerance of kGramMinTol the Gram
+//      matrix cannot resolve the stop rule and the plain pivoted-QR kernel
+//      runs on Y instead;
 //   5. forms B = Q^T C and, for every k <= k_Y, the largest residual column
 //      norm max_j ||c_j - Q_k Q_k^T c_j|| -- k_project, k_residual_scan;
 //   6. keeps the smallest k >= 1 whose largest residual is below
@@ -43,6 +50,9 @@ struct SketchTask {
   int* ell;         // sketch width (written by the predictor, then the sketch's QR rank)
   double* Y;        // row-major m x ell sketch (ld ldy)
   const double* Qc; // m x ell orthonormal basis of range(Y), column-major (ld m)
+  double* G;        // ell x ell Gram matrix Y^T Y, row-major (ld ldy)
+  double* Lt;       // ell x ell: Lt[k * ldy + c] = L(c, k) of the pivoted Cholesky of G
+  int* colat;       // ell: column of Y at each pivot position
   double* B;        // ell x w projections Q^T C, row-major (ld w)
   unsigned long long* M;  // ell + 1 largest squared residuals (bit patterns of doubles >= 0)
   int* rank;        // kept rank (output)
@@ -71,6 +81,17 @@ cudaError_t launch_rank_features(const SketchTask* t, int ntasks, double tol, in
 cudaError_t launch_rank_predict(const SketchTask* t, int ntasks, RankModel model, cudaStream_t st);
 // Y = C Omega over the given tiles (tile rows: rows of C; tile columns: columns of Y)
 cudaError_t launch_sketch(const SketchTask* t, const GemmTile* tiles, int ntiles, cudaStream_t st);
+// smallest stop tolerance (relative to |R(0,0)|) the Gram pivoting resolves:
+// |R(i,i)|^2 / |R(0,0)|^2 >= 1e-10 stays four orders above the rounding of G
+constexpr double kGramMinTol = 1e-5;
+// G = Y^T Y over the given tiles (r0 <= c0; both triangles are written)
+cudaError_t launch_gram(const SketchTask* t, const GemmTile* tiles, int ntiles, cudaStream_t st);
+// Pivoted Cholesky of G (one CTA per task, nmax >= every ell): the pivot order
+// to colat and the rank -- the first i with |L(i,i)| < stol |L(0,0)|, else
+// min(m, ell) -- over *ell.  Ties within pivot_rtol of the largest diagonal
+// go to the smallest position, as in the pivoted QR.
+size_t pchol_smem(int nmax);
+cudaError_t launch_pchol(const SketchTask* t, int ntasks, int nmax, double stol, double pivot_rtol, cudaStream_t st);
 // B = Q^T C over the given tiles (tile rows: basis vectors; tile columns: columns of C)
 cudaError_t launch_project(const SketchTask* t, const GemmTile* tiles, int ntiles, cudaStream_t st);
 // residual scan over column blocks of 256 (tile.c0), then the rank choice
