@@ -177,7 +177,7 @@ def run_ours(args):
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")  # 256 MB > L2
     import ctypes as C
 
-    def device_step():
+    def device_step(prof=False):
         t.assemble()
         b_dev.copy_(torch.from_numpy(b_host).to("cuda"))
         flush.zero_()
@@ -187,6 +187,8 @@ def run_ours(args):
         torch.cuda.synchronize()
         l0 = T.kernel_launches()
         e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+        if prof:  # the launches of this step alone under `ncu --profile-from-start off`
+            torch.cuda.cudart().cudaProfilerStart()
         e0.record(stream)
         t.factorize()
         e1.record(stream)
@@ -197,6 +199,8 @@ def run_ours(args):
             raise RuntimeError(lib.spq_last_error(t._h))
         e2.record(stream)
         torch.cuda.synchronize()
+        if prof:
+            torch.cuda.cudart().cudaProfilerStop()
         return e0.elapsed_time(e2) / 1e3, e0.elapsed_time(e1) / 1e3, it.value, rr.value, T.kernel_launches() - l0
 
     def e2e_step():
@@ -241,8 +245,8 @@ def run_ours(args):
             for _ in range(args.warmup):
                 device_step()
             r = {"times": [], "ftimes": [], "iters": [], "rels": [], "launches": []}
-            for _ in range(args.steps):
-                dt, ft, it, rr, nl = device_step()
+            for si in range(args.steps):
+                dt, ft, it, rr, nl = device_step(args.profile == name and si == 0)
                 r["times"].append(dt)
                 r["ftimes"].append(ft)
                 r["iters"].append(it)
@@ -408,6 +412,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile", default="", choices=["", "fp64", "mixed+learned"],
+                    help="bracket the first timed step of this variant with cudaProfilerStart/Stop")
     ap.add_argument("--size", type=int, default=64,
                     help="grid points per side (64 = the benchmark; smaller members of the family for profiling)")
     args = ap.parse_args()

@@ -155,6 +155,10 @@ int spq_times(spq_tree* t, double* times);
 /* Per level, 8 values (milliseconds): geqrt+tsqrt chains, trailing updates,
  * scaling QR, scaling applies, RRQR, compression applies, merge, level total. */
 int spq_level_times(spq_tree* t, float* ms);
+/* Per level, 6 values: nominal flops of the first six phases of spq_level_times
+ * (chains, updates, scaling QR, scaling applies, pivoted QR or learned ranks,
+ * compression applies). */
+int spq_level_flops(spq_tree* t, double* flops);
 /* Nominal FP64 flops of the last factorization (LAPACK Working Note 41 counts). */
 double spq_factor_flops(spq_tree* t);
 /* Bytes of compression-matrix data the pivoted QR of the last factorization

@@ -233,6 +233,14 @@ int spq_times(spq_tree* h, double* times) {
   times[4] = h->t->t_gmres;
   return 0;
 }
+int spq_level_flops(spq_tree* h, double* flops) {
+  if (!h || !flops) return -1;
+  const auto& lt = h->t->level_timing();
+  for (size_t l = 0; l < lt.size(); ++l)
+    for (int k = 0; k < 6; ++k) flops[6 * l + k] = lt[l].flops[k];
+  return 0;
+}
+
 int spq_level_times(spq_tree* h, float* ms) {
   if (!h || !ms) return -1;
   const auto& lt = h->t->level_timing();

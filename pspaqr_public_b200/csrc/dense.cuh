@@ -329,111 +329,184 @@ __device__ void apply_q_right(const T* V, int ldv, const T* Tm, int k, T* C, int
 
 
 // ---------------------------------------------------------------- tiled matrix applies
-// Register-tiled FP64 block reflector applies on matrices: rows are streamed
-// through shared memory in tiles of kRT, each thread owns a 4 x 2 micro-tile
-// of W = V^T C (kNB x kNC) and of the update C -= V W2.  `sm` holds
-// kTileSmem doubles.
+// Register-tiled block reflector applies on matrices: rows are streamed
+// through shared memory in tiles of kRT; the left apply keeps two tiles in
+// flight (the next tile's global loads are issued before the current tile's
+// products).  `sm` holds kTileSmem elements.
 constexpr int kNC = 64;   // columns (rows for right applies) per pass
 constexpr int kRT = 32;   // rows (columns) per shared-memory tile
-constexpr int kTileSmem = kRT * (kNB + 1) + kNC * (kRT + 1) + kNB * kNC;
+constexpr int kTileSmem = 2 * kRT * (kNB + 1) + 2 * kRT * (kNC + 1) + kNB * kNC;
+
+// Load through L2 (kCg: data written by another CTA of the cluster) or as is.
+template <bool kCg, typename T>
+__device__ __forceinline__ T ld_v(const T* p) {
+  if (kCg) return __ldcg(p);
+  return *p;
+}
 
 // C (m x nc <= kNC) <- Q^T C with one panel: unit = 1: V unit lower trapezoidal
 // (geqrt / RRQR reflectors), A unused; unit = 0: pentagonal tpqrt panel,
-// [A (kb x nc); C] <- Q^T [A; C] with V full (m x kb).
-template <typename T>
+// [A (kb x nc); C] <- Q^T [A; C] with V full (m x kb).  Column c of A and C
+// is column c + (c / kNB) * cgap of the arrays (cgap > 0: the column panels
+// a CTA owns in a cluster-distributed factorization).  kCg: V and T are read
+// through L2.
+template <typename T, bool kCg = false>
 __device__ void tile_left_qt(const T* V, int ldv, const T* Tm, int ldt, int kb, int unit, T* A, int lda,
-                             T* C, int ldc, int m, int nc, T* sm) {
-  T* sV = sm;                              // [kRT][kNB+1]
-  T* sC = sV + kRT * (kNB + 1);            // [kRT][kNC+1]; later W2 [kNB][kNC]
-  T* sW = sC + kNC * (kRT + 1);            // [kNB][kNC]
+                             T* C, int ldc, int m, int nc, T* sm, int cgap = 0) {
+  constexpr int kVS = kRT * (kNB + 1), kCS = kRT * (kNC + 1);
+  T* sV0 = sm;                 // two [kRT][kNB+1] tiles of V
+  T* sC0 = sV0 + 2 * kVS;      // two [kRT][kNC+1] tiles of C; later W2 [kNB][kNC]
+  T* sW = sC0 + 2 * kCS;       // [kNB][kNC]
   const int t = threadIdx.x;
-  const int ti = t & 7, tc = t >> 3;            // rows ti*4..+3, cols tc*2..+1
-  T acc[4][2] = {{0, 0}, {0, 0}, {0, 0}, {0, 0}};
-  for (int r0 = 0; r0 < m; r0 += kRT) {
-    const int rn = (m - r0) < kRT ? (m - r0) : kRT;
-    for (int idx = t; idx < kRT * kNB; idx += kThreads) {
-      const int r = idx % kRT, i = idx / kRT, gr = r0 + r;
+  auto col = [&](int c) { return (size_t)(c + (c / kNB) * cgap); };
+  // loads of one tile: V element (idx & 31, idx >> 5) and C element
+  // (idx & 31, idx >> 5) for idx = t + kThreads * s (rows fastest: coalesced)
+  constexpr int kSV = kRT * kNB / kThreads, kSC = kRT * kNC / kThreads;
+  T rv[kSV], rc[kSC];
+  auto vload = [&](int r0) {
+#pragma unroll
+    for (int q = 0; q < kSV; ++q) {
+      const int idx = t + q * kThreads, r = idx & (kRT - 1), i = idx / kRT, gr = r0 + r;
       T v = 0.0;
-      if (r < rn && i < kb) v = unit ? (gr == i ? 1.0 : (gr < i ? 0.0 : V[gr + (size_t)i * ldv])) : V[gr + (size_t)i * ldv];
-      sV[r * (kNB + 1) + i] = v;
+      if (gr < m && i < kb)
+        v = unit ? (gr == i ? (T)1.0 : (gr < i ? (T)0.0 : ld_v<kCg>(V + gr + (size_t)i * ldv)))
+                 : ld_v<kCg>(V + gr + (size_t)i * ldv);
+      rv[q] = v;
     }
-    for (int idx = t; idx < kRT * kNC; idx += kThreads) {
-      const int r = idx % kRT, c = idx / kRT;
-      sC[r * (kNC + 1) + c] = (r < rn && c < nc) ? C[(r0 + r) + (size_t)c * ldc] : 0.0;
-    }
-    __syncthreads();
-#pragma unroll 4
-    for (int r = 0; r < kRT; ++r) {
-      const T* vr = sV + r * (kNB + 1) + ti * 4;
-      const T* cr = sC + r * (kNC + 1) + tc * 2;
-      const T b0 = cr[0], b1 = cr[1];
+  };
+  auto vstash = [&](int b) {
 #pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        const T a = vr[q];
-        acc[q][0] += a * b0;
-        acc[q][1] += a * b1;
+    for (int q = 0; q < kSV; ++q) {
+      const int idx = t + q * kThreads;
+      sV0[b * kVS + (idx & (kRT - 1)) * (kNB + 1) + idx / kRT] = rv[q];
+    }
+  };
+  const int ntile = (m + kRT - 1) / kRT;
+  // W = V^T C: thread rows ti*4..+3 of W, columns tc*2..+1
+  {
+    const int ti = t & 7, tc = t >> 3;
+    T acc[4][2] = {{0, 0}, {0, 0}, {0, 0}, {0, 0}};
+    auto cload = [&](int r0) {
+#pragma unroll
+      for (int q = 0; q < kSC; ++q) {
+        const int idx = t + q * kThreads, r = idx & (kRT - 1), c = idx / kRT;
+        rc[q] = (r0 + r < m && c < nc) ? C[(r0 + r) + col(c) * ldc] : (T)0.0;
       }
+    };
+    vload(0);
+    cload(0);
+    vstash(0);
+#pragma unroll
+    for (int q = 0; q < kSC; ++q) {
+      const int idx = t + q * kThreads;
+      sC0[(idx & (kRT - 1)) * (kNC + 1) + idx / kRT] = rc[q];
     }
     __syncthreads();
-  }
-#pragma unroll
-  for (int q = 0; q < 4; ++q)
-#pragma unroll
-    for (int p = 0; p < 2; ++p) {
-      const int i = ti * 4 + q, c = tc * 2 + p;
-      T w = acc[q][p];
-      if (!unit && i < kb && c < nc) w += A[i + (size_t)c * lda];
-      sW[i * kNC + c] = w;
-    }
-  __syncthreads();
-  // W2 = T^T W  (T upper triangular: W2(i) = sum_{l <= i} T(l, i) W(l))
-  T* sW2 = sC;
-#pragma unroll
-  for (int q = 0; q < 4; ++q)
-#pragma unroll
-    for (int p = 0; p < 2; ++p) {
-      const int i = ti * 4 + q, c = tc * 2 + p;
-      T s = 0.0;
-      if (i < kb)
-        for (int l = 0; l <= i; ++l) s += Tm[l + (size_t)i * ldt] * sW[l * kNC + c];
-      sW2[i * kNC + c] = s;
-    }
-  __syncthreads();
-  if (!unit)
-    for (int idx = t; idx < kb * nc; idx += kThreads) {
-      const int i = idx % kb, c = idx / kb;
-      A[i + (size_t)c * lda] -= sW2[i * kNC + c];
-    }
-  // C -= V W2
-  const int tr = t & 7, tcc = t >> 3;  // rows tr*4..+3, cols tcc*2..+1
-  for (int r0 = 0; r0 < m; r0 += kRT) {
-    const int rn = (m - r0) < kRT ? (m - r0) : kRT;
-    for (int idx = t; idx < kRT * kNB; idx += kThreads) {
-      const int r = idx % kRT, i = idx / kRT, gr = r0 + r;
-      T v = 0.0;
-      if (r < rn && i < kb) v = unit ? (gr == i ? 1.0 : (gr < i ? 0.0 : V[gr + (size_t)i * ldv])) : V[gr + (size_t)i * ldv];
-      sV[r * (kNB + 1) + i] = v;
-    }
-    __syncthreads();
-    T u[4][2] = {{0, 0}, {0, 0}, {0, 0}, {0, 0}};
-#pragma unroll 4
-    for (int i = 0; i < kNB; ++i) {
-      const T w0 = sW2[i * kNC + tcc * 2], w1 = sW2[i * kNC + tcc * 2 + 1];
-#pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        const T a = sV[(tr * 4 + q) * (kNB + 1) + i];
-        u[q][0] += a * w0;
-        u[q][1] += a * w1;
+    for (int tt = 0; tt < ntile; ++tt) {
+      const int b = tt & 1;
+      const bool more = tt + 1 < ntile;
+      if (more) {
+        vload((tt + 1) * kRT);
+        cload((tt + 1) * kRT);
       }
+      const T* sV = sV0 + b * kVS;
+      const T* sC = sC0 + b * kCS;
+#pragma unroll 8
+      for (int r = 0; r < kRT; ++r) {
+        const T* vr = sV + r * (kNB + 1) + ti * 4;
+        const T* cr = sC + r * (kNC + 1) + tc * 2;
+        const T b0 = cr[0], b1 = cr[1];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          const T a = vr[q];
+          acc[q][0] += a * b0;
+          acc[q][1] += a * b1;
+        }
+      }
+      if (more) {
+        vstash(b ^ 1);
+#pragma unroll
+        for (int q = 0; q < kSC; ++q) {
+          const int idx = t + q * kThreads;
+          sC0[(b ^ 1) * kCS + (idx & (kRT - 1)) * (kNC + 1) + idx / kRT] = rc[q];
+        }
+      }
+      __syncthreads();
     }
 #pragma unroll
     for (int q = 0; q < 4; ++q)
 #pragma unroll
       for (int p = 0; p < 2; ++p) {
-        const int r = tr * 4 + q, c = tcc * 2 + p;
-        if (r < rn && c < nc) C[(r0 + r) + (size_t)c * ldc] -= u[q][p];
+        const int i = ti * 4 + q, c = tc * 2 + p;
+        T w = acc[q][p];
+        if (!unit && i < kb && c < nc) w += A[i + col(c) * lda];
+        sW[i * kNC + c] = w;
       }
+  }
+  __syncthreads();
+  // W2 = T^T W  (T upper triangular: W2(i) = sum_{l <= i} T(l, i) W(l))
+  T* sW2 = sC0;
+  for (int idx = t; idx < kNB * kNC; idx += kThreads) {
+    const int i = idx / kNC, c = idx % kNC;
+    T s = 0.0;
+    if (i < kb)
+      for (int l = 0; l <= i; ++l) s += ld_v<kCg>(Tm + l + (size_t)i * ldt) * sW[l * kNC + c];
+    sW2[i * kNC + c] = s;
+  }
+  __syncthreads();
+  if (!unit)
+    for (int idx = t; idx < kb * nc; idx += kThreads) {
+      const int i = idx % kb, c = idx / kb;
+      A[i + col(c) * lda] -= sW2[i * kNC + c];
+    }
+  // C -= V W2: thread row r = t & 31 of each tile, columns g*8..+7 (g = t >> 5);
+  // the next tile's V and C are loaded before the current tile's products
+  {
+    const int r = t & (kRT - 1), g = t / kRT;
+    constexpr int kCPT = kRT * kNC / kThreads;  // columns per thread
+    T cc[kCPT], cn[kCPT];
+    auto crow = [&](int r0, T* dst) {
+#pragma unroll
+      for (int p = 0; p < kCPT; ++p) {
+        const int c = g * kCPT + p;
+        dst[p] = (r0 + r < m && c < nc) ? C[(r0 + r) + col(c) * ldc] : (T)0.0;
+      }
+    };
+    vload(0);
+    crow(0, cc);
+    vstash(0);
     __syncthreads();
+    for (int tt = 0; tt < ntile; ++tt) {
+      const int b = tt & 1, r0 = tt * kRT;
+      const bool more = tt + 1 < ntile;
+      if (more) {
+        vload(r0 + kRT);
+        crow(r0 + kRT, cn);
+      }
+      const T* vr = sV0 + b * kVS + r * (kNB + 1);
+      T u[kCPT];
+#pragma unroll
+      for (int p = 0; p < kCPT; ++p) u[p] = 0.0;
+#pragma unroll 8
+      for (int i = 0; i < kNB; ++i) {
+        const T a = vr[i];
+        const T* w = sW2 + i * kNC + g * kCPT;
+#pragma unroll
+        for (int p = 0; p < kCPT; ++p) u[p] += a * w[p];
+      }
+      if (r0 + r < m)
+#pragma unroll
+        for (int p = 0; p < kCPT; ++p) {
+          const int c = g * kCPT + p;
+          if (c < nc) C[(r0 + r) + col(c) * ldc] = cc[p] - u[p];
+        }
+      if (more) {
+        vstash(b ^ 1);
+#pragma unroll
+        for (int p = 0; p < kCPT; ++p) cc[p] = cn[p];
+      }
+      __syncthreads();
+    }
   }
 }
 

@@ -318,6 +318,14 @@ int Tree::factorize() {
   auto ck = [&](cudaError_t e, const char* where) { return check_cuda(e, where); };
   for (int lvl = 0; lvl < L; ++lvl) {
     const Level& Lv = st_.levels[lvl];
+    const double h0 = wall();
+    double hwait = 0;  // host time blocked in the level's intermediate synchronisations
+    auto sync_timed = [&](const char* where) {
+      const double a = wall();
+      const cudaError_t e = cudaStreamSynchronize(stream_);
+      hwait += wall() - a;
+      return ck(e, where);
+    };
     cudaEventRecord(ev[0], stream_);
     // ---------------- elimination: geqrt + tsqrt chains, grouped by cluster size
     std::vector<ElimTask> et[3];
@@ -335,7 +343,7 @@ int Tree::factorize() {
       t.tau = scratch_.dalloc(std::max(nc, 1));
       t.n = nc;
       t.out_begin = (int)eo.size();
-      flops_ += 2.0 * nc * nc * (nc - nc / 3.0);
+      lt_[lvl].flops[0] += 2.0 * nc * nc * (nc - nc / 3.0);
       int vm = nc;
       for (int q = Lv.out_begin[ii]; q < Lv.out_end[ii]; ++q) {
         const int e = Lv.out_edges[q];
@@ -346,7 +354,7 @@ int Tree::factorize() {
         o.m = rows_[e];
         eo.push_back(o);
         vm = std::max(vm, o.m);
-        flops_ += 2.0 * rows_[e] * nc * nc;
+        lt_[lvl].flops[0] += 2.0 * rows_[e] * nc * nc;
       }
       t.out_end = (int)eo.size();
       if (!t.T || !t.tau) return fail(-11, "out of device memory (elimination)");
@@ -380,7 +388,7 @@ int Tree::factorize() {
         a.lda = ld_[ecm];
         a.ldb = 0;
         uo.push_back(a);
-        flops_ += 4.0 * nc * nc * ncol;
+        lt_[lvl].flops[1] += 4.0 * nc * nc * ncol;
         const int ii = (int)(std::lower_bound(Lv.interiors.begin(), Lv.interiors.end(), c) - Lv.interiors.begin());
         int j = Lv.col_emn_begin[q];
         for (int r = Lv.out_begin[ii]; r < Lv.out_end[ii]; ++r, ++j) {
@@ -398,7 +406,7 @@ int Tree::factorize() {
           b.lda = ld_[ecm];
           b.ldb = ld_[emn];
           uo.push_back(b);
-          flops_ += 4.0 * rows_[ecn] * nc * ncol;
+          lt_[lvl].flops[1] += 4.0 * rows_[ecn] * nc * ncol;
         }
       }
       const int op_end = (int)uo.size();
@@ -415,6 +423,18 @@ int Tree::factorize() {
         }
       printf("level %d elim groups (cs 1/4/%d): %zu/%zu/%zu tasks, nmax %d/%d/%d, outs %zu, sum n^3 %.3g, sum m n^2 %.3g\n",
              lvl, kBigCluster, et[0].size(), et[1].size(), et[2].size(), nmax[0], nmax[1], nmax[2], eo.size(), n3, mn2);
+      double fsum = 0, fmax = 0;
+      int omax = 0;
+      for (const UpdTask& u : ut) {
+        double f = 0;
+        for (int o = u.op_begin; o < u.op_end; ++o)
+          f += 4.0 * uo[o].k * (uo[o].kind == 0 ? uo[o].m : uo[o].m + uo[o].k) * u.ncols;
+        fsum += f;
+        fmax = std::max(fmax, f);
+        omax = std::max(omax, u.op_end - u.op_begin);
+      }
+      printf("level %d updates: %zu tasks, %zu ops, %.3g flops, mean %.3g max %.3g per task, max ops %d\n", lvl,
+             ut.size(), uo.size(), fsum, fsum / std::max<size_t>(ut.size(), 1), fmax, omax);
     }
     {
       auto* d_eo = static_cast<ElimOut*>(upload(eo.data(), sizeof(ElimOut) * eo.size()));
@@ -450,7 +470,7 @@ int Tree::factorize() {
         const int g = cs == 1 ? 0 : (cs == 4 ? 1 : 2);
         sc[g].push_back(t);
         smax[g] = std::max(smax[g], np);
-        flops_ += 2.0 * np * np * (np - np / 3.0);
+        lt_[lvl].flops[2] += 2.0 * np * np * (np - np / 3.0);
       }
       if (verbose >= 2) {
         double n3 = 0;
@@ -478,7 +498,7 @@ int Tree::factorize() {
             t.cnt = std::min(kChunk, t.nc - c0);
             rows_scale.push_back(t);
           }
-          flops_ += 4.0 * t.m * t.m * t.nc;
+          lt_[lvl].flops[3] += 4.0 * t.m * t.m * t.nc;
         }
         if (c) {
           t.V = ptr_[Lv.self_edge_of[E.n1 - Lv.first]];
@@ -489,7 +509,7 @@ int Tree::factorize() {
             t.cnt = std::min(kChunk, t.m - r0);
             cols_scale.push_back(t);
           }
-          flops_ += (double)t.m * t.nc * t.nc;
+          lt_[lvl].flops[3] += (double)t.m * t.nc * t.nc;
         }
       }
       // compression matrices C (m x w) of the level's interfaces, gathered
@@ -755,7 +775,7 @@ int Tree::factorize() {
         cudaEventRecord(le[0], stream_);
         std::vector<int> ell(nsp);
         if (ck(cudaMemcpyAsync(ell.data(), d_ell, sizeof(int) * nsp, cudaMemcpyDeviceToHost, stream_), "sketch widths") ||
-            ck(cudaStreamSynchronize(stream_), "rank prediction"))
+            sync_timed("rank prediction"))
           return -10;
         std::vector<GemmTile> sk_tiles, pj_tiles, scan_blocks, gram_tiles;
         RrqrGroups G;
@@ -859,7 +879,7 @@ int Tree::factorize() {
         cudaEventRecord(le[4], stream_);
         std::vector<int> fb(nsp);
         if (ck(cudaMemcpyAsync(fb.data(), d_fb, sizeof(int) * nsp, cudaMemcpyDeviceToHost, stream_), "fallback flags") ||
-            ck(cudaStreamSynchronize(stream_), "rank selection"))
+            sync_timed("rank selection"))
           return -10;
         RrqrGroups Fb;
         double fb_work = 0;
@@ -868,7 +888,7 @@ int Tree::factorize() {
         for (size_t q = 0; q < nsp; ++q) {
           const int p = Lv.spars_clusters[q];
           const SketchTask& t = sk[q];
-          flops_ += 4.0 * t.m * (double)t.w * ell[q];  // sketch + projection GEMMs
+          lt_[lvl].flops[4] += 4.0 * t.m * (double)t.w * ell[q];  // sketch + projection GEMMs
           learned_ell_ += ell[q];
           if (t.m <= 0 || t.w <= 0) continue;
           sketch_qr.push_back({(double)t.m, (double)ell[q], (double)ell[q]});
@@ -928,8 +948,21 @@ int Tree::factorize() {
       cudaEventRecord(ev[3], stream_);
       if (ck(cudaMemcpyAsync(host_rank.data(), d_rank_, sizeof(int) * host_rank.size(), cudaMemcpyDeviceToHost, stream_),
              "rank readback") ||
-          ck(cudaStreamSynchronize(stream_), "sparsification"))
+          sync_timed("sparsification"))
         return -10;
+      // compression applies: Q^T of the interface's r reflectors on the rows
+      // of its edges, Q on their columns (4 m r - 2 r^2 per vector)
+      for (int e : Lv.spars_edges) {
+        const Edge& E = st_.edges[e];
+        if (st_.clusters[E.n1].sparsify) {
+          const double n = size_[E.n1], r = host_rank[E.n1];
+          lt_[lvl].flops[5] += (4.0 * n * r - 2.0 * r * r) * rows_[e];
+        }
+        if (st_.clusters[E.n2].sparsify) {
+          const double m = size_[E.n2], r = host_rank[E.n2];
+          lt_[lvl].flops[5] += (4.0 * m * r - 2.0 * r * r) * cols_[e];
+        }
+      }
       for (int p : Lv.spars_clusters) size_[p] = host_rank[p];
       if (rank_log_ && nsp) {
         std::vector<float> f(kRankFeatures * nsp);
@@ -953,7 +986,7 @@ int Tree::factorize() {
       // the pivoted QR moves: the transposed gather (read + write), one pass
       // for the norms, one per pivot step over the active columns
       auto account = [&](double m, double w, double steps, double r) {
-        flops_ += 4.0 * m * w * r - 2.0 * r * r * (m + w) + 4.0 * r * r * r / 3.0 + m * r * r;
+        lt_[lvl].flops[4] += 4.0 * m * w * r - 2.0 * r * r * (m + w) + 4.0 * r * r * r / 3.0 + m * r * r;
         rrqr_bytes_ += 8.0 * m * (3.0 * w + steps * w - steps * (steps + 1.0) / 2.0);
       };
       for (const auto& e : sketch_qr) account(e[0], e[1], e[2], e[2]);
@@ -1016,7 +1049,14 @@ int Tree::factorize() {
       if (ck(launch_merge(d_mt, (int)mt.size(), stream_), "merge kernel")) return -10;
     }
     cudaEventRecord(ev[4], stream_);
+    const double h1 = wall();
     if (ck(cudaStreamSynchronize(stream_), "factorize level")) return -10;
+    if (verbose >= 2) {
+      float gpu_ms = 0;
+      cudaEventElapsedTime(&gpu_ms, ev[0], ev[4]);
+      printf("level %d host: busy %.2f ms, waits %.2f + final %.2f ms, GPU level %.2f ms\n", lvl,
+             1e3 * (h1 - h0 - hwait), 1e3 * hwait, 1e3 * (wall() - h1), gpu_ms);
+    }
     cudaEventElapsedTime(&lt_[lvl].elim_ms, ev[0], ev[1]);
     cudaEventElapsedTime(&lt_[lvl].scale_ms, ev[1], ev[2]);
     cudaEventElapsedTime(&lt_[lvl].spars_ms, ev[2], ev[3]);
@@ -1035,6 +1075,8 @@ int Tree::factorize() {
   }
   for (auto& e : ev) cudaEventDestroy(e);
   for (auto& e : fe) cudaEventDestroy(e);
+  for (const LevelTiming& t : lt_)
+    for (double f : t.flops) flops_ += f;
   factorized_ = true;
   int rc = build_solve_graph();
   if (rc) return rc;

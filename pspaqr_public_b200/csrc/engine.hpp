@@ -45,6 +45,9 @@ struct LevelTiming {
   // finer split: geqrt+tsqrt chains, trailing updates, scaling QR, scaling
   // applies, RRQR, compression applies
   float e1_ms = 0, e2_ms = 0, sqr_ms = 0, sapp_ms = 0, rrqr_ms = 0, capp_ms = 0;
+  // nominal flops of the same phases (chains, updates, scaling QR, scaling
+  // applies, pivoted QR / learned ranks, compression applies)
+  double flops[6] = {0, 0, 0, 0, 0, 0};
   int ntasks_elim = 0, ntasks_upd = 0, nspars = 0;
 };
 

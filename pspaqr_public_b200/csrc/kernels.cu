@@ -57,70 +57,85 @@ __global__ void k_scatter(int nnz, const double* __restrict__ val, double* const
 }
 
 // ------------------------------------------------------------ distributed Householder QR
-// Reflector j of a geqrt (unit = 1: v = [1; S(j+1:m, j)]) or of a tpqrt step
-// (unit = 0: v = [1 (on R(j,j)); B(:, j)]).  The owner of column j computes it;
-// after the cluster barrier every CTA loads the tail into shared `vb` and
-// applies H_j to its own columns k > j.  `lt` holds the owner's tau values for
-// its panels (T factors), `tg` broadcasts tau through global memory.
+// Blocked Householder QR over a cluster: a geqrt (unit = 1: reflector j is
+// v = [1; R(j+1:m, j)]) or a tpqrt (unit = 0: v = [1 (on R(j,j)); B(:, j)]).
+// The 32-column panels are dealt round-robin to the cluster's CTAs.  For each
+// panel its owner builds the kb reflectors, applying each only inside the
+// panel, and the panel's T factor; after one cluster barrier every CTA
+// applies the block reflector to its own later panels with the tiled apply
+// (two of its panels per pass).  `lt` holds the owner's tau values, `tg`
+// the global copy, `vb` a reflector tail, `tile` dev::kTileSmem elements.
 template <typename T>
 __device__ void dist_qr(T* R, int ldr, T* B, int ldb, int m, int n, int unit, T* Tout, T* tg,
-                        T* lt, T* vb, T* red, T* tmp, int cs) {
+                        T* lt, T* vb, T* red, T* tmp, T* tile, int cs) {
   const int rank = crank(cs);
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  // unit: reflector tails live in R itself (rows j+1..m-1 of column j), m rows
-  // pentagonal: tails are the m rows of B, the diagonal lives in R
-  for (int j = 0; j < n; ++j) {
-    const int vlen = unit ? (m - j - 1) : m;
-    T* tail = unit ? (R + (j + 1) + (size_t)j * ldr) : (B + (size_t)j * ldb);
-    if (owns(j, rank, cs)) {
-      T s = 0.0;
-      for (int i = threadIdx.x; i < vlen; i += kThreads) s += tail[i] * tail[i];
-      s = dev::cta_sum(s, red);
-      const T alpha = R[j + (size_t)j * ldr];
-      T beta, scal;
-      const T tj = dev::house(alpha, s, &beta, &scal);
-      if (tj != 0.0)
-        for (int i = threadIdx.x; i < vlen; i += kThreads) tail[i] *= scal;
-      __syncthreads();
-      if (threadIdx.x == 0) {
-        R[j + (size_t)j * ldr] = beta;
-        lt[j] = tj;
-        tg[j] = tj;
+  const int gap = (cs - 1) * kNB;  // columns between two panels of one CTA
+  for (int j0 = 0; j0 < n; j0 += kNB) {
+    const int kb = (n - j0) < kNB ? (n - j0) : kNB;
+    const int pend = j0 + kb;
+    if (owns(j0, rank, cs)) {
+      for (int j = j0; j < pend; ++j) {
+        const int vlen = unit ? (m - j - 1) : m;
+        T* tail = unit ? (R + (j + 1) + (size_t)j * ldr) : (B + (size_t)j * ldb);
+        T s = 0.0;
+        for (int i = threadIdx.x; i < vlen; i += kThreads) s += tail[i] * tail[i];
+        s = dev::cta_sum(s, red);
+        const T alpha = R[j + (size_t)j * ldr];
+        T beta, scal;
+        const T tj = dev::house(alpha, s, &beta, &scal);
+        if (tj != 0.0)
+          for (int i = threadIdx.x; i < vlen; i += kThreads) {
+            const T v = tail[i] * scal;
+            tail[i] = v;
+            vb[i] = v;
+          }
+        if (threadIdx.x == 0) {
+          R[j + (size_t)j * ldr] = beta;
+          lt[j] = tj;
+          tg[j] = tj;
+        }
+        __syncthreads();
+        // H_j on the panel's later columns
+        if (tj != 0.0)
+          for (int k = j + 1 + warp; k < pend; k += kWarps) {
+            T* rjk = R + j + (size_t)k * ldr;
+            T* tk = unit ? (R + (j + 1) + (size_t)k * ldr) : (B + (size_t)k * ldb);
+            T d = lane == 0 ? *rjk : 0.0;
+            for (int i = lane; i < vlen; i += 32) d += vb[i] * tk[i];
+            d = dev::warp_sum(d) * tj;
+            if (lane == 0) *rjk -= d;
+            for (int i = lane; i < vlen; i += 32) tk[i] -= vb[i] * d;
+          }
+        __syncthreads();
       }
+      if (unit)
+        dev::panel_t(R + j0 + (size_t)j0 * ldr, ldr, m - j0, kb, 1, lt + j0, Tout + (size_t)j0 * kNB, kNB, tmp);
+      else
+        dev::panel_t(B + (size_t)j0 * ldb, ldb, m, kb, 0, lt + j0, Tout + (size_t)j0 * kNB, kNB, tmp);
       __threadfence();
     }
     csync(cs);
-    const T tj = __ldcg(tg + j);
-    if (tj != 0.0) {
-      for (int i = threadIdx.x; i < vlen; i += kThreads) vb[i] = __ldcg(tail + i);
-      __syncthreads();
-      // apply H_j to own columns k > j
-      for (int k = j + 1 + warp; k < n; k += kWarps) {
-        if (!owns(k, rank, cs)) continue;
-        T* rjk = R + j + (size_t)k * ldr;
-        T* tk = unit ? (R + (j + 1) + (size_t)k * ldr) : (B + (size_t)k * ldb);
-        T d = lane == 0 ? *rjk : 0.0;
-        for (int i = lane; i < vlen; i += 32) d += vb[i] * tk[i];
-        d = dev::warp_sum(d) * tj;
-        if (lane == 0) *rjk -= d;
-        for (int i = lane; i < vlen; i += 32) tk[i] -= vb[i] * d;
-      }
+    // the panel's block reflector on own later panels, two per pass
+    const T* Tm = Tout + (size_t)j0 * kNB;
+    int q0 = pend;  // first column of own later panels
+    while (q0 < n && !owns(q0, rank, cs)) q0 += kNB;
+    for (; q0 < n; q0 += 2 * cs * kNB) {
+      const int second = q0 + cs * kNB;
+      const int nc = (q0 + kNB < n ? kNB : n - q0) + (second < n ? ((second + kNB < n ? kNB : n - second)) : 0);
+      if (unit)
+        dev::tile_left_qt<T, true>(R + j0 + (size_t)j0 * ldr, ldr, Tm, kNB, kb, 1, nullptr, 0,
+                                   R + j0 + (size_t)q0 * ldr, ldr, m - j0, nc, tile, gap);
+      else
+        dev::tile_left_qt<T, true>(B + (size_t)j0 * ldb, ldb, Tm, kNB, kb, 0, R + j0 + (size_t)q0 * ldr, ldr,
+                                   B + (size_t)q0 * ldb, ldb, m, nc, tile, gap);
     }
-    __syncthreads();
-  }
-  // block factors of own panels
-  for (int j0 = rank * kNB; j0 < n; j0 += cs * kNB) {
-    const int kb = (n - j0) < kNB ? (n - j0) : kNB;
-    if (unit)
-      dev::panel_t(R + j0 + (size_t)j0 * ldr, ldr, m - j0, kb, 1, lt + j0, Tout + (size_t)j0 * kNB, kNB, tmp);
-    else
-      dev::panel_t(B + (size_t)j0 * ldb, ldb, m, kb, 0, lt + j0, Tout + (size_t)j0 * kNB, kNB, tmp);
   }
   csync(cs);
 }
 
 template <typename T>
-__global__ void __launch_bounds__(kThreads) k_elim(const ElimTask* __restrict__ tasks, const ElimOut* __restrict__ outs,
+__global__ void __launch_bounds__(kThreads, 2) k_elim(const ElimTask* __restrict__ tasks, const ElimOut* __restrict__ outs,
                                                    int cs, int vmax) {
   extern __shared__ __align__(16) unsigned char smraw[];
   T* sm = reinterpret_cast<T*>(smraw);
@@ -129,16 +144,17 @@ __global__ void __launch_bounds__(kThreads) k_elim(const ElimTask* __restrict__ 
   T* tmp = red + kRed;
   T* lt = tmp + kNB;
   T* vb = lt + t.n;
-  (void)vmax;
-  dist_qr<T>(as<T>(t.S), t.n, nullptr, 0, t.n, t.n, 1, as<T>(t.T), as<T>(t.tau), lt, vb, red, tmp, cs);
+  T* tile = vb + vmax;
+  dist_qr<T>(as<T>(t.S), t.n, nullptr, 0, t.n, t.n, 1, as<T>(t.T), as<T>(t.tau), lt, vb, red, tmp, tile, cs);
   for (int o = t.out_begin; o < t.out_end; ++o) {
     const ElimOut e = outs[o];
-    dist_qr<T>(as<T>(t.S), t.n, as<T>(e.B), e.m, e.m, t.n, 0, as<T>(e.T), as<T>(t.tau), lt, vb, red, tmp, cs);
+    dist_qr<T>(as<T>(t.S), t.n, as<T>(e.B), e.m, e.m, t.n, 0, as<T>(e.T), as<T>(t.tau), lt, vb, red, tmp, tile,
+               cs);
   }
 }
 
 template <typename T>
-__global__ void __launch_bounds__(kThreads) k_scale(const ScaleTask* __restrict__ tasks, int cs) {
+__global__ void __launch_bounds__(kThreads, 2) k_scale(const ScaleTask* __restrict__ tasks, int cs) {
   extern __shared__ __align__(16) unsigned char smraw[];
   T* sm = reinterpret_cast<T*>(smraw);
   const ScaleTask t = tasks[blockIdx.x / cs];
@@ -146,12 +162,12 @@ __global__ void __launch_bounds__(kThreads) k_scale(const ScaleTask* __restrict_
   T* tmp = red + kRed;
   T* lt = tmp + kNB;
   T* vb = lt + t.n;
-  dist_qr<T>(as<T>(t.S), t.n, nullptr, 0, t.n, t.n, 1, as<T>(t.T), as<T>(t.tau), lt, vb, red, tmp, cs);
+  dist_qr<T>(as<T>(t.S), t.n, nullptr, 0, t.n, t.n, 1, as<T>(t.T), as<T>(t.tau), lt, vb, red, tmp, vb + t.n, cs);
 }
 
 // ------------------------------------------------------------ chunked applies
 template <typename T>
-__global__ void __launch_bounds__(kThreads) k_update(const UpdTask* __restrict__ tasks, const UpdOp* __restrict__ ops) {
+__global__ void __launch_bounds__(kThreads, 2) k_update(const UpdTask* __restrict__ tasks, const UpdOp* __restrict__ ops) {
   extern __shared__ __align__(16) unsigned char smraw[];
   T* sm = reinterpret_cast<T*>(smraw);
   const UpdTask t = tasks[blockIdx.x];
@@ -168,7 +184,7 @@ __global__ void __launch_bounds__(kThreads) k_update(const UpdTask* __restrict__
 
 // row scaling: columns [lo, lo+cnt) of A <- Qs^T A
 template <typename T>
-__global__ void __launch_bounds__(kThreads) k_edge_left(const EdgeChunk* __restrict__ tasks) {
+__global__ void __launch_bounds__(kThreads, 2) k_edge_left(const EdgeChunk* __restrict__ tasks) {
   extern __shared__ __align__(16) unsigned char smraw[];
   T* sm = reinterpret_cast<T*>(smraw);
   const EdgeChunk t = tasks[blockIdx.x];
@@ -364,6 +380,12 @@ __device__ __forceinline__ void warp_min_pos(int& bp, int& bc) {
   }
 }
 
+// Partial-sum scratch of k_rrqr; vn1, vn2 and it also hold the tiled-apply
+// scratch of the final QR (dev::kTileSmem doubles).
+__host__ __device__ constexpr int rrqr_gp_doubles(int nlmax) {
+  return 8 * kThreads > dev::kTileSmem - 2 * nlmax ? 8 * kThreads : dev::kTileSmem - 2 * nlmax;
+}
+
 // Shared-memory carve of k_rrqr (doubles, then ints); rrqr_smem mirrors it.
 struct RrqrSmem {
   double *red, *tmp, *spa, *spb, *s1, *s2, *sq, *cv, *qf, *vn1, *vn2, *gp;
@@ -381,7 +403,7 @@ struct RrqrSmem {
     vn1 = qf + mmax;
     vn2 = vn1 + nlmax;
     gp = vn2 + nlmax;
-    pos = reinterpret_cast<int*>(gp + 8 * kThreads);
+    pos = reinterpret_cast<int*>(gp + rrqr_gp_doubles(nlmax));
     flg = pos + nlmax;
   }
 };
@@ -749,7 +771,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_rrqr(const RrqrTask* __restrict
     for (int r = lane; r < m; r += 32) t.V[r + (size_t)l * m] = __ldg(Ct + (size_t)r * ldw + c);
   }
   __syncthreads();
-  dist_qr<double>(t.V, m, nullptr, 0, m, rk, 1, t.T, t.tau, S.s1, S.qf, S.red, S.tmp, cs);
+  dist_qr<double>(t.V, m, nullptr, 0, m, rk, 1, t.T, t.tau, S.s1, S.qf, S.red, S.tmp, S.vn1, cs);
   if (rank == 0 && threadIdx.x == 0) {
     *t.rank = rk;
     if (t.stats) t.stats[6] = (int)((clock64() - tq) >> 10);
@@ -774,7 +796,7 @@ __global__ void __launch_bounds__(kThreads) k_selected_qr(const RrqrTask* __rest
   double* lt = tmp + kNB;
   double* vb = lt + nmax;
   const int ldq = nmax + 1;
-  double* Qt = vb + mmax;      // rt x ldq: rows of the basis being solved
+  double* Qt = vb + mmax;      // rt x ldq: rows of the basis being solved (first the QR's tile scratch)
   double* Rb = Qt + (size_t)rt * ldq;  // 32 x 33 block of R
   const double* __restrict__ C = t.C;
   for (int l = warp; l < rk; l += kWarps) {
@@ -783,7 +805,7 @@ __global__ void __launch_bounds__(kThreads) k_selected_qr(const RrqrTask* __rest
     for (int r = lane; r < m; r += 32) t.V[r + (size_t)l * m] = __ldg(C + (size_t)r * ldw + c);
   }
   __syncthreads();
-  dist_qr<double>(t.V, m, nullptr, 0, m, rk, 1, t.T, t.tau, lt, vb, red, tmp, cs);
+  dist_qr<double>(t.V, m, nullptr, 0, m, rk, 1, t.T, t.tau, lt, vb, red, tmp, Qt, cs);
   // R(l, j) = V[l + j m] for l <= j, written by the owners of column j
   auto R = [&](int l, int j) { return __ldcg(t.V + l + (size_t)j * m); };
   const int rc = (m + cs - 1) / cs;
@@ -1154,7 +1176,7 @@ cudaError_t launch_elim(const ElimTask* t, const ElimOut* o, int ntasks, int cs,
                         cudaStream_t st) {
   if (cudaError_t pre = begin("launch_elim")) return pre;
   if (ntasks <= 0) return cudaSuccess;
-  const size_t b = smem_bytes(kRed + kNB + (size_t)nmax + (size_t)std::max(vmax, 1));
+  const size_t b = smem_bytes(kRed + kNB + (size_t)nmax + (size_t)std::max(vmax, 1) + kWcap);
   if (g_fp32) {
     if (cudaError_t e = prep(k_elim<float>, b)) return e;
     return launch_clustered(k_elim<float>, ntasks, cs, b, st, t, o, cs, vmax);
@@ -1166,7 +1188,7 @@ cudaError_t launch_elim(const ElimTask* t, const ElimOut* o, int ntasks, int cs,
 cudaError_t launch_scale(const ScaleTask* t, int ntasks, int cs, int nmax, cudaStream_t st) {
   if (cudaError_t pre = begin("launch_scale")) return pre;
   if (ntasks <= 0) return cudaSuccess;
-  const size_t b = smem_bytes(kRed + kNB + 2 * (size_t)nmax);
+  const size_t b = smem_bytes(kRed + kNB + 2 * (size_t)nmax + kWcap);
   if (g_fp32) {
     if (cudaError_t e = prep(k_scale<float>, b)) return e;
     return launch_clustered(k_scale<float>, ntasks, cs, b, st, t, cs);
@@ -1215,7 +1237,7 @@ cudaError_t launch_edge(int kind, const EdgeChunk* t, int ntasks, cudaStream_t s
 
 size_t rrqr_smem(int mmax, int kmax, int nlmax, int rcmax, size_t c_doubles) {
   const size_t d = kRed + kNB + 4 * ((size_t)kmax + 1) + 2 * (size_t)rcmax + (size_t)std::max(mmax, 1) +
-                   2 * (size_t)nlmax + 8 * (size_t)kThreads;
+                   2 * (size_t)nlmax + (size_t)rrqr_gp_doubles(nlmax);
   size_t b = smem_bytes(d) + sizeof(int) * 2 * (size_t)nlmax;
   if (c_doubles) b += 16 + smem_bytes(c_doubles);
   return b;
@@ -1285,7 +1307,7 @@ int selected_qr_rows(int nmax) { return std::max(1, std::min(32, 12288 / (std::m
 size_t selected_qr_smem(int mmax, int nmax) {
   const int rt = selected_qr_rows(nmax);
   return smem_bytes(kRed + kNB + (size_t)std::max(nmax, 1) + (size_t)std::max(mmax, 1) +
-                    (size_t)rt * (std::max(nmax, 1) + 1) + 32 * 33);
+                    std::max((size_t)rt * (std::max(nmax, 1) + 1) + 32 * 33, (size_t)kWcap));
 }
 
 cudaError_t launch_selected_qr(const RrqrTask* t, int ntasks, int cs, int mmax, int nmax, cudaStream_t st) {

@@ -92,6 +92,7 @@ def lib():
             "spq_get_block": (i32, [vp, i32, i32, pd, pi]),
             "spq_times": (i32, [vp, pd]),
             "spq_level_times": (i32, [vp, pf]),
+            "spq_level_flops": (i32, [vp, pd]),
             "spq_factor_flops": (f64, [vp]),
             "spq_rrqr_bytes": (f64, [vp]),
             "spq_pool_bytes": (f64, [vp]),
@@ -389,6 +390,12 @@ class ParTree:
         out = np.zeros(8 * self.nlevels, np.float32)
         lib().spq_level_times(self._h, out.ctypes.data_as(C.POINTER(C.c_float)))
         return out.reshape(self.nlevels, 8)
+
+    def level_flops(self) -> np.ndarray:
+        """(nlevels, 6) nominal flops per phase, columns as LEVEL_PHASES[:6]."""
+        out = np.zeros(6 * self.nlevels, np.float64)
+        lib().spq_level_flops(self._h, out.ctypes.data_as(C.POINTER(C.c_double)))
+        return out.reshape(self.nlevels, 6)
 
     def factor_flops(self) -> float:
         return lib().spq_factor_flops(self._h)
