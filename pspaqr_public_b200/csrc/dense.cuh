@@ -630,6 +630,88 @@ __device__ void mat_apply_q_right(const T* V, int ldv, const T* Tm, int k, T* C,
 }
 
 
+// ---------------------------------------------------------------- single-vector applies
+// Shared scratch of vec_panel (elements): partial sums, W2, the panel's T.
+constexpr int kVecRed = (kWarps + 1) * 32 + kNB * (kNB + 1);
+
+// One panel of kb <= kNB reflectors on a vector in shared memory:
+//   unit = 1: x (m) <- (I - V T V^T)^T x (trans) or (I - V T V^T) x, V unit
+//             lower trapezoidal from the panel's diagonal;
+//   unit = 0: [a (kb); x (m)] <- Q^T [a; x], Q = I - [I; V] T [I; V]^T, V full.
+// Every thread takes rows t, t + kThreads, ... and issues the kb loads of a row
+// together; the kb partial sums are reduce-scattered across each warp (lane i
+// ends with reflector i's sum) and across the warps through `red`.
+template <typename T>
+__device__ void vec_panel(const T* V, int ldv, const T* Tm, int ldt, int kb, int unit, bool trans, T* a, T* x,
+                          int m, T* red) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  // the panel's T (upper triangle) to shared memory while the rows stream
+  T* sT = red + (kWarps + 1) * 32;  // [kNB][kNB+1], sT[l * (kNB+1) + i] = T(l, i)
+  for (int e = threadIdx.x; e < kNB * kNB; e += kThreads) {
+    const int l = e & (kNB - 1), i = e / kNB;
+    sT[l * (kNB + 1) + i] = (l <= i && i < kb) ? Tm[l + (size_t)i * ldt] : (T)0.0;
+  }
+  T acc[kNB];
+#pragma unroll
+  for (int i = 0; i < kNB; ++i) acc[i] = 0.0;
+  for (int r = threadIdx.x; r < m; r += kThreads) {
+    const T xr = x[r];
+#pragma unroll
+    for (int i = 0; i < kNB; ++i) {
+      T v = 0.0;
+      if (i < kb) v = unit ? (r == i ? (T)1.0 : (r < i ? (T)0.0 : V[r + (size_t)i * ldv])) : V[r + (size_t)i * ldv];
+      acc[i] += v * xr;
+    }
+  }
+#pragma unroll
+  for (int o = 16; o >= 1; o >>= 1) {
+    const bool up = (lane & o) != 0;
+#pragma unroll
+    for (int q = 0; q < o; ++q) {
+      const T send = up ? acc[q] : acc[q + o];
+      const T keep = up ? acc[q + o] : acc[q];
+      acc[q] = keep + __shfl_xor_sync(0xffffffffu, send, o);
+    }
+  }
+  red[warp * 32 + lane] = acc[0];
+  __syncthreads();
+  T* w2 = red + kWarps * 32;
+  if (warp == 0) {
+    T w = 0.0;
+    for (int q = 0; q < kWarps; ++q) w += red[q * 32 + lane];
+    if (!unit && lane < kb) w += a[lane];
+    T s = 0.0;
+#pragma unroll
+    for (int l = 0; l < kNB; ++l) {
+      const T tl = trans ? sT[l * (kNB + 1) + lane] : sT[lane * (kNB + 1) + l];
+      s += tl * __shfl_sync(0xffffffffu, w, l);
+    }
+    w2[lane] = lane < kb ? s : (T)0.0;
+    if (!unit && lane < kb) a[lane] -= s;
+  }
+  __syncthreads();
+  for (int r = threadIdx.x; r < m; r += kThreads) {
+    T s = 0.0;
+#pragma unroll
+    for (int i = 0; i < kNB; ++i) {
+      T v = 0.0;
+      if (i < kb) v = unit ? (r == i ? (T)1.0 : (r < i ? (T)0.0 : V[r + (size_t)i * ldv])) : V[r + (size_t)i * ldv];
+      s += v * w2[i];
+    }
+    x[r] -= s;
+  }
+  __syncthreads();
+}
+
+// [a (k); x (m)] <- Q^T [a; x] for a pentagonal (tpqrt) factor, V full (m x k).
+template <typename T>
+__device__ void vec_apply_tpqt(const T* V, int ldv, const T* Tm, int k, T* a, T* x, int m, T* red) {
+  for (int j0 = 0; j0 < k; j0 += kNB) {
+    const int kb = (k - j0) < kNB ? (k - j0) : kNB;
+    vec_panel<T>(V + (size_t)j0 * ldv, ldv, Tm + (size_t)j0 * kNB, kNB, kb, 0, true, a + j0, x, m, red);
+  }
+}
+
 // C (m <= kNC rows x n) <- C R^{-1}, R upper triangular (n x n), blocked by 32
 // columns: C(:, J) -= C(:, 0:j0) R(0:j0, J) through shared-memory tiles, then
 // the 32 x 32 diagonal block is solved one row per thread.

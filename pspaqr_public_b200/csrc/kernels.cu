@@ -915,12 +915,12 @@ __global__ void __launch_bounds__(kThreads) k_fwd_elim(const FwdElimTask* __rest
   const int ti = s_task;
   if (ti >= ntasks) return;
   const FwdElimTask t = tasks[ti];
-  T* w = sm;
-  T* xc = w + 2 * kNB;
+  T* red = sm;
+  T* xc = red + dev::kVecRed;
   T* xn = xc + (nmax > 0 ? nmax : 1);
   for (int i = threadIdx.x; i < t.n; i += kThreads) xc[i] = __ldcg(as<T>(t.x) + i);
   __syncthreads();
-  dev::apply_qt<T>(as<T>(t.S), t.n, as<T>(t.T), t.n, xc, t.n, t.n, 1, w, 2 * kNB);
+  dev::apply_qt<T>(as<T>(t.S), t.n, as<T>(t.T), t.n, xc, t.n, t.n, 1, red, 2 * kNB);
   for (int o = t.out_begin; o < t.out_end; ++o) {
     const FwdOut e = outs[o];
     if (threadIdx.x == 0) {
@@ -945,7 +945,7 @@ __global__ void __launch_bounds__(kThreads) k_fwd_elim(const FwdElimTask* __rest
     if (s_abort) return;
     for (int i = threadIdx.x; i < e.m; i += kThreads) xn[i] = __ldcg(as<T>(e.xn) + i);
     __syncthreads();
-    dev::apply_tpqt<T>(as<T>(e.V), e.m, as<T>(e.T), t.n, xc, t.n, xn, e.m, e.m, 1, w, 2 * kNB);
+    dev::vec_apply_tpqt<T>(as<T>(e.V), e.m, as<T>(e.T), t.n, xc, xn, e.m, red);
     for (int i = threadIdx.x; i < e.m; i += kThreads) __stcg(as<T>(e.xn) + i, xn[i]);
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -961,12 +961,12 @@ __global__ void __launch_bounds__(kThreads) k_fwd_spars(const FwdSparsTask* __re
   extern __shared__ __align__(16) unsigned char smraw[];
   T* sm = reinterpret_cast<T*>(smraw);
   const FwdSparsTask t = tasks[blockIdx.x];
-  T* w = sm;
+  T* red = sm;
   T* x = sm + 2 * kNB;
   for (int i = threadIdx.x; i < t.n; i += kThreads) x[i] = as<T>(t.x)[i];
   __syncthreads();
-  dev::apply_qt<T>(as<T>(t.Qs), t.n, as<T>(t.Ts), t.n, x, t.n, t.n, 1, w, 2 * kNB);
-  dev::apply_qt<T>(as<T>(t.V), t.n, as<T>(t.T), *t.rank, x, t.n, t.n, 1, w, 2 * kNB);
+  dev::apply_qt<T>(as<T>(t.Qs), t.n, as<T>(t.Ts), t.n, x, t.n, t.n, 1, red, 2 * kNB);
+  dev::apply_qt<T>(as<T>(t.V), t.n, as<T>(t.T), *t.rank, x, t.n, t.n, 1, red, 2 * kNB);
   for (int i = threadIdx.x; i < t.n; i += kThreads) as<T>(t.x)[i] = x[i];
 }
 
@@ -975,32 +975,88 @@ __global__ void __launch_bounds__(kThreads) k_bwd_spars(const FwdSparsTask* __re
   extern __shared__ __align__(16) unsigned char smraw[];
   T* sm = reinterpret_cast<T*>(smraw);
   const FwdSparsTask t = tasks[blockIdx.x];
-  T* w = sm;
-  T* xs = w + 2 * kNB;
+  T* red = sm;
+  T* xs = red + 2 * kNB;
   T* x = xs + 32;
   for (int i = threadIdx.x; i < t.n; i += kThreads) x[i] = as<T>(t.x)[i];
   __syncthreads();
-  dev::apply_q<T>(as<T>(t.V), t.n, as<T>(t.T), *t.rank, x, t.n, t.n, 1, w, 2 * kNB);
+  dev::apply_q<T>(as<T>(t.V), t.n, as<T>(t.T), *t.rank, x, t.n, t.n, 1, red, 2 * kNB);
   dev::trsv_upper<T>(as<T>(t.Qs), t.n, x, t.n, xs);
   for (int i = threadIdx.x; i < t.n; i += kThreads) as<T>(t.x)[i] = x[i];
 }
 
-template <typename T>
+// kBwdRows: rows per lane of the backward GEMV (interiors of <= 32 kBwdRows
+// rows); 0: one thread per row.
+template <typename T, int kBwdRows>
 __global__ void __launch_bounds__(kThreads) k_bwd_elim(const BwdElimTask* __restrict__ tasks,
-                                                       const BwdIn* __restrict__ ins) {
+                                                       const BwdIn* __restrict__ ins, int nmax) {
   extern __shared__ __align__(16) unsigned char smraw[];
   T* sm = reinterpret_cast<T*>(smraw);
   const BwdElimTask t = tasks[blockIdx.x];
   T* xs = sm;
   T* x = sm + 32;
+  T* part = x + nmax;  // kWarps x nmax partial sums (kBwdRows > 0)
   for (int i = threadIdx.x; i < t.n; i += kThreads) x[i] = as<T>(t.x)[i];
-  __syncthreads();
-  for (int q = t.in_begin; q < t.in_end; ++q) {
-    const BwdIn e = ins[q];
+  if (kBwdRows > 0) {
+    // x -= sum over in-edges of R_e x_e: warp w streams the columns j = w mod
+    // kWarps (lanes over rows, coalesced), two columns' loads in flight, into
+    // a partial vector held in registers; the warps' partials meet in `part`
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int nrs = (t.n + 31) / 32;
+    constexpr int kR = kBwdRows > 0 ? kBwdRows : 1;
+    T y[kR];
+#pragma unroll
+    for (int u = 0; u < kR; ++u) y[u] = 0.0;
+    for (int q = t.in_begin; q < t.in_end; ++q) {
+      const BwdIn e = ins[q];
+      const T* R = as<T>(e.R);
+      const T* xm = as<T>(e.xm);
+      int j = warp;
+      for (; j + kWarps < e.s; j += 2 * kWarps) {
+        const T* c0 = R + (size_t)j * e.ldr;
+        const T* c1 = c0 + (size_t)kWarps * e.ldr;
+        T v0[kR], v1[kR];
+#pragma unroll
+        for (int u = 0; u < kR; ++u) {
+          const int r = lane + 32 * u;
+          const bool ok = u < nrs && r < t.n;
+          v0[u] = ok ? c0[r] : (T)0.0;
+          v1[u] = ok ? c1[r] : (T)0.0;
+        }
+        const T x0 = xm[j], x1 = xm[j + kWarps];
+#pragma unroll
+        for (int u = 0; u < kR; ++u) y[u] += v0[u] * x0 + v1[u] * x1;
+      }
+      if (j < e.s) {
+        const T* c0 = R + (size_t)j * e.ldr;
+        const T x0 = xm[j];
+#pragma unroll
+        for (int u = 0; u < kR; ++u) {
+          const int r = lane + 32 * u;
+          if (u < nrs && r < t.n) y[u] += c0[r] * x0;
+        }
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < kR; ++u) {
+      const int r = lane + 32 * u;
+      if (u < nrs && r < t.n) part[warp * nmax + r] = y[u];
+    }
+    __syncthreads();
     for (int i = threadIdx.x; i < t.n; i += kThreads) {
       T s = 0.0;
-      for (int j = 0; j < e.s; ++j) s += as<T>(e.R)[i + (size_t)j * e.ldr] * as<T>(e.xm)[j];
+      for (int w = 0; w < kWarps; ++w) s += part[w * nmax + i];
       x[i] -= s;
+    }
+  } else {
+    __syncthreads();
+    for (int q = t.in_begin; q < t.in_end; ++q) {
+      const BwdIn e = ins[q];
+      for (int i = threadIdx.x; i < t.n; i += kThreads) {
+        T s = 0.0;
+        for (int j = 0; j < e.s; ++j) s += as<T>(e.R)[i + (size_t)j * e.ldr] * as<T>(e.xm)[j];
+        x[i] -= s;
+      }
     }
   }
   __syncthreads();
@@ -1332,7 +1388,7 @@ cudaError_t launch_fwd_elim(const FwdElimTask* t, const FwdOut* o, int ntasks, i
                             int* status, long long spin_limit, cudaStream_t st) {
   if (cudaError_t pre = begin("launch_fwd_elim")) return pre;
   if (ntasks <= 0) return cudaSuccess;
-  const size_t b = smem_bytes(2 * kNB + (size_t)std::max(nmax, 1) + (size_t)std::max(mmax, 1));
+  const size_t b = smem_bytes(dev::kVecRed + (size_t)std::max(nmax, 1) + (size_t)std::max(mmax, 1));
   counted();
   if (g_fp32) {
     if (cudaError_t e = prep(k_fwd_elim<float>, b)) return e;
@@ -1377,15 +1433,23 @@ cudaError_t launch_bwd_spars(const FwdSparsTask* t, int ntasks, int nmax, cudaSt
 cudaError_t launch_bwd_elim(const BwdElimTask* t, const BwdIn* in, int ntasks, int nmax, cudaStream_t st) {
   if (cudaError_t pre = begin("launch_bwd_elim")) return pre;
   if (ntasks <= 0) return cudaSuccess;
-  const size_t b = smem_bytes(32 + (size_t)nmax);
+  nmax = std::max(nmax, 1);
+  const int rows = nmax <= 128 ? 4 : nmax <= 384 ? 12 : nmax <= 1024 ? 32 : 0;
+  const size_t b = smem_bytes(32 + (size_t)nmax + (rows ? (size_t)kWarps * nmax : 0));
   counted();
-  if (g_fp32) {
-    if (cudaError_t e = prep(k_bwd_elim<float>, b)) return e;
-    k_bwd_elim<float><<<ntasks, kThreads, b, st>>>(t, in);
-  } else {
-    if (cudaError_t e = prep(k_bwd_elim<double>, b)) return e;
-    k_bwd_elim<double><<<ntasks, kThreads, b, st>>>(t, in);
-  }
+  auto go = [&](auto kern) -> cudaError_t {
+    if (cudaError_t e = prep(kern, b)) return e;
+    kern<<<ntasks, kThreads, b, st>>>(t, in, nmax);
+    return cudaSuccess;
+  };
+  cudaError_t e;
+  if (g_fp32)
+    e = rows == 4 ? go(k_bwd_elim<float, 4>) : rows == 12 ? go(k_bwd_elim<float, 12>)
+        : rows == 32 ? go(k_bwd_elim<float, 32>) : go(k_bwd_elim<float, 0>);
+  else
+    e = rows == 4 ? go(k_bwd_elim<double, 4>) : rows == 12 ? go(k_bwd_elim<double, 12>)
+        : rows == 32 ? go(k_bwd_elim<double, 32>) : go(k_bwd_elim<double, 0>);
+  if (e) return e;
   return last();
 }
 
