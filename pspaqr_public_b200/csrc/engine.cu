@@ -87,6 +87,8 @@ void Arena::release() {
 Tree::Tree(int L, int s) : nlevels(L), skip(s) {}
 
 Tree::~Tree() {
+  if (stream_) cudaStreamSynchronize(stream_);
+  for (auto& c : pin_) cudaFreeHost(c.first);
   cudaFree(d_model_);
   if (solve_exec_) cudaGraphExecDestroy(solve_exec_);
   if (solve_graph_) cudaGraphDestroy(solve_graph_);
@@ -131,9 +133,35 @@ int Tree::device_status() {
   return s;
 }
 
+void* Tree::stage(size_t bytes) {
+  bytes = (bytes + 255) / 256 * 256;
+  while (pin_cur_ < pin_.size() && pin_off_ + bytes > pin_[pin_cur_].second) {
+    ++pin_cur_;
+    pin_off_ = 0;
+  }
+  if (pin_cur_ == pin_.size()) {
+    const size_t sz = std::max<size_t>(size_t(64) << 20, bytes);
+    void* p = nullptr;
+    if (cudaHostAlloc(&p, sz, cudaHostAllocDefault) != cudaSuccess) {
+      cudaGetLastError();
+      return nullptr;
+    }
+    pin_.push_back({static_cast<char*>(p), sz});
+  }
+  char* r = pin_[pin_cur_].first + pin_off_;
+  pin_off_ += bytes;
+  return r;
+}
+
 void* Tree::upload(const void* host, size_t bytes) {
   void* d = scratch_.alloc(std::max<size_t>(bytes, 1));
-  if (d && bytes && host) cudaMemcpyAsync(d, host, bytes, cudaMemcpyHostToDevice, stream_);
+  if (!d || !bytes || !host) return d;
+  if (void* p = stage(bytes)) {
+    std::memcpy(p, host, bytes);
+    cudaMemcpyAsync(d, p, bytes, cudaMemcpyHostToDevice, stream_);
+  } else {
+    cudaMemcpyAsync(d, host, bytes, cudaMemcpyHostToDevice, stream_);
+  }
   return d;
 }
 
@@ -193,6 +221,8 @@ int Tree::assemble() {
     if (check_cuda(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "stream")) return -10;
     own_stream_ = true;
   }
+  if (check_cuda(cudaStreamSynchronize(stream_), "assemble")) return -10;
+  stage_reset();
   const int n = st_.n;
   const int ncl = (int)st_.clusters.size();
   const int ned = (int)st_.edges.size();
@@ -318,6 +348,7 @@ int Tree::factorize() {
   auto ck = [&](cudaError_t e, const char* where) { return check_cuda(e, where); };
   for (int lvl = 0; lvl < L; ++lvl) {
     const Level& Lv = st_.levels[lvl];
+    stage_reset();  // the previous level (or assemble) ended with a stream synchronisation
     const double h0 = wall();
     double hwait = 0;  // host time blocked in the level's intermediate synchronisations
     auto sync_timed = [&](const char* where) {

@@ -150,7 +150,12 @@ class Tree {
     return code;
   }
   int check_cuda(cudaError_t e, const char* where);
-  void* upload(const void* host, size_t bytes);   // into the per-level scratch arena
+  // into the per-level scratch arena, staged through pinned host memory so
+  // that the copy does not wait for the stream's earlier work
+  void* upload(const void* host, size_t bytes);
+  // pinned staging area of upload(): reused after the stream has drained
+  void* stage(size_t bytes);
+  void stage_reset() { pin_cur_ = 0, pin_off_ = 0; }
   int build_solve_graph();
   // one zeroed region for the blocks of `edges`; sets ptr_/ld_ (rows_/cols_ must be set)
   int alloc_level_blocks(const std::vector<int>& edges);
@@ -165,6 +170,8 @@ class Tree {
   bool own_stream_ = false;
   Arena arena_;        // blocks and factors (lives until destruction)
   Arena scratch_;      // descriptors of the factorization (released after it)
+  std::vector<std::pair<char*, size_t>> pin_;  // pinned staging chunks
+  size_t pin_cur_ = 0, pin_off_ = 0;
 
   // per cluster
   std::vector<int> size_, size_org_, rpos_;

@@ -492,7 +492,6 @@ __global__ void __launch_bounds__(kT) k_gram(const SketchTask* __restrict__ task
   }
 }
 
-constexpr int kPT = 1024;  // threads of the pivoted Cholesky
 
 // (position, column) with the smallest position across the warp
 __device__ __forceinline__ void warp_min_pos(int& bp, int& bc) {
@@ -515,6 +514,7 @@ __device__ __forceinline__ void warp_min_pos(int& bp, int& bc) {
 //   L(c, i) = (G(c, p) - sum_{k<i} L(c, k) L(p, k)) / L(i, i).
 // Threads are (k-group, column) pairs so that short columns still keep the
 // CTA's loads in flight.
+template <int kPT>
 __global__ void __launch_bounds__(kPT) k_pchol(const SketchTask* __restrict__ tasks, double stol, double pivot_rtol) {
   extern __shared__ double psm[];
   __shared__ double s_v[kPT / 32];
@@ -605,19 +605,21 @@ __global__ void __launch_bounds__(kPT) k_pchol(const SketchTask* __restrict__ ta
     for (int c0 = 0; c0 < n; c0 += cw) {
       const int c = c0 + slot;
       const bool act = grp < ng && c < n && pos[c] > i;
-      double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
+      double a[8] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
       if (act) {
         const double* col = t.Lt + c;
         int k = grp;
-        for (; k + 3 * ng < i; k += 4 * ng) {
-          a0 += col[(size_t)k * ld] * lp[k];
-          a1 += col[(size_t)(k + ng) * ld] * lp[k + ng];
-          a2 += col[(size_t)(k + 2 * ng) * ld] * lp[k + 2 * ng];
-          a3 += col[(size_t)(k + 3 * ng) * ld] * lp[k + 3 * ng];
+        // eight rows of Lt in flight per thread
+        for (; k + 7 * ng < i; k += 8 * ng) {
+          double v[8];
+#pragma unroll
+          for (int u = 0; u < 8; ++u) v[u] = col[(size_t)(k + u * ng) * ld];
+#pragma unroll
+          for (int u = 0; u < 8; ++u) a[u] += v[u] * lp[k + u * ng];
         }
-        for (; k < i; k += ng) a0 += col[(size_t)k * ld] * lp[k];
+        for (; k < i; k += ng) a[0] += col[(size_t)k * ld] * lp[k];
       }
-      const double acc = (a0 + a1) + (a2 + a3);
+      const double acc = ((a[0] + a[1]) + (a[2] + a[3])) + ((a[4] + a[5]) + (a[6] + a[7]));
       if (ng > 1) {
         part[threadIdx.x] = acc;
         __syncthreads();
@@ -726,9 +728,12 @@ cudaError_t launch_gram(const SketchTask* t, const GemmTile* tiles, int ntiles, 
   return done_launch("launch_gram");
 }
 
+// threads of the pivoted Cholesky: 128 for sketches of at most 64 columns
+static int pchol_threads(int nmax) { return nmax <= 64 ? 128 : 1024; }
+
 size_t pchol_smem(int nmax) {
   const size_t n = (size_t)std::max(nmax, 1);
-  return sizeof(double) * (2 * n + kPT) + sizeof(int) * 2 * n;
+  return sizeof(double) * (2 * n + pchol_threads(nmax)) + sizeof(int) * 2 * n;
 }
 
 cudaError_t launch_pchol(const SketchTask* t, int ntasks, int nmax, double stol, double pivot_rtol, cudaStream_t st) {
@@ -736,9 +741,14 @@ cudaError_t launch_pchol(const SketchTask* t, int ntasks, int nmax, double stol,
   if (ntasks <= 0) return cudaSuccess;
   const size_t smem = pchol_smem(nmax);
   if (smem > 227 * 1024) return cudaErrorInvalidValue;
-  cudaError_t e = cudaFuncSetAttribute(k_pchol, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  auto go = [&](auto kern, int threads) -> cudaError_t {
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e) return e;
+    kern<<<ntasks, threads, smem, st>>>(t, stol, pivot_rtol);
+    return cudaSuccess;
+  };
+  const cudaError_t e = pchol_threads(nmax) == 128 ? go(k_pchol<128>, 128) : go(k_pchol<1024>, 1024);
   if (e) return e;
-  k_pchol<<<ntasks, kPT, smem, st>>>(t, stol, pivot_rtol);
   return done_launch("launch_pchol");
 }
 
