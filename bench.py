@@ -51,6 +51,9 @@ METRIC = "time to 1e-10 rel. residual (factor+GMRES), 64^3 diffusion: mixed+lear
 # capture of the 48^3 member of the workload family
 # (profiles/k_rrqr_diff3d_48_traffic.md)
 RRQR_DRAM_PER_ALGO_BYTE = 0.78
+# DRAM bytes per nominal flop of the FP32 trailing-update launches (k_update),
+# from an ncu capture of the same step (None: not captured)
+UPDATE_DRAM_PER_FLOP = None
 # sketch columns beyond the predicted rank in the learned-rank variant
 LEARNED_OVERSAMPLE = 32
 
@@ -141,6 +144,28 @@ def fp64_gemm_peak(torch) -> float:
         e1.record()
         torch.cuda.synchronize()
         best = min(best, e0.elapsed_time(e1) / 1e3)
+    del a, b
+    return 2.0 * n ** 3 / best / 1e12
+
+
+def fp32_simt_peak(torch) -> float:
+    """cuBLAS SGEMM 8192^3 with TF32 off (FP32 on the CUDA cores), TFLOP/s: the
+    roofline denominator of the FP32 factor kernels (MEASURED_PEAKS.json carries
+    HBM and bf16 tensor figures only)."""
+    n = 8192
+    prev = torch.backends.cuda.matmul.allow_tf32
+    torch.backends.cuda.matmul.allow_tf32 = False
+    a = torch.randn(n, n, dtype=torch.float32, device="cuda")
+    b = torch.randn(n, n, dtype=torch.float32, device="cuda")
+    best = 1e30
+    for _ in range(4):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        torch.matmul(a, b)
+        e1.record()
+        torch.cuda.synchronize()
+        best = min(best, e0.elapsed_time(e1) / 1e3)
+    torch.backends.cuda.matmul.allow_tf32 = prev
     del a, b
     return 2.0 * n ** 3 / best / 1e12
 
@@ -256,6 +281,7 @@ def run_ours(args):
             r["ranks"] = ranks()
             r["counts"] = t.learned_counts()
             r["flops"] = t.factor_flops()
+            r["level_flops"] = t.level_flops()
             r["rrqr_bytes"] = t.rrqr_bytes()
             res[name] = r
     head = res["mixed+learned"]
@@ -270,6 +296,15 @@ def run_ours(args):
         e2e = float(np.mean(e2e_times))
     peaks = measured_peaks()
     fp64_peak = fp64_gemm_peak(torch) if rank == 0 else 0.0
+    fp32_peak = fp32_simt_peak(torch) if rank == 0 else 0.0
+    # dominant kernel of the headline step: the FP32 trailing updates (k_update,
+    # one launch per level), compute-bound on the CUDA cores; nominal flops of
+    # the updates phase over its event-timed duration (same stream)
+    ui = ParTree.LEVEL_PHASES.index("updates")
+    upd_s = float(head["level_ms"][:, ui].sum()) / 1e3
+    upd_flops = float(head["level_flops"][:, ui].sum())
+    upd_launches = int(np.count_nonzero(head["level_flops"][:, ui]))
+    upd_tflops = upd_flops / upd_s / 1e12 if upd_s > 0 else 0.0
     fact = float(np.mean(head["ftimes"]))
     # dominant kernel of the plain factorization: the pivoted QR
     # (k_rrqr_assemble + k_rrqr launches of every level), HBM-bound;
@@ -318,7 +353,19 @@ def run_ours(args):
                     "oversample": LEARNED_OVERSAMPLE},
         "e2e": {"value": e2e, "unit": "s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": 8 * N},
         "gpu_launches": int(np.median(head["launches"])),
-        "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
+        "roofline": {"bound": "fp32", "achieved": upd_tflops, "peak": fp32_peak, "unit": "TFLOP/s",
+                     "frac": upd_tflops / fp32_peak if fp32_peak else None,
+                     "traffic": UPDATE_DRAM_PER_FLOP * upd_flops / max(upd_launches, 1)
+                     if UPDATE_DRAM_PER_FLOP else None,
+                     "kernel": "k_update<float>: FP32 trailing updates of the headline step (share of its kernel "
+                               "time: the largest in the ncu launch list)",
+                     "algorithmic_flops": upd_flops, "launches": upd_launches, "duration_s": upd_s,
+                     "per_launch_flops": upd_flops / max(upd_launches, 1),
+                     "peak_source": "cuBLAS SGEMM 8192^3, TF32 off, measured in this run (FP32 on the CUDA cores; "
+                                    "MEASURED_PEAKS.json has no FP32 figure)",
+                     "traffic_source": "per launch: dram__bytes_read.sum + dram__bytes_write.sum per nominal flop "
+                                       "(ncu) x flops per launch" if UPDATE_DRAM_PER_FLOP else "not captured"},
+        "roofline_fp64_rrqr": {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
                      "frac": achieved / hbm_peak,
                      "traffic": RRQR_DRAM_PER_ALGO_BYTE * rrqr_bytes if RRQR_DRAM_PER_ALGO_BYTE else None,
                      "kernel": "pivoted QR (k_rrqr_assemble + k_rrqr, all levels of one plain FP64 factorization)",

@@ -335,7 +335,13 @@ __device__ void apply_q_right(const T* V, int ldv, const T* Tm, int k, T* C, int
 // products).  `sm` holds kTileSmem elements.
 constexpr int kNC = 64;   // columns (rows for right applies) per pass
 constexpr int kRT = 32;   // rows (columns) per shared-memory tile
-constexpr int kTileSmem = 2 * kRT * (kNB + 1) + 2 * kRT * (kNC + 1) + kNB * kNC;
+// Row strides of the V and C tiles of the left apply: 16-byte aligned rows
+// whose starts fall on distinct 16-byte bank groups for 8 consecutive rows.
+template <typename T>
+__host__ __device__ constexpr int tile_lv() { return kNB + (sizeof(T) == 4 ? 4 : 2); }
+template <typename T>
+__host__ __device__ constexpr int tile_lc() { return kNC + (sizeof(T) == 4 ? 4 : 2); }
+constexpr int kTileSmem = 2 * kRT * tile_lv<float>() + 2 * kRT * tile_lc<float>() + kNB * kNC;
 
 // Load through L2 (kCg: data written by another CTA of the cluster) or as is.
 template <bool kCg, typename T>
@@ -353,20 +359,25 @@ __device__ __forceinline__ T ld_v(const T* p) {
 template <typename T, bool kCg = false>
 __device__ void tile_left_qt(const T* V, int ldv, const T* Tm, int ldt, int kb, int unit, T* A, int lda,
                              T* C, int ldc, int m, int nc, T* sm, int cgap = 0) {
-  constexpr int kVS = kRT * (kNB + 1), kCS = kRT * (kNC + 1);
-  T* sV0 = sm;                 // two [kRT][kNB+1] tiles of V
-  T* sC0 = sV0 + 2 * kVS;      // two [kRT][kNC+1] tiles of C; later W2 [kNB][kNC]
-  T* sW = sC0 + 2 * kCS;       // [kNB][kNC]
+  static_assert(kThreads == 256 && kNB == 32 && kNC == 64 && kRT == 32, "tile shapes");
+  constexpr int kLV = tile_lv<T>(), kLC = tile_lc<T>();
+  constexpr int kVS = kRT * kLV, kCS = kRT * kLC;
+  T* sV0 = sm;               // two [kRT][kLV] tiles of V
+  T* sC0 = sV0 + 2 * kVS;    // two [kRT][kLC] tiles of C
+  T* sW = sC0 + 2 * kCS;     // [kNB][kNC]: W, then the partial sums' landing area is sV0..sC0
   const int t = threadIdx.x;
   auto col = [&](int c) { return (size_t)(c + (c / kNB) * cgap); };
-  // loads of one tile: V element (idx & 31, idx >> 5) and C element
-  // (idx & 31, idx >> 5) for idx = t + kThreads * s (rows fastest: coalesced)
+  // global loads of one tile: lane = row (a warp reads 32 consecutive rows of
+  // one column: coalesced), warp w = columns kSV w .. (V) and kSC w .. (C), so
+  // that a thread stashes one row segment with 16-byte stores
   constexpr int kSV = kRT * kNB / kThreads, kSC = kRT * kNC / kThreads;
+  const int lr = t & (kRT - 1), lw = t / kRT;
   T rv[kSV], rc[kSC];
   auto vload = [&](int r0) {
+    const int gr = r0 + lr;
 #pragma unroll
     for (int q = 0; q < kSV; ++q) {
-      const int idx = t + q * kThreads, r = idx & (kRT - 1), i = idx / kRT, gr = r0 + r;
+      const int i = lw * kSV + q;
       T v = 0.0;
       if (gr < m && i < kb)
         v = unit ? (gr == i ? (T)1.0 : (gr < i ? (T)0.0 : ld_v<kCg>(V + gr + (size_t)i * ldv)))
@@ -375,32 +386,55 @@ __device__ void tile_left_qt(const T* V, int ldv, const T* Tm, int ldt, int kb, 
     }
   };
   auto vstash = [&](int b) {
+    T* d = sV0 + b * kVS + lr * kLV + lw * kSV;
 #pragma unroll
-    for (int q = 0; q < kSV; ++q) {
-      const int idx = t + q * kThreads;
-      sV0[b * kVS + (idx & (kRT - 1)) * (kNB + 1) + idx / kRT] = rv[q];
+    for (int q = 0; q < kSV; ++q) d[q] = rv[q];
+  };
+  auto cload = [&](int r0) {
+    const int gr = r0 + lr;
+#pragma unroll
+    for (int q = 0; q < kSC; ++q) {
+      const int c = lw * kSC + q;
+      rc[q] = (gr < m && c < nc) ? C[gr + col(c) * ldc] : (T)0.0;
     }
   };
-  const int ntile = (m + kRT - 1) / kRT;
-  // W = V^T C: thread rows ti*4..+3 of W, columns tc*2..+1
-  {
-    const int ti = t & 7, tc = t >> 3;
-    T acc[4][2] = {{0, 0}, {0, 0}, {0, 0}, {0, 0}};
-    auto cload = [&](int r0) {
+  auto cstash = [&](int b) {
+    T* d = sC0 + b * kCS + lr * kLC + lw * kSC;
 #pragma unroll
-      for (int q = 0; q < kSC; ++q) {
-        const int idx = t + q * kThreads, r = idx & (kRT - 1), c = idx / kRT;
-        rc[q] = (r0 + r < m && c < nc) ? C[(r0 + r) + col(c) * ldc] : (T)0.0;
-      }
-    };
+    for (int q = 0; q < kSC; ++q) d[q] = rc[q];
+  };
+  const int ntile = (m + kRT - 1) / kRT;
+  // T (and the top block A of a pentagonal panel) are read now, used after
+  // the products: element idx = t + kThreads q, T(l = idx & 31, i = idx >> 5)
+  // and A(i = idx & 31, c = idx >> 5)
+  constexpr int kST = kNB * kNB / kThreads, kSA = kNB * kNC / kThreads;
+  T rt[kST], ra[kSA];
+#pragma unroll
+  for (int q = 0; q < kST; ++q) {
+    const int idx = t + q * kThreads, l = idx & (kNB - 1), i = idx / kNB;
+    rt[q] = (l <= i && i < kb) ? ld_v<kCg>(Tm + l + (size_t)i * ldt) : (T)0.0;
+  }
+#pragma unroll
+  for (int q = 0; q < kSA; ++q) {
+    const int idx = t + q * kThreads, i = idx & (kNB - 1), c = idx / kNB;
+    ra[q] = (!unit && i < kb && c < nc) ? A[i + col(c) * lda] : (T)0.0;
+  }
+  // ---- W = V^T C.  A thread accumulates W(i0:i0+kIW, c0:c0+4); the kSets
+  // row sets of kTPO threads each take kRows consecutive rows of every tile
+  {
+    constexpr int kIW = sizeof(T) == 4 ? 8 : 4;           // reflectors per thread
+    constexpr int kTPO = (kNB / kIW) * (kNC / 4);          // threads per set
+    constexpr int kSets = kThreads / kTPO, kRows = kRT / kSets;
+    const int set = t / kTPO, i0 = ((t % kTPO) / (kNC / 4)) * kIW, c0 = (t % (kNC / 4)) * 4;
+    T acc[kIW][4];
+#pragma unroll
+    for (int a = 0; a < kIW; ++a)
+#pragma unroll
+      for (int b = 0; b < 4; ++b) acc[a][b] = 0.0;
     vload(0);
     cload(0);
     vstash(0);
-#pragma unroll
-    for (int q = 0; q < kSC; ++q) {
-      const int idx = t + q * kThreads;
-      sC0[(idx & (kRT - 1)) * (kNC + 1) + idx / kRT] = rc[q];
-    }
+    cstash(0);
     __syncthreads();
     for (int tt = 0; tt < ntile; ++tt) {
       const int b = tt & 1;
@@ -409,48 +443,71 @@ __device__ void tile_left_qt(const T* V, int ldv, const T* Tm, int ldt, int kb, 
         vload((tt + 1) * kRT);
         cload((tt + 1) * kRT);
       }
-      const T* sV = sV0 + b * kVS;
-      const T* sC = sC0 + b * kCS;
+      const T* sV = sV0 + b * kVS + (set * kRows) * kLV + i0;
+      const T* sC = sC0 + b * kCS + (set * kRows) * kLC + c0;
 #pragma unroll 8
-      for (int r = 0; r < kRT; ++r) {
-        const T* vr = sV + r * (kNB + 1) + ti * 4;
-        const T* cr = sC + r * (kNC + 1) + tc * 2;
-        const T b0 = cr[0], b1 = cr[1];
+      for (int r = 0; r < kRows; ++r) {
+        T v[kIW], c[4];
 #pragma unroll
-        for (int q = 0; q < 4; ++q) {
-          const T a = vr[q];
-          acc[q][0] += a * b0;
-          acc[q][1] += a * b1;
-        }
+        for (int a = 0; a < kIW; ++a) v[a] = sV[r * kLV + a];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) c[q] = sC[r * kLC + q];
+#pragma unroll
+        for (int a = 0; a < kIW; ++a)
+#pragma unroll
+          for (int q = 0; q < 4; ++q) acc[a][q] += v[a] * c[q];
       }
       if (more) {
         vstash(b ^ 1);
-#pragma unroll
-        for (int q = 0; q < kSC; ++q) {
-          const int idx = t + q * kThreads;
-          sC0[(b ^ 1) * kCS + (idx & (kRT - 1)) * (kNC + 1) + idx / kRT] = rc[q];
-        }
+        cstash(b ^ 1);
       }
       __syncthreads();
     }
+    // sets 1.. park their partial sums in the tile buffers, set 0 adds them in
+    // set order
+    static_assert((kSets - 1) * kNB * kNC <= 2 * kVS + 2 * kCS, "park area");
+    T* park = sV0;
+    if (set > 0)
 #pragma unroll
-    for (int q = 0; q < 4; ++q)
+      for (int a = 0; a < kIW; ++a)
 #pragma unroll
-      for (int p = 0; p < 2; ++p) {
-        const int i = ti * 4 + q, c = tc * 2 + p;
-        T w = acc[q][p];
-        if (!unit && i < kb && c < nc) w += A[i + col(c) * lda];
-        sW[i * kNC + c] = w;
-      }
+        for (int q = 0; q < 4; ++q) park[(set - 1) * kNB * kNC + (i0 + a) * kNC + c0 + q] = acc[a][q];
+    __syncthreads();
+    if (set == 0)
+#pragma unroll
+      for (int a = 0; a < kIW; ++a)
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          const int i = i0 + a, c = c0 + q;
+          T w = acc[a][q];
+#pragma unroll
+          for (int p = 0; p < kSets - 1; ++p) w += park[p * kNB * kNC + i * kNC + c];
+          sW[i * kNC + c] = w;
+        }
   }
   __syncthreads();
-  // W2 = T^T W  (T upper triangular: W2(i) = sum_{l <= i} T(l, i) W(l))
-  T* sW2 = sC0;
+  // T to shared memory (the tail of the tile buffers), A into W
+  T* sT = sV0 + 2 * kVS + 2 * kCS - kNB * (kNB + 1);  // sT[l * (kNB+1) + i] = T(l, i)
+#pragma unroll
+  for (int q = 0; q < kST; ++q) {
+    const int idx = t + q * kThreads;
+    sT[(idx & (kNB - 1)) * (kNB + 1) + idx / kNB] = rt[q];
+  }
+  if (!unit)
+#pragma unroll
+    for (int q = 0; q < kSA; ++q) {
+      const int idx = t + q * kThreads;
+      sW[(idx & (kNB - 1)) * kNC + idx / kNB] += ra[q];
+    }
+  __syncthreads();
+  // ---- W2 = T^T W (T upper triangular: W2(i) = sum_{l <= i} T(l, i) W(l))
+  T* sW2 = sV0;
+  static_assert(kNB * kNC <= 2 * kVS + 2 * kCS - kNB * (kNB + 1), "W2 and T areas");
   for (int idx = t; idx < kNB * kNC; idx += kThreads) {
     const int i = idx / kNC, c = idx % kNC;
     T s = 0.0;
     if (i < kb)
-      for (int l = 0; l <= i; ++l) s += ld_v<kCg>(Tm + l + (size_t)i * ldt) * sW[l * kNC + c];
+      for (int l = 0; l <= i; ++l) s += sT[l * (kNB + 1) + i] * sW[l * kNC + c];
     sW2[i * kNC + c] = s;
   }
   __syncthreads();
@@ -459,82 +516,125 @@ __device__ void tile_left_qt(const T* V, int ldv, const T* Tm, int ldt, int kb, 
       const int i = idx % kb, c = idx / kb;
       A[i + col(c) * lda] -= sW2[i * kNC + c];
     }
-  // C -= V W2: thread row r = t & 31 of each tile, columns g*8..+7 (g = t >> 5);
-  // the next tile's V and C are loaded before the current tile's products
-  {
-    const int r = t & (kRT - 1), g = t / kRT;
-    constexpr int kCPT = kRT * kNC / kThreads;  // columns per thread
-    T cc[kCPT], cn[kCPT];
-    auto crow = [&](int r0, T* dst) {
+  // ---- C -= V W2.  A thread keeps W2(:, its kCW columns) in registers and
+  // owns kRW rows of each tile (a warp shares its rows: V rows are broadcast)
+  constexpr int kCW = sizeof(T) == 4 ? 2 : 1;     // columns per thread
+  constexpr int kRW = kRT * kNC / kThreads / kCW;  // rows per thread
+  const int cq = (t % (kNC / kCW)) * kCW, rq = (t / (kNC / kCW)) * kRW;
+  T w2[kNB][kCW];
 #pragma unroll
-      for (int p = 0; p < kCPT; ++p) {
-        const int c = g * kCPT + p;
-        dst[p] = (r0 + r < m && c < nc) ? C[(r0 + r) + col(c) * ldc] : (T)0.0;
-      }
-    };
-    vload(0);
-    crow(0, cc);
-    vstash(0);
-    __syncthreads();
-    for (int tt = 0; tt < ntile; ++tt) {
-      const int b = tt & 1, r0 = tt * kRT;
-      const bool more = tt + 1 < ntile;
-      if (more) {
-        vload(r0 + kRT);
-        crow(r0 + kRT, cn);
-      }
-      const T* vr = sV0 + b * kVS + r * (kNB + 1);
-      T u[kCPT];
+  for (int i = 0; i < kNB; ++i)
 #pragma unroll
-      for (int p = 0; p < kCPT; ++p) u[p] = 0.0;
-#pragma unroll 8
+    for (int q = 0; q < kCW; ++q) w2[i][q] = sW2[i * kNC + cq + q];
+  __syncthreads();
+  vload(0);
+  cload(0);
+  vstash(0);
+  cstash(0);
+  __syncthreads();
+  for (int tt = 0; tt < ntile; ++tt) {
+    const int b = tt & 1, r0 = tt * kRT;
+    const bool more = tt + 1 < ntile;
+    if (more) {
+      vload(r0 + kRT);
+      cload(r0 + kRT);
+    }
+    const T* sV = sV0 + b * kVS;
+    T* sC = sC0 + b * kCS;
+#pragma unroll
+    for (int r = 0; r < kRW; ++r) {
+      const T* vr = sV + (rq + r) * kLV;
+      T u[kCW];
+#pragma unroll
+      for (int q = 0; q < kCW; ++q) u[q] = 0.0;
+#pragma unroll
       for (int i = 0; i < kNB; ++i) {
         const T a = vr[i];
-        const T* w = sW2 + i * kNC + g * kCPT;
 #pragma unroll
-        for (int p = 0; p < kCPT; ++p) u[p] += a * w[p];
+        for (int q = 0; q < kCW; ++q) u[q] += a * w2[i][q];
       }
-      if (r0 + r < m)
 #pragma unroll
-        for (int p = 0; p < kCPT; ++p) {
-          const int c = g * kCPT + p;
-          if (c < nc) C[(r0 + r) + col(c) * ldc] = cc[p] - u[p];
-        }
-      if (more) {
-        vstash(b ^ 1);
-#pragma unroll
-        for (int p = 0; p < kCPT; ++p) cc[p] = cn[p];
-      }
-      __syncthreads();
+      for (int q = 0; q < kCW; ++q) sC[(rq + r) * kLC + cq + q] -= u[q];
     }
+    __syncthreads();
+    // the updated tile back to global memory, coalesced
+    if (r0 + lr < m)
+#pragma unroll
+      for (int q = 0; q < kSC; ++q) {
+        const int c = lw * kSC + q;
+        if (c < nc) C[(r0 + lr) + col(c) * ldc] = sC[lr * kLC + c];
+      }
+    if (more) {
+      vstash(b ^ 1);
+      cstash(b ^ 1);
+    }
+    __syncthreads();
   }
 }
 
 // C (m <= kNC rows x n) <- C (I - V T V^T) with one panel, V unit lower
-// trapezoidal (n x kb).
+// trapezoidal (n x kb).  Column tiles of kRT stream through two shared
+// buffers: the next tile's global loads are issued before the current tile's
+// products.
 template <typename T>
 __device__ void tile_right_q(const T* V, int ldv, const T* Tm, int ldt, int kb, T* C, int ldc, int m,
                              int n, T* sm) {
-  T* sV = sm;                              // [kRT][kNB+1]: V rows c0..c0+31
-  T* sC = sV + kRT * (kNB + 1);            // [kNC][kRT+1]: C(r, c0+c)
-  T* sW = sC + kNC * (kRT + 1);            // [kNC][kNB] W(r, i)
+  constexpr int kVS = kRT * (kNB + 1), kCS = kNC * (kRT + 1);
+  static_assert(2 * kVS + 2 * kCS + kNC * kNB <= kTileSmem, "right apply scratch");
+  T* sV0 = sm;               // two [kRT][kNB+1] tiles: V rows c0..c0+31
+  T* sC0 = sV0 + 2 * kVS;    // two [kNC][kRT+1] tiles: C(r, c0+c)
+  T* sW = sC0 + 2 * kCS;     // [kNC][kNB] W(r, i)
   const int t = threadIdx.x;
-  const int ti = t & 7, tr = t >> 3;            // i = ti*4..+3, r = tr*2..+1
-  T acc[2][4] = {{0, 0, 0, 0}, {0, 0, 0, 0}};
-  for (int c0 = 0; c0 < n; c0 += kRT) {
-    const int cn = (n - c0) < kRT ? (n - c0) : kRT;
-    for (int idx = t; idx < kRT * kNB; idx += kThreads) {
-      const int c = idx % kRT, i = idx / kRT, gc = c0 + c;
+  constexpr int kSV = kRT * kNB / kThreads, kSC = kNC * kRT / kThreads;
+  T rv[kSV], rc[kSC];
+  auto vload = [&](int c0) {
+#pragma unroll
+    for (int q = 0; q < kSV; ++q) {
+      const int idx = t + q * kThreads, c = idx % kRT, i = idx / kRT, gc = c0 + c;
       T v = 0.0;
-      if (c < cn && i < kb) v = gc == i ? 1.0 : (gc < i ? 0.0 : V[gc + (size_t)i * ldv]);
-      sV[c * (kNB + 1) + i] = v;
+      if (gc < n && i < kb) v = gc == i ? (T)1.0 : (gc < i ? (T)0.0 : V[gc + (size_t)i * ldv]);
+      rv[q] = v;
     }
-    for (int idx = t; idx < kNC * kRT; idx += kThreads) {
-      const int r = idx % kNC, c = idx / kNC;
-      sC[r * (kRT + 1) + c] = (r < m && c < cn) ? C[r + (size_t)(c0 + c) * ldc] : 0.0;
+  };
+  auto vstash = [&](int b) {
+#pragma unroll
+    for (int q = 0; q < kSV; ++q) {
+      const int idx = t + q * kThreads;
+      sV0[b * kVS + (idx % kRT) * (kNB + 1) + idx / kRT] = rv[q];
     }
-    __syncthreads();
-#pragma unroll 4
+  };
+  auto cload = [&](int c0) {
+#pragma unroll
+    for (int q = 0; q < kSC; ++q) {
+      const int idx = t + q * kThreads, r = idx % kNC, c = idx / kNC;
+      rc[q] = (r < m && c0 + c < n) ? C[r + (size_t)(c0 + c) * ldc] : (T)0.0;
+    }
+  };
+  auto cstash = [&](int b) {
+#pragma unroll
+    for (int q = 0; q < kSC; ++q) {
+      const int idx = t + q * kThreads;
+      sC0[b * kCS + (idx % kNC) * (kRT + 1) + idx / kNC] = rc[q];
+    }
+  };
+  const int ntile = (n + kRT - 1) / kRT;
+  const int ti = t & 7, tr = t >> 3;  // i = ti*4..+3, r = tr*2..+1
+  T acc[2][4] = {{0, 0, 0, 0}, {0, 0, 0, 0}};
+  vload(0);
+  cload(0);
+  vstash(0);
+  cstash(0);
+  __syncthreads();
+  for (int tt = 0; tt < ntile; ++tt) {
+    const int b = tt & 1;
+    const bool more = tt + 1 < ntile;
+    if (more) {
+      vload((tt + 1) * kRT);
+      cload((tt + 1) * kRT);
+    }
+    const T* sV = sV0 + b * kVS;
+    const T* sC = sC0 + b * kCS;
+#pragma unroll 8
     for (int c = 0; c < kRT; ++c) {
       const T a0 = sC[(tr * 2) * (kRT + 1) + c], a1 = sC[(tr * 2 + 1) * (kRT + 1) + c];
 #pragma unroll
@@ -544,6 +644,10 @@ __device__ void tile_right_q(const T* V, int ldv, const T* Tm, int ldt, int kb, 
         acc[1][q] += a1 * v;
       }
     }
+    if (more) {
+      vstash(b ^ 1);
+      cstash(b ^ 1);
+    }
     __syncthreads();
   }
 #pragma unroll
@@ -551,8 +655,14 @@ __device__ void tile_right_q(const T* V, int ldv, const T* Tm, int ldt, int kb, 
 #pragma unroll
     for (int q = 0; q < 4; ++q) sW[(tr * 2 + p) * kNB + ti * 4 + q] = acc[p][q];
   __syncthreads();
-  // W2 = W T (W2(r,i) = sum_{l <= i} W(r,l) T(l,i))
-  T* sW2 = sC;  // [kNC][kNB]
+  // W2 = W T (W2(r,i) = sum_{l <= i} W(r,l) T(l,i)), T staged in shared memory
+  T* sT = sC0;                 // [kNB][kNB+1]
+  T* sW2 = sC0 + kNB * (kNB + 1);  // [kNC][kNB]
+  for (int idx = t; idx < kNB * kNB; idx += kThreads) {
+    const int l = idx % kNB, i = idx / kNB;
+    sT[l * (kNB + 1) + i] = (l <= i && i < kb) ? Tm[l + (size_t)i * ldt] : (T)0.0;
+  }
+  __syncthreads();
 #pragma unroll
   for (int p = 0; p < 2; ++p)
 #pragma unroll
@@ -560,23 +670,23 @@ __device__ void tile_right_q(const T* V, int ldv, const T* Tm, int ldt, int kb, 
       const int r = tr * 2 + p, i = ti * 4 + q;
       T s = 0.0;
       if (i < kb)
-        for (int l = 0; l <= i; ++l) s += sW[r * kNB + l] * Tm[l + (size_t)i * ldt];
+        for (int l = 0; l <= i; ++l) s += sW[r * kNB + l] * sT[l * (kNB + 1) + i];
       sW2[r * kNB + i] = s;
     }
   __syncthreads();
-  // C(r, c) -= sum_i W2(r, i) V(c, i)
-  const int rr = t & 31, cc = t >> 5;  // rows rr, rr+32; cols cc*4..+3 of the tile
-  for (int c0 = 0; c0 < n; c0 += kRT) {
-    const int cn = (n - c0) < kRT ? (n - c0) : kRT;
-    for (int idx = t; idx < kRT * kNB; idx += kThreads) {
-      const int c = idx % kRT, i = idx / kRT, gc = c0 + c;
-      T v = 0.0;
-      if (c < cn && i < kb) v = gc == i ? 1.0 : (gc < i ? 0.0 : V[gc + (size_t)i * ldv]);
-      sV[c * (kNB + 1) + i] = v;
-    }
-    __syncthreads();
+  // C(r, c) -= sum_i W2(r, i) V(c, i): thread rows rr, rr+32, columns cc*4..+3
+  // of each tile; the next tile's V is loaded before the current products
+  const int rr = t & 31, cc = t >> 5;
+  vload(0);
+  vstash(0);
+  __syncthreads();
+  for (int tt = 0; tt < ntile; ++tt) {
+    const int b = tt & 1, c0 = tt * kRT;
+    const bool more = tt + 1 < ntile;
+    if (more) vload(c0 + kRT);
+    const T* sV = sV0 + b * kVS;
     T u[2][4] = {{0, 0, 0, 0}, {0, 0, 0, 0}};
-#pragma unroll 4
+#pragma unroll 8
     for (int i = 0; i < kNB; ++i) {
       const T w0 = sW2[rr * kNB + i], w1 = sW2[(rr + 32) * kNB + i];
 #pragma unroll
@@ -591,8 +701,9 @@ __device__ void tile_right_q(const T* V, int ldv, const T* Tm, int ldt, int kb, 
 #pragma unroll
       for (int q = 0; q < 4; ++q) {
         const int r = rr + 32 * p, c = cc * 4 + q;
-        if (r < m && c < cn) C[r + (size_t)(c0 + c) * ldc] -= u[p][q];
+        if (r < m && c0 + c < n) C[r + (size_t)(c0 + c) * ldc] -= u[p][q];
       }
+    if (more) vstash(b ^ 1);
     __syncthreads();
   }
 }
