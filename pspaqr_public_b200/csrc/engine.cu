@@ -101,6 +101,10 @@ Tree::~Tree() {
   cudaFree(d_tickets_);
   cudaFree(d_status_);
   cudaFree(d_tmp_);
+  cudaFree(d_dst_);
+  cudaFree(d_perm_);
+  cudaFree(d_cval_);
+  cudaFreeHost(h_cval_);
   cudaFree(d_krylov_);
   scratch_.release();
   arena_.release();
@@ -209,6 +213,7 @@ int Tree::partition(int nrows, int ncols, const int* colptr, const int* rowidx, 
   if (rc != 0) return fail(rc, st_.error);
   partitioned_ = true;
   assembled_ = factorized_ = false;
+  asm_valid_ = false;
   t_partition = wall() - t0;
   if (verbose) printf("Time to partition: %g\n", t_partition);
   return 0;
@@ -260,58 +265,79 @@ int Tree::assemble() {
   }
   if (int rc = alloc_level_blocks(L0.edges)) return rc;
   const Csc& P = st_.App;
-  std::vector<int> leaf_of(n);
-  for (int o = L0.first; o < L0.first + L0.count; ++o)
-    for (int k = st_.clusters[o].cstart; k < st_.clusters[o].cstart + st_.clusters[o].size0; ++k) leaf_of[k] = o;
   const int nnz = (int)P.rowidx.size();
-  std::vector<double*> dst(nnz);
-  for (int j = 0; j < n; ++j) {
-    const int cj = leaf_of[j];
-    for (int k = P.colptr[j]; k < P.colptr[j + 1]; ++k) {
-      const int i = P.rowidx[k];
-      const int ri = leaf_of[i];
-      const int e = st_.find_edge(cj, ri);
-      dst[k] = elem(ptr_[e], (i - st_.clusters[ri].cstart) + (size_t)(j - st_.clusters[cj].cstart) * ld_[e]);
-    }
-  }
-  // CSR of App for the SpMV (y = App x)
-  std::vector<int> rowptr(n + 1, 0), col(nnz);
-  std::vector<double> val(nnz);
-  for (int k = 0; k < nnz; ++k) rowptr[P.rowidx[k] + 1]++;
-  std::partial_sum(rowptr.begin(), rowptr.end(), rowptr.begin());
-  {
-    std::vector<int> pos(rowptr.begin(), rowptr.end() - 1);
-    for (int j = 0; j < n; ++j)
+  std::vector<double*> ptr0;
+  for (int e : L0.edges) ptr0.push_back(ptr_[e]);
+  if (!asm_valid_ || asm_fp32_ != (fp32_ ? 1 : 0) || ptr0 != asm_ptr0_) {
+    // maps of this partition and block layout: the destination of every
+    // nonzero and the CSR (row-major) order of the SpMV copy
+    std::vector<int> leaf_of(n);
+    for (int o = L0.first; o < L0.first + L0.count; ++o)
+      for (int k = st_.clusters[o].cstart; k < st_.clusters[o].cstart + st_.clusters[o].size0; ++k) leaf_of[k] = o;
+    std::vector<double*> dst(nnz);
+    for (int j = 0; j < n; ++j) {
+      const int cj = leaf_of[j];
       for (int k = P.colptr[j]; k < P.colptr[j + 1]; ++k) {
-        int p = pos[P.rowidx[k]]++;
-        col[p] = j;
-        val[p] = P.val[k];
+        const int i = P.rowidx[k];
+        const int ri = leaf_of[i];
+        const int e = st_.find_edge(cj, ri);
+        dst[k] = elem(ptr_[e], (i - st_.clusters[ri].cstart) + (size_t)(j - st_.clusters[cj].cstart) * ld_[e]);
       }
+    }
+    std::vector<int> rowptr(n + 1, 0), col(nnz), perm(nnz);
+    for (int k = 0; k < nnz; ++k) rowptr[P.rowidx[k] + 1]++;
+    std::partial_sum(rowptr.begin(), rowptr.end(), rowptr.begin());
+    {
+      std::vector<int> pos(rowptr.begin(), rowptr.end() - 1);
+      for (int j = 0; j < n; ++j)
+        for (int k = P.colptr[j]; k < P.colptr[j + 1]; ++k) {
+          const int q = pos[P.rowidx[k]]++;
+          col[q] = j;
+          perm[k] = q;
+        }
+    }
+    cudaFree(d_rowptr_);
+    cudaFree(d_col_);
+    cudaFree(d_val_);
+    cudaFree(d_dst_);
+    cudaFree(d_perm_);
+    cudaFree(d_cval_);
+    cudaFree(d_rank_);
+    cudaFree(d_status_);
+    cudaFree(d_tmp_);
+    cudaFreeHost(h_cval_);
+    d_rowptr_ = nullptr, d_col_ = nullptr, d_val_ = nullptr, d_dst_ = nullptr, d_perm_ = nullptr;
+    d_cval_ = nullptr, d_rank_ = nullptr, d_status_ = nullptr, d_tmp_ = nullptr, h_cval_ = nullptr;
+    const size_t nz = (size_t)std::max(nnz, 1);
+    if (check_cuda(cudaMalloc(&d_rowptr_, sizeof(int) * (n + 1)), "malloc") ||
+        check_cuda(cudaMalloc(&d_col_, sizeof(int) * nz), "malloc") ||
+        check_cuda(cudaMalloc(&d_val_, sizeof(double) * nz), "malloc") ||
+        check_cuda(cudaMalloc(&d_dst_, sizeof(double*) * nz), "malloc") ||
+        check_cuda(cudaMalloc(&d_perm_, sizeof(int) * nz), "malloc") ||
+        check_cuda(cudaMalloc(&d_cval_, sizeof(double) * nz), "malloc") ||
+        check_cuda(cudaMalloc(&d_rank_, sizeof(int) * ncl), "malloc") ||
+        check_cuda(cudaMalloc(&d_status_, sizeof(int)), "malloc") ||
+        check_cuda(cudaMalloc(&d_tmp_, sizeof(double) * 2 * n), "malloc") ||
+        check_cuda(cudaHostAlloc(&h_cval_, sizeof(double) * nz, cudaHostAllocDefault), "host alloc"))
+      return -10;
+    if (check_cuda(cudaMemcpy(d_rowptr_, rowptr.data(), sizeof(int) * (n + 1), cudaMemcpyHostToDevice), "upload") ||
+        check_cuda(cudaMemcpy(d_col_, col.data(), sizeof(int) * nnz, cudaMemcpyHostToDevice), "upload") ||
+        check_cuda(cudaMemcpy(d_dst_, dst.data(), sizeof(double*) * nnz, cudaMemcpyHostToDevice), "upload") ||
+        check_cuda(cudaMemcpy(d_perm_, perm.data(), sizeof(int) * nnz, cudaMemcpyHostToDevice), "upload"))
+      return -10;
+    asm_ptr0_ = ptr0;
+    asm_fp32_ = fp32_ ? 1 : 0;
+    asm_valid_ = true;
   }
-  cudaFree(d_rowptr_);
-  cudaFree(d_col_);
-  cudaFree(d_val_);
-  cudaFree(d_rank_);
-  cudaFree(d_status_);
-  cudaFree(d_tmp_);
-  if (check_cuda(cudaMalloc(&d_rowptr_, sizeof(int) * (n + 1)), "malloc") ||
-      check_cuda(cudaMalloc(&d_col_, sizeof(int) * std::max(nnz, 1)), "malloc") ||
-      check_cuda(cudaMalloc(&d_val_, sizeof(double) * std::max(nnz, 1)), "malloc") ||
-      check_cuda(cudaMalloc(&d_rank_, sizeof(int) * ncl), "malloc") ||
-      check_cuda(cudaMalloc(&d_status_, sizeof(int)), "malloc") ||
-      check_cuda(cudaMalloc(&d_tmp_, sizeof(double) * 2 * n), "malloc"))
-    return -10;
   scratch_.reset();
-  cudaMemcpyAsync(d_rowptr_, rowptr.data(), sizeof(int) * (n + 1), cudaMemcpyHostToDevice, stream_);
-  cudaMemcpyAsync(d_col_, col.data(), sizeof(int) * nnz, cudaMemcpyHostToDevice, stream_);
-  cudaMemcpyAsync(d_val_, val.data(), sizeof(double) * nnz, cudaMemcpyHostToDevice, stream_);
   cudaMemsetAsync(d_status_, 0, sizeof(int), stream_);
-  // scatter values of App (CSC order) into the blocks
-  std::vector<double> cval(P.val);
-  double* d_cval = static_cast<double*>(upload(cval.data(), sizeof(double) * nnz));
-  double** d_dst = static_cast<double**>(upload(dst.data(), sizeof(double*) * nnz));
-  if (!d_cval || !d_dst) return fail(-11, "out of device memory (assembly)");
-  if (check_cuda(launch_scatter(nnz, d_cval, d_dst, stream_), "scatter")) return -10;
+  // the values of App (CSC order): one copy from pinned memory, scattered into
+  // the blocks and permuted into the SpMV's CSR order on the device
+  std::memcpy(h_cval_, P.val.data(), sizeof(double) * nnz);
+  if (check_cuda(cudaMemcpyAsync(d_cval_, h_cval_, sizeof(double) * nnz, cudaMemcpyHostToDevice, stream_), "values") ||
+      check_cuda(launch_scatter(nnz, d_cval_, d_dst_, stream_), "scatter") ||
+      check_cuda(launch_permute(nnz, d_perm_, d_cval_, d_val_, stream_), "value permutation"))
+    return -10;
   if (check_cuda(cudaStreamSynchronize(stream_), "assemble")) return -10;
   scratch_.reset();
   assembled_ = true;
@@ -754,7 +780,8 @@ int Tree::factorize() {
       int* d_fb = nullptr;
       if (rank_model_ || rank_log_) {
         sk.resize(nsp);
-        int mmax = 1, wmax = 1;
+        int mmax = 1;
+        std::vector<GemmTile> fblocks;  // column blocks of the feature pass
         d_feat = static_cast<float*>(scratch_.alloc(sizeof(float) * kRankFeatures * std::max<size_t>(nsp, 1)));
         double* d_cmax2 = scratch_.dalloc(std::max<size_t>(nsp, 1));
         d_ell = static_cast<int*>(scratch_.alloc(sizeof(int) * std::max<size_t>(nsp, 1)));
@@ -769,6 +796,9 @@ int Tree::factorize() {
           t.w = sp_w[q];
           t.ldw = sp_ldw[q];
           t.cn2 = scratch_.dalloc(std::max(t.w, 1));
+          const int nblk = (t.w + kFeatCols - 1) / kFeatCols;
+          t.y4p = scratch_.dalloc((size_t)std::max(nblk, 1) * 4 * std::max(t.m, 1));
+          for (int b = 0; b < nblk; ++b) fblocks.push_back({(int)q, 0, b * kFeatCols});
           t.feat = d_feat + q * kRankFeatures;
           t.cmax2 = d_cmax2 + q;
           t.ell = d_ell + q;
@@ -776,13 +806,15 @@ int Tree::factorize() {
           t.fallback = d_fb + q;
           t.seed = 0x5EEDull ^ ((unsigned long long)lvl << 40) ^ ((unsigned long long)p * 0x9E3779B97F4A7C15ull);
           t.level = lvl;
-          if (!t.cn2) return fail(-11, "out of device memory (rank features)");
+          if (!t.cn2 || !t.y4p) return fail(-11, "out of device memory (rank features)");
           mmax = std::max(mmax, t.m);
-          wmax = std::max(wmax, t.w);
         }
         auto* d_sk = static_cast<SketchTask*>(up_any(sk));
-        if (!d_sk) return fail(-11, "out of device memory (rank features)");
-        if (ck(launch_rank_features(d_sk, (int)nsp, tol, mmax, wmax, stream_), "rank features")) return -10;
+        auto* d_fb_blocks = static_cast<GemmTile*>(up_any(fblocks));
+        if (!d_sk || !d_fb_blocks) return fail(-11, "out of device memory (rank features)");
+        if (ck(launch_rank_features(d_sk, (int)nsp, d_fb_blocks, (int)fblocks.size(), tol, mmax, stream_),
+               "rank features"))
+          return -10;
         if (rank_model_) {
           RankModel model{d_model_, d_model_ + kMlpParams, d_model_ + kMlpParams + kRankFeatures, oversample_};
           if (ck(launch_rank_predict(d_sk, (int)nsp, model, stream_), "rank prediction")) return -10;
@@ -841,10 +873,10 @@ int Tree::factorize() {
           moff += (size_t)ell[q] + 1;
           if (!t.Y || !Qc || !t.B) return fail(-11, "out of device memory (sketch)");
           if (t.m <= 0 || t.w <= 0) continue;
-          for (int r0 = 0; r0 < t.m; r0 += 64)
-            for (int c0 = 0; c0 < ell[q]; c0 += 64) sk_tiles.push_back({(int)q, r0, c0});
-          for (int l0 = 0; l0 < ell[q]; l0 += 64)
-            for (int j0 = 0; j0 < t.w; j0 += 64) pj_tiles.push_back({(int)q, l0, j0});
+          for (int r0 = 0; r0 < t.m; r0 += kSketchRows)
+            for (int c0 = 0; c0 < ell[q]; c0 += kSketchCols) sk_tiles.push_back({(int)q, r0, c0});
+          for (int l0 = 0; l0 < ell[q]; l0 += kProjectRows)
+            for (int j0 = 0; j0 < t.w; j0 += kProjectCols) pj_tiles.push_back({(int)q, l0, j0});
           for (int j0 = 0; j0 < t.w; j0 += 256) scan_blocks.push_back({(int)q, 0, j0});
           // the sketch's pivoted QR stops at sketch_tol * tol and writes its
           // rank over the sketch width: later stages use only those vectors

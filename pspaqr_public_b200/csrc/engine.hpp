@@ -187,6 +187,15 @@ class Tree {
   int* d_rowptr_ = nullptr;
   int* d_col_ = nullptr;
   double* d_val_ = nullptr;
+  // assembly maps built once per partition and storage precision: the block
+  // element of each nonzero (CSC order), its CSR position, the CSC values
+  double** d_dst_ = nullptr;
+  int* d_perm_ = nullptr;
+  double* d_cval_ = nullptr;
+  double* h_cval_ = nullptr;  // pinned copy of the values for the upload
+  std::vector<double*> asm_ptr0_;  // level-0 block addresses the maps were built for
+  int asm_fp32_ = -1;
+  bool asm_valid_ = false;
   double* d_xw_ = nullptr;     // solve workspace (all cluster vectors)
   int64_t xw_size_ = 0;
   int* d_turn_ = nullptr;      // per cluster turn counters

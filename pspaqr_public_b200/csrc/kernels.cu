@@ -1064,6 +1064,10 @@ __global__ void __launch_bounds__(kThreads) k_bwd_elim(const BwdElimTask* __rest
   for (int i = threadIdx.x; i < t.n; i += kThreads) as<T>(t.x)[i] = x[i];
 }
 
+__global__ void k_permute(int n, const int* __restrict__ perm, const double* __restrict__ src, double* dst) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) dst[perm[i]] = src[i];
+}
+
 template <typename T>
 __global__ void k_copy_idx(int n, const int* __restrict__ src, const int* __restrict__ dst, double* xd) {
   T* x = as<T>(xd);
@@ -1225,6 +1229,14 @@ cudaError_t launch_scatter(int nnz, const double* val, double* const* dst, cudaS
   counted();
   if (g_fp32) k_scatter<float><<<grid_for(nnz), 256, 0, st>>>(nnz, val, dst);
   else k_scatter<double><<<grid_for(nnz), 256, 0, st>>>(nnz, val, dst);
+  return last();
+}
+
+cudaError_t launch_permute(int n, const int* perm, const double* src, double* dst, cudaStream_t st) {
+  if (cudaError_t pre = begin("launch_permute")) return pre;
+  if (n <= 0) return cudaSuccess;
+  counted();
+  k_permute<<<grid_for(n), 256, 0, st>>>(n, perm, src, dst);
   return last();
 }
 

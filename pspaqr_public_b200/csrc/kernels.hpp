@@ -27,6 +27,8 @@ cudaError_t launch_to_f32_batch(const ConvTask* t, int ntasks, cudaStream_t st);
 void add_kernel_launches(long long n);
 
 cudaError_t launch_scatter(int nnz, const double* val, double* const* dst, cudaStream_t st);
+// dst[perm[i]] = src[i], i < n
+cudaError_t launch_permute(int n, const int* perm, const double* src, double* dst, cudaStream_t st);
 // cs = CTAs per task (thread-block cluster size); vmax = longest reflector tail
 cudaError_t launch_elim(const ElimTask* t, const ElimOut* o, int ntasks, int cs, int nmax, int vmax, cudaStream_t st);
 cudaError_t launch_scale(const ScaleTask* t, int ntasks, int cs, int nmax, cudaStream_t st);

@@ -63,8 +63,68 @@ __device__ double block_max(double v, double* red) {
 }
 
 // ---------------------------------------------------------------- features
-// One CTA per interface.  Dynamic shared memory: 4 * mmax doubles (the
-// 4-column sketch) + wmax bytes (its signs).
+// Signs of the 4-column feature sketch of column j: bit c set = +1.
+__device__ __forceinline__ unsigned feat_signs(unsigned long long seed, int j) {
+  return (unsigned)(omega_bits(seed ^ 0x5DEECE66Dull, j, 0) & 15u);
+}
+
+// One CTA per block of kFeatCols columns (tile.c0): squared norms of its
+// columns (a thread per column, eight rows in flight), then its part of the
+// 4-column Rademacher sketch (a warp per row, the block's columns over the
+// lanes) into y4p[(block * 4 + c) * m + r].
+__global__ void __launch_bounds__(kT) k_feature_blocks(const SketchTask* __restrict__ tasks,
+                                                       const GemmTile* __restrict__ blocks) {
+  const GemmTile g = blocks[blockIdx.x];
+  const SketchTask t = tasks[g.task];
+  const int m = t.m, w = t.w;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int j = g.c0 + threadIdx.x;
+  if (j < w) {
+    const double* col = t.C + j;
+    double a[8] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+    int r = 0;
+    for (; r + 8 <= m; r += 8) {
+      double v[8];
+#pragma unroll
+      for (int u = 0; u < 8; ++u) v[u] = __ldg(col + (size_t)(r + u) * t.ldw);
+#pragma unroll
+      for (int u = 0; u < 8; ++u) a[u] += v[u] * v[u];
+    }
+    for (; r < m; ++r) {
+      const double v = __ldg(col + (size_t)r * t.ldw);
+      a[0] += v * v;
+    }
+    t.cn2[j] = ((a[0] + a[1]) + (a[2] + a[3])) + ((a[4] + a[5]) + (a[6] + a[7]));
+  }
+  constexpr int kPer = kFeatCols / 32;
+  unsigned sg[kPer];
+#pragma unroll
+  for (int u = 0; u < kPer; ++u) {
+    const int jj = g.c0 + lane + 32 * u;
+    sg[u] = jj < w ? feat_signs(t.seed, jj) : 0u;
+  }
+  const int blk = g.c0 / kFeatCols;
+  for (int r = warp; r < m; r += kT / 32) {
+    const double* row = t.C + (size_t)r * t.ldw;
+    double y[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+    for (int u = 0; u < kPer; ++u) {
+      const int jj = g.c0 + lane + 32 * u;
+      const double v = jj < w ? __ldg(row + jj) : 0.0;
+#pragma unroll
+      for (int c = 0; c < 4; ++c) y[c] += ((sg[u] >> c) & 1u) ? v : -v;
+    }
+#pragma unroll
+    for (int c = 0; c < 4; ++c) y[c] = warp_sumd(y[c]);
+    if (lane == 0)
+#pragma unroll
+      for (int c = 0; c < 4; ++c) t.y4p[((size_t)blk * 4 + c) * m + r] = y[c];
+  }
+}
+
+// One CTA per interface: the sketch (partials summed in block order), its QR
+// diagonal, the norm statistics and the 11 features.  Dynamic shared memory:
+// 4 * mmax doubles.
 __global__ void __launch_bounds__(kT) k_rank_features(const SketchTask* __restrict__ tasks, double tol) {
   extern __shared__ double sm[];
   __shared__ double red[kT / 32];
@@ -72,20 +132,18 @@ __global__ void __launch_bounds__(kT) k_rank_features(const SketchTask* __restri
   const int m = t.m, w = t.w;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   double* y4 = sm;
-  unsigned char* sg = reinterpret_cast<unsigned char*>(sm + 4 * (size_t)(m > 0 ? m : 1));
-  // squared column norms
+  const int nblk = (w + kFeatCols - 1) / kFeatCols;
+  for (int e = threadIdx.x; e < 4 * m; e += kT) {
+    const int c = e / m, r = e % m;
+    double s = 0.0;
+    for (int b = 0; b < nblk; ++b) s += t.y4p[((size_t)b * 4 + c) * m + r];
+    y4[e] = s;
+  }
   double cmax = 0.0, fro = 0.0;
   for (int j = threadIdx.x; j < w; j += kT) {
-    double s = 0.0;
-#pragma unroll 4
-    for (int r = 0; r < m; ++r) {
-      const double v = __ldg(t.C + (size_t)r * t.ldw + j);
-      s += v * v;
-    }
-    t.cn2[j] = s;
+    const double s = t.cn2[j];
     cmax = fmax(cmax, s);
     fro += s;
-    sg[j] = (unsigned char)(omega_bits(t.seed ^ 0x5DEECE66Dull, j, 0) & 15u);
   }
   cmax = block_max(cmax, red);
   fro = block_sum(fro, red);
@@ -100,29 +158,6 @@ __global__ void __launch_bounds__(kT) k_rank_features(const SketchTask* __restri
   double cq[3];
 #pragma unroll
   for (int q = 0; q < 3; ++q) cq[q] = block_sum((double)cnt[q], red);
-  // 4-column Rademacher sketch, one warp per row
-  for (int r = warp; r < m; r += kT / 32) {
-    double a0 = 0, a1 = 0, a2 = 0, a3 = 0;
-    const double* row = t.C + (size_t)r * t.ldw;
-    for (int j = lane; j < w; j += 32) {
-      const double v = __ldg(row + j);
-      const unsigned s = sg[j];
-      a0 += (s & 1u) ? v : -v;
-      a1 += (s & 2u) ? v : -v;
-      a2 += (s & 4u) ? v : -v;
-      a3 += (s & 8u) ? v : -v;
-    }
-    a0 = warp_sumd(a0);
-    a1 = warp_sumd(a1);
-    a2 = warp_sumd(a2);
-    a3 = warp_sumd(a3);
-    if (lane == 0) {
-      y4[r] = a0;
-      y4[m + r] = a1;
-      y4[2 * m + r] = a2;
-      y4[3 * m + r] = a3;
-    }
-  }
   __syncthreads();
   // diagonal of R in a QR of the sketch (modified Gram-Schmidt, warp 0)
   double d[4] = {0, 0, 0, 0};
@@ -685,17 +720,20 @@ cudaError_t done_launch(const char* name) {
 }  // namespace
 
 // ---------------------------------------------------------------- launchers
-size_t rank_features_smem(int mmax, int wmax) {
-  return sizeof(double) * (4 * (size_t)std::max(mmax, 1) + ((size_t)std::max(wmax, 1) + 7) / 8);
-}
+size_t rank_features_smem(int mmax) { return sizeof(double) * 4 * (size_t)std::max(mmax, 1); }
 
-cudaError_t launch_rank_features(const SketchTask* t, int ntasks, double tol, int mmax, int wmax, cudaStream_t st) {
+cudaError_t launch_rank_features(const SketchTask* t, int ntasks, const GemmTile* blocks, int nblocks, double tol,
+                                 int mmax, cudaStream_t st) {
   if (cudaError_t e = cudaGetLastError()) return e;
   if (ntasks <= 0) return cudaSuccess;
-  const size_t smem = rank_features_smem(mmax, wmax);
+  const size_t smem = rank_features_smem(mmax);
   if (smem > 227 * 1024) return cudaErrorInvalidValue;
   cudaError_t e = cudaFuncSetAttribute(k_rank_features, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e) return e;
+  if (nblocks > 0) {
+    k_feature_blocks<<<nblocks, kT, 0, st>>>(t, blocks);
+    if ((e = done_launch("launch_feature_blocks"))) return e;
+  }
   k_rank_features<<<ntasks, kT, smem, st>>>(t, tol);
   return done_launch("launch_rank_features");
 }

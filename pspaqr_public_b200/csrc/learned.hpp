@@ -53,6 +53,7 @@ struct SketchTask {
   double* G;        // ell x ell Gram matrix Y^T Y, row-major (ld ldy)
   double* Lt;       // ell x ell: Lt[k * ldy + c] = L(c, k) of the pivoted Cholesky of G
   int* colat;       // ell: column of Y at each pivot position
+  double* y4p;      // 4 x m partial sketches per block of kFeatCols columns (features)
   double* B;        // ell x w projections Q^T C, row-major (ld w)
   unsigned long long* M;  // ell + 1 largest squared residuals (bit patterns of doubles >= 0)
   int* rank;        // kept rank (output)
@@ -75,11 +76,18 @@ struct RankModel {
   int oversample;
 };
 
-// one CTA per task; mmax / wmax bound the tasks' m and w
-size_t rank_features_smem(int mmax, int wmax);
-cudaError_t launch_rank_features(const SketchTask* t, int ntasks, double tol, int mmax, int wmax, cudaStream_t st);
+// Features in two launches: per block of kFeatCols columns of an interface
+// (tile.c0) the squared column norms and the partial 4-column sketch; then one
+// CTA per interface (mmax bounds m) sums the partials in block order and forms
+// the features.
+constexpr int kFeatCols = 256;
+size_t rank_features_smem(int mmax);
+cudaError_t launch_rank_features(const SketchTask* t, int ntasks, const GemmTile* blocks, int nblocks, double tol,
+                                 int mmax, cudaStream_t st);
 cudaError_t launch_rank_predict(const SketchTask* t, int ntasks, RankModel model, cudaStream_t st);
-// Y = C Omega over the given tiles (tile rows: rows of C; tile columns: columns of Y)
+// Y = C Omega over the given tiles (tile rows: kSketchRows rows of C; tile
+// columns: kSketchCols columns of Y)
+constexpr int kSketchRows = 64, kSketchCols = 64;
 cudaError_t launch_sketch(const SketchTask* t, const GemmTile* tiles, int ntiles, cudaStream_t st);
 // smallest stop tolerance (relative to |R(0,0)|) the Gram pivoting resolves:
 // |R(i,i)|^2 / |R(0,0)|^2 >= 1e-10 stays four orders above the rounding of G
@@ -92,7 +100,9 @@ cudaError_t launch_gram(const SketchTask* t, const GemmTile* tiles, int ntiles, 
 // go to the smallest position, as in the pivoted QR.
 size_t pchol_smem(int nmax);
 cudaError_t launch_pchol(const SketchTask* t, int ntasks, int nmax, double stol, double pivot_rtol, cudaStream_t st);
-// B = Q^T C over the given tiles (tile rows: basis vectors; tile columns: columns of C)
+// B = Q^T C over the given tiles (tile rows: kProjectRows basis vectors; tile
+// columns: kProjectCols columns of C)
+constexpr int kProjectRows = 64, kProjectCols = 64;
 cudaError_t launch_project(const SketchTask* t, const GemmTile* tiles, int ntiles, cudaStream_t st);
 // residual scan over column blocks of 256 (tile.c0), then the rank choice
 cudaError_t launch_residual_scan(const SketchTask* t, const GemmTile* blocks, int nblocks, cudaStream_t st);
