@@ -742,8 +742,8 @@ __device__ void mat_apply_q_right(const T* V, int ldv, const T* Tm, int k, T* C,
 
 
 // ---------------------------------------------------------------- single-vector applies
-// Shared scratch of vec_panel (elements): partial sums, W2, the panel's T.
-constexpr int kVecRed = (kWarps + 1) * 32 + kNB * (kNB + 1);
+// Shared scratch of vec_panel (elements): partial sums and W2.
+constexpr int kVecRed = (kWarps + 1) * 32;
 
 // One panel of kb <= kNB reflectors on a vector in shared memory:
 //   unit = 1: x (m) <- (I - V T V^T)^T x (trans) or (I - V T V^T) x, V unit
@@ -756,11 +756,15 @@ template <typename T>
 __device__ void vec_panel(const T* V, int ldv, const T* Tm, int ldt, int kb, int unit, bool trans, T* a, T* x,
                           int m, T* red) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  // the panel's T (upper triangle) to shared memory while the rows stream
-  T* sT = red + (kWarps + 1) * 32;  // [kNB][kNB+1], sT[l * (kNB+1) + i] = T(l, i)
-  for (int e = threadIdx.x; e < kNB * kNB; e += kThreads) {
-    const int l = e & (kNB - 1), i = e / kNB;
-    sT[l * (kNB + 1) + i] = (l <= i && i < kb) ? Tm[l + (size_t)i * ldt] : (T)0.0;
+  // warp 0: column `lane` (trans) or row `lane` of T, loaded now and used
+  // after the rows' products, so that its latency overlaps them
+  T tv[kNB];
+  if (warp == 0) {
+#pragma unroll
+    for (int l = 0; l < kNB; ++l) {
+      const bool ok = l < kb && lane < kb && (trans ? l <= lane : l >= lane);
+      tv[l] = ok ? (trans ? Tm[l + (size_t)lane * ldt] : Tm[lane + (size_t)l * ldt]) : (T)0.0;
+    }
   }
   T acc[kNB];
 #pragma unroll
@@ -793,10 +797,7 @@ __device__ void vec_panel(const T* V, int ldv, const T* Tm, int ldt, int kb, int
     if (!unit && lane < kb) w += a[lane];
     T s = 0.0;
 #pragma unroll
-    for (int l = 0; l < kNB; ++l) {
-      const T tl = trans ? sT[l * (kNB + 1) + lane] : sT[lane * (kNB + 1) + l];
-      s += tl * __shfl_sync(0xffffffffu, w, l);
-    }
+    for (int l = 0; l < kNB; ++l) s += tv[l] * __shfl_sync(0xffffffffu, w, l);
     w2[lane] = lane < kb ? s : (T)0.0;
     if (!unit && lane < kb) a[lane] -= s;
   }
