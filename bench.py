@@ -51,9 +51,11 @@ METRIC = "time to 1e-10 rel. residual (factor+GMRES), 64^3 diffusion: mixed+lear
 # capture of the 48^3 member of the workload family
 # (profiles/k_rrqr_diff3d_48_traffic.md)
 RRQR_DRAM_PER_ALGO_BYTE = 0.78
-# DRAM bytes per nominal flop of the FP32 trailing-update launches (k_update),
-# from an ncu capture of the same step (None: not captured)
-UPDATE_DRAM_PER_FLOP = None
+# DRAM bytes per nominal flop of the FP32 trailing-update launches (k_update):
+# 337.2 MB over the 2.24e10 update flops of the mixed+learned step of the 32^3
+# member (ncu dram__bytes_read.sum + dram__bytes_write.sum, all 8 launches;
+# profiles/k_update_diff3d_32.md), scaled by flops to the 64^3 step
+UPDATE_DRAM_PER_FLOP = 0.0151
 # sketch columns beyond the predicted rank in the learned-rank variant
 LEARNED_OVERSAMPLE = 32
 
@@ -365,8 +367,9 @@ def run_ours(args):
                      "per_launch_flops": upd_flops / max(upd_launches, 1),
                      "peak_source": "cuBLAS SGEMM 8192^3, TF32 off, measured in this run (FP32 on the CUDA cores; "
                                     "MEASURED_PEAKS.json has no FP32 figure)",
-                     "traffic_source": "per launch: dram__bytes_read.sum + dram__bytes_write.sum per nominal flop "
-                                       "(ncu) x flops per launch" if UPDATE_DRAM_PER_FLOP else "not captured"},
+                     "traffic_source": "per launch: DRAM bytes per nominal flop of the k_update launches of the "
+                                       "32^3 member (ncu) x flops per launch of this step"
+                     if UPDATE_DRAM_PER_FLOP else "not captured"},
         "roofline_fp64_rrqr": {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
                      "frac": achieved / hbm_peak,
                      "traffic": RRQR_DRAM_PER_ALGO_BYTE * rrqr_bytes if RRQR_DRAM_PER_ALGO_BYTE else None,
@@ -381,6 +384,8 @@ def run_ours(args):
                         "note": "nominal LAWN 41 flops of the plain factorization / its time; "
                                 "peak = cuBLAS DGEMM 8192^3 in this run"},
         "level_ms": {k: head["level_ms"][:, i].round(3).tolist() for i, k in enumerate(ParTree.LEVEL_PHASES)},
+        "level_gflop": {k: (head["level_flops"][:, i] / 1e9).round(4).tolist()
+                        for i, k in enumerate(ParTree.LEVEL_PHASES[:6])},
         "level_ms_fp64": {k: plt[:, i].round(3).tolist() for i, k in enumerate(ParTree.LEVEL_PHASES)},
         "clocks": clk.summary(),
         "hbm_peak_gbs": peaks.get("hbm_gbs"),
