@@ -783,7 +783,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_rrqr(const RrqrTask* __restrict
 // basis Qc = C_sel R^{-1} (column-major, ld m) over the cluster's row blocks:
 // tiles of rt rows, 32-column blocks of R, a blocked update from the solved
 // columns and a triangular solve on the diagonal block.
-__global__ void __launch_bounds__(kThreads) k_selected_qr(const RrqrTask* __restrict__ tasks, int cs, int mmax,
+__global__ void __launch_bounds__(kThreads, 2) k_selected_qr(const RrqrTask* __restrict__ tasks, int cs, int mmax,
                                                           int nmax, int rt) {
   extern __shared__ double sm[];
   const RrqrTask t = tasks[blockIdx.x / cs];
