@@ -847,7 +847,9 @@ int Tree::factorize() {
         const double stol = sketch_tol * tol;
         const bool gram = stol >= kGramMinTol;
         std::vector<RrqrTask> sel[3];
-        int sel_m[3] = {1, 1, 1}, sel_n[3] = {1, 1, 1}, ellmax = 1;
+        int sel_m[3] = {1, 1, 1}, sel_n[3] = {1, 1, 1};
+        std::vector<int> pc_order[2];  // pivoted Cholesky: sketches of <= 64 columns, wider ones
+        int pc_max[2] = {1, 1};
         const int sel_cs[3] = {1, 4, kBigCluster};
         size_t mtot = 0;
         double sketch_work = 0;
@@ -903,7 +905,9 @@ int Tree::factorize() {
             sel[g].push_back(r);
             sel_m[g] = std::max(sel_m[g], t.m);
             sel_n[g] = std::max(sel_n[g], ell[q]);
-            ellmax = std::max(ellmax, ell[q]);
+            const int pg = ell[q] <= 64 ? 0 : 1;
+            pc_order[pg].push_back((int)q);
+            pc_max[pg] = std::max(pc_max[pg], ell[q]);
           } else if (!add_rrqr(G, t.Y, t.m, ell[q], t.ldy, p, d_ell + q, Qc, d_stats ? d_stats + 8 * q : nullptr,
                                work_cap(sketch_work, 4096), sketch_smem)) {
             return -12;
@@ -920,9 +924,15 @@ int Tree::factorize() {
         if (gram) {
           auto* d_gt = static_cast<GemmTile*>(up_any(gram_tiles));
           if (!d_gt) return fail(-11, "out of device memory (sketch)");
-          if (ck(launch_gram(d_sk, d_gt, (int)gram_tiles.size(), stream_), "sketch Gram matrix") ||
-              ck(launch_pchol(d_sk, (int)nsp, ellmax, stol, pivot_rtol, stream_), "sketch pivots"))
-            return -10;
+          if (ck(launch_gram(d_sk, d_gt, (int)gram_tiles.size(), stream_), "sketch Gram matrix")) return -10;
+          for (int pg = 0; pg < 2; ++pg) {
+            if (pc_order[pg].empty()) continue;
+            auto* d_ord = static_cast<int*>(up_any(pc_order[pg]));
+            if (!d_ord) return fail(-11, "out of device memory (sketch)");
+            if (ck(launch_pchol(d_sk, d_ord, (int)pc_order[pg].size(), pc_max[pg], stol, pivot_rtol, stream_),
+                   "sketch pivots"))
+              return -10;
+          }
           for (int g = 0; g < 3; ++g) {
             if (sel[g].empty()) continue;
             auto* d_sel = static_cast<RrqrTask*>(up_any(sel[g]));

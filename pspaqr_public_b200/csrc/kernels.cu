@@ -901,7 +901,7 @@ __device__ __forceinline__ void st_release(int* p, int v) {
 // only target lower tickets, which are held by running CTAs, so the sweep
 // cannot deadlock; a wait that exceeds `spin_limit` cycles sets *status = 2.
 template <typename T>
-__global__ void __launch_bounds__(kThreads) k_fwd_elim(const FwdElimTask* __restrict__ tasks,
+__global__ void __launch_bounds__(kThreads, 2) k_fwd_elim(const FwdElimTask* __restrict__ tasks,
                                                        const FwdOut* __restrict__ outs, int ntasks, int* ticket,
                                                        int* status, long long spin_limit, int nmax) {
   extern __shared__ __align__(16) unsigned char smraw[];

@@ -550,12 +550,13 @@ __device__ __forceinline__ void warp_min_pos(int& bp, int& bc) {
 // Threads are (k-group, column) pairs so that short columns still keep the
 // CTA's loads in flight.
 template <int kPT>
-__global__ void __launch_bounds__(kPT) k_pchol(const SketchTask* __restrict__ tasks, double stol, double pivot_rtol) {
+__global__ void __launch_bounds__(kPT) k_pchol(const SketchTask* __restrict__ tasks, const int* __restrict__ order,
+                                               double stol, double pivot_rtol) {
   extern __shared__ double psm[];
   __shared__ double s_v[kPT / 32];
   __shared__ int s_p[kPT / 32], s_c[kPT / 32];
   __shared__ int s_piv[2];
-  const SketchTask t = tasks[blockIdx.x];
+  const SketchTask t = tasks[order[blockIdx.x]];
   const int n = *t.ell, ld = t.ldy;
   if (n <= 0 || t.m <= 0 || t.w <= 0 || !t.G) return;
   const int kmin = min(t.m, n);
@@ -774,7 +775,8 @@ size_t pchol_smem(int nmax) {
   return sizeof(double) * (2 * n + pchol_threads(nmax)) + sizeof(int) * 2 * n;
 }
 
-cudaError_t launch_pchol(const SketchTask* t, int ntasks, int nmax, double stol, double pivot_rtol, cudaStream_t st) {
+cudaError_t launch_pchol(const SketchTask* t, const int* order, int ntasks, int nmax, double stol, double pivot_rtol,
+                         cudaStream_t st) {
   if (cudaError_t e = cudaGetLastError()) return e;
   if (ntasks <= 0) return cudaSuccess;
   const size_t smem = pchol_smem(nmax);
@@ -782,7 +784,7 @@ cudaError_t launch_pchol(const SketchTask* t, int ntasks, int nmax, double stol,
   auto go = [&](auto kern, int threads) -> cudaError_t {
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e) return e;
-    kern<<<ntasks, threads, smem, st>>>(t, stol, pivot_rtol);
+    kern<<<ntasks, threads, smem, st>>>(t, order, stol, pivot_rtol);
     return cudaSuccess;
   };
   const cudaError_t e = pchol_threads(nmax) == 128 ? go(k_pchol<128>, 128) : go(k_pchol<1024>, 1024);

@@ -94,12 +94,14 @@ cudaError_t launch_sketch(const SketchTask* t, const GemmTile* tiles, int ntiles
 constexpr double kGramMinTol = 1e-5;
 // G = Y^T Y over the given tiles (r0 <= c0; both triangles are written)
 cudaError_t launch_gram(const SketchTask* t, const GemmTile* tiles, int ntiles, cudaStream_t st);
-// Pivoted Cholesky of G (one CTA per task, nmax >= every ell): the pivot order
+// Pivoted Cholesky of G (one CTA per task tasks[order[i]], nmax >= their ell;
+// 128 threads when nmax <= 64, else 1024): the pivot order
 // to colat and the rank -- the first i with |L(i,i)| < stol |L(0,0)|, else
 // min(m, ell) -- over *ell.  Ties within pivot_rtol of the largest diagonal
 // go to the smallest position, as in the pivoted QR.
 size_t pchol_smem(int nmax);
-cudaError_t launch_pchol(const SketchTask* t, int ntasks, int nmax, double stol, double pivot_rtol, cudaStream_t st);
+cudaError_t launch_pchol(const SketchTask* t, const int* order, int ntasks, int nmax, double stol, double pivot_rtol,
+                         cudaStream_t st);
 // B = Q^T C over the given tiles (tile rows: kProjectRows basis vectors; tile
 // columns: kProjectCols columns of C)
 constexpr int kProjectRows = 64, kProjectCols = 64;
