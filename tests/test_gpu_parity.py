@@ -160,3 +160,30 @@ def test_gmres_64cube_manufactured_solution():
     assert rr < 1e-10
     assert k <= 20
     assert _relerr(x, x_true) < 1e-6
+
+
+def test_reassembly_is_bit_identical():
+    """A second assemble of the same partition reuses the nonzeros' block maps
+    and the CSR permutation built by the first: the factors, the preconditioner
+    apply and the GMRES solve are bit-identical, in FP64 and in float storage
+    (which rebuilds the maps for the float layout)."""
+    cp, ri, v = _matrix("diff", 16, 3)
+    t = ParTree(6, 0)
+    t.set_tol(1e-2)
+    t.set_coords_tensor(16, 3)
+    t.partition((cp, ri, scale_columns(cp, v)))
+    b = random_reference(16 ** 3, 9)
+    for prec in (64, 32, 64):
+        t.set_precision(prec)
+        out = []
+        for _ in range(2):
+            t.assemble()
+            t.factorize()
+            top = len(t.clusters()) - 1
+            x = t.solve_inplace(b.copy())
+            k, rr = dist_gmres(None, b.copy(), t, 100, 1e-10)
+            out.append((t.block(top, top), x, k, rr, [c["rank"] for c in t.clusters()]))
+        (B0, x0, k0, r0, rk0), (B1, x1, k1, r1, rk1) = out
+        assert rk0 == rk1 and k0 == k1 and r0 == r1
+        assert np.array_equal(B0, B1) and np.array_equal(x0, x1)
+        assert r0 <= 1e-10

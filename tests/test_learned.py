@@ -193,3 +193,32 @@ def test_trained_network_gains_over_constant_prediction(model):
     n = tr["accepted"] + tr["fallback"]
     assert tr["sketch_columns"] < co["sketch_columns"]
     assert tr["fallback"] <= co["fallback"] + 0.01 * n
+
+
+@pytest.mark.gpu
+def test_gram_pivots_match_pivoted_qr_on_the_sketch(model):
+    """The sketch's pivots come from a pivoted Cholesky of its Gram matrix when
+    the sketch's stop tolerance (sketch_tol * tol) is at least 1e-5, else from
+    the pivoted-QR kernel run on the sketch.  Both follow the same pivot order,
+    and the kept rank is chosen by the residual rule on the sketch's basis, so
+    the two paths keep ranks within +-2 of each other on nearly every
+    interface and both solves converge alike.  Near-ties in the column norms
+    (binary coefficients) are resolved by the tie rule under each path's own
+    rounding, so exact equality is not expected everywhere (about 80 % of the
+    ranks are equal on this matrix)."""
+    m, meta = model
+    n = 32
+    res = {}
+    for name, sketch_tol in (("gram", 0.1), ("pivoted_qr", 1e-4)):
+        t = _tree(n, 53, 1e-2)
+        t.set_rank_model(m, meta["oversample"])
+        t.set_sketch_tuning(sketch_tol)
+        t.assemble()
+        t.factorize()
+        res[name] = (_ranks(t), _solve(t, n))
+    (rg, (kg, rrg)), (rq, (kq, rrq)) = res["gram"], res["pivoted_qr"]
+    assert len(rg) == len(rq)
+    assert np.mean(rg == rq) >= 0.7
+    assert np.mean(np.abs(rg - rq) <= 2) >= 0.9
+    assert abs(int(rg.sum()) - int(rq.sum())) <= 0.02 * rq.sum()
+    assert rrg <= 1e-10 and rrq <= 1e-10 and abs(kg - kq) <= 1
