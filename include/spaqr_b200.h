@@ -114,7 +114,10 @@ int spq_gmres_device(spq_tree* t, double* b, int maxit, double tol, int* iters, 
  * before any stream capture on the device.  The array is shared by every tree
  * on a device: calls that overlap in time (several host threads or streams)
  * race on it and must be serialised.  b, iters and relres as spq_gmres_device;
- * no residual history. */
+ * no residual history.  It always runs the reference's left-preconditioned
+ * GMRES, which is what spq_gmres_device runs with double factors; with float
+ * factors spq_gmres_device defaults to flexible GMRES instead, and the left
+ * method's stopping test is then only reliable to about 1e-7. */
 int spq_gmres_device_noalloc(spq_tree* t, double* b, int maxit, double tol, int* iters, double* relres);
 
 /* ParTree::distribute_x / extract_x (src/ptree.cpp:3264-3303), single rank:
