@@ -829,33 +829,68 @@ __device__ void vec_apply_tpqt(const T* V, int ldv, const T* Tm, int k, T* a, T*
 // the 32 x 32 diagonal block is solved one row per thread.
 template <typename T>
 __device__ void tile_trsm_right_upper(const T* R, int ldr, T* C, int ldc, int m, int n, T* sm) {
-  T* sR = sm;                      // [kRT][kNB+1]  R(l0+l, j0+j)
-  T* sC = sR + kRT * (kNB + 1);    // [kNC][kRT+1]  C(r, l0+l), later the solved block
+  constexpr int kRS = kRT * (kNB + 1), kCS = kNC * (kRT + 1);
+  static_assert(2 * kRS + 2 * kCS <= kTileSmem, "right solve scratch");
+  T* sR0 = sm;                 // two [kRT][kNB+1] tiles: R(l0+l, j0+j)
+  T* sC0 = sR0 + 2 * kRS;      // two [kNC][kRT+1] tiles: C(r, l0+l)
+  T* sR = sR0;                 // the diagonal block, after the products
+  T* sC = sC0;                 // the block being solved
   const int t = threadIdx.x;
   const int tj = t & 7, tr = t >> 3;    // cols tj*4..+3, rows tr*2..+1
+  constexpr int kSR = kRT * kNB / kThreads, kSC = kNC * kRT / kThreads;
+  T rr[kSR], rc[kSC];
+  // tiles of the already solved columns, the next one loaded before the
+  // current one's products
+  auto load = [&](int l0, int j0, int jb) {
+#pragma unroll
+    for (int q = 0; q < kSR; ++q) {
+      const int idx = t + q * kThreads, l = idx % kRT, j = idx / kRT;
+      rr[q] = (j < jb) ? R[(l0 + l) + (size_t)(j0 + j) * ldr] : (T)0.0;
+    }
+#pragma unroll
+    for (int q = 0; q < kSC; ++q) {
+      const int idx = t + q * kThreads, r = idx % kNC, l = idx / kNC;
+      rc[q] = (r < m) ? C[r + (size_t)(l0 + l) * ldc] : (T)0.0;
+    }
+  };
+  auto stash = [&](int b) {
+#pragma unroll
+    for (int q = 0; q < kSR; ++q) {
+      const int idx = t + q * kThreads;
+      sR0[b * kRS + (idx % kRT) * (kNB + 1) + idx / kRT] = rr[q];
+    }
+#pragma unroll
+    for (int q = 0; q < kSC; ++q) {
+      const int idx = t + q * kThreads;
+      sC0[b * kCS + (idx % kNC) * (kRT + 1) + idx / kNC] = rc[q];
+    }
+  };
   for (int j0 = 0; j0 < n; j0 += kNB) {
     const int jb = (n - j0) < kNB ? (n - j0) : kNB;
     T acc[2][4] = {{0, 0, 0, 0}, {0, 0, 0, 0}};
-    for (int l0 = 0; l0 < j0; l0 += kRT) {
-      for (int idx = t; idx < kRT * kNB; idx += kThreads) {
-        const int l = idx % kRT, j = idx / kRT;
-        sR[l * (kNB + 1) + j] = (j < jb) ? R[(l0 + l) + (size_t)(j0 + j) * ldr] : 0.0;
-      }
-      for (int idx = t; idx < kNC * kRT; idx += kThreads) {
-        const int r = idx % kNC, l = idx / kNC;
-        sC[r * (kRT + 1) + l] = (r < m) ? C[r + (size_t)(l0 + l) * ldc] : 0.0;
-      }
+    const int nl = (j0 + kRT - 1) / kRT;
+    if (nl > 0) {
+      load(0, j0, jb);
+      stash(0);
       __syncthreads();
+    }
+    for (int it = 0; it < nl; ++it) {
+      const int b = it & 1;
+      const bool more = it + 1 < nl;
+      if (more) load((it + 1) * kRT, j0, jb);
+      const T* tR = sR0 + b * kRS;
+      const T* tC = sC0 + b * kCS;
 #pragma unroll 4
       for (int l = 0; l < kRT; ++l) {
-        const T a0 = sC[(tr * 2) * (kRT + 1) + l], a1 = sC[(tr * 2 + 1) * (kRT + 1) + l];
+        const T a0 = tC[(tr * 2) * (kRT + 1) + l], a1 = tC[(tr * 2 + 1) * (kRT + 1) + l];
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
-          const T rv = sR[l * (kNB + 1) + tj * 4 + q];
+          const T rv = tR[l * (kNB + 1) + tj * 4 + q];
           acc[0][q] += a0 * rv;
           acc[1][q] += a1 * rv;
         }
       }
+      if (more) stash(b ^ 1);
       __syncthreads();
     }
     // subtract into the block, stage it in shared memory with the diagonal R block
