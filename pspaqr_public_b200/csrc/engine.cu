@@ -721,46 +721,57 @@ int Tree::factorize() {
         }
         return 0;
       };
-      std::vector<EdgeChunk> right, left;
-      for (int e : Lv.spars_edges) {
-        const Edge& E = st_.edges[e];
-        const bool r = st_.clusters[E.n2].sparsify, c = st_.clusters[E.n1].sparsify;
-        EdgeChunk t{};
-        t.A = ptr_[e];
-        t.lda = ld_[e];
-        t.m = rows_[e];
-        t.nc = cols_[e];
-        if (c) {
-          t.V = Qsp_[E.n1];
-          t.T = Tsp_[E.n1];
-          t.kdev = d_rank_ + E.n1;
-          t.ldv = size_[E.n1];
-          for (int r0 = 0; r0 < t.m; r0 += kChunk) {
-            t.lo = r0;
-            t.cnt = std::min(kChunk, t.m - r0);
-            right.push_back(t);
-          }
-        }
-        if (r) {
-          t.V = Qsp_[E.n2];
-          t.T = Tsp_[E.n2];
-          t.kdev = d_rank_ + E.n2;
-          t.ldv = size_[E.n2];
-          t.limdev = c ? d_rank_ + E.n1 : nullptr;
-          for (int c0 = 0; c0 < t.nc; c0 += kChunk) {
-            t.lo = c0;
-            t.cnt = std::min(kChunk, t.nc - c0);
-            left.push_back(t);
-          }
-        }
-      }
       auto up_vec = [&](auto& v) { return upload(v.data(), sizeof(v[0]) * v.size()); };
       auto* d_rs = static_cast<RrqrSrc*>(up_vec(rs));
       auto* d_rows = static_cast<EdgeChunk*>(up_vec(rows_scale));
       auto* d_cols = static_cast<EdgeChunk*>(up_vec(cols_scale));
-      auto* d_right = static_cast<EdgeChunk*>(up_vec(right));
-      auto* d_left = static_cast<EdgeChunk*>(up_vec(left));
-      if (!d_rs || !d_rows || !d_cols || !d_right || !d_left) return fail(-11, "out of device memory (sparsification)");
+      if (!d_rs || !d_rows || !d_cols) return fail(-11, "out of device memory (sparsification)");
+      // chunk lists of the compression applies: built while the GPU runs the
+      // scaling and the pivoted-QR or rank-prediction stages queued before them
+      std::vector<EdgeChunk> right, left;
+      EdgeChunk* d_right = nullptr;
+      EdgeChunk* d_left = nullptr;
+      bool compress_built = false;
+      auto build_compress = [&]() -> int {
+        if (compress_built) return 0;
+        compress_built = true;
+        for (int e : Lv.spars_edges) {
+          const Edge& E = st_.edges[e];
+          const bool r = st_.clusters[E.n2].sparsify, c = st_.clusters[E.n1].sparsify;
+          EdgeChunk t{};
+          t.A = ptr_[e];
+          t.lda = ld_[e];
+          t.m = rows_[e];
+          t.nc = cols_[e];
+          if (c) {
+            t.V = Qsp_[E.n1];
+            t.T = Tsp_[E.n1];
+            t.kdev = d_rank_ + E.n1;
+            t.ldv = size_[E.n1];
+            for (int r0 = 0; r0 < t.m; r0 += kChunk) {
+              t.lo = r0;
+              t.cnt = std::min(kChunk, t.m - r0);
+              right.push_back(t);
+            }
+          }
+          if (r) {
+            t.V = Qsp_[E.n2];
+            t.T = Tsp_[E.n2];
+            t.kdev = d_rank_ + E.n2;
+            t.ldv = size_[E.n2];
+            t.limdev = c ? d_rank_ + E.n1 : nullptr;
+            for (int c0 = 0; c0 < t.nc; c0 += kChunk) {
+              t.lo = c0;
+              t.cnt = std::min(kChunk, t.nc - c0);
+              left.push_back(t);
+            }
+          }
+        }
+        d_right = static_cast<EdgeChunk*>(up_vec(right));
+        d_left = static_cast<EdgeChunk*>(up_vec(left));
+        if (!d_right || !d_left) return fail(-11, "out of device memory (compression)");
+        return 0;
+      };
       for (int g = 0; g < 3; ++g) {
         if (sc[g].empty()) continue;
         auto* d = static_cast<ScaleTask*>(up_vec(sc[g]));
@@ -818,6 +829,7 @@ int Tree::factorize() {
         if (rank_model_) {
           RankModel model{d_model_, d_model_ + kMlpParams, d_model_ + kMlpParams + kRankFeatures, oversample_};
           if (ck(launch_rank_predict(d_sk, (int)nsp, model, stream_), "rank prediction")) return -10;
+          if (int rc = build_compress()) return rc;
         }
       }
       if (!rank_model_) {
@@ -829,6 +841,7 @@ int Tree::factorize() {
           if (!rr_cs[q]) return -12;
         }
         if (int rc = run_rrqr(G, tol)) return rc;
+        if (int rc = build_compress()) return rc;
       } else {
         // learned ranks: sketch widths back on the host to plan the sketch
         // GEMMs; pivoted QR of the sketches, projections, rank choice; the
@@ -1014,6 +1027,7 @@ int Tree::factorize() {
         auto* d_cv = static_cast<ConvTask*>(up_any(cv));
         if (!d_cv || ck(launch_to_f32_batch(d_cv, (int)cv.size(), stream_), "factor conversion")) return -10;
       }
+      if (int rc = build_compress()) return rc;
       cudaEventRecord(fe[2], stream_);
       if (ck(launch_edge(2, d_right, (int)right.size(), stream_), "right compression") ||
           ck(launch_edge(0, d_left, (int)left.size(), stream_), "left compression"))
