@@ -536,6 +536,15 @@ int Tree::factorize() {
         printf("level %d scale groups: %zu/%zu/%zu tasks, nmax %d/%d/%d, sum n^3 %.3g\n", lvl, sc[0].size(),
                sc[1].size(), sc[2].size(), smax[0], smax[1], smax[2], n3);
       }
+      // each stage is launched as soon as its descriptors exist, so that the
+      // host builds the next lists while the GPU runs it
+      auto up_vec = [&](auto& v) { return upload(v.data(), sizeof(v[0]) * v.size()); };
+      for (int g = 0; g < 3; ++g) {
+        if (sc[g].empty()) continue;
+        auto* d = static_cast<ScaleTask*>(up_vec(sc[g]));
+        if (!d || ck(launch_scale(d, (int)sc[g].size(), csz[g], smax[g], stream_), "scaling kernel")) return -10;
+      }
+      cudaEventRecord(fe[1], stream_);
       std::vector<EdgeChunk> rows_scale, cols_scale;
       for (int e : Lv.spars_edges) {
         const Edge& E = st_.edges[e];
@@ -569,6 +578,15 @@ int Tree::factorize() {
           lt_[lvl].flops[3] += (double)t.m * t.nc * t.nc;
         }
       }
+      {
+        auto* d_rows = static_cast<EdgeChunk*>(up_vec(rows_scale));
+        auto* d_cols = static_cast<EdgeChunk*>(up_vec(cols_scale));
+        if (!d_rows || !d_cols) return fail(-11, "out of device memory (scaling)");
+        if (ck(launch_edge(0, d_rows, (int)rows_scale.size(), stream_), "row scaling") ||
+            ck(launch_edge(1, d_cols, (int)cols_scale.size(), stream_), "column scaling"))
+          return -10;
+      }
+      cudaEventRecord(ev[2], stream_);
       // compression matrices C (m x w) of the level's interfaces, gathered
       // transposed into scratch by k_rrqr_assemble
       const size_t nsp = Lv.spars_clusters.size();
@@ -721,11 +739,9 @@ int Tree::factorize() {
         }
         return 0;
       };
-      auto up_vec = [&](auto& v) { return upload(v.data(), sizeof(v[0]) * v.size()); };
       auto* d_rs = static_cast<RrqrSrc*>(up_vec(rs));
-      auto* d_rows = static_cast<EdgeChunk*>(up_vec(rows_scale));
-      auto* d_cols = static_cast<EdgeChunk*>(up_vec(cols_scale));
-      if (!d_rs || !d_rows || !d_cols) return fail(-11, "out of device memory (sparsification)");
+      if (!d_rs) return fail(-11, "out of device memory (sparsification)");
+      if (ck(launch_rrqr_assemble(d_rs, (int)rs.size(), stream_), "rrqr assembly")) return -10;
       // chunk lists of the compression applies: built while the GPU runs the
       // scaling and the pivoted-QR or rank-prediction stages queued before them
       std::vector<EdgeChunk> right, left;
@@ -772,17 +788,6 @@ int Tree::factorize() {
         if (!d_right || !d_left) return fail(-11, "out of device memory (compression)");
         return 0;
       };
-      for (int g = 0; g < 3; ++g) {
-        if (sc[g].empty()) continue;
-        auto* d = static_cast<ScaleTask*>(up_vec(sc[g]));
-        if (!d || ck(launch_scale(d, (int)sc[g].size(), csz[g], smax[g], stream_), "scaling kernel")) return -10;
-      }
-      cudaEventRecord(fe[1], stream_);
-      if (ck(launch_edge(0, d_rows, (int)rows_scale.size(), stream_), "row scaling") ||
-          ck(launch_edge(1, d_cols, (int)cols_scale.size(), stream_), "column scaling"))
-        return -10;
-      cudaEventRecord(ev[2], stream_);
-      if (ck(launch_rrqr_assemble(d_rs, (int)rs.size(), stream_), "rrqr assembly")) return -10;
       // interface features: inputs of the rank model, or logged with the
       // plain ranks as its training pairs
       std::vector<SketchTask> sk;
