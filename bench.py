@@ -51,13 +51,16 @@ METRIC = "time to 1e-10 rel. residual (factor+GMRES), 64^3 diffusion: mixed+lear
 # capture of the 48^3 member of the workload family
 # (profiles/k_rrqr_diff3d_48_traffic.md)
 RRQR_DRAM_PER_ALGO_BYTE = 0.78
-# DRAM bytes per nominal flop of the FP32 trailing-update launches (k_update):
-# 337.2 MB over the 2.24e10 update flops of the mixed+learned step of the 32^3
-# member (ncu dram__bytes_read.sum + dram__bytes_write.sum, all 8 launches;
-# profiles/k_update_diff3d_32.md), scaled by flops to the 64^3 step
-UPDATE_DRAM_PER_FLOP = 0.0151
+# DRAM bytes per nominal flop of the tensor-core trailing-update launches
+# (k_update_tc), from an ncu capture of the 32^3 member of the workload family,
+# scaled by flops to the 64^3 step (None: not captured for this kernel yet)
+UPDATE_DRAM_PER_FLOP = None
 # sketch columns beyond the predicted rank in the learned-rank variant
 LEARNED_OVERSAMPLE = 32
+# wall-clock budget of the reference arm's timed steps (seconds)
+REFERENCE_BUDGET_S = 240.0
+# backward-error probes per variant
+N_PROBES = 2
 
 
 def build_matrix():
@@ -285,6 +288,9 @@ def run_ours(args):
             r["flops"] = t.factor_flops()
             r["level_flops"] = t.level_flops()
             r["rrqr_bytes"] = t.rrqr_bytes()
+            # the factorization's backward error ||(A P - Q R) z|| / ||Q R z|| in
+            # N_PROBES seeded directions (outside the timed steps)
+            r["backward_error"] = t.backward_error(N_PROBES, seed=2021).tolist()
             res[name] = r
     head = res["mixed+learned"]
     e2e_times = [e2e_step()[0] for _ in range(max(1, min(args.steps, 3)))]
@@ -323,6 +329,12 @@ def run_ours(args):
     cnt = head["counts"]
     nint = max(cnt["accepted"] + cnt["fallback"], 1)
     dr = head["ranks"] - res["fp64"]["ranks"]
+    # effective ceiling of the 3xTF32 updates: three kind::tf32 MMAs per
+    # product, TF32 at half the measured bf16 tensor rate
+    bf16 = peaks.get("bf16_tflops_sustained") or peaks.get("bf16_tflops")
+    tc_peak = bf16 / 2.0 / 3.0 if bf16 else 1590.0 / 2.0 / 3.0
+    tc_src = ("MEASURED_PEAKS.json bf16_tflops_sustained / 2 (TF32 rate) / 3 (MMAs per 3xTF32 product), of measured"
+              if bf16 else "fallback 1590 TFLOP/s bf16 / 2 / 3, of fallback")
     out = {
         "metric": METRIC,
         "value": step,
@@ -334,65 +346,57 @@ def run_ours(args):
         "higher_is_better": False,
         "scaling": "weak",
         "vs_baseline": None,
-        "dtype": "f32 factors and preconditioner / f64 SpMV, Krylov and pivoted QR",
+        "dtype": "f32 factors (3xTF32 tensor-core left applies) and preconditioner / f64 SpMV, Krylov, pivoted QR",
         "data": "synthetic (seeded Gaussian random field coefficients, N(0,1) right-hand side)",
-        "variant": "mixed precision + learned ranks: float factor blocks and preconditioner apply, ranks from an "
-                   "MLP-sized randomized range finder with the pivoted QR's residual rule (pivoted-QR fallback), "
-                   "flexible right-preconditioned GMRES in FP64; fp64_plain = the reference method on the GPU",
-        "config": {"workload": W["name"], "matrix": W["matrix"], "nlevels": W["nlevels"], "tol": W["tol"],
-                   "skip": W["skip"], "gmres_tol": W["gmres_tol"], "parallelism": f"replicas x{world}",
-                   "l2": "factor pool (GBs) > L2; 256 MB buffer written before every timed step"},
+        "ratio_vs_fp64": step / fp64_step,
+        "fp64_plain": {"value": fp64_step, "factorize_s": float(np.mean(res["fp64"]["ftimes"])),
+                       "gmres_iters": int(np.median(res["fp64"]["iters"])),
+                       "true_relres": float(max(res["fp64"]["rels"])),
+                       "backward_error": res["fp64"]["backward_error"]},
         "factorize_s": fact,
         "gmres_s": step - fact,
         "gmres_iters": int(np.median(head["iters"])),
         "true_relres": float(max(head["rels"])),
-        "partition_s": t_part,
-        "fp64_plain": {"value": fp64_step, "factorize_s": float(np.mean(res["fp64"]["ftimes"])),
-                       "gmres_iters": int(np.median(res["fp64"]["iters"])),
-                       "true_relres": float(max(res["fp64"]["rels"]))},
-        "ratio_vs_fp64": step / fp64_step,
+        "backward_error": head["backward_error"],
         "learned": {"interfaces": int(nint), "fallback_rate": cnt["fallback"] / nint,
                     "ranks_within_2": float(np.mean(np.abs(dr) <= 2)) if len(dr) else None,
                     "sketch_columns_per_interface": cnt["sketch_columns"] / nint,
                     "oversample": LEARNED_OVERSAMPLE},
+        "partition_s": t_part,
+        "config": {"workload": W["name"], "nlevels": W["nlevels"], "tol": W["tol"], "skip": W["skip"],
+                   "gmres_tol": W["gmres_tol"], "parallelism": f"replicas x{world}",
+                   "l2": "factor pool (GBs) > L2; 256 MB buffer written before every timed step"},
         "e2e": {"value": e2e, "unit": "s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": 8 * N},
         "gpu_launches": int(np.median(head["launches"])),
-        "roofline": {"bound": "fp32", "achieved": upd_tflops, "peak": fp32_peak, "unit": "TFLOP/s",
-                     "frac": upd_tflops / fp32_peak if fp32_peak else None,
+        "roofline": {"bound": "tensor", "achieved": upd_tflops, "peak": tc_peak, "unit": "TFLOP/s",
+                     "frac": upd_tflops / tc_peak,
                      "traffic": UPDATE_DRAM_PER_FLOP * upd_flops / max(upd_launches, 1)
                      if UPDATE_DRAM_PER_FLOP else None,
-                     "kernel": "k_update<float>: FP32 trailing updates of the headline step (share of its kernel "
-                               "time: the largest in the ncu launch list)",
+                     "kernel": "k_update_tc: 3xTF32 tcgen05 trailing updates of the headline step",
                      "algorithmic_flops": upd_flops, "launches": upd_launches, "duration_s": upd_s,
-                     "per_launch_flops": upd_flops / max(upd_launches, 1),
-                     "peak_source": "cuBLAS SGEMM 8192^3, TF32 off, measured in this run (FP32 on the CUDA cores; "
-                                    "MEASURED_PEAKS.json has no FP32 figure)",
-                     "traffic_source": "per launch: DRAM bytes per nominal flop of the k_update launches of the "
-                                       "32^3 member (ncu) x flops per launch of this step"
-                     if UPDATE_DRAM_PER_FLOP else "not captured"},
+                     "per_launch_flops": upd_flops / max(upd_launches, 1), "peak_source": tc_src,
+                     "fp32_simt_sgemm_tflops": fp32_peak},
         "roofline_fp64_rrqr": {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
-                     "frac": achieved / hbm_peak,
-                     "traffic": RRQR_DRAM_PER_ALGO_BYTE * rrqr_bytes if RRQR_DRAM_PER_ALGO_BYTE else None,
-                     "kernel": "pivoted QR (k_rrqr_assemble + k_rrqr, all levels of one plain FP64 factorization)",
-                     "algorithmic_bytes": rrqr_bytes, "duration_s": rrqr_s, "launches": "per factorization",
-                     "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if peaks.get("hbm_gbs")
-                     else "fallback 6650 GB/s (of fallback)",
-                     "traffic_source": "dram__bytes_read.sum + dram__bytes_write.sum per algorithmic byte of the "
-                                       "k_rrqr* launches of the 48^3 member (ncu), scaled to this step"},
-        "factor_fp64": {"achieved_tflops": res["fp64"]["flops"] / float(np.mean(res["fp64"]["ftimes"])) / 1e12,
-                        "dgemm_peak_tflops": fp64_peak,
-                        "note": "nominal LAWN 41 flops of the plain factorization / its time; "
-                                "peak = cuBLAS DGEMM 8192^3 in this run"},
+                               "frac": achieved / hbm_peak,
+                               "traffic": RRQR_DRAM_PER_ALGO_BYTE * rrqr_bytes if RRQR_DRAM_PER_ALGO_BYTE else None,
+                               "duration_s": rrqr_s},
+        "factor_fp64_tflops": res["fp64"]["flops"] / float(np.mean(res["fp64"]["ftimes"])) / 1e12,
+        "dgemm_peak_tflops": fp64_peak,
+        "clocks": clk.summary(),
+        "hbm_peak_gbs": peaks.get("hbm_gbs"),
+    }
+    # per-level phase times and flops: a second record on stderr (the headline
+    # line stays short)
+    detail = {
         "level_ms": {k: head["level_ms"][:, i].round(3).tolist() for i, k in enumerate(ParTree.LEVEL_PHASES)},
         "level_gflop": {k: (head["level_flops"][:, i] / 1e9).round(4).tolist()
                         for i, k in enumerate(ParTree.LEVEL_PHASES[:6])},
         "level_ms_fp64": {k: plt[:, i].round(3).tolist() for i, k in enumerate(ParTree.LEVEL_PHASES)},
-        "clocks": clk.summary(),
-        "hbm_peak_gbs": peaks.get("hbm_gbs"),
     }
     if rank == 0 and not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline(cp, ri, v, b_host)
     if rank == 0:
+        print(json.dumps(detail), file=sys.stderr)
         print(json.dumps(out))
     if dist:
         dist.barrier()
@@ -444,16 +448,25 @@ def run_reference(args):
         o.partition()
         o.assemble()
         o.factorize()
-    vals = [cpu_baseline(cp, ri, v, b, threads) for _ in range(args.steps)]
+    # every step is one full time-to-solution run (about 45 s on 16 cores);
+    # steps beyond a 4-minute budget are not run, so that the arm ends within
+    # a few minutes at any --steps
+    vals, t_start = [], time.perf_counter()
+    for _ in range(args.steps):
+        vals.append(cpu_baseline(cp, ri, v, b, threads))
+        if time.perf_counter() - t_start + vals[-1]["value"] > REFERENCE_BUDGET_S:
+            break
     val = float(np.mean([x["value"] for x in vals]))
     out = {
         "metric": METRIC, "value": val, "unit": "s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": val * 1e3, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f32 factors and preconditioner / f64 SpMV, Krylov and pivoted QR", "data": "synthetic", "impl": "reference",
+        "steps_timed": len(vals), "ms_per_step": val * 1e3, "higher_is_better": False, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64 (plain FP64 factors, preconditioner and Krylov)", "data": "synthetic",
+        "impl": "reference",
         "config": {"workload": W["name"], "matrix": W["matrix"], "nlevels": W["nlevels"], "tol": W["tol"],
                    "skip": W["skip"], "gmres_tol": W["gmres_tol"], "parallelism": f"cpu x{threads} threads"},
         "cpu_baseline": {"value": val, "unit": "s", "cores": threads, "kind": "port",
-                         "sample": vals[-1]["sample"] + f"; warm-up on the 32^3 member x{args.warmup}"},
+                         "sample": vals[-1]["sample"] + f"; warm-up on the 32^3 member x{args.warmup}; "
+                                   f"{len(vals)} of {args.steps} steps timed ({REFERENCE_BUDGET_S:.0f} s budget)"},
         "e2e": {"value": val, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(out))

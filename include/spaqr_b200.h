@@ -11,7 +11,8 @@
  * Status codes: -1 bad argument, -2 unsupported input (non-square, levels),
  * -3 coordinates missing or mismatched, -4 call out of order, -5 / -6 symbolic
  * structure inconsistent, -10 CUDA error, -11 device memory exhausted,
- * -12 device-side wait timed out / preconditioner failure.
+ * -12 device-side wait timed out / preconditioner failure, -13 zero or
+ * non-finite pivot in the factorization, -14 fixed workspace too small.
  */
 #ifndef SPAQR_B200_H
 #define SPAQR_B200_H
@@ -59,6 +60,35 @@ int spq_set_rrqr_work(spq_tree* t, double elems, double fill);
  * pivoted QR of the compression matrices stay in double; bits = 64 (default)
  * is the plain FP64 method.  Takes effect at the next assemble. */
 int spq_set_precision(spq_tree* t, int bits);
+/* Tensor cores of the mixed-precision factorization (no reference counterpart):
+ * on = 1 (default) runs the left block-reflector applies of float factors --
+ * the trailing updates (the reference's larfb / tpmqrt, ptree.cpp:216-266),
+ * the row scaling and the left compression applies (ptree.cpp:1613-1659,
+ * 1860-1903) -- as 3xTF32 tcgen05 MMAs with FP32 accumulation; on = 0 runs them
+ * in FP32 on the CUDA cores.  No effect on FP64 factors.  Takes effect at the
+ * next factorize. */
+int spq_set_tensor_cores(spq_tree* t, int on);
+/* Failure detection (no reference counterpart; the reference asserts, which
+ * its Release build compiles out, or exits).
+ * spq_set_spin_limit: clock-cycle budget of each bounded wait of the
+ * preconditioner apply's forward sweep (default 2e9); a wait that runs out
+ * makes the solve / GMRES call fail with -12.  Takes effect at the next
+ * factorize.
+ * spq_set_checks: on = 1 checks on the host, before every upload, that the
+ * trailing-update, compression and merge descriptors address memory inside
+ * the block pool; a bad descriptor fails factorize with -5 before anything is
+ * launched for its stage.
+ * spq_debug_corrupt_descriptor: fault injection for tests of those checks --
+ * the next factorize moves one trailing-update descriptor's block address far
+ * outside the pool on the host, and turns the checks on so that it is never
+ * launched.
+ * factorize also fails with -13 when a QR factorization of the elimination or
+ * of the scaling meets a zero or non-finite pivot (a device status word set by
+ * the kernels, read after each level), and partition fails with -2 on a
+ * non-finite matrix value. */
+int spq_set_spin_limit(spq_tree* t, long long cycles);
+int spq_set_checks(spq_tree* t, int on);
+int spq_debug_corrupt_descriptor(spq_tree* t);
 /* Krylov method of spq_gmres / spq_gmres_device (no reference counterpart):
  * 0 = left-preconditioned GMRES of is.cpp:447-527; 1 = flexible
  * right-preconditioned GMRES, whose residual is the true ||b - A x|| however
@@ -91,6 +121,14 @@ int spq_solve_inplace_device(spq_tree* t, double* x);
 int spq_solve_global(spq_tree* t, const double* b, double* x);
 /* VectorXd ParTree::spmv(VectorXd x) const  -- src/ptree.cpp:3212-3262 (permuted order). */
 int spq_spmv(spq_tree* t, const double* x, double* y);
+/* Factor backward error (no single reference counterpart; the reference prints
+ * the one-shot residual ||A x - b|| / ||b|| of x = M^{-1} b for one b at
+ * pspaQR.cpp:207-225): eta[p] = ||A z_p - u_p|| / ||u_p|| with z_p = M^{-1} u_p
+ * for nprobe probe vectors, i.e. ||(A P - Q R) z_p|| / ||Q R z_p||, the relative
+ * backward error of the factorization QR ~ A P in the direction z_p.  U (host,
+ * n x nprobe column-major, permuted order) holds the probes; U = NULL draws
+ * u_p ~ N(0,1) from std::mt19937_64(seed + p). */
+int spq_factor_backward_error(spq_tree* t, int nprobe, const double* U, unsigned long long seed, double* eta);
 /* unsigned long dist_gmres(A, b, M, iter, tol, verb)  -- src/is.cpp:447-527.
  * b (host, permuted order) is overwritten by the solution; iters = the
  * reference's k; relres = true ||b - A x|| / ||b|| (pspaQR.cpp:264-268);
@@ -109,9 +147,13 @@ int spq_gmres_device(spq_tree* t, double* b, int maxit, double tol, int* iters, 
  * array of 6,291,456 doubles (48 MiB) built into the library, which bounds
  * the problem: n * (maxit + 3) + maxit + 1028 <= 6,291,456 (the 64^3 grid,
  * n = 262,144, allows maxit <= 20), and maxit <= 100.  Larger requests fail
- * with an error naming the size; nothing is truncated.  The array's device
- * address is looked up by the first call on each device, so make that call
- * before any stream capture on the device.  The array is shared by every tree
+ * with an error naming the size; nothing is truncated.  The array lives in a
+ * code module of its own, which CUDA 12.2 and later load lazily: the first
+ * call on each device loads it, which commits the 48 MiB on that device, and
+ * looks up the array's device address.  So make that first call (a small solve
+ * will do) before the caller reserves the rest of the device's memory and
+ * before any stream capture on the device, or run with
+ * CUDA_MODULE_LOADING=EAGER; later calls commit nothing.  The array is shared by every tree
  * on a device: calls that overlap in time (several host threads or streams)
  * race on it and must be serialised.  b, iters and relres as spq_gmres_device;
  * no residual history.  It always runs the reference's left-preconditioned
@@ -219,6 +261,25 @@ int spq_mlp_predict(const float* params, const float* X, int n, float* out);
 int spq_mlp_train(float* params, const float* X, const float* y, int n, int epochs, int batch, float lr,
                   unsigned long long seed, float* loss_hist);
 const char* spq_mlp_last_error(void);
+
+/* ---- nested-dissection subtree sharding over ranks (one GPU per rank) ----
+ * ParTree::get_rank / cluster2rank / edge2rank (ptree.cpp:65-91): the owner of
+ * every cluster (cluster_owner, one per cluster order), of every permuted
+ * unknown (row_owner, n), and per level the number of transfers between ranks
+ * (nexchange, nlevels): the reference's active messages of factors
+ * (ptree.cpp:1081-1098, 1419-1441, 1500-1531, 1662-1693), of compression
+ * blocks, and of blocks merged into a parent owned elsewhere (send_edge_am,
+ * ptree.cpp:2005-2038).  nranks: a power of two <= 2^(nlevels-1).  Any output
+ * may be NULL.  Available after spq_partition. */
+int spq_shard_plan(spq_tree* t, int nranks, int* cluster_owner, int* row_owner, int* nexchange);
+/* The transfers of level lvl, 5 ints each: kind (0 merge of block `id` into
+ * parent block `dst`, 1 elimination factors of interior cluster `id`, 2
+ * scaling/sparsification factors of interface `id`, 3 compression block `id`
+ * to its interface's owner), id, dst (-1 unless kind 0), from rank, to rank. */
+int spq_shard_exchange(spq_tree* t, int nranks, int lvl, int* out);
+/* Every block of the symbolic structure, 3 ints each: column cluster n1, row
+ * cluster n2, level (edge index = position). */
+int spq_get_edges(spq_tree* t, int* out);
 
 const char* spq_last_error(spq_tree* t);
 

@@ -17,9 +17,9 @@ LIB = os.path.join(HERE, "libspaqr_b200.so")
 DRIVER = os.path.join(HERE, "spaqr")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-SOURCES = ["structure.cpp", "engine.cu", "kernels.cu", "learned.cu", "noalloc.cu", "capi.cpp", "capi_learned.cpp"]
-HEADERS = ["structure.hpp", "engine.hpp", "tasks.hpp", "kernels.hpp", "dense.cuh", "noalloc.hpp", "learned.hpp",
-           "capi_internal.hpp"]
+SOURCES = ["structure.cpp", "engine.cu", "kernels.cu", "learned.cu", "noalloc.cu", "shard.cpp", "capi.cpp", "capi_learned.cpp"]
+HEADERS = ["structure.hpp", "engine.hpp", "tasks.hpp", "kernels.hpp", "dense.cuh", "tc_apply.cuh", "noalloc.hpp", "learned.hpp",
+           "capi_internal.hpp", "shard.hpp"]
 
 
 def _stale(target: str, deps) -> bool:

@@ -1,4 +1,5 @@
 // capi.cpp -- extern "C" boundary (include/spaqr_b200.h) over spq::Tree.
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <random>
@@ -10,6 +11,7 @@
 #include "engine.hpp"
 #include "kernels.hpp"
 #include "noalloc.hpp"
+#include "shard.hpp"
 
 
 namespace {
@@ -74,6 +76,30 @@ int spq_set_precision(spq_tree* h, int bits) {
   return 0;
 }
 
+int spq_set_spin_limit(spq_tree* h, long long cycles) {
+  if (!h || cycles < 0) return -1;
+  h->t->spin_limit = cycles;
+  return 0;
+}
+
+int spq_set_checks(spq_tree* h, int on) {
+  if (!h || on < 0 || on > 1) return -1;
+  h->t->check_descriptors = on != 0;
+  return 0;
+}
+
+int spq_debug_corrupt_descriptor(spq_tree* h) {
+  if (!h) return -1;
+  h->t->corrupt_next_descriptor = true;
+  return 0;
+}
+
+int spq_set_tensor_cores(spq_tree* h, int on) {
+  if (!h || on < 0 || on > 1) return -1;
+  h->t->tensor_cores = on != 0;
+  return 0;
+}
+
 int spq_set_krylov(spq_tree* h, int method) {
   if (!h || method < -1 || method > 1) return -1;
   h->t->krylov = method;
@@ -109,11 +135,18 @@ int spq_partition(spq_tree* h, int nrows, int ncols, const int* colptr, const in
 int spq_assemble(spq_tree* h) { return h ? done(h, h->t->assemble()) : -1; }
 int spq_factorize(spq_tree* h) { return h ? done(h, h->t->factorize()) : -1; }
 int spq_solve_inplace(spq_tree* h, double* x) { return (h && x) ? done(h, h->t->solve_host(x)) : -1; }
-int spq_solve_inplace_device(spq_tree* h, double* x) { return (h && x) ? done(h, h->t->solve_device(x)) : -1; }
+int spq_solve_inplace_device(spq_tree* h, double* x) {
+  if (!h || !x) return -1;
+  h->t->clear_status();
+  return done(h, h->t->solve_device(x));
+}
 int spq_solve_global(spq_tree* h, const double* b, double* x) {
   return (h && b && x) ? done(h, h->t->solve_global(b, x)) : -1;
 }
 int spq_spmv(spq_tree* h, const double* x, double* y) { return (h && x && y) ? done(h, h->t->spmv_host(x, y)) : -1; }
+int spq_factor_backward_error(spq_tree* h, int nprobe, const double* U, unsigned long long seed, double* eta) {
+  return h ? done(h, h->t->backward_error(nprobe, U, seed, eta)) : -1;
+}
 int spq_gmres(spq_tree* h, double* b, int maxit, double tol, int* iters, double* relres, double* hist, int hist_cap) {
   if (!h || !b || !iters || !relres) return -1;
   return done(h, h->t->gmres_host(b, maxit, tol, iters, relres, hist, hist_cap));
@@ -261,6 +294,53 @@ double spq_factor_flops(spq_tree* h) { return h ? h->t->factor_flops() : -1.0; }
 double spq_rrqr_bytes(spq_tree* h) { return h ? h->t->rrqr_bytes() : -1.0; }
 double spq_pool_bytes(spq_tree* h) { return h ? (double)h->t->pool_bytes() : -1.0; }
 long long spq_kernel_launches(void) { return spq::kernel_launches(); }
+int spq_shard_plan(spq_tree* h, int nranks, int* cluster_owner, int* row_owner, int* nexchange) {
+  if (!h || nranks < 1) return -1;
+  const auto& s = h->t->structure();
+  if (s.clusters.empty()) {
+    h->err = "shard plan requested before partition";
+    return -4;
+  }
+  spq::ShardPlan p;
+  if (spq::build_shard_plan(s, nranks, p)) {
+    h->err = "nranks must be a power of two no larger than the number of leaf parts";
+    return -1;
+  }
+  if (cluster_owner) std::copy(p.cluster_owner.begin(), p.cluster_owner.end(), cluster_owner);
+  if (row_owner) std::copy(p.row_owner.begin(), p.row_owner.end(), row_owner);
+  if (nexchange)
+    for (int l = 0; l < s.nlevels; ++l) nexchange[l] = (int)p.exchange[l].size();
+  return 0;
+}
+
+int spq_shard_exchange(spq_tree* h, int nranks, int lvl, int* out) {
+  if (!h || nranks < 1) return -1;
+  const auto& s = h->t->structure();
+  if (lvl < 0 || lvl >= s.nlevels) return -1;
+  spq::ShardPlan p;
+  if (spq::build_shard_plan(s, nranks, p)) return -1;
+  int k = 0;
+  for (const auto& x : p.exchange[lvl]) {
+    out[k++] = x.kind;
+    out[k++] = x.id;
+    out[k++] = x.dst;
+    out[k++] = x.from;
+    out[k++] = x.to;
+  }
+  return 0;
+}
+
+int spq_get_edges(spq_tree* h, int* out) {
+  if (!h || !out) return -1;
+  const auto& s = h->t->structure();
+  for (size_t e = 0; e < s.edges.size(); ++e) {
+    out[3 * e] = s.edges[e].n1;
+    out[3 * e + 1] = s.edges[e].n2;
+    out[3 * e + 2] = s.edges[e].level;
+  }
+  return 0;
+}
+
 const char* spq_last_error(spq_tree* h) {
   if (!h) return "null handle";
   return h->err.c_str();

@@ -2,6 +2,7 @@
 #include "engine.hpp"
 
 #include <algorithm>
+#include <random>
 #include <array>
 #include <chrono>
 #include <cmath>
@@ -22,7 +23,6 @@ double wall() {
 constexpr size_t kAlign = 256;
 constexpr size_t kArenaChunk = size_t(1) << 30;
 // bounded wait of the forward sweep: ~1 s at 2 GHz
-constexpr long long kSpinLimit = 2000000000LL;
 constexpr int kChunk = 64;        // columns (rows) per CTA of the chunked applies
 constexpr int kBigCluster = 8;    // CTAs per task for blocks of >= 8 panels
 constexpr int kRrqrMaxCols = 1024;  // own columns of C per CTA (four per thread)
@@ -68,6 +68,13 @@ void* Arena::alloc(size_t bytes) {
   c.off += bytes;
   used_ += bytes;
   return r;
+}
+
+bool Arena::contains(const void* p, size_t bytes) const {
+  const char* q = static_cast<const char*>(p);
+  for (const Chunk& c : chunks_)
+    if (q >= c.base && q + bytes <= c.base + c.size) return true;
+  return false;
 }
 
 void Arena::reset() {
@@ -129,6 +136,10 @@ int Tree::set_stream(cudaStream_t s) {
     if (factorized_) return build_solve_graph();
   }
   return 0;
+}
+
+void Tree::clear_status() {
+  if (d_status_) cudaMemsetAsync(d_status_, 0, sizeof(int), stream_);
 }
 
 int Tree::device_status() {
@@ -209,6 +220,12 @@ int Tree::partition(int nrows, int ncols, const int* colptr, const int* rowidx, 
     if (colptr[j + 1] < colptr[j]) return fail(-1, "colptr is not monotone");
   for (int k = 0; k < nnz; ++k)
     if (rowidx[k] < 0 || rowidx[k] >= nrows) return fail(-1, "row index out of range");
+  // a NaN or infinite value would reach every kernel of the factorization
+  for (int j = 0; j < ncols; ++j)
+    for (int k = colptr[j]; k < colptr[j + 1]; ++k)
+      if (!std::isfinite(val[k]))
+        return fail(-2, "matrix value (row " + std::to_string(rowidx[k]) + ", column " + std::to_string(j) +
+                            ") is not finite");
   int rc = build_structure(st_, A_, nlevels, skip, tol, X_, dim_);
   if (rc != 0) return fail(rc, st_.error);
   partitioned_ = true;
@@ -360,7 +377,10 @@ static int cluster_for(int ncols) {
 int Tree::factorize() {
   if (!assembled_) return fail(-4, "factorize called before assemble");
   set_factor_fp32(fp32_);
+  set_tensor_cores(fp32_ && tensor_cores);
+  set_status_word(d_status_);
   if (factorized_) return fail(-4, "factorize called twice; assemble again first");
+  clear_status();
   double t0 = wall();
   const int L = st_.nlevels;
   const int NB = dev_nb();
@@ -503,6 +523,26 @@ int Tree::factorize() {
           return -10;
       }
       cudaEventRecord(fe[0], stream_);
+      if (corrupt_next_descriptor && !uo.empty()) {
+        corrupt_next_descriptor = false;
+        check_descriptors = true;
+        uo[uo.size() / 2].B = uo[uo.size() / 2].A + ((size_t)1 << 40);  // far outside the pool
+        uo[uo.size() / 2].kind = 1;
+      }
+      if (check_descriptors) {
+        const size_t es = fp32_ ? 4 : 8;
+        for (const UpdTask& u : ut)
+          for (int o = u.op_begin; o < u.op_end; ++o) {
+            const UpdOp& op = uo[o];
+            const size_t ncol = (size_t)u.col0 + u.ncols;
+            if (!arena_.contains(op.V, es * ((size_t)op.ldv * (op.k - 1) + op.m)) ||
+                !arena_.contains(op.T, es * (size_t)NB * op.k) ||
+                !arena_.contains(op.A, es * ((size_t)op.lda * (ncol - 1) + (op.kind ? op.k : op.m))) ||
+                (op.kind == 1 && !arena_.contains(op.B, es * ((size_t)op.ldb * (ncol - 1) + op.m))))
+              return fail(-5, "trailing-update descriptor " + std::to_string(o) + " of level " + std::to_string(lvl) +
+                                  " addresses memory outside the block pool; nothing launched");
+          }
+      }
       auto* d_ut = static_cast<UpdTask*>(upload(ut.data(), sizeof(UpdTask) * ut.size()));
       auto* d_uo = static_cast<UpdOp*>(upload(uo.data(), sizeof(UpdOp) * uo.size()));
       if (!d_ut || !d_uo) return fail(-11, "out of device memory (update descriptors)");
@@ -782,6 +822,15 @@ int Tree::factorize() {
               left.push_back(t);
             }
           }
+        }
+        if (check_descriptors) {
+          const size_t es = fp32_ ? 4 : 8;
+          for (const auto* lst : {&right, &left})
+            for (const EdgeChunk& c : *lst)
+              if (!arena_.contains(c.A, es * ((size_t)c.lda * (c.nc - 1) + c.m)) ||
+                  !arena_.contains(c.V, es * (size_t)c.ldv * c.ldv))  // Q_sp: size x size
+                return fail(-5, "compression descriptor of level " + std::to_string(lvl) +
+                                    " addresses memory outside the block pool; nothing launched");
         }
         d_right = static_cast<EdgeChunk*>(up_vec(right));
         d_left = static_cast<EdgeChunk*>(up_vec(left));
@@ -1136,6 +1185,14 @@ int Tree::factorize() {
         t.identity = (E.n1 == E.n2 && st_.clusters[E.n1].sparsify) ? 1 : 0;
         if (t.rows > 0 && t.cols > 0) mt.push_back(t);
       }
+      if (check_descriptors) {
+        const size_t es = fp32_ ? 4 : 8;
+        for (const MergeTask& m : mt)
+          if (!arena_.contains(m.src, es * ((size_t)m.ld_src * (m.cols - 1) + m.rows)) ||
+              !arena_.contains(m.dst, es * ((size_t)m.ld_dst * (m.coff + m.cols - 1) + m.roff + m.rows)))
+            return fail(-5, "merge descriptor of level " + std::to_string(lvl) +
+                                " addresses memory outside the block pool; nothing launched");
+      }
       auto* d_mt = static_cast<MergeTask*>(upload(mt.data(), sizeof(MergeTask) * mt.size()));
       if (!d_mt) return fail(-11, "out of device memory (merge)");
       if (ck(launch_merge(d_mt, (int)mt.size(), stream_), "merge kernel")) return -10;
@@ -1143,6 +1200,12 @@ int Tree::factorize() {
     cudaEventRecord(ev[4], stream_);
     const double h1 = wall();
     if (ck(cudaStreamSynchronize(stream_), "factorize level")) return -10;
+    if (const int ds = device_status()) {
+      clear_status();
+      if (ds & 2) return fail(-12, "tensor-core MMA wait timed out on the device at level " + std::to_string(lvl));
+      return fail(-13, std::string(ds & 4 ? "non-finite" : "zero") + " pivot in the QR factorizations of level " +
+                           std::to_string(lvl));
+    }
     if (verbose >= 2) {
       float gpu_ms = 0;
       cudaEventElapsedTime(&gpu_ms, ev[0], ev[4]);
@@ -1348,7 +1411,7 @@ int Tree::build_solve_graph() {
   cudaMemsetAsync(d_tickets_, 0, sizeof(int) * L, stream_);
   for (int lvl = 0; lvl < L; ++lvl) {
     LevelSolve& S = ls[lvl];
-    cerr = cerr ? cerr : launch_fwd_elim(S.fe, S.fo, S.nfe, S.fe_nmax, S.fe_mmax, d_tickets_ + lvl, d_status_, kSpinLimit, stream_);
+    cerr = cerr ? cerr : launch_fwd_elim(S.fe, S.fo, S.nfe, S.fe_nmax, S.fe_mmax, d_tickets_ + lvl, d_status_, spin_limit, stream_);
     cerr = cerr ? cerr : launch_fwd_spars(S.fs, S.nfs, S.fs_nmax, stream_);
     cerr = cerr ? cerr : launch_copy_idx(S.ng, S.gsrc, S.gdst, d_xw_, stream_);
   }
@@ -1390,6 +1453,7 @@ int Tree::solve_host(double* x) {
   double t0 = wall();
   const int n = st_.n;
   if (!factorized_) return fail(-4, "solve called before factorize");
+  clear_status();
   cudaMemcpyAsync(d_tmp_, x, sizeof(double) * n, cudaMemcpyHostToDevice, stream_);
   int rc = solve_device(d_tmp_);
   if (rc) return rc;
@@ -1397,6 +1461,36 @@ int Tree::solve_host(double* x) {
   if (check_cuda(cudaStreamSynchronize(stream_), "solve")) return -10;
   if (device_status() != 0) return fail(-12, "forward sweep wait timed out on the device");
   t_solve = wall() - t0;
+  return 0;
+}
+
+int Tree::backward_error(int nprobe, const double* U, unsigned long long seed, double* eta) {
+  if (!factorized_) return fail(-4, "backward error called before factorize");
+  if (nprobe < 1 || !eta) return fail(-1, "backward error: nprobe >= 1 and an output array are required");
+  const int n = st_.n;
+  std::vector<double> u(n), y(n);
+  for (int p = 0; p < nprobe; ++p) {
+    if (U) {
+      std::copy(U + (size_t)p * n, U + (size_t)(p + 1) * n, u.begin());
+    } else {
+      std::mt19937_64 gen(seed + (unsigned long long)p);
+      std::normal_distribution<double> nd(0.0, 1.0);
+      for (double& v : u) v = nd(gen);
+    }
+    clear_status();
+    cudaMemcpyAsync(d_tmp_, u.data(), sizeof(double) * n, cudaMemcpyHostToDevice, stream_);
+    if (int rc = solve_device(d_tmp_)) return rc;
+    if (int rc = spmv_device(d_tmp_, d_tmp_ + n)) return rc;
+    cudaMemcpyAsync(y.data(), d_tmp_ + n, sizeof(double) * n, cudaMemcpyDeviceToHost, stream_);
+    if (check_cuda(cudaStreamSynchronize(stream_), "backward error")) return -10;
+    if (device_status() != 0) return fail(-12, "forward sweep wait timed out on the device");
+    double r2 = 0, u2 = 0;
+    for (int i = 0; i < n; ++i) {
+      r2 += (y[i] - u[i]) * (y[i] - u[i]);
+      u2 += u[i] * u[i];
+    }
+    eta[p] = std::sqrt(r2) / std::sqrt(u2);
+  }
   return 0;
 }
 
@@ -1431,6 +1525,7 @@ int Tree::gmres_device(double* b, int maxit, double gtol, int* iters, double* re
   if (!factorized_) return fail(-4, "gmres called before factorize");
   if (krylov == 1 || (krylov < 0 && fp32_)) return fgmres_device(b, maxit, gtol, iters, relres, hist, hist_cap);
   if (maxit < 1) return fail(-1, "maxit must be >= 1");
+  clear_status();
   double t0 = wall();
   const int n = st_.n;
   const size_t ldq = (size_t)n;
@@ -1533,6 +1628,7 @@ int Tree::gmres_device_fixed(double* b, int maxit, double gtol, int* iters, doub
   if (!factorized_) return fail(-4, "gmres called before factorize");
   if (maxit < 1 || maxit > kNoAllocMaxit)
     return fail(-1, "maxit must be in [1, " + std::to_string(kNoAllocMaxit) + "] for the allocation-free GMRES");
+  clear_status();
   double t0 = wall();
   const int n = st_.n;
   const size_t ldq = (size_t)n;
@@ -1658,6 +1754,7 @@ int Tree::set_rank_model(const float* params, const float* mean, const float* st
 int Tree::fgmres_device(double* b, int maxit, double gtol, int* iters, double* relres, double* hist, int hist_cap) {
   if (!factorized_) return fail(-4, "gmres called before factorize");
   if (maxit < 1) return fail(-1, "maxit must be >= 1");
+  clear_status();
   double t0 = wall();
   const int n = st_.n;
   const size_t ldq = (size_t)n;

@@ -26,6 +26,8 @@ class Arena {
   double* dalloc(size_t n) { return static_cast<double*>(alloc(n * sizeof(double))); }
   // forget every allocation but keep the chunks for reuse (no cudaFree)
   void reset();
+  // [p, p + bytes) lies inside one chunk
+  bool contains(const void* p, size_t bytes) const;
   void release();
   size_t used() const { return used_; }
   size_t reserved() const { return reserved_; }
@@ -78,6 +80,22 @@ class Tree {
   // 1 = flexible right-preconditioned GMRES, -1 (default) = flexible exactly
   // when the factors are float
   int krylov = -1;
+  // float factors: left block-reflector applies (trailing updates, row
+  // scaling, left compression) on the tensor cores (3xTF32) or on the CUDA
+  // cores
+  bool tensor_cores = true;
+  // cycle budget of every bounded spin wait of the preconditioner apply's
+  // forward sweep (takes effect at the next factorize, which captures the
+  // apply); a wait that runs out fails the apply with status -12
+  long long spin_limit = 2000000000LL;
+  // host-side checks of the trailing-update, compression and merge
+  // descriptors before each upload: every block address lies in the block
+  // pool (failure: status -5, nothing launched)
+  bool check_descriptors = false;
+  // fault injection for the checks above (tests): the next factorize moves
+  // one trailing-update descriptor's block address out of the pool before the
+  // check; forces check_descriptors on
+  bool corrupt_next_descriptor = false;
   // learned ranks: the sketch's pivoted QR stops at sketch_tol * tol (the
   // kept rank is then chosen on C itself)
   double sketch_tol = 0.1;
@@ -96,6 +114,11 @@ class Tree {
   int solve_global(const double* b, double* x);
   int spmv_device(const double* x, double* y);
   int spmv_host(const double* x, double* y);
+  // Factor backward error in nprobe directions: eta[p] = ||A z - u_p|| / ||u_p||
+  // with z = M^{-1} u_p, which is ||(A P - Q R) z|| / ||Q R z||.  U (n x nprobe,
+  // column-major, permuted order) gives the probes; U = null draws u_p ~ N(0,1)
+  // from std::mt19937_64(seed + p).
+  int backward_error(int nprobe, const double* U, unsigned long long seed, double* eta);
   int gmres_host(double* b, int maxit, double tol, int* iters, double* relres, double* hist, int hist_cap);
   int gmres_device(double* b_dev, int maxit, double tol, int* iters, double* relres, double* hist, int hist_cap);
   int fgmres_device(double* b, int maxit, double gtol, int* iters, double* relres, double* hist, int hist_cap);
@@ -143,6 +166,10 @@ class Tree {
     *ell = learned_ell_;
   }
   int device_status();
+  // zero the device status word (stream-ordered): every factorize, solve and
+  // GMRES entry starts from a clean status, so a wait that ran out once does
+  // not fail the calls after it
+  void clear_status();
 
  private:
   int fail(int code, const std::string& msg) {

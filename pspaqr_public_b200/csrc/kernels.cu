@@ -18,6 +18,7 @@
 #include "dense.cuh"
 #include "kernels.hpp"
 #include "tasks.hpp"
+#include "tc_apply.cuh"
 
 namespace cg = cooperative_groups;
 
@@ -67,7 +68,7 @@ __global__ void k_scatter(int nnz, const double* __restrict__ val, double* const
 // the global copy, `vb` a reflector tail, `tile` dev::kTileSmem elements.
 template <typename T>
 __device__ void dist_qr(T* R, int ldr, T* B, int ldb, int m, int n, int unit, T* Tout, T* tg,
-                        T* lt, T* vb, T* red, T* tmp, T* tile, int cs) {
+                        T* lt, T* vb, T* red, T* tmp, T* tile, int cs, int* status = nullptr) {
   const int rank = crank(cs);
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int gap = (cs - 1) * kNB;  // columns between two panels of one CTA
@@ -94,6 +95,8 @@ __device__ void dist_qr(T* R, int ldr, T* B, int ldb, int m, int n, int unit, T*
           R[j + (size_t)j * ldr] = beta;
           lt[j] = tj;
           tg[j] = tj;
+          // R(j, j) = 0 or not finite: the triangular solves would break down
+          if (status && !(isfinite(beta) && beta != (T)0)) atomicOr(status, isfinite(beta) ? 8 : 4);
         }
         __syncthreads();
         // H_j on the panel's later columns
@@ -136,7 +139,7 @@ __device__ void dist_qr(T* R, int ldr, T* B, int ldb, int m, int n, int unit, T*
 
 template <typename T>
 __global__ void __launch_bounds__(kThreads, 2) k_elim(const ElimTask* __restrict__ tasks, const ElimOut* __restrict__ outs,
-                                                   int cs, int vmax) {
+                                                   int cs, int vmax, int* status) {
   extern __shared__ __align__(16) unsigned char smraw[];
   T* sm = reinterpret_cast<T*>(smraw);
   const ElimTask t = tasks[blockIdx.x / cs];
@@ -145,16 +148,16 @@ __global__ void __launch_bounds__(kThreads, 2) k_elim(const ElimTask* __restrict
   T* lt = tmp + kNB;
   T* vb = lt + t.n;
   T* tile = vb + vmax;
-  dist_qr<T>(as<T>(t.S), t.n, nullptr, 0, t.n, t.n, 1, as<T>(t.T), as<T>(t.tau), lt, vb, red, tmp, tile, cs);
+  dist_qr<T>(as<T>(t.S), t.n, nullptr, 0, t.n, t.n, 1, as<T>(t.T), as<T>(t.tau), lt, vb, red, tmp, tile, cs, status);
   for (int o = t.out_begin; o < t.out_end; ++o) {
     const ElimOut e = outs[o];
     dist_qr<T>(as<T>(t.S), t.n, as<T>(e.B), e.m, e.m, t.n, 0, as<T>(e.T), as<T>(t.tau), lt, vb, red, tmp, tile,
-               cs);
+               cs, status);
   }
 }
 
 template <typename T>
-__global__ void __launch_bounds__(kThreads, 2) k_scale(const ScaleTask* __restrict__ tasks, int cs) {
+__global__ void __launch_bounds__(kThreads, 2) k_scale(const ScaleTask* __restrict__ tasks, int cs, int* status) {
   extern __shared__ __align__(16) unsigned char smraw[];
   T* sm = reinterpret_cast<T*>(smraw);
   const ScaleTask t = tasks[blockIdx.x / cs];
@@ -162,7 +165,8 @@ __global__ void __launch_bounds__(kThreads, 2) k_scale(const ScaleTask* __restri
   T* tmp = red + kRed;
   T* lt = tmp + kNB;
   T* vb = lt + t.n;
-  dist_qr<T>(as<T>(t.S), t.n, nullptr, 0, t.n, t.n, 1, as<T>(t.T), as<T>(t.tau), lt, vb, red, tmp, vb + t.n, cs);
+  dist_qr<T>(as<T>(t.S), t.n, nullptr, 0, t.n, t.n, 1, as<T>(t.T), as<T>(t.tau), lt, vb, red, tmp, vb + t.n, cs,
+             status);
 }
 
 // ------------------------------------------------------------ chunked applies
@@ -196,6 +200,59 @@ __global__ void __launch_bounds__(kThreads, 2) k_edge_left(const EdgeChunk* __re
     cnt = min(cnt, lim - t.lo);
   }
   dev::mat_apply_qt<T>(as<T>(t.V), t.ldv, as<T>(t.T), k, as<T>(t.A) + (size_t)t.lo * t.lda, t.lda, t.m, cnt, sm);
+}
+
+// ------------------------------------------------------------ tensor-core applies (float factors)
+// The panel loops of dev::mat_apply_qt / mat_apply_tpqt on the tensor cores
+// (tc::left_qt, 3xTF32); chunks of at most 64 columns.
+__device__ void tc_apply_qt(tc::Ctx& x, const float* V, int ldv, const float* Tm, int k, float* C, int ldc, int m,
+                            int nc) {
+  for (int j0 = 0; j0 < k; j0 += kNB) {
+    const int kb = min(k - j0, kNB);
+    for (int c0 = 0; c0 < nc; c0 += 64)
+      tc::left_qt(x, V + j0 + (size_t)j0 * ldv, ldv, Tm + (size_t)j0 * kNB, kNB, kb, 1, nullptr, 0,
+                  C + j0 + (size_t)c0 * ldc, ldc, m - j0, min(nc - c0, 64));
+  }
+}
+__device__ void tc_apply_tpqt(tc::Ctx& x, const float* V, int ldv, const float* Tm, int k, float* A, int lda,
+                              float* B, int ldb, int m, int nc) {
+  for (int j0 = 0; j0 < k; j0 += kNB) {
+    const int kb = min(k - j0, kNB);
+    for (int c0 = 0; c0 < nc; c0 += 64)
+      tc::left_qt(x, V + (size_t)j0 * ldv, ldv, Tm + (size_t)j0 * kNB, kNB, kb, 0, A + j0 + (size_t)c0 * lda, lda,
+                  B + (size_t)c0 * ldb, ldb, m, min(nc - c0, 64));
+  }
+}
+
+// k_update on the tensor cores (float factors)
+__global__ void __launch_bounds__(kThreads, 2) k_update_tc(const UpdTask* __restrict__ tasks,
+                                                         const UpdOp* __restrict__ ops, int* status) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  tc::Ctx x = tc::begin(smraw, status);
+  const UpdTask t = tasks[blockIdx.x];
+  for (int o = t.op_begin; o < t.op_end; ++o) {
+    const UpdOp op = ops[o];
+    if (op.kind == 0)
+      tc_apply_qt(x, as<float>(op.V), op.ldv, as<float>(op.T), op.k, as<float>(op.A) + (size_t)t.col0 * op.lda,
+                  op.lda, op.m, t.ncols);
+    else
+      tc_apply_tpqt(x, as<float>(op.V), op.ldv, as<float>(op.T), op.k, as<float>(op.A) + (size_t)t.col0 * op.lda,
+                    op.lda, as<float>(op.B) + (size_t)t.col0 * op.ldb, op.ldb, op.m, t.ncols);
+  }
+  tc::end(x);
+}
+
+// k_edge_left on the tensor cores (float factors)
+__global__ void __launch_bounds__(kThreads, 2) k_edge_left_tc(const EdgeChunk* __restrict__ tasks, int* status) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  tc::Ctx x = tc::begin(smraw, status);
+  const EdgeChunk t = tasks[blockIdx.x];
+  const int k = t.kdev ? *t.kdev : t.k;
+  int cnt = t.cnt;
+  if (t.limdev) cnt = min(cnt, *t.limdev - t.lo);
+  if (cnt > 0) tc_apply_qt(x, as<float>(t.V), t.ldv, as<float>(t.T), k, as<float>(t.A) + (size_t)t.lo * t.lda, t.lda,
+                           t.m, cnt);
+  tc::end(x);
 }
 
 // column scaling: rows [lo, lo+cnt) of A <- A R^{-1}
@@ -1173,6 +1230,8 @@ __global__ void k_to_f32_batch(const ConvTask* __restrict__ tasks) {
 namespace {
 std::atomic<long long> g_launches{0};
 thread_local bool g_fp32 = false;  // factor storage of the next launches
+thread_local bool g_tc = false;     // float left applies on the tensor cores
+thread_local int* g_status = nullptr;  // status word of the factorization kernels
 inline void counted() { g_launches.fetch_add(1, std::memory_order_relaxed); }
 
 constexpr size_t kSmemMax = 227 * 1024;
@@ -1217,6 +1276,9 @@ inline cudaError_t begin(const char* name) {
 
 const char* last_launch_name() { return g_last_launch; }
 void set_factor_fp32(bool on) { g_fp32 = on; }
+void set_tensor_cores(bool on) { g_tc = on; }
+void set_status_word(int* status) { g_status = status; }
+bool tensor_cores() { return g_tc; }
 bool factor_fp32() { return g_fp32; }
 void set_last_launch(const char* name) { g_last_launch = name; }
 
@@ -1247,10 +1309,10 @@ cudaError_t launch_elim(const ElimTask* t, const ElimOut* o, int ntasks, int cs,
   const size_t b = smem_bytes(kRed + kNB + (size_t)nmax + (size_t)std::max(vmax, 1) + kWcap);
   if (g_fp32) {
     if (cudaError_t e = prep(k_elim<float>, b)) return e;
-    return launch_clustered(k_elim<float>, ntasks, cs, b, st, t, o, cs, vmax);
+    return launch_clustered(k_elim<float>, ntasks, cs, b, st, t, o, cs, vmax, g_status);
   }
   if (cudaError_t e = prep(k_elim<double>, b)) return e;
-  return launch_clustered(k_elim<double>, ntasks, cs, b, st, t, o, cs, vmax);
+  return launch_clustered(k_elim<double>, ntasks, cs, b, st, t, o, cs, vmax, g_status);
 }
 
 cudaError_t launch_scale(const ScaleTask* t, int ntasks, int cs, int nmax, cudaStream_t st) {
@@ -1259,10 +1321,10 @@ cudaError_t launch_scale(const ScaleTask* t, int ntasks, int cs, int nmax, cudaS
   const size_t b = smem_bytes(kRed + kNB + 2 * (size_t)nmax + kWcap);
   if (g_fp32) {
     if (cudaError_t e = prep(k_scale<float>, b)) return e;
-    return launch_clustered(k_scale<float>, ntasks, cs, b, st, t, cs);
+    return launch_clustered(k_scale<float>, ntasks, cs, b, st, t, cs, g_status);
   }
   if (cudaError_t e = prep(k_scale<double>, b)) return e;
-  return launch_clustered(k_scale<double>, ntasks, cs, b, st, t, cs);
+  return launch_clustered(k_scale<double>, ntasks, cs, b, st, t, cs, g_status);
 }
 
 cudaError_t launch_update(const UpdTask* t, const UpdOp* o, int ntasks, cudaStream_t st) {
@@ -1270,7 +1332,10 @@ cudaError_t launch_update(const UpdTask* t, const UpdOp* o, int ntasks, cudaStre
   if (ntasks <= 0) return cudaSuccess;
   const size_t b = smem_bytes(kWcap);
   counted();
-  if (g_fp32) {
+  if (g_fp32 && g_tc) {
+    if (cudaError_t e = prep(k_update_tc, tc::kSmemBytes)) return e;
+    k_update_tc<<<ntasks, kThreads, tc::kSmemBytes, st>>>(t, o, g_status);
+  } else if (g_fp32) {
     if (cudaError_t e = prep(k_update<float>, b)) return e;
     k_update<float><<<ntasks, kThreads, b, st>>>(t, o);
   } else {
@@ -1299,6 +1364,11 @@ cudaError_t launch_edge(int kind, const EdgeChunk* t, int ntasks, cudaStream_t s
     }
     return last();
   };
+  if (g_fp32 && g_tc && kind == 0) {
+    if ((e = prep(k_edge_left_tc, tc::kSmemBytes))) return e;
+    k_edge_left_tc<<<ntasks, kThreads, tc::kSmemBytes, st>>>(t, g_status);
+    return last();
+  }
   return g_fp32 ? go(k_edge_left<float>, k_edge_trsm<float>, k_edge_right<float>)
                 : go(k_edge_left<double>, k_edge_trsm<double>, k_edge_right<double>);
 }

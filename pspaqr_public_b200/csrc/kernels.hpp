@@ -20,6 +20,15 @@ void set_last_launch(const char* name);
 // Descriptors carry block addresses as double* either way.
 void set_factor_fp32(bool on);
 bool factor_fp32();
+// Left block-reflector applies of float factors (trailing updates, row
+// scaling, left compression) on the tensor cores (tcgen05, 3xTF32) for the
+// launchers of this thread that follow.
+void set_tensor_cores(bool on);
+bool tensor_cores();
+// Device status word of the factorization kernels launched by this thread:
+// bit 2 (value 2) a tensor-core wait ran out, 4 a non-finite pivot, 8 a zero
+// pivot in a QR factorization (elimination chains, scaling QR).
+void set_status_word(int* status);
 // n doubles -> n floats stored at dst, and back (vectors, factors)
 cudaError_t launch_to_f32(long long n, const double* src, double* dst, cudaStream_t st);
 cudaError_t launch_to_f64(long long n, const double* src, double* dst, cudaStream_t st);

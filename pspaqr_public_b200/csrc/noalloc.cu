@@ -6,7 +6,11 @@
 // preconditioned GMRES on 262,144 unknowns (the 64^3 grid) with up to 20
 // iterations.  Its address is taken once per device with cudaGetSymbolAddress
 // while that device is current; the first call on a device does this set-up,
-// so that call should come before any stream capture on the device.  All
+// so that call should come before any stream capture on the device.  This
+// file holds no kernel, so it compiles to a module of its own that CUDA 12.2+
+// loads lazily, at that same first call: the 48 MiB are committed then, and
+// the first call must come before a caller reserves the rest of device memory
+// (or the process runs with CUDA_MODULE_LOADING=EAGER).  All
 // trees on a device share the array: calls that overlap in time (other host
 // threads, other streams) race on it and must be serialised by the caller.
 #include <cuda_runtime.h>

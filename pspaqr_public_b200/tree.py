@@ -51,6 +51,10 @@ def lib():
             "spq_set_rrqr_work": (i32, [vp, f64, f64]),
             "spq_set_precision": (i32, [vp, i32]),
             "spq_set_krylov": (i32, [vp, i32]),
+            "spq_set_tensor_cores": (i32, [vp, i32]),
+            "spq_set_spin_limit": (i32, [vp, C.c_longlong]),
+            "spq_set_checks": (i32, [vp, i32]),
+            "spq_debug_corrupt_descriptor": (i32, [vp]),
             "spq_get_factor": (i32, [vp, i32, i32, pd, pi]),
             "spq_set_coords": (i32, [vp, i32, i32, pd]),
             "spq_set_coords_tensor": (i32, [vp, i32, i32]),
@@ -61,6 +65,7 @@ def lib():
             "spq_solve_inplace_device": (i32, [vp, vp]),
             "spq_solve_global": (i32, [vp, pd, pd]),
             "spq_spmv": (i32, [vp, pd, pd]),
+            "spq_factor_backward_error": (i32, [vp, i32, pd, C.c_ulonglong, pd]),
             "spq_gmres": (i32, [vp, pd, i32, f64, pi, pd, pd, i32]),
             "spq_gmres_device": (i32, [vp, vp, i32, f64, pi, pd, pd, i32]),
             "spq_gmres_device_noalloc": (i32, [vp, vp, i32, f64, pi, pd]),
@@ -90,6 +95,9 @@ def lib():
             "spq_num_edges": (i32, [vp]),
             "spq_find_edge": (i32, [vp, i32, i32]),
             "spq_get_block": (i32, [vp, i32, i32, pd, pi]),
+            "spq_shard_plan": (i32, [vp, i32, pi, pi, pi]),
+            "spq_shard_exchange": (i32, [vp, i32, i32, pi]),
+            "spq_get_edges": (i32, [vp, pi]),
             "spq_times": (i32, [vp, pd]),
             "spq_level_times": (i32, [vp, pf]),
             "spq_level_flops": (i32, [vp, pd]),
@@ -224,6 +232,22 @@ class ParTree:
         pivoted QR); 64: plain FP64.  Takes effect at the next assemble."""
         self._chk(lib().spq_set_precision(self._h, bits), "set_precision")
 
+    def set_tensor_cores(self, on: bool):
+        """Float factors: left block-reflector applies as 3xTF32 tcgen05 MMAs (default) or FP32 SIMT."""
+        self._chk(lib().spq_set_tensor_cores(self._h, int(bool(on))), "set_tensor_cores")
+
+    def set_spin_limit(self, cycles: int):
+        """Cycle budget of the preconditioner apply's bounded waits (next factorize)."""
+        self._chk(lib().spq_set_spin_limit(self._h, int(cycles)), "set_spin_limit")
+
+    def set_checks(self, on: bool):
+        """Host-side bounds checks of the factorization's descriptors before upload."""
+        self._chk(lib().spq_set_checks(self._h, int(bool(on))), "set_checks")
+
+    def debug_corrupt_descriptor(self):
+        """Fault injection (tests): the next factorize corrupts one descriptor on the host."""
+        self._chk(lib().spq_debug_corrupt_descriptor(self._h), "debug_corrupt_descriptor")
+
     def set_krylov(self, method: int):
         """0: left GMRES (reference); 1: flexible right-preconditioned GMRES;
         -1: flexible exactly with float factors (default)."""
@@ -314,6 +338,18 @@ class ParTree:
         y = np.empty_like(x)
         self._chk(lib().spq_spmv(self._h, _pd(x), _pd(y)), "spmv")
         return y
+
+    def backward_error(self, nprobe: int = 3, probes: Optional[np.ndarray] = None, seed: int = 2021) -> np.ndarray:
+        """||A z - u|| / ||u||, z = M^{-1} u, for nprobe probe vectors u (permuted
+        order): the factorization's relative backward error ||(A P - Q R) z|| / ||Q R z||.
+        ``probes`` (n x nprobe) gives them; otherwise u ~ N(0,1) from mt19937_64(seed + p)."""
+        eta = np.zeros(nprobe)
+        U = None
+        if probes is not None:
+            U = np.asfortranarray(probes, dtype=np.float64).reshape(self.nrows_local(), nprobe, order="F")
+        self._chk(lib().spq_factor_backward_error(self._h, nprobe, _pd(U) if U is not None else None, seed, _pd(eta)),
+                  "backward_error")
+        return eta
 
     def nrows_local(self) -> int:
         return lib().spq_n(self._h)

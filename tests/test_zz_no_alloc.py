@@ -69,3 +69,45 @@ def test_noalloc_rejects_oversized_requests(tree):
     b = random_reference(N**D, 12)
     rc, msg, _, _, _ = _gmres(tree, b, noalloc=True, maxit=101)
     assert rc != 0 and "maxit" in msg
+
+
+def test_noalloc_later_calls_commit_no_device_memory(tree):
+    """The first call loads the library module that holds the fixed array (48 MiB);
+    a later call must leave the device's free memory unchanged."""
+    import torch
+    from pspaqr_public_b200 import random_reference
+
+    b = random_reference(N**D, 13)
+    x = torch.from_numpy(b.copy()).cuda()
+    rc, msg, _, _, _ = _gmres(tree, b, noalloc=True)
+    assert rc == 0, msg
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    rc, msg, _, _, _ = _gmres(tree, b, noalloc=True)
+    assert rc == 0, msg
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info()
+    del x
+    assert free1 == free0
+
+
+def test_noalloc_rejects_a_basis_larger_than_the_array():
+    """48^3 unknowns with maxit 100 need 110,592 * 103 + 1128 doubles and more:
+    beyond the fixed 6,291,456 the call fails with the size it needed."""
+    from pspaqr_public_b200 import ParTree, random_reference, scale_columns
+    from pspaqr_public_b200 import matrices as M
+
+    n = 48
+    cp, ri, v = M.laplacian(n, 3)
+    t = ParTree(8, 0)
+    t.set_tol(1e-1)
+    t.set_coords_tensor(n, 3)
+    t.partition((cp, ri, scale_columns(cp, v)))
+    t.assemble()
+    t.factorize()
+    assert n**3 * (100 + 3) > 6_291_456
+    rc, msg, _, _, _ = _gmres(t, random_reference(n**3, 14), noalloc=True, maxit=100)
+    assert rc == -14 and "doubles" in msg, (rc, msg)
+    # within the bound the same tree solves
+    rc, msg, _, _, rr = _gmres(t, random_reference(n**3, 14), noalloc=True, maxit=40)
+    assert rc == 0, msg
