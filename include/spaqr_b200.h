@@ -162,6 +162,23 @@ int spq_gmres_device(spq_tree* t, double* b, int maxit, double tol, int* iters, 
  * method's stopping test is then only reliable to about 1e-7. */
 int spq_gmres_device_noalloc(spq_tree* t, double* b, int maxit, double tol, int* iters, double* relres);
 
+/* Several right-hand sides at once (no reference counterpart; the reference
+ * solves one right-hand side per dist_gmres call, is.cpp:447-527).
+ * spq_solve_block_device: X (device, column r at X + r * ldx, permuted order)
+ * is overwritten by M^{-1} X; the nrhs sweeps run as parallel branches of one
+ * CUDA graph, built on the first call per factorization and nrhs (allocates).
+ * spq_gmres_block / spq_gmres_block_device: flexible right-preconditioned GMRES
+ * of the nrhs systems in lockstep, one block apply per iteration and one host
+ * synchronisation per iteration for all of them; B (host / device, column r at
+ * B + r * ldb) is overwritten by the solutions; iters[r] and relres[r] (true
+ * ||b_r - A x_r|| / ||b_r||) per right-hand side.  Krylov storage grows to
+ * nrhs * n * (2 maxit + 3) doubles: size maxit to the iterations expected. */
+int spq_solve_block_device(spq_tree* t, double* X, int nrhs, long long ldx);
+int spq_gmres_block(spq_tree* t, double* B, int nrhs, long long ldb, int maxit, double tol, int* iters,
+                    double* relres);
+int spq_gmres_block_device(spq_tree* t, double* B, int nrhs, long long ldb, int maxit, double tol, int* iters,
+                           double* relres);
+
 /* ParTree::distribute_x / extract_x (src/ptree.cpp:3264-3303), single rank:
  * x_local = x[rperm]  and  x[cperm] = x_local. */
 int spq_distribute_x(spq_tree* t, const double* x, double* x_local);

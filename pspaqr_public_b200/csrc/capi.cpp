@@ -165,6 +165,20 @@ int spq_gmres_device_noalloc(spq_tree* h, double* b, int maxit, double tol, int*
   }
   return done(h, h->t->gmres_device_fixed(b, maxit, tol, iters, relres, ws, spq::kNoAllocDoubles));
 }
+int spq_solve_block_device(spq_tree* h, double* X, int nrhs, long long ldx) {
+  if (!h || !X || nrhs < 1 || ldx < 1) return -1;
+  return done(h, h->t->solve_block_device(X, nrhs, (size_t)ldx));
+}
+int spq_gmres_block(spq_tree* h, double* B, int nrhs, long long ldb, int maxit, double tol, int* iters,
+                    double* relres) {
+  if (!h || !B || !iters || !relres || nrhs < 1 || ldb < 1) return -1;
+  return done(h, h->t->block_gmres_host(B, nrhs, (size_t)ldb, maxit, tol, iters, relres));
+}
+int spq_gmres_block_device(spq_tree* h, double* B, int nrhs, long long ldb, int maxit, double tol, int* iters,
+                           double* relres) {
+  if (!h || !B || !iters || !relres || nrhs < 1 || ldb < 1) return -1;
+  return done(h, h->t->block_fgmres_device(B, nrhs, (size_t)ldb, maxit, tol, iters, relres));
+}
 int spq_distribute_x(spq_tree* h, const double* x, double* xl) {
   if (!h || !x || !xl) return -1;
   const auto& s = h->t->structure();

@@ -99,6 +99,7 @@ Tree::~Tree() {
   cudaFree(d_model_);
   if (solve_exec_) cudaGraphExecDestroy(solve_exec_);
   if (solve_graph_) cudaGraphDestroy(solve_graph_);
+  release_block_solve();
   cudaFree(d_rank_);
   cudaFree(d_rowptr_);
   cudaFree(d_col_);
@@ -1263,40 +1264,13 @@ int Tree::alloc_level_blocks(const std::vector<int>& edges) {
 
 // Cluster vectors: level-0 clusters at their permuted columns [0, n); every
 // later cluster gets its own segment of its level size.
-int Tree::build_solve_graph() {
-  set_factor_fp32(fp32_);
+// Descriptors of one vector's preconditioner apply: per level the forward
+// elimination / sparsification tasks, the backward ones and the merge index
+// maps, all addressing the cluster vectors of the workspace xw (turn counters
+// in turn).  Uploaded into the block pool.
+int Tree::plan_solve(double* xw, int* turn, std::vector<SolvePlan>& ls) {
   const int L = st_.nlevels;
-  const int ncl = (int)st_.clusters.size();
-  xoff_.assign(ncl, 0);
-  int64_t off = st_.n;
-  const Level& L0 = st_.levels[0];
-  for (int o = L0.first; o < L0.first + L0.count; ++o) xoff_[o] = st_.clusters[o].cstart;
-  for (int o = L0.first + L0.count; o < ncl; ++o) {
-    xoff_[o] = off;
-    off += size_org_[o];
-  }
-  xw_size_ = off;
-  cudaFree(d_xw_);
-  cudaFree(d_turn_);
-  cudaFree(d_tickets_);
-  if (check_cuda(cudaMalloc(&d_xw_, sizeof(double) * std::max<int64_t>(xw_size_, 1)), "malloc") ||
-      check_cuda(cudaMalloc(&d_turn_, sizeof(int) * ncl), "malloc") ||
-      check_cuda(cudaMalloc(&d_tickets_, sizeof(int) * L), "malloc"))
-    return -10;
-  struct LevelSolve {
-    FwdElimTask* fe = nullptr;
-    FwdOut* fo = nullptr;
-    int nfe = 0, fe_nmax = 1, fe_mmax = 1;
-    FwdSparsTask* fs = nullptr;
-    int nfs = 0, fs_nmax = 1;
-    BwdElimTask* be = nullptr;
-    BwdIn* bi = nullptr;
-    int nbe = 0, be_nmax = 1;
-    int* gsrc = nullptr;
-    int* gdst = nullptr;
-    int ng = 0;
-  };
-  std::vector<LevelSolve> ls(L);
+  ls.assign(L, SolvePlan());
   auto up = [&](const void* h, size_t bytes) -> void* {
     void* d = arena_.alloc(std::max<size_t>(bytes, 1));
     if (d && bytes && h) cudaMemcpyAsync(d, h, bytes, cudaMemcpyHostToDevice, stream_);
@@ -1304,7 +1278,7 @@ int Tree::build_solve_graph() {
   };
   for (int lvl = 0; lvl < L; ++lvl) {
     const Level& Lv = st_.levels[lvl];
-    LevelSolve& S = ls[lvl];
+    SolvePlan& S = ls[lvl];
     // turn order per neighbour: interiors ascending
     std::vector<int> seen(Lv.count, 0);
     std::vector<FwdElimTask> fe;
@@ -1314,7 +1288,7 @@ int Tree::build_solve_graph() {
       FwdElimTask t;
       t.S = ptr_[Lv.self_edge_of[c - Lv.first]];
       t.T = T_[c];
-      t.x = elem(d_xw_, xoff_[c]);
+      t.x = elem(xw, xoff_[c]);
       t.n = size_[c];
       t.out_begin = (int)fo.size();
       for (int q = Lv.out_begin[ii]; q < Lv.out_end[ii]; ++q) {
@@ -1323,8 +1297,8 @@ int Tree::build_solve_graph() {
         FwdOut o;
         o.V = ptr_[e];
         o.T = tsqrtT_[e];
-        o.xn = elem(d_xw_, xoff_[nb]);
-        o.turn = d_turn_ + nb;
+        o.xn = elem(xw, xoff_[nb]);
+        o.turn = turn + nb;
         o.m = rows_[e];
         o.my_turn = seen[nb - Lv.first]++;
         fo.push_back(o);
@@ -1342,7 +1316,7 @@ int Tree::build_solve_graph() {
       t.V = Qsp_[p];
       t.T = Tsp_[p];
       t.rank = d_rank_ + p;
-      t.x = elem(d_xw_, xoff_[p]);
+      t.x = elem(xw, xoff_[p]);
       t.n = size_org_[p];
       fs.push_back(t);
       S.fs_nmax = std::max(S.fs_nmax, t.n);
@@ -1353,7 +1327,7 @@ int Tree::build_solve_graph() {
       const int c = Lv.interiors[ii];
       BwdElimTask t;
       t.S = ptr_[Lv.self_edge_of[c - Lv.first]];
-      t.x = elem(d_xw_, xoff_[c]);
+      t.x = elem(xw, xoff_[c]);
       t.n = size_[c];
       t.in_begin = (int)bi.size();
       for (int q = Lv.in_begin[ii]; q < Lv.in_end[ii]; ++q) {
@@ -1362,7 +1336,7 @@ int Tree::build_solve_graph() {
         b.R = ptr_[e];
         b.ldr = ld_[e];
         b.s = cols_[e];
-        b.xm = elem(d_xw_, xoff_[st_.edges[e].n1]);
+        b.xm = elem(xw, xoff_[st_.edges[e].n1]);
         bi.push_back(b);
       }
       t.in_end = (int)bi.size();
@@ -1397,36 +1371,300 @@ int Tree::build_solve_graph() {
     if (!S.fe || !S.fo || !S.fs || !S.be || !S.bi || !S.gsrc || !S.gdst)
       return fail(-11, "out of device memory (solve descriptors)");
   }
-  if (check_cuda(cudaStreamSynchronize(stream_), "solve descriptors")) return -10;
-  // capture the sweep
+  return check_cuda(cudaStreamSynchronize(stream_), "solve descriptors");
+}
+
+// Captures one vector's sweep (forward levels, then backward levels) into *g.
+int Tree::capture_solve(const std::vector<SolvePlan>& ls, double* xw, int* turn, int* tickets, cudaGraph_t* g,
+                        long long* kernels) {
+  const int L = st_.nlevels;
+  const int ncl = (int)st_.clusters.size();
+  if (check_cuda(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal), "capture")) return -10;
+  const long long launches_before = kernel_launches();
+  cudaError_t cerr = cudaSuccess;
+  cudaMemsetAsync(turn, 0, sizeof(int) * ncl, stream_);
+  cudaMemsetAsync(tickets, 0, sizeof(int) * L, stream_);
+  for (int lvl = 0; lvl < L; ++lvl) {
+    const SolvePlan& S = ls[lvl];
+    cerr = cerr ? cerr : launch_fwd_elim(S.fe, S.fo, S.nfe, S.fe_nmax, S.fe_mmax, tickets + lvl, d_status_, spin_limit, stream_);
+    cerr = cerr ? cerr : launch_fwd_spars(S.fs, S.nfs, S.fs_nmax, stream_);
+    cerr = cerr ? cerr : launch_copy_idx(S.ng, S.gsrc, S.gdst, xw, stream_);
+  }
+  for (int lvl = L - 1; lvl >= 0; --lvl) {
+    const SolvePlan& S = ls[lvl];
+    cerr = cerr ? cerr : launch_bwd_spars(S.fs, S.nfs, S.fs_nmax, stream_);
+    cerr = cerr ? cerr : launch_bwd_elim(S.be, S.bi, S.nbe, S.be_nmax, stream_);
+    if (lvl > 0) cerr = cerr ? cerr : launch_copy_idx(ls[lvl - 1].ng, ls[lvl - 1].gdst, ls[lvl - 1].gsrc, xw, stream_);
+  }
+  *kernels = kernel_launches() - launches_before;
+  add_kernel_launches(-*kernels);  // captured, not executed
+  cudaError_t ce = cudaStreamEndCapture(stream_, g);
+  if (check_cuda(cerr, "solve kernel launch") || check_cuda(ce, "end capture")) return -10;
+  return 0;
+}
+
+int Tree::build_solve_graph() {
+  set_factor_fp32(fp32_);
+  const int L = st_.nlevels;
+  const int ncl = (int)st_.clusters.size();
+  xoff_.assign(ncl, 0);
+  int64_t off = st_.n;
+  const Level& L0 = st_.levels[0];
+  for (int o = L0.first; o < L0.first + L0.count; ++o) xoff_[o] = st_.clusters[o].cstart;
+  for (int o = L0.first + L0.count; o < ncl; ++o) {
+    xoff_[o] = off;
+    off += size_org_[o];
+  }
+  xw_size_ = off;
+  cudaFree(d_xw_);
+  cudaFree(d_turn_);
+  cudaFree(d_tickets_);
+  d_xw_ = nullptr, d_turn_ = nullptr, d_tickets_ = nullptr;
+  release_block_solve();
+  if (check_cuda(cudaMalloc(&d_xw_, sizeof(double) * std::max<int64_t>(xw_size_, 1)), "malloc") ||
+      check_cuda(cudaMalloc(&d_turn_, sizeof(int) * ncl), "malloc") ||
+      check_cuda(cudaMalloc(&d_tickets_, sizeof(int) * L), "malloc"))
+    return -10;
+  std::vector<SolvePlan> ls;
+  if (int rc = plan_solve(d_xw_, d_turn_, ls)) return rc;
   if (solve_exec_) {
     cudaGraphExecDestroy(solve_exec_);
     cudaGraphDestroy(solve_graph_);
     solve_exec_ = nullptr;
   }
-  if (check_cuda(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal), "capture")) return -10;
-  const long long launches_before = kernel_launches();
-  cudaError_t cerr = cudaSuccess;
-  cudaMemsetAsync(d_turn_, 0, sizeof(int) * ncl, stream_);
-  cudaMemsetAsync(d_tickets_, 0, sizeof(int) * L, stream_);
-  for (int lvl = 0; lvl < L; ++lvl) {
-    LevelSolve& S = ls[lvl];
-    cerr = cerr ? cerr : launch_fwd_elim(S.fe, S.fo, S.nfe, S.fe_nmax, S.fe_mmax, d_tickets_ + lvl, d_status_, spin_limit, stream_);
-    cerr = cerr ? cerr : launch_fwd_spars(S.fs, S.nfs, S.fs_nmax, stream_);
-    cerr = cerr ? cerr : launch_copy_idx(S.ng, S.gsrc, S.gdst, d_xw_, stream_);
-  }
-  for (int lvl = L - 1; lvl >= 0; --lvl) {
-    LevelSolve& S = ls[lvl];
-    cerr = cerr ? cerr : launch_bwd_spars(S.fs, S.nfs, S.fs_nmax, stream_);
-    cerr = cerr ? cerr : launch_bwd_elim(S.be, S.bi, S.nbe, S.be_nmax, stream_);
-    if (lvl > 0) cerr = cerr ? cerr : launch_copy_idx(ls[lvl - 1].ng, ls[lvl - 1].gdst, ls[lvl - 1].gsrc, d_xw_, stream_);
-  }
-  solve_graph_kernels_ = kernel_launches() - launches_before;
-  add_kernel_launches(-solve_graph_kernels_);  // captured, not executed
-  cudaError_t ce = cudaStreamEndCapture(stream_, &solve_graph_);
-  if (check_cuda(cerr, "solve kernel launch") || check_cuda(ce, "end capture")) return -10;
+  if (int rc = capture_solve(ls, d_xw_, d_turn_, d_tickets_, &solve_graph_, &solve_graph_kernels_)) return rc;
   if (check_cuda(cudaGraphInstantiate(&solve_exec_, solve_graph_, 0), "instantiate")) return -10;
   return 0;
+}
+
+void Tree::release_block_solve() {
+  if (block_exec_) cudaGraphExecDestroy(block_exec_);
+  if (block_graph_) cudaGraphDestroy(block_graph_);
+  block_exec_ = nullptr;
+  block_graph_ = nullptr;
+  cudaFree(d_xwb_);
+  cudaFree(d_turnb_);
+  cudaFree(d_ticketsb_);
+  d_xwb_ = nullptr, d_turnb_ = nullptr, d_ticketsb_ = nullptr;
+  block_nrhs_ = 0;
+  block_graph_kernels_ = 0;
+}
+
+// The preconditioner apply of nrhs vectors as one graph: nrhs independent
+// sweeps (own workspace, turn counters and tickets each) as parallel branches,
+// so that the GPU runs them concurrently.  Built on first use per factorization
+// and nrhs (it allocates), reused after.
+int Tree::build_block_solve(int nrhs) {
+  if (block_exec_ && block_nrhs_ == nrhs) return 0;
+  release_block_solve();
+  const int L = st_.nlevels;
+  const int ncl = (int)st_.clusters.size();
+  if (check_cuda(cudaMalloc(&d_xwb_, sizeof(double) * (size_t)std::max<int64_t>(xw_size_, 1) * nrhs), "malloc") ||
+      check_cuda(cudaMalloc(&d_turnb_, sizeof(int) * (size_t)ncl * nrhs), "malloc") ||
+      check_cuda(cudaMalloc(&d_ticketsb_, sizeof(int) * (size_t)L * nrhs), "malloc"))
+    return -11;
+  if (check_cuda(cudaGraphCreate(&block_graph_, 0), "graph")) return -10;
+  set_factor_fp32(fp32_);
+  for (int r = 0; r < nrhs; ++r) {
+    double* xw = elem(d_xwb_, (size_t)r * xw_size_);
+    std::vector<SolvePlan> ls;
+    if (int rc = plan_solve(xw, d_turnb_ + (size_t)r * ncl, ls)) return rc;
+    cudaGraph_t g = nullptr;
+    long long nk = 0;
+    if (int rc = capture_solve(ls, xw, d_turnb_ + (size_t)r * ncl, d_ticketsb_ + (size_t)r * L, &g, &nk)) return rc;
+    cudaGraphNode_t node;
+    const cudaError_t e = cudaGraphAddChildGraphNode(&node, block_graph_, nullptr, 0, g);
+    cudaGraphDestroy(g);  // the child node holds a copy
+    if (check_cuda(e, "block solve graph")) return -10;
+    block_graph_kernels_ += nk;
+  }
+  if (check_cuda(cudaGraphInstantiate(&block_exec_, block_graph_, 0), "instantiate block solve")) return -10;
+  block_nrhs_ = nrhs;
+  return 0;
+}
+
+// M^{-1} x in place for the device vectors cols[0..nrhs) (permuted order), as
+// one block graph launch.
+int Tree::solve_block_cols(const std::vector<double*>& cols) {
+  if (!factorized_) return fail(-4, "solve called before factorize");
+  const int nrhs = (int)cols.size();
+  if (int rc = build_block_solve(nrhs)) return rc;
+  const int n = st_.n;
+  set_factor_fp32(fp32_);
+  for (int r = 0; r < nrhs; ++r) {
+    double* xw = elem(d_xwb_, (size_t)r * xw_size_);
+    if (fp32_) {
+      if (check_cuda(launch_to_f32(n, cols[r], xw, stream_), "block solve input")) return -10;
+    } else {
+      cudaMemcpyAsync(xw, cols[r], sizeof(double) * n, cudaMemcpyDeviceToDevice, stream_);
+    }
+  }
+  if (check_cuda(cudaGraphLaunch(block_exec_, stream_), "block solve graph")) return -10;
+  add_kernel_launches(block_graph_kernels_);
+  for (int r = 0; r < nrhs; ++r) {
+    double* xw = elem(d_xwb_, (size_t)r * xw_size_);
+    if (fp32_) {
+      if (check_cuda(launch_to_f64(n, xw, cols[r], stream_), "block solve output")) return -10;
+    } else {
+      cudaMemcpyAsync(cols[r], xw, sizeof(double) * n, cudaMemcpyDeviceToDevice, stream_);
+    }
+  }
+  return 0;
+}
+
+// M^{-1} X for nrhs device vectors (column r at X + r * ldx, permuted order).
+int Tree::solve_block_device(double* X, int nrhs, size_t ldx) {
+  if (nrhs < 1 || ldx < (size_t)st_.n) return fail(-1, "solve_block: nrhs >= 1 and ldx >= n required");
+  clear_status();
+  std::vector<double*> cols(nrhs);
+  for (int r = 0; r < nrhs; ++r) cols[r] = X + (size_t)r * ldx;
+  return solve_block_cols(cols);
+}
+
+// Flexible GMRES for nrhs right-hand sides in lockstep: every iteration applies
+// the preconditioner to all of them in one block graph, runs the SpMV and the
+// modified Gram-Schmidt of each, and reads all Hessenberg columns back with one
+// synchronisation.  A right-hand side that has converged is frozen (its later
+// columns are computed but not used).  B (device, column r at B + r * ldb) is
+// overwritten by the solutions; iters[r] / relres[r] as fgmres_device.
+int Tree::block_fgmres_device(double* B, int nrhs, size_t ldb, int maxit, double gtol, int* iters,
+                              double* relres) {
+  if (!factorized_) return fail(-4, "gmres called before factorize");
+  if (maxit < 1 || nrhs < 1 || ldb < (size_t)st_.n) return fail(-1, "block gmres: maxit, nrhs >= 1, ldb >= n");
+  clear_status();
+  double t0 = wall();
+  const int n = st_.n;
+  const size_t ldq = (size_t)n;
+  const int grid = mgs_grid(n);
+  // per right-hand side: V (n x maxit+1) | Z (n x maxit) | q | b | H column;
+  // then the shared partial sums and counter
+  const size_t hcap = (size_t)maxit + 3;
+  const size_t per = ldq * (2 * (size_t)maxit + 1) + 2 * ldq + hcap;
+  if (int erc = ensure_krylov(per * nrhs + grid + 1)) return erc;
+  auto Vr = [&](int r) { return d_krylov_ + per * r; };
+  auto Zr = [&](int r) { return Vr(r) + ldq * (maxit + 1); };
+  auto qr = [&](int r) { return Zr(r) + ldq * maxit; };
+  auto br = [&](int r) { return qr(r) + ldq; };
+  auto hr = [&](int r) { return br(r) + ldq; };
+  double* partial = d_krylov_ + per * nrhs;
+  unsigned int* done = reinterpret_cast<unsigned int*>(partial + grid);
+  cudaError_t ge = cudaSuccess;
+  auto g = [&](cudaError_t e) {
+    if (!ge) ge = e;
+  };
+  g(cudaMemsetAsync(done, 0, sizeof(unsigned int), stream_));
+  for (int r = 0; r < nrhs; ++r) {
+    g(cudaMemcpyAsync(br(r), B + (size_t)r * ldb, sizeof(double) * n, cudaMemcpyDeviceToDevice, stream_));
+    g(cudaMemcpyAsync(qr(r), br(r), sizeof(double) * n, cudaMemcpyDeviceToDevice, stream_));
+    g(launch_mgs_step(n, qr(r), nullptr, nullptr, nullptr, partial, done, hr(r), 1, stream_));  // ||b||
+    g(launch_scale_copy(n, qr(r), hr(r), Vr(r), stream_));
+  }
+  std::vector<double> hk(hcap * nrhs, 0.0);
+  auto readback = [&](int cnt) {
+    for (int r = 0; r < nrhs; ++r)
+      g(cudaMemcpyAsync(hk.data() + hcap * r, hr(r), sizeof(double) * cnt, cudaMemcpyDeviceToHost, stream_));
+    return check_cuda(ge ? ge : cudaStreamSynchronize(stream_), "block gmres");
+  };
+  int rc = readback(1);
+  std::vector<double> rnorm(nrhs);
+  for (int r = 0; r < nrhs; ++r) rnorm[r] = hk[hcap * r];
+  const size_t hs = (size_t)(maxit + 1) * maxit;
+  std::vector<double> H(hs * nrhs, 0.0), cs((size_t)maxit * nrhs, 0.0), sn((size_t)maxit * nrhs, 0.0),
+      beta((size_t)(maxit + 1) * nrhs, 0.0);
+  std::vector<int> kfin(nrhs, -1);
+  for (int r = 0; r < nrhs; ++r) {
+    beta[(size_t)(maxit + 1) * r] = rnorm[r];
+    if (!rc && !(rnorm[r] > 0)) rc = fail(-1, "zero or invalid right-hand side " + std::to_string(r));
+  }
+  int k = 0, active = nrhs;
+  for (; !rc && k < maxit && active > 0; ++k) {
+    // Z(:, k) = M^{-1} V(:, k) for every right-hand side: the block apply works
+    // on the columns Z_r(:, k) in place
+    for (int r = 0; r < nrhs; ++r)
+      g(cudaMemcpyAsync(Zr(r) + (size_t)k * ldq, Vr(r) + (size_t)k * ldq, sizeof(double) * n,
+                        cudaMemcpyDeviceToDevice, stream_));
+    if (ge) break;
+    std::vector<double*> zk(nrhs);
+    for (int r = 0; r < nrhs; ++r) zk[r] = Zr(r) + (size_t)k * ldq;
+    if ((rc = solve_block_cols(zk))) break;
+    for (int r = 0; r < nrhs; ++r) {
+      double* zk = Zr(r) + (size_t)k * ldq;
+      double* Q = Vr(r);
+      double* q = qr(r);
+      double* hcol = hr(r);
+      if ((rc = spmv_device(zk, q))) break;
+      for (int i = 0; i <= k; ++i)
+        g(launch_mgs_step(n, q, i ? Q + (size_t)(i - 1) * ldq : nullptr, i ? hcol + (i - 1) : nullptr,
+                          Q + (size_t)i * ldq, partial, done, hcol + i, 0, stream_));
+      g(launch_mgs_step(n, q, Q + (size_t)k * ldq, hcol + k, nullptr, partial, done, hcol + k + 1, 1, stream_));
+      g(launch_scale_copy(n, q, hcol + k + 1, Q + (size_t)(k + 1) * ldq, stream_));
+    }
+    if (rc || (rc = readback(k + 2))) break;
+    for (int r = 0; r < nrhs; ++r) {
+      if (kfin[r] >= 0) continue;
+      double* Hr = H.data() + hs * r;
+      double* c = cs.data() + (size_t)maxit * r;
+      double* s2 = sn.data() + (size_t)maxit * r;
+      double* be = beta.data() + (size_t)(maxit + 1) * r;
+      auto Hc = [&](int i, int j) -> double& { return Hr[(size_t)j * (maxit + 1) + i]; };
+      for (int i = 0; i <= k + 1; ++i) Hc(i, k) = hk[hcap * r + i];
+      for (int i = 0; i < k; ++i) {
+        const double temp = c[i] * Hc(i, k) + s2[i] * Hc(i + 1, k);
+        Hc(i + 1, k) = -s2[i] * Hc(i, k) + c[i] * Hc(i + 1, k);
+        Hc(i, k) = temp;
+      }
+      if (Hc(k, k) == 0) {
+        c[k] = 0;
+        s2[k] = 1;
+      } else {
+        const double t = std::sqrt(Hc(k, k) * Hc(k, k) + Hc(k + 1, k) * Hc(k + 1, k));
+        c[k] = std::fabs(Hc(k, k)) / t;
+        s2[k] = c[k] * Hc(k + 1, k) / Hc(k, k);
+      }
+      Hc(k, k) = c[k] * Hc(k, k) + s2[k] * Hc(k + 1, k);
+      Hc(k + 1, k) = 0.0;
+      be[k + 1] = -s2[k] * be[k];
+      be[k] = c[k] * be[k];
+      const double err = std::fabs(be[k + 1]) / rnorm[r];
+      if (verbose) printf("block FGMRES: rhs %d error at step %d is %e\n", r, k, err);
+      if (err <= gtol || k + 1 == maxit) {
+        kfin[r] = k;
+        --active;
+      }
+    }
+  }
+  if (!rc && device_status() != 0) rc = fail(-12, "forward sweep wait timed out on the device");
+  if (!rc) {
+    std::vector<double> nr(2 * nrhs, 1.0);
+    for (int r = 0; r < nrhs; ++r) {
+      const int kr = kfin[r] >= 0 ? kfin[r] : std::min(k, maxit) - 1;
+      double* Hr = H.data() + hs * r;
+      double* be = beta.data() + (size_t)(maxit + 1) * r;
+      auto Hc = [&](int i, int j) -> double& { return Hr[(size_t)j * (maxit + 1) + i]; };
+      std::vector<double> y(kr + 1, 0.0);
+      for (int i = kr; i >= 0; --i) {
+        y[i] = be[i];
+        for (int j = i + 1; j < kr + 1; ++j) y[i] -= Hc(i, j) * y[j];
+        y[i] /= Hc(i, i);
+      }
+      double* x = B + (size_t)r * ldb;
+      double* q = qr(r);
+      double* hcol = hr(r);
+      g(cudaMemcpyAsync(hcol, y.data(), sizeof(double) * (kr + 1), cudaMemcpyHostToDevice, stream_));
+      g(launch_combine(n, kr + 1, Zr(r), ldq, hcol, x, stream_));
+      g(spmv_device(x, q) ? cudaErrorUnknown : cudaSuccess);
+      g(launch_sub(n, br(r), q, q, stream_));
+      g(launch_mgs_step(n, q, nullptr, nullptr, nullptr, partial, done, hcol, 1, stream_));
+      g(launch_mgs_step(n, br(r), nullptr, nullptr, nullptr, partial, done, hcol + 1, 1, stream_));
+      g(cudaMemcpyAsync(nr.data() + 2 * r, hcol, sizeof(double) * 2, cudaMemcpyDeviceToHost, stream_));
+      // the host copy of y must stay alive until the copy has run
+      if ((rc = check_cuda(ge ? ge : cudaStreamSynchronize(stream_), "block gmres finish"))) break;
+      iters[r] = kr;
+    }
+    for (int r = 0; !rc && r < nrhs; ++r) relres[r] = nr[2 * r] / nr[2 * r + 1];
+  }
+  t_gmres = wall() - t0;
+  return rc;
 }
 
 int Tree::solve_device(double* x) {
@@ -1845,6 +2083,26 @@ int Tree::fgmres_device(double* b, int maxit, double gtol, int* iters, double* r
     last_gmres_iters = k;
   }
   t_gmres = wall() - t0;
+  return rc;
+}
+
+// block_fgmres_device with host right-hand sides / solutions (column r at
+// B + r * ldb): uploaded into one device buffer per call.
+int Tree::block_gmres_host(double* B, int nrhs, size_t ldb, int maxit, double gtol, int* iters, double* relres) {
+  if (!factorized_) return fail(-4, "gmres called before factorize");
+  if (nrhs < 1 || ldb < (size_t)st_.n) return fail(-1, "block gmres: nrhs >= 1, ldb >= n");
+  const size_t n = st_.n;
+  double* d = nullptr;
+  if (check_cuda(cudaMalloc(&d, sizeof(double) * n * nrhs), "malloc block right-hand sides")) return -11;
+  for (int r = 0; r < nrhs; ++r)
+    cudaMemcpyAsync(d + n * r, B + ldb * r, sizeof(double) * n, cudaMemcpyHostToDevice, stream_);
+  int rc = block_fgmres_device(d, nrhs, n, maxit, gtol, iters, relres);
+  if (!rc) {
+    for (int r = 0; r < nrhs; ++r)
+      cudaMemcpyAsync(B + ldb * r, d + n * r, sizeof(double) * n, cudaMemcpyDeviceToHost, stream_);
+    rc = check_cuda(cudaStreamSynchronize(stream_), "block gmres download");
+  }
+  cudaFree(d);
   return rc;
 }
 

@@ -126,6 +126,14 @@ class Tree {
   // with fixed host arrays (maxit <= kNoAllocMaxit); allocates nothing
   int gmres_device_fixed(double* b, int maxit, double gtol, int* iters, double* relres, double* ws, size_t ws_doubles);
 
+  // preconditioner apply of nrhs vectors at once (column r at X + r * ldx):
+  // one graph of nrhs concurrent sweeps, built on first use (allocates)
+  int solve_block_device(double* X, int nrhs, size_t ldx);
+  // flexible GMRES of nrhs right-hand sides in lockstep (block preconditioner
+  // apply, one host synchronisation per iteration for all of them)
+  int block_fgmres_device(double* B, int nrhs, size_t ldb, int maxit, double gtol, int* iters, double* relres);
+  int block_gmres_host(double* B, int nrhs, size_t ldb, int maxit, double gtol, int* iters, double* relres);
+
   int set_stream(cudaStream_t s);
   cudaStream_t stream() const { return stream_; }
 
@@ -184,6 +192,26 @@ class Tree {
   void* stage(size_t bytes);
   void stage_reset() { pin_cur_ = 0, pin_off_ = 0; }
   int build_solve_graph();
+  // one vector's apply: descriptors for workspace xw / turn counters, and its capture
+  struct SolvePlan {
+    FwdElimTask* fe = nullptr;
+    FwdOut* fo = nullptr;
+    int nfe = 0, fe_nmax = 1, fe_mmax = 1;
+    FwdSparsTask* fs = nullptr;
+    int nfs = 0, fs_nmax = 1;
+    BwdElimTask* be = nullptr;
+    BwdIn* bi = nullptr;
+    int nbe = 0, be_nmax = 1;
+    int* gsrc = nullptr;
+    int* gdst = nullptr;
+    int ng = 0;
+  };
+  int plan_solve(double* xw, int* turn, std::vector<SolvePlan>& ls);
+  int capture_solve(const std::vector<SolvePlan>& ls, double* xw, int* turn, int* tickets, cudaGraph_t* g,
+                    long long* kernels);
+  int build_block_solve(int nrhs);
+  void release_block_solve();
+  int solve_block_cols(const std::vector<double*>& cols);
   // one zeroed region for the blocks of `edges`; sets ptr_/ld_ (rows_/cols_ must be set)
   int alloc_level_blocks(const std::vector<int>& edges);
 
@@ -231,6 +259,14 @@ class Tree {
   cudaGraphExec_t solve_exec_ = nullptr;
   cudaGraph_t solve_graph_ = nullptr;
   long long solve_graph_kernels_ = 0;
+  // block apply of block_nrhs_ vectors: workspaces, turn counters, tickets
+  cudaGraphExec_t block_exec_ = nullptr;
+  cudaGraph_t block_graph_ = nullptr;
+  long long block_graph_kernels_ = 0;
+  int block_nrhs_ = 0;
+  double* d_xwb_ = nullptr;
+  int* d_turnb_ = nullptr;
+  int* d_ticketsb_ = nullptr;
   double* d_tmp_ = nullptr;    // 2 vectors for host-pointer entry points
   // Krylov workspace kept across GMRES calls
   double* d_krylov_ = nullptr;

@@ -84,7 +84,7 @@ def constant_model(mean_y, nf):
     return {"params": p, "mean": np.zeros(F, np.float32), "std": np.ones(F, np.float32)}
 
 
-def evaluate(model, const, seeds, tols, n=64):
+def evaluate(model, const, seeds, tols, n=64, oversample=OVERSAMPLE):
     rows = []
     for tol in tols:
         agg = {"tol": tol, "interfaces": 0}
@@ -105,7 +105,7 @@ def evaluate(model, const, seeds, tols, n=64):
             sp = np.array([c["sparsify"] for c in cl]) > 0
             plain = np.array([c["rank"] for c in cl])[sp]
             for name, m in (("learned", model), ("constant", const)):
-                t.set_rank_model(m, OVERSAMPLE)
+                t.set_rank_model(m, oversample)
                 t.assemble()
                 t.factorize()
                 cnt = t.learned_counts()
@@ -119,7 +119,7 @@ def evaluate(model, const, seeds, tols, n=64):
             del t
         N = max(agg["interfaces"], 1)
         rows.append({
-            "tol": tol, "interfaces": agg["interfaces"],
+            "tol": tol, "interfaces": agg["interfaces"], "oversample": oversample,
             "learned": {"within2": agg["within2"] / N, "fallback_rate": agg["fallback"] / N,
                         "sketch_columns": agg["sketch_cols"], "factorize_s": agg["learned_s"] / len(seeds)},
             "constant": {"within2": agg["c_within2"] / N, "fallback_rate": agg["c_fallback"] / N,
@@ -139,6 +139,9 @@ def main():
     ap.add_argument("--epochs", type=int, default=60)
     ap.add_argument("--no-eval", action="store_true")
     ap.add_argument("--eval-only", action="store_true", help="evaluate the model already in --out")
+    ap.add_argument("--oversample", type=int, default=OVERSAMPLE,
+                    help="sketch columns beyond the predicted rank in the evaluation")
+    ap.add_argument("--report", default="report.json", help="report file name (in --out)")
     args = ap.parse_args()
 
     def rng(s):
@@ -150,8 +153,9 @@ def main():
         meta = json.loads(str(z["meta"]))
         model = {k: z[k].astype(np.float32) for k in ("params", "mean", "std")}
         const = constant_model(meta["mean_target"], len(model["mean"]))
-        report = {"meta": meta, "loss": z["loss"].tolist(), "eval": evaluate(model, const, rng(args.eval_seeds), TOLS)}
-        with open(os.path.join(args.out, "report.json"), "w") as f:
+        report = {"meta": meta, "loss": z["loss"].tolist(),
+                  "eval": evaluate(model, const, rng(args.eval_seeds), TOLS, oversample=args.oversample)}
+        with open(os.path.join(args.out, args.report), "w") as f:
             json.dump(report, f, indent=1)
         return
     t0 = time.time()

@@ -82,6 +82,9 @@ def lib():
             "spq_mlp_train": (i32, [pf, pf, pf, i32, i32, i32, f32, C.c_ulonglong, pf]),
             "spq_mlp_last_error": (C.c_char_p, []),
             "spq_distribute_x": (i32, [vp, pd, pd]),
+            "spq_solve_block_device": (i32, [vp, vp, i32, C.c_longlong]),
+            "spq_gmres_block": (i32, [vp, pd, i32, C.c_longlong, i32, f64, pi, pd]),
+            "spq_gmres_block_device": (i32, [vp, vp, i32, C.c_longlong, i32, f64, pi, pd]),
             "spq_extract_x": (i32, [vp, pd, pd]),
             "spq_n": (i32, [vp]),
             "spq_set_stream": (i32, [vp, vp]),
@@ -442,6 +445,19 @@ class ParTree:
 
     def pool_bytes(self) -> float:
         return lib().spq_pool_bytes(self._h)
+
+
+def block_gmres(M: ParTree, B: np.ndarray, iters: int = 100, tol: float = 1e-10):
+    """Flexible GMRES of the columns of B (n x nrhs, permuted local order) in
+    lockstep, one block preconditioner apply per iteration; B is overwritten by
+    the solutions.  Returns (iterations, true relative residuals) per column."""
+    if B.dtype != np.float64 or not B.flags.f_contiguous or B.ndim != 2:
+        raise TypeError("B must be a Fortran-ordered float64 n x nrhs array")
+    n, nrhs = B.shape
+    k = np.zeros(nrhs, np.int32)
+    rr = np.zeros(nrhs)
+    M._chk(lib().spq_gmres_block(M._h, _pd(B), nrhs, n, iters, tol, _pi(k), _pd(rr)), "gmres_block")
+    return k, rr
 
 
 def dist_gmres(A, b: np.ndarray, M: ParTree, iters: int = 300, tol: float = 1e-12, verb: bool = True,
