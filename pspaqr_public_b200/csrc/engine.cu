@@ -7,6 +7,7 @@
 #include <chrono>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <numeric>
 
@@ -91,7 +92,11 @@ void Arena::release() {
 }
 
 // ---------------------------------------------------------------- Tree
-Tree::Tree(int L, int s) : nlevels(L), skip(s) {}
+Tree::Tree(int L, int s) : nlevels(L), skip(s) {
+  // SPQ_TENSOR_CORES=0 in the environment starts trees with the float applies
+  // on the CUDA cores (spq_set_tensor_cores changes it per tree)
+  if (const char* e = std::getenv("SPQ_TENSOR_CORES")) tensor_cores = std::atoi(e) != 0;
+}
 
 Tree::~Tree() {
   if (stream_) cudaStreamSynchronize(stream_);
