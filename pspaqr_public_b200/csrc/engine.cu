@@ -447,6 +447,18 @@ int Tree::factorize() {
       nmax[g] = std::max(nmax[g], nc);
       vmax[g] = std::max(vmax[g], vm);
     }
+    // the chains run while the host builds the update lists
+    {
+      auto* d_eo = static_cast<ElimOut*>(upload(eo.data(), sizeof(ElimOut) * eo.size()));
+      for (int g = 0; g < 3; ++g) {
+        if (et[g].empty()) continue;
+        auto* d_et = static_cast<ElimTask*>(upload(et[g].data(), sizeof(ElimTask) * et[g].size()));
+        if (!d_et || !d_eo) return fail(-11, "out of device memory (elimination descriptors)");
+        if (ck(launch_elim(d_et, d_eo, (int)et[g].size(), csz[g], nmax[g], vmax[g], stream_), "elimination kernel"))
+          return -10;
+      }
+      cudaEventRecord(fe[0], stream_);
+    }
     // trailing updates: one task per (column cluster, chunk of kChunk columns)
     std::vector<UpdTask> ut;
     std::vector<UpdOp> uo;
@@ -520,15 +532,6 @@ int Tree::factorize() {
              ut.size(), uo.size(), fsum, fsum / std::max<size_t>(ut.size(), 1), fmax, omax);
     }
     {
-      auto* d_eo = static_cast<ElimOut*>(upload(eo.data(), sizeof(ElimOut) * eo.size()));
-      for (int g = 0; g < 3; ++g) {
-        if (et[g].empty()) continue;
-        auto* d_et = static_cast<ElimTask*>(upload(et[g].data(), sizeof(ElimTask) * et[g].size()));
-        if (!d_et || !d_eo) return fail(-11, "out of device memory (elimination descriptors)");
-        if (ck(launch_elim(d_et, d_eo, (int)et[g].size(), csz[g], nmax[g], vmax[g], stream_), "elimination kernel"))
-          return -10;
-      }
-      cudaEventRecord(fe[0], stream_);
       if (corrupt_next_descriptor && !uo.empty()) {
         corrupt_next_descriptor = false;
         check_descriptors = true;

@@ -224,6 +224,17 @@ __device__ void tc_apply_tpqt(tc::Ctx& x, const float* V, int ldv, const float* 
   }
 }
 
+// C (m x n) <- C Q, panels in order (dev::mat_apply_q_right), on the tensor
+// cores: each panel is the left apply Q^T of the transposed chunk.  m <= 64.
+__device__ void tc_apply_q_right(tc::Ctx& x, const float* V, int ldv, const float* Tm, int k, float* C, int ldc,
+                                 int m, int n) {
+  for (int j0 = 0; j0 < k; j0 += kNB) {
+    const int kb = min(k - j0, kNB);
+    tc::left_qt<true>(x, V + j0 + (size_t)j0 * ldv, ldv, Tm + (size_t)j0 * kNB, kNB, kb, 1, nullptr, 0,
+                      C + (size_t)j0 * ldc, ldc, n - j0, m);
+  }
+}
+
 // k_update on the tensor cores (float factors)
 __global__ void __launch_bounds__(kThreads, 2) k_update_tc(const UpdTask* __restrict__ tasks,
                                                          const UpdOp* __restrict__ ops, int* status) {
@@ -252,6 +263,16 @@ __global__ void __launch_bounds__(kThreads, 2) k_edge_left_tc(const EdgeChunk* _
   if (t.limdev) cnt = min(cnt, *t.limdev - t.lo);
   if (cnt > 0) tc_apply_qt(x, as<float>(t.V), t.ldv, as<float>(t.T), k, as<float>(t.A) + (size_t)t.lo * t.lda, t.lda,
                            t.m, cnt);
+  tc::end(x);
+}
+
+// k_edge_right on the tensor cores (float factors): rows [lo, lo+cnt) of A <- A Q
+__global__ void __launch_bounds__(kThreads, 2) k_edge_right_tc(const EdgeChunk* __restrict__ tasks, int* status) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  tc::Ctx x = tc::begin(smraw, status);
+  const EdgeChunk t = tasks[blockIdx.x];
+  const int k = t.kdev ? *t.kdev : t.k;
+  if (t.cnt > 0) tc_apply_q_right(x, as<float>(t.V), t.ldv, as<float>(t.T), k, as<float>(t.A) + t.lo, t.lda, t.cnt, t.nc);
   tc::end(x);
 }
 
@@ -1367,6 +1388,11 @@ cudaError_t launch_edge(int kind, const EdgeChunk* t, int ntasks, cudaStream_t s
   if (g_fp32 && g_tc && kind == 0) {
     if ((e = prep(k_edge_left_tc, tc::kSmemBytes))) return e;
     k_edge_left_tc<<<ntasks, kThreads, tc::kSmemBytes, st>>>(t, g_status);
+    return last();
+  }
+  if (g_fp32 && g_tc && kind == 2) {
+    if ((e = prep(k_edge_right_tc, tc::kSmemBytes))) return e;
+    k_edge_right_tc<<<ntasks, kThreads, tc::kSmemBytes, st>>>(t, g_status);
     return last();
   }
   return g_fp32 ? go(k_edge_left<float>, k_edge_trsm<float>, k_edge_right<float>)

@@ -219,7 +219,10 @@ __device__ __forceinline__ void wait_mma(Ctx& x) {
 // [A (kb x nc); C (m x nc)] <- Q^T [A; C] for one panel, as dev::tile_left_qt:
 // unit = 1: V unit lower trapezoidal (m x kb) from the panel's diagonal, A
 // unused; unit = 0: V full (m x kb), pentagonal top block A.  nc <= 64,
-// kb <= 32.  Called by all threads of the CTA.
+// kb <= 32.  kTrans: the operand is the transpose of the array at C, element
+// (r, c) at C[c + r * ldc] -- the right apply D (I - V T V^T) of a chunk of
+// nc rows of D, since (D Q)^T = Q^T D^T.  Called by all threads of the CTA.
+template <bool kTrans = false>
 __device__ void left_qt(Ctx& x, const float* V, int ldv, const float* Tm, int ldt, int kb, int unit, float* A,
                         int lda, float* C, int ldc, int m, int nc) {
   if (m <= 0 || nc <= 0 || kb <= 0 || x.failed) return;
@@ -243,12 +246,25 @@ __device__ void left_qt(Ctx& x, const float* V, int ldv, const float* Tm, int ld
   const int nt1 = (m + kCRows - 1) / kCRows;
   constexpr int kLC = kCRows * 64 / kThreads, kLV = kCRows * kNB / kThreads;
   float rc[kLC], rv[kLV];
+  // element (r, c) of the operand; a warp reads consecutive addresses (rows of
+  // C, or columns of the transposed operand)
+  auto cidx = [&](int idx, int& r, int& c) {
+    if (kTrans) {
+      c = idx & 63;
+      r = idx >> 6;
+    } else {
+      r = idx & (kCRows - 1);
+      c = idx >> 6;
+    }
+  };
+  auto cptr = [&](int r, int c) { return kTrans ? C + c + (size_t)r * ldc : C + r + (size_t)c * ldc; };
   auto load1 = [&](int rt) {
     const int r0 = rt * kCRows;
 #pragma unroll
     for (int q = 0; q < kLC; ++q) {
-      const int idx = t + q * kThreads, r = idx & (kCRows - 1), c = idx >> 6;
-      rc[q] = (r0 + r < m && c < nc) ? C[(r0 + r) + (size_t)c * ldc] : 0.f;
+      int r, c;
+      cidx(t + q * kThreads, r, c);
+      rc[q] = (r0 + r < m && c < nc) ? *cptr(r0 + r, c) : 0.f;
     }
 #pragma unroll
     for (int q = 0; q < kLV; ++q) {
@@ -260,7 +276,8 @@ __device__ void left_qt(Ctx& x, const float* V, int ldv, const float* Tm, int ld
     const int vr = (rt & 1) * kCRows;
 #pragma unroll
     for (int q = 0; q < kLC; ++q) {
-      const int idx = t + q * kThreads, r = idx & (kCRows - 1), c = idx >> 6;
+      int r, c;
+      cidx(t + q * kThreads, r, c);
       const float hi = tf32_hi(rc[q]);
       *reinterpret_cast<float*>(sm + kOffChi + c_off(r, c)) = hi;
       *reinterpret_cast<float*>(sm + kOffClo + c_off(r, c)) = rc[q] - hi;
@@ -378,7 +395,7 @@ __device__ void left_qt(Ctx& x, const float* V, int ldv, const float* Tm, int ld
       for (int j = 0; j < 32; ++j) {
         const int c = 32 * half + j;
         if (c < nc) {
-          float* p = C + r + (size_t)c * ldc;
+          float* p = cptr(r, c);
           float old;
           if (c_in_smem)
             old = *reinterpret_cast<const float*>(sm + kOffChi + c_off(rl, c)) +
