@@ -68,6 +68,15 @@ int spq_set_precision(spq_tree* t, int bits);
  * in FP32 on the CUDA cores.  No effect on FP64 factors.  Takes effect at the
  * next factorize. */
 int spq_set_tensor_cores(spq_tree* t, int on);
+/* Reuse of descriptor lists across factorizations of one partition (no
+ * reference counterpart; the reference rebuilds its task graph every time,
+ * ptree.cpp:885-2123).  A level's lists depend only on its cluster sizes and on
+ * the allocators' states, so when a later factorize meets the same sizes (the
+ * same kept ranks below that level) it reuses them; the merge list is reused
+ * when the level's kept ranks are equal too.  on = 1 (default) enables it;
+ * spq_plan_hits counts the levels that reused their lists. */
+int spq_set_plan_cache(spq_tree* t, int on);
+long long spq_plan_hits(spq_tree* t);
 /* Failure detection (no reference counterpart; the reference asserts, which
  * its Release build compiles out, or exits).
  * spq_set_spin_limit: clock-cycle budget of each bounded wait of the

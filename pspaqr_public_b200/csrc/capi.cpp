@@ -76,6 +76,13 @@ int spq_set_precision(spq_tree* h, int bits) {
   return 0;
 }
 
+int spq_set_plan_cache(spq_tree* h, int on) {
+  if (!h || on < 0 || on > 1) return -1;
+  h->t->plan_cache = on != 0;
+  return 0;
+}
+long long spq_plan_hits(spq_tree* h) { return h ? h->t->plan_hits() : -1; }
+
 int spq_set_spin_limit(spq_tree* h, long long cycles) {
   if (!h || cycles < 0) return -1;
   h->t->spin_limit = cycles;

@@ -71,6 +71,16 @@ void* Arena::alloc(size_t bytes) {
   return r;
 }
 
+void Arena::state(std::vector<const char*>& base, std::vector<size_t>& off, size_t& cur) const {
+  base.clear();
+  off.clear();
+  for (const Chunk& c : chunks_) {
+    base.push_back(c.base);
+    off.push_back(c.off);
+  }
+  cur = cur_;
+}
+
 bool Arena::contains(const void* p, size_t bytes) const {
   const char* q = static_cast<const char*>(p);
   for (const Chunk& c : chunks_)
@@ -237,6 +247,7 @@ int Tree::partition(int nrows, int ncols, const int* colptr, const int* rowidx, 
   partitioned_ = true;
   assembled_ = factorized_ = false;
   asm_valid_ = false;
+  plans_.clear();
   t_partition = wall() - t0;
   if (verbose) printf("Time to partition: %g\n", t_partition);
   return 0;
@@ -410,6 +421,27 @@ int Tree::factorize() {
       return ck(e, where);
     };
     cudaEventRecord(ev[0], stream_);
+    // descriptor lists of an earlier factorization with equal sizes and
+    // allocator states are reused (LevelPlan)
+    if ((int)plans_.size() != L) plans_.assign(L, LevelPlan());
+    LevelPlan& P = plans_[lvl];
+    bool hit = false;
+    {
+      LevelPlanKey key;
+      arena_.state(key.abase, key.aoff, key.acur);
+      std::vector<size_t> soff;
+      size_t scur = 0;
+      scratch_.state(key.sbase, soff, scur);
+      key.sizes.assign(size_.begin() + Lv.first, size_.begin() + Lv.first + Lv.count);
+      key.flags = (fp32_ ? 1 : 0) | (rank_model_ ? 2 : 0) | (rank_log_ ? 4 : 0) | (verbose >= 2 ? 8 : 0);
+      hit = plan_cache && P.valid && P.key == key;
+      if (!hit) {
+        P = LevelPlan();
+        P.key = std::move(key);
+      } else {
+        ++plan_hits_;
+      }
+    }
     // ---------------- elimination: geqrt + tsqrt chains, grouped by cluster size
     std::vector<ElimTask> et[3];
     std::vector<ElimOut> eo;
@@ -460,9 +492,9 @@ int Tree::factorize() {
       cudaEventRecord(fe[0], stream_);
     }
     // trailing updates: one task per (column cluster, chunk of kChunk columns)
-    std::vector<UpdTask> ut;
-    std::vector<UpdOp> uo;
-    for (size_t ct = 0; ct < Lv.col_m.size(); ++ct) {
+    std::vector<UpdTask>& ut = P.ut;
+    std::vector<UpdOp>& uo = P.uo;
+    for (size_t ct = 0; !hit && ct < Lv.col_m.size(); ++ct) {
       const int m = Lv.col_m[ct];
       const int op_begin = (int)uo.size();
       const int ncol = size_[m];
@@ -483,7 +515,7 @@ int Tree::factorize() {
         a.lda = ld_[ecm];
         a.ldb = 0;
         uo.push_back(a);
-        lt_[lvl].flops[1] += 4.0 * nc * nc * ncol;
+        P.fl_upd += 4.0 * nc * nc * ncol;
         const int ii = (int)(std::lower_bound(Lv.interiors.begin(), Lv.interiors.end(), c) - Lv.interiors.begin());
         int j = Lv.col_emn_begin[q];
         for (int r = Lv.out_begin[ii]; r < Lv.out_end[ii]; ++r, ++j) {
@@ -501,12 +533,13 @@ int Tree::factorize() {
           b.lda = ld_[ecm];
           b.ldb = ld_[emn];
           uo.push_back(b);
-          lt_[lvl].flops[1] += 4.0 * rows_[ecn] * nc * ncol;
+          P.fl_upd += 4.0 * rows_[ecn] * nc * ncol;
         }
       }
       const int op_end = (int)uo.size();
       for (int c0 = 0; c0 < ncol; c0 += kChunk) ut.push_back({op_begin, op_end, c0, std::min(kChunk, ncol - c0)});
     }
+    lt_[lvl].flops[1] += P.fl_upd;
     lt_[lvl].ntasks_elim = (int)Lv.interiors.size();
     lt_[lvl].ntasks_upd = (int)ut.size();
     if (verbose >= 2) {
@@ -532,17 +565,21 @@ int Tree::factorize() {
              ut.size(), uo.size(), fsum, fsum / std::max<size_t>(ut.size(), 1), fmax, omax);
     }
     {
+      std::vector<UpdOp> uo_bad;  // the fault-injection copy (the cached list stays intact)
+      const std::vector<UpdOp>* uop = &uo;
       if (corrupt_next_descriptor && !uo.empty()) {
         corrupt_next_descriptor = false;
         check_descriptors = true;
-        uo[uo.size() / 2].B = uo[uo.size() / 2].A + ((size_t)1 << 40);  // far outside the pool
-        uo[uo.size() / 2].kind = 1;
+        uo_bad = uo;
+        uo_bad[uo.size() / 2].B = uo_bad[uo.size() / 2].A + ((size_t)1 << 40);  // far outside the pool
+        uo_bad[uo.size() / 2].kind = 1;
+        uop = &uo_bad;
       }
       if (check_descriptors) {
         const size_t es = fp32_ ? 4 : 8;
         for (const UpdTask& u : ut)
           for (int o = u.op_begin; o < u.op_end; ++o) {
-            const UpdOp& op = uo[o];
+            const UpdOp& op = (*uop)[o];
             const size_t ncol = (size_t)u.col0 + u.ncols;
             if (!arena_.contains(op.V, es * ((size_t)op.ldv * (op.k - 1) + op.m)) ||
                 !arena_.contains(op.T, es * (size_t)NB * op.k) ||
@@ -553,7 +590,7 @@ int Tree::factorize() {
           }
       }
       auto* d_ut = static_cast<UpdTask*>(upload(ut.data(), sizeof(UpdTask) * ut.size()));
-      auto* d_uo = static_cast<UpdOp*>(upload(uo.data(), sizeof(UpdOp) * uo.size()));
+      auto* d_uo = static_cast<UpdOp*>(upload(uop->data(), sizeof(UpdOp) * uop->size()));
       if (!d_ut || !d_uo) return fail(-11, "out of device memory (update descriptors)");
       if (ck(launch_update(d_ut, d_uo, (int)ut.size(), stream_), "update kernel")) return -10;
     }
@@ -594,8 +631,10 @@ int Tree::factorize() {
         if (!d || ck(launch_scale(d, (int)sc[g].size(), csz[g], smax[g], stream_), "scaling kernel")) return -10;
       }
       cudaEventRecord(fe[1], stream_);
-      std::vector<EdgeChunk> rows_scale, cols_scale;
-      for (int e : Lv.spars_edges) {
+      std::vector<EdgeChunk>& rows_scale = P.rows_scale;
+      std::vector<EdgeChunk>& cols_scale = P.cols_scale;
+      for (size_t ei = 0; !hit && ei < Lv.spars_edges.size(); ++ei) {
+        const int e = Lv.spars_edges[ei];
         const Edge& E = st_.edges[e];
         const bool r = st_.clusters[E.n2].sparsify, c = st_.clusters[E.n1].sparsify;
         EdgeChunk t{};
@@ -613,7 +652,7 @@ int Tree::factorize() {
             t.cnt = std::min(kChunk, t.nc - c0);
             rows_scale.push_back(t);
           }
-          lt_[lvl].flops[3] += 4.0 * t.m * t.m * t.nc;
+          P.fl_sapp += 4.0 * t.m * t.m * t.nc;
         }
         if (c) {
           t.V = ptr_[Lv.self_edge_of[E.n1 - Lv.first]];
@@ -624,9 +663,10 @@ int Tree::factorize() {
             t.cnt = std::min(kChunk, t.m - r0);
             cols_scale.push_back(t);
           }
-          lt_[lvl].flops[3] += (double)t.m * t.nc * t.nc;
+          P.fl_sapp += (double)t.m * t.nc * t.nc;
         }
       }
+      lt_[lvl].flops[3] += P.fl_sapp;
       {
         auto* d_rows = static_cast<EdgeChunk*>(up_vec(rows_scale));
         auto* d_cols = static_cast<EdgeChunk*>(up_vec(cols_scale));
@@ -639,8 +679,10 @@ int Tree::factorize() {
       // compression matrices C (m x w) of the level's interfaces, gathered
       // transposed into scratch by k_rrqr_assemble
       const size_t nsp = Lv.spars_clusters.size();
-      std::vector<RrqrSrc> rs;
-      std::vector<int> sp_w(nsp), sp_ldw(nsp);
+      std::vector<RrqrSrc>& rs = P.rs;
+      std::vector<int>& sp_w = P.sp_w;
+      if (!hit) sp_w.assign(nsp, 0);
+      std::vector<int> sp_ldw(nsp);
       std::vector<double*> sp_C(nsp), spV(nsp), spT(nsp);
       std::vector<int> sp_q(st_.clusters.size(), -1);  // interface -> index in this level's list
       for (size_t q = 0; q < nsp; ++q) sp_q[Lv.spars_clusters[q]] = (int)q;
@@ -653,22 +695,25 @@ int Tree::factorize() {
       for (size_t q = 0; q < nsp; ++q) {
         const int p = Lv.spars_clusters[q];
         const int mp = size_[p];
-        int w = 0;
-        for (int k = Lv.sp_out_begin[q]; k < Lv.sp_out_end[q]; ++k) w += rows_[Lv.sp_out[k]];
-        for (int k = Lv.sp_in_begin[q]; k < Lv.sp_in_end[q]; ++k) w += cols_[Lv.sp_in[k]];
-        sp_w[q] = w;
+        if (!hit) {
+          int w = 0;
+          for (int k = Lv.sp_out_begin[q]; k < Lv.sp_out_end[q]; ++k) w += rows_[Lv.sp_out[k]];
+          for (int k = Lv.sp_in_begin[q]; k < Lv.sp_in_end[q]; ++k) w += cols_[Lv.sp_in[k]];
+          sp_w[q] = w;
+        }
+        const int w = sp_w[q];
         sp_ldw[q] = (w + 3) / 4 * 4;
         level_work += (double)mp * w;
         double* Ct = scratch_.dalloc((size_t)std::max(mp, 1) * std::max(sp_ldw[q], 4));
         if (!Ct) return fail(-11, "out of device memory (rrqr)");
         sp_C[q] = Ct;
         int c0 = 0;
-        for (int k = Lv.sp_out_begin[q]; k < Lv.sp_out_end[q]; ++k) {
+        for (int k = Lv.sp_out_begin[q]; !hit && k < Lv.sp_out_end[q]; ++k) {
           const int e = Lv.sp_out[k];
           if (rows_[e] > 0 && mp > 0) rs.push_back({ptr_[e], ld_[e], rows_[e], cols_[e], 1, Ct, sp_ldw[q], c0});
           c0 += rows_[e];
         }
-        for (int k = Lv.sp_in_begin[q]; k < Lv.sp_in_end[q]; ++k) {
+        for (int k = Lv.sp_in_begin[q]; !hit && k < Lv.sp_in_end[q]; ++k) {
           const int e = Lv.sp_in[k];
           if (cols_[e] > 0 && mp > 0) rs.push_back({ptr_[e], ld_[e], rows_[e], cols_[e], 0, Ct, sp_ldw[q], c0});
           c0 += cols_[e];
@@ -793,14 +838,21 @@ int Tree::factorize() {
       if (ck(launch_rrqr_assemble(d_rs, (int)rs.size(), stream_), "rrqr assembly")) return -10;
       // chunk lists of the compression applies: built while the GPU runs the
       // scaling and the pivoted-QR or rank-prediction stages queued before them
-      std::vector<EdgeChunk> right, left;
+      std::vector<EdgeChunk>& right = P.right;
+      std::vector<EdgeChunk>& left = P.left;
       EdgeChunk* d_right = nullptr;
       EdgeChunk* d_left = nullptr;
       bool compress_built = false;
       auto build_compress = [&]() -> int {
         if (compress_built) return 0;
         compress_built = true;
-        for (int e : Lv.spars_edges) {
+        const bool reuse = hit && P.compress_valid;
+        if (!reuse) {
+          right.clear();
+          left.clear();
+        }
+        for (size_t ei = 0; !reuse && ei < Lv.spars_edges.size(); ++ei) {
+          const int e = Lv.spars_edges[ei];
           const Edge& E = st_.edges[e];
           const bool r = st_.clusters[E.n2].sparsify, c = st_.clusters[E.n1].sparsify;
           EdgeChunk t{};
@@ -832,6 +884,7 @@ int Tree::factorize() {
             }
           }
         }
+        P.compress_valid = true;
         if (check_descriptors) {
           const size_t es = fp32_ ? 4 : 8;
           for (const auto* lst : {&right, &left})
@@ -1178,8 +1231,17 @@ int Tree::factorize() {
         cols_[e] = size_[E.n1];
       }
       if (int rc = alloc_level_blocks(N.edges)) return rc;
-      std::vector<MergeTask> mt;
-      for (size_t q = 0; q < Lv.merge_src.size(); ++q) {
+      // the merge list also depends on the kept ranks of the level's interfaces
+      std::vector<int> mkey;
+      mkey.reserve(Lv.spars_clusters.size());
+      for (int p : Lv.spars_clusters) mkey.push_back(size_[p]);
+      const bool mreuse = hit && P.merge_valid && P.merge_key == mkey;
+      std::vector<MergeTask>& mt = P.mt;
+      if (!mreuse) {
+        mt.clear();
+        P.merge_key = std::move(mkey);
+      }
+      for (size_t q = 0; !mreuse && q < Lv.merge_src.size(); ++q) {
         const int s = Lv.merge_src[q], d = Lv.merge_dst[q];
         const Edge& E = st_.edges[s];
         MergeTask t;
@@ -1194,6 +1256,7 @@ int Tree::factorize() {
         t.identity = (E.n1 == E.n2 && st_.clusters[E.n1].sparsify) ? 1 : 0;
         if (t.rows > 0 && t.cols > 0) mt.push_back(t);
       }
+      P.merge_valid = true;
       if (check_descriptors) {
         const size_t es = fp32_ ? 4 : 8;
         for (const MergeTask& m : mt)
@@ -1206,6 +1269,7 @@ int Tree::factorize() {
       if (!d_mt) return fail(-11, "out of device memory (merge)");
       if (ck(launch_merge(d_mt, (int)mt.size(), stream_), "merge kernel")) return -10;
     }
+    P.valid = true;  // every list of the level is stored
     cudaEventRecord(ev[4], stream_);
     const double h1 = wall();
     if (ck(cudaStreamSynchronize(stream_), "factorize level")) return -10;

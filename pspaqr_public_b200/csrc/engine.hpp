@@ -26,6 +26,9 @@ class Arena {
   double* dalloc(size_t n) { return static_cast<double*>(alloc(n * sizeof(double))); }
   // forget every allocation but keep the chunks for reuse (no cudaFree)
   void reset();
+  // the allocator's state: chunk bases, fill offsets and current chunk (two
+  // equal states hand out the same addresses for the same requests)
+  void state(std::vector<const char*>& base, std::vector<size_t>& off, size_t& cur) const;
   // [p, p + bytes) lies inside one chunk
   bool contains(const void* p, size_t bytes) const;
   void release();
@@ -40,6 +43,40 @@ class Arena {
   std::vector<Chunk> chunks_;
   size_t cur_ = 0;  // chunk being filled
   size_t used_ = 0, reserved_ = 0;
+};
+
+// Descriptor lists of one level kept for the next factorization of the same
+// partition.  Every list is a deterministic function of the level's cluster
+// sizes, the flags below and the allocators' states at the level's start
+// (which fix every block, factor and scratch address the lists hold), so a
+// later factorization whose key is equal reuses them instead of rebuilding;
+// the merge list also depends on the level's kept ranks.  The allocations
+// themselves are still made in the same order, so addresses stay identical.
+struct LevelPlanKey {
+  std::vector<const char*> abase, sbase;
+  std::vector<size_t> aoff;
+  size_t acur = 0;
+  std::vector<int> sizes;
+  int flags = 0;
+  bool operator==(const LevelPlanKey& o) const {
+    return acur == o.acur && flags == o.flags && sizes == o.sizes && aoff == o.aoff && abase == o.abase &&
+           sbase == o.sbase;
+  }
+};
+struct LevelPlan {
+  bool valid = false;
+  LevelPlanKey key;
+  std::vector<UpdTask> ut;
+  std::vector<UpdOp> uo;
+  double fl_upd = 0, fl_sapp = 0;
+  std::vector<EdgeChunk> rows_scale, cols_scale;
+  std::vector<int> sp_w;
+  std::vector<RrqrSrc> rs;
+  bool compress_valid = false;
+  std::vector<EdgeChunk> right, left;
+  bool merge_valid = false;
+  std::vector<int> merge_key;  // kept ranks of the level's sparsified interfaces
+  std::vector<MergeTask> mt;
 };
 
 struct LevelTiming {
@@ -96,6 +133,10 @@ class Tree {
   // one trailing-update descriptor's block address out of the pool before the
   // check; forces check_descriptors on
   bool corrupt_next_descriptor = false;
+  // reuse a level's descriptor lists when a later factorization meets the
+  // same sizes and allocator states (LevelPlan)
+  bool plan_cache = true;
+  long long plan_hits() const { return plan_hits_; }
   // learned ranks: the sketch's pivoted QR stops at sketch_tol * tol (the
   // kept rank is then chosen on C itself)
   double sketch_tol = 0.1;
@@ -273,6 +314,8 @@ class Tree {
   size_t krylov_doubles_ = 0;
   int ensure_krylov(size_t doubles);
   std::vector<LevelTiming> lt_;
+  std::vector<LevelPlan> plans_;  // per level, cleared by partition
+  long long plan_hits_ = 0;       // levels whose lists were reused
   double flops_ = 0;
   double rrqr_bytes_ = 0;
   bool fp32_ = false;  // factor blocks hold float (set by assemble)

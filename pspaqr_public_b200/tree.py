@@ -54,6 +54,8 @@ def lib():
             "spq_set_tensor_cores": (i32, [vp, i32]),
             "spq_set_spin_limit": (i32, [vp, C.c_longlong]),
             "spq_set_checks": (i32, [vp, i32]),
+            "spq_set_plan_cache": (i32, [vp, i32]),
+            "spq_plan_hits": (C.c_longlong, [vp]),
             "spq_debug_corrupt_descriptor": (i32, [vp]),
             "spq_get_factor": (i32, [vp, i32, i32, pd, pi]),
             "spq_set_coords": (i32, [vp, i32, i32, pd]),
@@ -242,6 +244,14 @@ class ParTree:
     def set_spin_limit(self, cycles: int):
         """Cycle budget of the preconditioner apply's bounded waits (next factorize)."""
         self._chk(lib().spq_set_spin_limit(self._h, int(cycles)), "set_spin_limit")
+
+    def set_plan_cache(self, on: bool):
+        """Reuse a level's descriptor lists when a later factorize meets the same sizes."""
+        self._chk(lib().spq_set_plan_cache(self._h, int(bool(on))), "set_plan_cache")
+
+    def plan_hits(self) -> int:
+        """Levels whose descriptor lists were reused so far."""
+        return int(lib().spq_plan_hits(self._h))
 
     def set_checks(self, on: bool):
         """Host-side bounds checks of the factorization's descriptors before upload."""

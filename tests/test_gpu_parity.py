@@ -187,3 +187,50 @@ def test_reassembly_is_bit_identical():
         assert rk0 == rk1 and k0 == k1 and r0 == r1
         assert np.array_equal(B0, B1) and np.array_equal(x0, x1)
         assert r0 <= 1e-10
+
+
+@pytest.mark.parametrize("precision,learned", [(64, False), (32, True)])
+def test_reused_plans_are_bit_identical(precision, learned):
+    """A re-factorization that meets the same sizes reuses every level's
+    descriptor lists; its factors, apply and GMRES are bit-identical to a
+    factorization that rebuilds them.  A new tolerance changes the kept ranks:
+    the levels above the first changed rank rebuild their lists, and the result
+    equals an uncached factorization at that tolerance."""
+    from pspaqr_public_b200.tree import load_rank_model
+
+    cp, ri, v = _matrix("diff", 16, 3)
+    b = random_reference(16 ** 3, 9)
+
+    def run(cache, tol, reps):
+        t = ParTree(6, 0)
+        t.set_tol(tol)
+        t.set_coords_tensor(16, 3)
+        t.set_precision(precision)
+        t.set_plan_cache(cache)
+        t.partition((cp, ri, scale_columns(cp, v)))
+        if learned:
+            t.set_rank_model(load_rank_model(), 32)
+        outs = []
+        for tol_i in tol if isinstance(tol, list) else [tol] * reps:
+            t.set_tol(tol_i)
+            t.assemble()
+            t.factorize()
+            top = len(t.clusters()) - 1
+            x = t.solve_inplace(b.copy())
+            k, rr = dist_gmres(None, b.copy(), t, 100, 1e-10)
+            outs.append((t.block(top, top), x, k, rr, [c["rank"] for c in t.clusters()]))
+        return t, outs
+
+    t, cached = run(True, 1e-2, 3)
+    assert t.plan_hits() == 2 * 6  # every level of the 2nd and 3rd factorization
+    _, fresh = run(False, 1e-2, 1)
+    for B, x, k, rr, rk in cached:
+        B0, x0, k0, rr0, rk0 = fresh[0]
+        assert rk == rk0 and k == k0 and rr == rr0
+        assert np.array_equal(B, B0) and np.array_equal(x, x0)
+    t2, mixed = run(True, [1e-2, 1e-3], 0)
+    assert t2.plan_hits() < 6
+    _, fresh3 = run(False, 1e-3, 1)
+    B, x, k, rr, rk = mixed[1]
+    B0, x0, k0, rr0, rk0 = fresh3[0]
+    assert rk == rk0 and k == k0 and np.array_equal(B, B0) and np.array_equal(x, x0)
