@@ -68,6 +68,14 @@ int spq_set_precision(spq_tree* t, int bits);
  * in FP32 on the CUDA cores.  No effect on FP64 factors.  Takes effect at the
  * next factorize. */
 int spq_set_tensor_cores(spq_tree* t, int on);
+/* Diagnostic of the tensor-core operand layouts (no reference counterpart):
+ * runs the two GEMMs of one panel apply once, on host inputs C (m x 64,
+ * column-major, ld m, m <= 64), V (m x 32, ld m) and W2 (32 x 64, ld 32), and
+ * returns every TMEM lane: out1 (128 x 32, row = lane) holds C^T V (M = 64
+ * layout), out2 (128 x 64) holds V W2.  flags (0..15) swap the leading and
+ * stride byte offsets of the descriptors (bit 0 / 1: first GEMM A / B, bit 2 /
+ * 3: second GEMM A / B). */
+int spq_debug_tc_probe(const float* C, const float* V, const float* W2, int m, int flags, float* out1, float* out2);
 /* Reuse of descriptor lists across factorizations of one partition (no
  * reference counterpart; the reference rebuilds its task graph every time,
  * ptree.cpp:885-2123).  A level's lists depend only on its cluster sizes and on

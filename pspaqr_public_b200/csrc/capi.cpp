@@ -101,6 +101,32 @@ int spq_debug_corrupt_descriptor(spq_tree* h) {
   return 0;
 }
 
+int spq_debug_tc_probe(const float* C, const float* V, const float* W2, int m, int flags, float* out1, float* out2) {
+  if (!C || !V || !W2 || !out1 || !out2 || m < 1 || m > 64 || flags < 0 || flags > 15) return -1;
+  float* d = nullptr;
+  int* st = nullptr;
+  const size_t nc = (size_t)m * 64, nv = (size_t)m * 32, nw = 32 * 64, n1 = 128 * 32, n2 = 128 * 64;
+  if (cudaMalloc(&d, sizeof(float) * (nc + nv + nw + n1 + n2)) != cudaSuccess) return -11;
+  if (cudaMalloc(&st, sizeof(int)) != cudaSuccess) {
+    cudaFree(d);
+    return -11;
+  }
+  float *dC = d, *dV = dC + nc, *dW = dV + nv, *d1 = dW + nw, *d2 = d1 + n1;
+  cudaMemset(st, 0, sizeof(int));
+  cudaMemcpy(dC, C, sizeof(float) * nc, cudaMemcpyHostToDevice);
+  cudaMemcpy(dV, V, sizeof(float) * nv, cudaMemcpyHostToDevice);
+  cudaMemcpy(dW, W2, sizeof(float) * nw, cudaMemcpyHostToDevice);
+  cudaError_t e = spq::launch_tc_probe(dC, dV, dW, m, flags, d1, d2, st, nullptr);
+  if (!e) e = cudaDeviceSynchronize();
+  int status = 0;
+  if (!e) e = cudaMemcpy(out1, d1, sizeof(float) * n1, cudaMemcpyDeviceToHost);
+  if (!e) e = cudaMemcpy(out2, d2, sizeof(float) * n2, cudaMemcpyDeviceToHost);
+  if (!e) e = cudaMemcpy(&status, st, sizeof(int), cudaMemcpyDeviceToHost);
+  cudaFree(d);
+  cudaFree(st);
+  return e ? -10 : (status ? -12 : 0);
+}
+
 int spq_set_tensor_cores(spq_tree* h, int on) {
   if (!h || on < 0 || on > 1) return -1;
   h->t->tensor_cores = on != 0;

@@ -266,6 +266,15 @@ __global__ void __launch_bounds__(kThreads, 2) k_edge_left_tc(const EdgeChunk* _
   tc::end(x);
 }
 
+// the operand-layout diagnostic of tc_apply.cuh (one CTA)
+__global__ void __launch_bounds__(kThreads, 1) k_tc_probe(const float* C, const float* V, const float* W2, int m,
+                                                       int flags, float* out1, float* out2, int* status) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  tc::Ctx x = tc::begin(smraw, status);
+  tc::probe(x, C, V, W2, m, flags, out1, out2);
+  tc::end(x);
+}
+
 // k_edge_right on the tensor cores (float factors): rows [lo, lo+cnt) of A <- A Q
 __global__ void __launch_bounds__(kThreads, 2) k_edge_right_tc(const EdgeChunk* __restrict__ tasks, int* status) {
   extern __shared__ __align__(16) unsigned char smraw[];
@@ -1397,6 +1406,16 @@ cudaError_t launch_edge(int kind, const EdgeChunk* t, int ntasks, cudaStream_t s
   }
   return g_fp32 ? go(k_edge_left<float>, k_edge_trsm<float>, k_edge_right<float>)
                 : go(k_edge_left<double>, k_edge_trsm<double>, k_edge_right<double>);
+}
+
+cudaError_t launch_tc_probe(const float* C, const float* V, const float* W2, int m, int flags, float* out1,
+                            float* out2, int* status, cudaStream_t st) {
+  if (cudaError_t pre = begin("launch_tc_probe")) return pre;
+  if (m < 1 || m > 64) return cudaErrorInvalidValue;
+  if (cudaError_t e = prep(k_tc_probe, tc::kSmemBytes)) return e;
+  counted();
+  k_tc_probe<<<1, kThreads, tc::kSmemBytes, st>>>(C, V, W2, m, flags, out1, out2, status);
+  return last();
 }
 
 size_t rrqr_smem(int mmax, int kmax, int nlmax, int rcmax, size_t c_doubles) {

@@ -29,6 +29,9 @@ bool tensor_cores();
 // bit 2 (value 2) a tensor-core wait ran out, 4 a non-finite pivot, 8 a zero
 // pivot in a QR factorization (elimination chains, scaling QR).
 void set_status_word(int* status);
+// Diagnostic of the tensor-core operand layouts (tc_apply.cuh tc::probe).
+cudaError_t launch_tc_probe(const float* C, const float* V, const float* W2, int m, int flags, float* out1,
+                            float* out2, int* status, cudaStream_t st);
 // n doubles -> n floats stored at dst, and back (vectors, factors)
 cudaError_t launch_to_f32(long long n, const double* src, double* dst, cudaStream_t st);
 cudaError_t launch_to_f64(long long n, const double* src, double* dst, cudaStream_t st);

@@ -152,6 +152,23 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, float (&v)[32]) {
   for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
 }
 
+// 32 lanes x 32 consecutive 32-bit columns of tensor memory from v.
+__device__ __forceinline__ void tmem_st32(uint32_t taddr, const float (&v)[32]) {
+  uint32_t r[32];
+#pragma unroll
+  for (int i = 0; i < 32; ++i) r[i] = __float_as_uint(v[i]);
+  asm volatile(
+      "tcgen05.st.sync.aligned.32x32b.x32.b32 [%0], "
+      "{%1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, %16, "
+      "%17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31, %32};" ::"r"(taddr),
+      "r"(r[0]), "r"(r[1]), "r"(r[2]), "r"(r[3]), "r"(r[4]), "r"(r[5]), "r"(r[6]), "r"(r[7]), "r"(r[8]), "r"(r[9]),
+      "r"(r[10]), "r"(r[11]), "r"(r[12]), "r"(r[13]), "r"(r[14]), "r"(r[15]), "r"(r[16]), "r"(r[17]), "r"(r[18]),
+      "r"(r[19]), "r"(r[20]), "r"(r[21]), "r"(r[22]), "r"(r[23]), "r"(r[24]), "r"(r[25]), "r"(r[26]), "r"(r[27]),
+      "r"(r[28]), "r"(r[29]), "r"(r[30]), "r"(r[31])
+      : "memory");
+  asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
+}
+
 // ---------------------------------------------------------------- context
 // Per-CTA state: shared-memory buffers, the TMEM allocation, the mbarrier's
 // phase and the error state.  Created by begin() (all threads), released by
@@ -438,6 +455,80 @@ __device__ void left_qt(Ctx& x, const float* V, int ldv, const float* Tm, int ld
   }
   fence_before();
   __syncthreads();  // the buffers and accumulators are free for the next panel
+}
+
+// ---------------------------------------------------------------- layout probe
+// Diagnostic of the operand layouts (one CTA): stages C (m <= 64 rows x 64
+// columns, ld m) and V (m x 32, ld m) exactly as left_qt does, runs the first
+// GEMM (D1 = C^T V, M = 64) into TMEM columns 0..31 and the second (D2 = V W2
+// with W2 32 x 64, ld 32, M = 128) into columns 64..127, and dumps every TMEM
+// lane: out1 (128 x 32) and out2 (128 x 64), row = lane.  TMEM is zeroed first,
+// so lanes an MMA does not write read 0.  flags bit b swaps the leading and
+// stride byte offsets of: 0 the first GEMM's A, 1 its B, 2 the second GEMM's A,
+// 3 its B.  Every variant reads inside the staged buffers.
+__device__ void probe(Ctx& x, const float* C, const float* V, const float* W2, int m, int flags, float* out1,
+                      float* out2) {
+  unsigned char* sm = x.sm;
+  const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+  const uint32_t base = saddr(sm);
+  if (warp < 4) {
+    float z[32];
+#pragma unroll
+    for (int i = 0; i < 32; ++i) z[i] = 0.f;
+    for (int c0 = 0; c0 < 128; c0 += 32) tmem_st32(x.tmem + ((uint32_t)(32 * warp) << 16) + c0, z);
+  }
+  for (int idx = t; idx < 64 * 64; idx += kThreads) {
+    const int r = idx & 63, c = idx >> 6;
+    const float v = r < m ? C[r + (size_t)c * m] : 0.f, hi = tf32_hi(v);
+    *reinterpret_cast<float*>(sm + kOffChi + c_off(r, c)) = hi;
+    *reinterpret_cast<float*>(sm + kOffClo + c_off(r, c)) = v - hi;
+  }
+  for (int idx = t; idx < kVRows * 32; idx += kThreads) {
+    const int r = idx & (kVRows - 1), i = idx >> 7;
+    const float v = r < m ? V[r + (size_t)i * m] : 0.f, hi = tf32_hi(v);
+    *reinterpret_cast<float*>(sm + kOffVhi + v_off(r, i)) = hi;
+    *reinterpret_cast<float*>(sm + kOffVlo + v_off(r, i)) = v - hi;
+  }
+  for (int idx = t; idx < 32 * 64; idx += kThreads) {
+    const int i = idx & 31, c = idx >> 5;
+    const float v = W2[i + (size_t)c * 32], hi = tf32_hi(v);
+    *reinterpret_cast<float*>(sm + kOffWhi + w_off(c, i)) = hi;
+    *reinterpret_cast<float*>(sm + kOffWlo + w_off(c, i)) = v - hi;
+  }
+  fence_smem_async();
+  fence_before();
+  __syncthreads();
+  auto d = [&](uint32_t a, int lbo, int sbo, bool swap) { return swap ? sdesc(a, sbo, lbo) : sdesc(a, lbo, sbo); };
+  if (t == 0) {
+    fence_after();
+    constexpr uint32_t kId1 = idesc_tf32(64, 32, 0, 0), kId2 = idesc_tf32(128, 64, 1, 0);
+    for (int ks = 0; ks < (m + 7) / 8; ++ks) {
+      const uint32_t ah = base + kOffChi + 2 * ks * kCChunk, al = base + kOffClo + 2 * ks * kCChunk;
+      const uint32_t bh = base + kOffVhi + 2 * ks * kVChunk, bl = base + kOffVlo + 2 * ks * kVChunk;
+      mma(x.tmem, d(ah, kCChunk, kCGroup, flags & 1), d(bh, kVChunk, kVGroup, flags & 2), kId1, ks > 0);
+      mma(x.tmem, d(ah, kCChunk, kCGroup, flags & 1), d(bl, kVChunk, kVGroup, flags & 2), kId1, 1u);
+      mma(x.tmem, d(al, kCChunk, kCGroup, flags & 1), d(bh, kVChunk, kVGroup, flags & 2), kId1, 1u);
+    }
+    for (int ks = 0; ks < 4; ++ks) {
+      const uint32_t ah = base + kOffVhi + ks * kVGroup, al = base + kOffVlo + ks * kVGroup;
+      const uint32_t bh = base + kOffWhi + 2 * ks * kWChunk, bl = base + kOffWlo + 2 * ks * kWChunk;
+      mma(x.tmem + 64, d(ah, kVGroup, kVChunk, flags & 4), d(bh, kWChunk, kWGroup, flags & 8), kId2, ks > 0);
+      mma(x.tmem + 64, d(ah, kVGroup, kVChunk, flags & 4), d(bl, kWChunk, kWGroup, flags & 8), kId2, 1u);
+      mma(x.tmem + 64, d(al, kVGroup, kVChunk, flags & 4), d(bh, kWChunk, kWGroup, flags & 8), kId2, 1u);
+    }
+    commit(x.bar);
+  }
+  wait_mma(x);
+  if (warp < 4 && !x.failed) {
+    const int row = 32 * warp + lane;
+    float v[32];
+    tmem_ld32(x.tmem + ((uint32_t)(32 * warp) << 16), v);
+    for (int j = 0; j < 32; ++j) out1[(size_t)row * 32 + j] = v[j];
+    for (int h = 0; h < 2; ++h) {
+      tmem_ld32(x.tmem + ((uint32_t)(32 * warp) << 16) + 64 + 32 * h, v);
+      for (int j = 0; j < 32; ++j) out2[(size_t)row * 64 + 32 * h + j] = v[j];
+    }
+  }
 }
 
 }  // namespace tc

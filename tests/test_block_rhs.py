@@ -43,8 +43,10 @@ def test_block_apply_equals_single_applies():
     n = N * N
     B = M.rhs_normal(n, 4, NRHS)
     X = torch.from_numpy(np.ascontiguousarray(B.T)).cuda()  # column r = row r of X (contiguous)
+    torch.cuda.synchronize()
     rc = lib().spq_solve_block_device(t._h, C.c_void_p(X.data_ptr()), NRHS, n)
     assert rc == 0, lib().spq_last_error(t._h)
+    torch.cuda.synchronize()  # the library runs on its own stream
     Xb = X.cpu().numpy()
     for r in range(NRHS):
         x = t.solve_inplace(np.ascontiguousarray(B[:, r]))
