@@ -269,6 +269,11 @@ int spq_rank_model_size(int* nparams, int* nfeatures);
  * standardise the features); params = NULL restores the plain pivoted QR.
  * Resets the counters of spq_learned_counts. */
 int spq_set_rank_model(spq_tree* t, const float* params, const float* mean, const float* stdev, int oversample);
+/* Margin (0..1, default 0) added to the predicted kept fraction before the
+ * sketch is sized: ell = ceil(min(pred + margin, 1) min(m, w)) + oversample.
+ * An upper quantile of the predictor's error on its training pairs keeps the
+ * fallback rate near the quantile's complement. */
+int spq_set_rank_margin(spq_tree* t, float margin);
 /* Tuning of the learned path: the sketch's pivoted QR stops at
  * sketch_tol * tol (default 0.1); smem = 1 holds each CTA's block of the
  * sketch in shared memory when it fits (default 0: reads it from global memory,

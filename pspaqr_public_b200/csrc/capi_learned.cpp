@@ -56,6 +56,12 @@ int spq_set_rank_model(spq_tree* h, const float* params, const float* mean, cons
   return rc;
 }
 
+int spq_set_rank_margin(spq_tree* h, float margin) {
+  if (!h || !(margin >= 0.0f && margin <= 1.0f)) return -1;
+  h->t->rank_margin = margin;
+  return 0;
+}
+
 int spq_set_sketch_tuning(spq_tree* h, double sketch_tol, int smem) {
   if (!h || !(sketch_tol > 0 && sketch_tol <= 1)) return -1;
   h->t->sketch_tol = sketch_tol;

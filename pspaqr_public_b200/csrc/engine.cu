@@ -943,7 +943,8 @@ int Tree::factorize() {
                "rank features"))
           return -10;
         if (rank_model_) {
-          RankModel model{d_model_, d_model_ + kMlpParams, d_model_ + kMlpParams + kRankFeatures, oversample_};
+          RankModel model{d_model_, d_model_ + kMlpParams, d_model_ + kMlpParams + kRankFeatures, oversample_,
+                          rank_margin};
           if (ck(launch_rank_predict(d_sk, (int)nsp, model, stream_), "rank prediction")) return -10;
           if (int rc = build_compress()) return rc;
         }

@@ -143,6 +143,9 @@ class Tree {
   // the sketch's pivoted QR holds each CTA's block of the sketch in shared
   // memory when it fits
   bool sketch_smem = false;
+  // learned ranks: added to the predicted kept fraction before the sketch is
+  // sized (an upper quantile of the predictor's error on its training pairs)
+  float rank_margin = 0.0f;
 
   int set_coords(int dim, int n, const double* X);
   int set_coords_tensor(int n, int d);

@@ -234,7 +234,8 @@ __global__ void k_rank_predict(const SketchTask* __restrict__ tasks, int ntasks,
   const int kmin = t.m < t.w ? t.m : t.w;
   float x[kRankFeatures];
   for (int f = 0; f < kRankFeatures; ++f) x[f] = (t.feat[f] - model.mean[f]) / model.stdev[f];
-  const float p = mlp_forward(model.params, x);
+  float p = mlp_forward(model.params, x) + model.margin;
+  p = p < 1.0f ? p : 1.0f;
   int ell = (int)ceilf(p * (float)kmin) + model.oversample;
   ell = ell < 1 ? 1 : ell;
   *t.ell = kmin < ell ? kmin : ell;

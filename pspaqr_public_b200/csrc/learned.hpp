@@ -74,6 +74,7 @@ struct RankModel {
   const float* mean;    // kRankFeatures
   const float* stdev;   // kRankFeatures
   int oversample;
+  float margin;  // added to the predicted kept fraction before sizing the sketch
 };
 
 // Features in two launches: per block of kFeatCols columns of an interface

@@ -84,9 +84,39 @@ def constant_model(mean_y, nf):
     return {"params": p, "mean": np.zeros(F, np.float32), "std": np.ones(F, np.float32)}
 
 
-def evaluate(model, const, seeds, tols, n=64, oversample=OVERSAMPLE):
+def calibrate(model, mean_y, seeds, tols, q=0.95, n=64):
+    """Sketch margins per tolerance: the q-quantile of (kept fraction - prediction)
+    over the plain factorizations' pairs of the training seeds, for the network
+    and for the constant predictor (prediction = training mean)."""
+    out, cout = {}, {}
+    for tol in tols:
+        feats, ys = [], []
+        for s in seeds:
+            t = make_tree(n, "binary", s)
+            t.set_tol(tol)
+            t.set_rank_log(True)
+            t.assemble()
+            t.factorize()
+            log = t.rank_log()
+            feats.append(log["features"])
+            ys.append(log["rank"] / np.maximum(log["kmin"], 1))
+            del t
+        X = np.concatenate(feats)
+        y = np.concatenate(ys)
+        p = T.mlp_predict(model["params"], (X - model["mean"]) / model["std"])
+        out[repr(tol)] = float(max(np.quantile(y - p, q), 0.0))
+        cout[repr(tol)] = float(max(np.quantile(y - mean_y, q), 0.0))
+        print(f"calibration tol {tol}: {len(y)} pairs, margin {out[repr(tol)]:.4f} (network), "
+              f"{cout[repr(tol)]:.4f} (constant)", flush=True)
+    return out, cout
+
+
+def evaluate(model, const, seeds, tols, n=64, oversample=OVERSAMPLE, margins=None, cmargins=None):
     rows = []
     for tol in tols:
+        if margins is not None:
+            model = dict(model, margin=margins[repr(tol)])
+            const = dict(const, margin=cmargins[repr(tol)])
         agg = {"tol": tol, "interfaces": 0}
         for name in ("plain", "learned", "constant"):
             agg[name + "_s"] = 0.0
@@ -120,6 +150,7 @@ def evaluate(model, const, seeds, tols, n=64, oversample=OVERSAMPLE):
         N = max(agg["interfaces"], 1)
         rows.append({
             "tol": tol, "interfaces": agg["interfaces"], "oversample": oversample,
+            "margin": model.get("margin", 0.0), "constant_margin": const.get("margin", 0.0),
             "learned": {"within2": agg["within2"] / N, "fallback_rate": agg["fallback"] / N,
                         "sketch_columns": agg["sketch_cols"], "factorize_s": agg["learned_s"] / len(seeds)},
             "constant": {"within2": agg["c_within2"] / N, "fallback_rate": agg["c_fallback"] / N,
@@ -142,6 +173,9 @@ def main():
     ap.add_argument("--oversample", type=int, default=OVERSAMPLE,
                     help="sketch columns beyond the predicted rank in the evaluation")
     ap.add_argument("--report", default="report.json", help="report file name (in --out)")
+    ap.add_argument("--calibrate", default="",
+                    help="training seeds (e.g. 10-19) to calibrate the sketch margins on; stored in the model's meta")
+    ap.add_argument("--quantile", type=float, default=0.95, help="quantile of the calibrated margins")
     args = ap.parse_args()
 
     def rng(s):
@@ -149,12 +183,21 @@ def main():
         return list(range(a, b + 1))
 
     if args.eval_only:
-        z = np.load(os.path.join(args.out, "rank_mlp.npz"))
+        path = os.path.join(args.out, "rank_mlp.npz")
+        z = np.load(path)
         meta = json.loads(str(z["meta"]))
         model = {k: z[k].astype(np.float32) for k in ("params", "mean", "std")}
         const = constant_model(meta["mean_target"], len(model["mean"]))
+        if args.calibrate:
+            m, c = calibrate(model, meta["mean_target"], rng(args.calibrate), TOLS, args.quantile)
+            meta.update(margin_by_tol=m, const_margin_by_tol=c, margin_quantile=args.quantile,
+                        margin_seeds=args.calibrate)
+            np.savez(path, params=model["params"], mean=model["mean"], std=model["std"], loss=z["loss"],
+                     meta=json.dumps(meta))
+        margins = meta.get("margin_by_tol")
         report = {"meta": meta, "loss": z["loss"].tolist(),
-                  "eval": evaluate(model, const, rng(args.eval_seeds), TOLS, oversample=args.oversample)}
+                  "eval": evaluate(model, const, rng(args.eval_seeds), TOLS, oversample=args.oversample,
+                                   margins=margins, cmargins=meta.get("const_margin_by_tol"))}
         with open(os.path.join(args.out, args.report), "w") as f:
             json.dump(report, f, indent=1)
         return

@@ -10,6 +10,7 @@ unloadable library raises.
 from __future__ import annotations
 
 import ctypes as C
+import json
 import os
 from typing import Optional
 
@@ -75,6 +76,7 @@ def lib():
             "spq_set_rank_model": (i32, [vp, pf, pf, pf, i32]),
             "spq_learned_counts": (i32, [vp, C.POINTER(C.c_longlong)]),
             "spq_set_sketch_tuning": (i32, [vp, f64, i32]),
+            "spq_set_rank_margin": (i32, [vp, f32]),
             "spq_set_rank_log": (i32, [vp, i32]),
             "spq_rank_log_count": (i32, [vp]),
             "spq_rank_log": (i32, [vp, pf, pi, pi, pi]),
@@ -277,6 +279,7 @@ class ParTree:
         m = self._model
         self._chk(lib().spq_set_rank_model(self._h, _pf(m["params"]), _pf(m["mean"]), _pf(m["std"]), oversample),
                   "set_rank_model")
+        self._chk(lib().spq_set_rank_margin(self._h, float(model.get("margin", 0.0))), "set_rank_margin")
 
     def set_sketch_tuning(self, sketch_tol: float = 0.1, smem: bool = False):
         """Stop of the sketch's pivoted QR (x tol) and its shared-memory mode."""
@@ -549,8 +552,17 @@ def mlp_init(seed: int = 0):
     return p
 
 
-def load_rank_model(path: Optional[str] = None) -> dict:
-    """The trained rank model shipped with the package (rank_model/rank_mlp.npz)."""
+def load_rank_model(path: Optional[str] = None, tol: Optional[float] = None) -> dict:
+    """The trained rank model shipped with the package (rank_model/rank_mlp.npz).
+    With ``tol``, the sketch margin calibrated for the nearest training tolerance
+    (``margin``: an upper quantile of the network's error on its training pairs)
+    comes with it; without, the margin is 0."""
     path = path or os.path.join(_HERE, "rank_model", "rank_mlp.npz")
     z = np.load(path)
-    return {k: z[k].astype(np.float32) for k in ("params", "mean", "std")}
+    out = {k: z[k].astype(np.float32) for k in ("params", "mean", "std")}
+    meta = json.loads(str(z["meta"])) if "meta" in z.files else {}
+    if tol is not None and meta.get("margin_by_tol"):
+        tols = [float(k) for k in meta["margin_by_tol"]]
+        near = min(tols, key=lambda x: abs(np.log10(x) - np.log10(tol)))
+        out["margin"] = float(meta["margin_by_tol"][repr(near) if repr(near) in meta["margin_by_tol"] else str(near)])
+    return out
