@@ -428,13 +428,22 @@ int Tree::factorize() {
     bool hit = false;
     {
       LevelPlanKey key;
-      arena_.state(key.abase, key.aoff, key.acur);
+      std::vector<const char*> abase, sbase;
       std::vector<size_t> soff;
       size_t scur = 0;
-      scratch_.state(key.sbase, soff, scur);
+      arena_.state(abase, key.aoff, key.acur);
+      scratch_.state(sbase, soff, scur);
+      // the chunks up to the current one (later ones are still empty)
+      const size_t na = std::min(abase.size(), key.acur + 1);
+      key.abase.assign(abase.begin(), abase.begin() + na);
+      key.aoff.resize(na);
+      key.sbase.assign(sbase.begin(), sbase.begin() + std::min<size_t>(sbase.size(), 1));
       key.sizes.assign(size_.begin() + Lv.first, size_.begin() + Lv.first + Lv.count);
       key.flags = (fp32_ ? 1 : 0) | (rank_model_ ? 2 : 0) | (rank_log_ ? 4 : 0) | (verbose >= 2 ? 8 : 0);
-      hit = plan_cache && P.valid && P.key == key;
+      auto prefix = [](const std::vector<const char*>& have, const std::vector<const char*>& rec) {
+        return have.size() >= rec.size() && std::equal(rec.begin(), rec.end(), have.begin());
+      };
+      hit = plan_cache && P.valid && P.key == key && prefix(abase, P.abase_end) && prefix(sbase, P.sbase_end);
       if (!hit) {
         P = LevelPlan();
         P.key = std::move(key);
@@ -1270,7 +1279,13 @@ int Tree::factorize() {
       if (!d_mt) return fail(-11, "out of device memory (merge)");
       if (ck(launch_merge(d_mt, (int)mt.size(), stream_), "merge kernel")) return -10;
     }
-    P.valid = true;  // every list of the level is stored
+    if (!P.valid) {  // every list of the level is stored
+      std::vector<size_t> off;
+      size_t cur = 0;
+      arena_.state(P.abase_end, off, cur);
+      scratch_.state(P.sbase_end, off, cur);
+      P.valid = true;
+    }
     cudaEventRecord(ev[4], stream_);
     const double h1 = wall();
     if (ck(cudaStreamSynchronize(stream_), "factorize level")) return -10;

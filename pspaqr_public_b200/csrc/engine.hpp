@@ -65,7 +65,10 @@ struct LevelPlanKey {
 };
 struct LevelPlan {
   bool valid = false;
-  LevelPlanKey key;
+  LevelPlanKey key;  // allocator chunks up to the current one, sizes, flags
+  // chunk bases of both allocators once the level was planned: a later run
+  // whose chunk lists start with these lands every allocation at the same place
+  std::vector<const char*> abase_end, sbase_end;
   std::vector<UpdTask> ut;
   std::vector<UpdOp> uo;
   double fl_upd = 0, fl_sapp = 0;

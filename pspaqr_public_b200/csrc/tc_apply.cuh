@@ -36,34 +36,52 @@ using dev::kNB;
 using dev::kThreads;
 
 // ---------------------------------------------------------------- layouts (bytes)
-constexpr int kVRows = 128;                   // rows of the V buffer (one M = 128 tile)
-constexpr int kVGroup = 128;                  // 8 reflectors x 16 B
-constexpr int kVChunk = 4 * kVGroup + 16;     // one 4-row chunk of all 32 reflectors, padded
-constexpr int kVBytes = (kVRows / 4) * kVChunk;
-constexpr int kCRows = 64;                    // rows of a staged C tile (first GEMM)
-constexpr int kCGroup = 128;                  // 8 columns x 16 B
-constexpr int kCChunk = 8 * kCGroup + 16;     // one 4-row chunk of all 64 columns, padded
-constexpr int kCBytes = (kCRows / 4) * kCChunk;
-constexpr int kWChunk = 128;                  // 4 reflectors x 8 columns x 4 B... (one core matrix)
-constexpr int kWGroup = 8 * kWChunk;          // 8 columns x all 32 reflectors
+// Every operand is K-major (no-swizzle canonical layout: core matrices of 8
+// rows x 16 bytes, the 16 bytes holding 4 consecutive K elements).  V is kept
+// twice: VR with K = rows (B operand of the first GEMM) and VI with K =
+// reflectors (A operand of the second).  Tiles are 64 rows; both GEMMs use
+// M = 64 (accumulator rows r at TMEM lanes (r % 16) + 32 (r / 16)).
+constexpr int kRows = 64;                     // rows of a staged tile
+constexpr int kVGroup = 128;                  // VR: 8 reflectors x 16 B
+constexpr int kVChunk = 4 * kVGroup + 16;     // VR: one 4-row chunk of all 32 reflectors, padded
+constexpr int kVBytes = (kRows / 4) * kVChunk;
+constexpr int kIChunk = 128;                  // VI: 8 rows x 4 reflectors
+constexpr int kIGroup = 8 * kIChunk;          // VI: 8 rows x all 32 reflectors
+constexpr int kIBytes = (kRows / 8) * kIGroup;
+constexpr int kCGroup = 128;                  // C: 8 columns x 16 B
+constexpr int kCChunk = 8 * kCGroup + 16;     // C: one 4-row chunk of all 64 columns, padded
+constexpr int kCBytes = (kRows / 4) * kCChunk;
+constexpr int kWChunk = 128;                  // W2^T: 8 columns x 4 reflectors
+constexpr int kWGroup = 8 * kWChunk;          // W2^T: 8 columns x all 32 reflectors
 constexpr int kWBytes = 8 * kWGroup;          // 64 columns
 constexpr int kOffVhi = 0;
 constexpr int kOffVlo = kOffVhi + kVBytes;
-constexpr int kOffChi = kOffVlo + kVBytes;
+constexpr int kOffIhi = kOffVlo + kVBytes;
+constexpr int kOffIlo = kOffIhi + kIBytes;
+constexpr int kOffChi = kOffIlo + kIBytes;
 constexpr int kOffClo = kOffChi + kCBytes;
 constexpr int kOffWhi = kOffClo + kCBytes;
 constexpr int kOffWlo = kOffWhi + kWBytes;
 constexpr int kOffT = kOffWlo + kWBytes;            // T (32 x 33 floats), then W (32 x 64 floats)
 constexpr int kOffWs = kOffT + kNB * (kNB + 1) * 4;
 constexpr int kOffBar = kOffWs + kNB * 64 * 4;      // mbarrier (8 B) + TMEM address (4 B)
-constexpr int kSmemBytes = kOffBar + 64 + 2048;     // + slack beyond every descriptor's reach
+constexpr int kSmemBytes = kOffBar + 256;
 constexpr uint32_t kTmemCols = 128;                 // two 64-column accumulators
-static_assert(kOffVlo % 16 == 0 && kOffChi % 16 == 0 && kOffClo % 16 == 0 && kOffWhi % 16 == 0 &&
-                  kOffWlo % 16 == 0 && kOffT % 16 == 0 && kOffBar % 16 == 0,
+static_assert(kOffVlo % 16 == 0 && kOffIhi % 16 == 0 && kOffIlo % 16 == 0 && kOffChi % 16 == 0 &&
+                  kOffClo % 16 == 0 && kOffWhi % 16 == 0 && kOffWlo % 16 == 0 && kOffT % 16 == 0 &&
+                  kOffBar % 16 == 0,
               "UMMA operands start on 16-byte boundaries");
+static_assert(2 * kSmemBytes + 2048 <= 228 * 1024, "two CTAs per SM");
 
+// VR (K = rows): element (r, i); a warp storing 32 consecutive rows of one
+// reflector hits 32 distinct banks (the 16-byte pad of kVChunk)
 __host__ __device__ constexpr int v_off(int r, int i) {
   return (r >> 2) * kVChunk + (i >> 3) * kVGroup + (i & 7) * 16 + (r & 3) * 4;
+}
+// VI (K = reflectors): element (r, i); 16-byte stores of 4 consecutive
+// reflectors by 8 consecutive rows fill one core matrix
+__host__ __device__ constexpr int vi_off(int r, int i) {
+  return (r >> 3) * kIGroup + (i >> 2) * kIChunk + (r & 7) * 16 + (i & 3) * 4;
 }
 __host__ __device__ constexpr int c_off(int r, int c) {
   return (r >> 2) * kCChunk + (c >> 3) * kCGroup + (c & 7) * 16 + (r & 3) * 4;
@@ -258,11 +276,6 @@ __device__ void left_qt(Ctx& x, const float* V, int ldv, const float* Tm, int ld
     if (unit) return gr == i ? 1.f : (gr < i ? 0.f : V[gr + (size_t)i * ldv]);
     return V[gr + (size_t)i * ldv];
   };
-  // ---- first GEMM over 64-row tiles: D1 (TMEM lanes by the M = 64 layout,
-  // columns 0..31) = C^T V.  Tile rt goes to V buffer rows 64 (rt & 1) ..
-  const int nt1 = (m + kCRows - 1) / kCRows;
-  constexpr int kLC = kCRows * 64 / kThreads, kLV = kCRows * kNB / kThreads;
-  float rc[kLC], rv[kLV];
   // element (r, c) of the operand; a warp reads consecutive addresses (rows of
   // C, or columns of the transposed operand)
   auto cidx = [&](int idx, int& r, int& c) {
@@ -270,27 +283,24 @@ __device__ void left_qt(Ctx& x, const float* V, int ldv, const float* Tm, int ld
       c = idx & 63;
       r = idx >> 6;
     } else {
-      r = idx & (kCRows - 1);
+      r = idx & (kRows - 1);
       c = idx >> 6;
     }
   };
   auto cptr = [&](int r, int c) { return kTrans ? C + c + (size_t)r * ldc : C + r + (size_t)c * ldc; };
-  auto load1 = [&](int rt) {
-    const int r0 = rt * kCRows;
+  const int nt = (m + kRows - 1) / kRows;
+  constexpr int kLC = kRows * 64 / kThreads;
+  float rc[kLC], rv[8];
+  auto loadc = [&](int rt) {
+    const int r0 = rt * kRows;
 #pragma unroll
     for (int q = 0; q < kLC; ++q) {
       int r, c;
       cidx(t + q * kThreads, r, c);
       rc[q] = (r0 + r < m && c < nc) ? *cptr(r0 + r, c) : 0.f;
     }
-#pragma unroll
-    for (int q = 0; q < kLV; ++q) {
-      const int idx = t + q * kThreads, r = idx & (kCRows - 1), i = idx >> 6;
-      rv[q] = vval(r0 + r, i);
-    }
   };
-  auto store1 = [&](int rt) {
-    const int vr = (rt & 1) * kCRows;
+  auto storec = [&]() {
 #pragma unroll
     for (int q = 0; q < kLC; ++q) {
       int r, c;
@@ -299,35 +309,64 @@ __device__ void left_qt(Ctx& x, const float* V, int ldv, const float* Tm, int ld
       *reinterpret_cast<float*>(sm + kOffChi + c_off(r, c)) = hi;
       *reinterpret_cast<float*>(sm + kOffClo + c_off(r, c)) = rc[q] - hi;
     }
-#pragma unroll
-    for (int q = 0; q < kLV; ++q) {
-      const int idx = t + q * kThreads, r = idx & (kCRows - 1), i = idx >> 6;
-      const float hi = tf32_hi(rv[q]);
-      *reinterpret_cast<float*>(sm + kOffVhi + v_off(vr + r, i)) = hi;
-      *reinterpret_cast<float*>(sm + kOffVlo + v_off(vr + r, i)) = rv[q] - hi;
-    }
-    fence_smem_async();
   };
-  constexpr uint32_t kId1 = idesc_tf32(64, 32, 0, 0);
-  load1(0);
-  for (int rt = 0; rt < nt1; ++rt) {
+  // V: thread (row t & 63, reflector groups 4 g .. 4 g + 3 for g = (t >> 6) and
+  // (t >> 6) + 4); a warp reads 32 consecutive rows of one reflector
+  auto loadv = [&](int rt) {
+    const int gr = rt * kRows + (t & (kRows - 1));
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int g = (t >> 6) + 4 * h;
+#pragma unroll
+      for (int j = 0; j < 4; ++j) rv[4 * h + j] = vval(gr, 4 * g + j);
+    }
+  };
+  auto storev = [&](bool vr) {  // VI always, VR when vr
+    const int r = t & (kRows - 1);
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int g = (t >> 6) + 4 * h;
+      float hi[4], lo[4];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        hi[j] = tf32_hi(rv[4 * h + j]);
+        lo[j] = rv[4 * h + j] - hi[j];
+      }
+      *reinterpret_cast<float4*>(sm + kOffIhi + vi_off(r, 4 * g)) = make_float4(hi[0], hi[1], hi[2], hi[3]);
+      *reinterpret_cast<float4*>(sm + kOffIlo + vi_off(r, 4 * g)) = make_float4(lo[0], lo[1], lo[2], lo[3]);
+      if (vr)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          *reinterpret_cast<float*>(sm + kOffVhi + v_off(r, 4 * g + j)) = hi[j];
+          *reinterpret_cast<float*>(sm + kOffVlo + v_off(r, 4 * g + j)) = lo[j];
+        }
+    }
+  };
+  // ---- first GEMM over 64-row tiles: D1 (TMEM columns 0..31) = C^T V
+  constexpr uint32_t kId = idesc_tf32(64, 32, 0, 0);
+  loadc(0);
+  loadv(0);
+  for (int rt = 0; rt < nt; ++rt) {
     if (rt > 0) wait_mma(x);  // the previous tile's MMAs have read the buffers
-    store1(rt);
+    storec();
+    storev(true);
+    fence_smem_async();
     fence_before();
     __syncthreads();
-    if (rt + 1 < nt1) load1(rt + 1);  // next tile's loads overlap these MMAs
+    if (rt + 1 < nt) {  // next tile's loads overlap these MMAs
+      loadc(rt + 1);
+      loadv(rt + 1);
+    }
     if (t == 0 && !x.failed) {
       fence_after();
-      const int vr = (rt & 1) * kCRows;
-      const int ksteps = ((m - rt * kCRows < kCRows ? m - rt * kCRows : kCRows) + 7) / 8;
+      const int ksteps = ((m - rt * kRows < kRows ? m - rt * kRows : kRows) + 7) / 8;
       for (int ks = 0; ks < ksteps; ++ks) {
         const uint32_t a_hi = base + kOffChi + 2 * ks * kCChunk, a_lo = base + kOffClo + 2 * ks * kCChunk;
-        const uint32_t b_hi = base + kOffVhi + (vr / 4 + 2 * ks) * kVChunk;
-        const uint32_t b_lo = base + kOffVlo + (vr / 4 + 2 * ks) * kVChunk;
+        const uint32_t b_hi = base + kOffVhi + 2 * ks * kVChunk, b_lo = base + kOffVlo + 2 * ks * kVChunk;
         const uint32_t acc0 = (rt > 0 || ks > 0) ? 1u : 0u;
-        mma(x.tmem, sdesc(a_hi, kCChunk, kCGroup), sdesc(b_hi, kVChunk, kVGroup), kId1, acc0);
-        mma(x.tmem, sdesc(a_hi, kCChunk, kCGroup), sdesc(b_lo, kVChunk, kVGroup), kId1, 1u);
-        mma(x.tmem, sdesc(a_lo, kCChunk, kCGroup), sdesc(b_hi, kVChunk, kVGroup), kId1, 1u);
+        mma(x.tmem, sdesc(a_hi, kCChunk, kCGroup), sdesc(b_hi, kVChunk, kVGroup), kId, acc0);
+        mma(x.tmem, sdesc(a_hi, kCChunk, kCGroup), sdesc(b_lo, kVChunk, kVGroup), kId, 1u);
+        mma(x.tmem, sdesc(a_lo, kCChunk, kCGroup), sdesc(b_hi, kVChunk, kVGroup), kId, 1u);
       }
       commit(x.bar);
     }
@@ -378,43 +417,24 @@ __device__ void left_qt(Ctx& x, const float* V, int ldv, const float* Tm, int ld
     }
     fence_smem_async();
   }
-  // ---- second GEMM over 128-row tiles into alternating 64-column
-  // accumulators; the epilogue of tile rt - 1 overlaps the MMAs of tile rt
-  const int nt2 = (m + kVRows - 1) / kVRows;
-  const bool c_in_smem = m <= kCRows;  // the single C tile is still staged
-  constexpr uint32_t kId2 = idesc_tf32(128, 64, 1, 0);
-  constexpr int kL2 = kVRows * kNB / kThreads;
-  float r2[kL2];
-  auto load2 = [&](int rt) {
-#pragma unroll
-    for (int q = 0; q < kL2; ++q) {
-      const int idx = t + q * kThreads, r = idx & (kVRows - 1), i = idx >> 7;
-      r2[q] = vval(rt * kVRows + r, i);
-    }
-  };
-  auto store2 = [&]() {
-#pragma unroll
-    for (int q = 0; q < kL2; ++q) {
-      const int idx = t + q * kThreads, r = idx & (kVRows - 1), i = idx >> 7;
-      const float hi = tf32_hi(r2[q]);
-      *reinterpret_cast<float*>(sm + kOffVhi + v_off(r, i)) = hi;
-      *reinterpret_cast<float*>(sm + kOffVlo + v_off(r, i)) = r2[q] - hi;
-    }
-    fence_smem_async();
-  };
+  // ---- second GEMM over 64-row tiles into alternating 64-column
+  // accumulators: D2 = V W2 (A = VI, B = W2^T, M = 64, N = 64, K = 32); the
+  // epilogue of tile rt - 1 overlaps the MMAs of tile rt
+  const bool restage = nt > 1;  // a single tile's VI is still staged
+  constexpr uint32_t kId2 = idesc_tf32(64, 64, 0, 0);
   auto epilogue = [&](int rt) {
     const int q4 = warp & 3, half = warp >> 2;
     float d[32];
     tmem_ld32(x.tmem + ((uint32_t)(32 * q4) << 16) + 64u * (uint32_t)(rt & 1) + 32u * (uint32_t)half, d);
-    const int rl = 32 * q4 + lane, r = rt * kVRows + rl;
-    if (r < m) {
+    const int rl = 16 * q4 + lane, r = rt * kRows + rl;  // M = 64: row rl at lane (rl % 16) + 32 (rl / 16)
+    if (lane < 16 && r < m) {
 #pragma unroll
       for (int j = 0; j < 32; ++j) {
         const int c = 32 * half + j;
         if (c < nc) {
           float* p = cptr(r, c);
           float old;
-          if (c_in_smem)
+          if (!restage)  // the single C tile is still staged
             old = *reinterpret_cast<const float*>(sm + kOffChi + c_off(rl, c)) +
                   *reinterpret_cast<const float*>(sm + kOffClo + c_off(rl, c));
           else
@@ -424,12 +444,12 @@ __device__ void left_qt(Ctx& x, const float* V, int ldv, const float* Tm, int ld
       }
     }
   };
-  for (int rt = 0; rt < nt2; ++rt) {
-    const bool restage = nt2 > 1 || m > kVRows;
+  for (int rt = 0; rt < nt; ++rt) {
     if (restage) {
-      load2(rt);
-      if (rt > 0) wait_mma(x);  // MMAs of tile rt - 1 are done with the V buffer
-      store2();
+      loadv(rt);
+      if (rt > 0) wait_mma(x);  // MMAs of tile rt - 1 are done with VI
+      storev(false);
+      fence_smem_async();
     }
     fence_before();
     __syncthreads();
@@ -437,20 +457,19 @@ __device__ void left_qt(Ctx& x, const float* V, int ldv, const float* Tm, int ld
       fence_after();
       const uint32_t d = x.tmem + 64u * (uint32_t)(rt & 1);
       for (int ks = 0; ks < 4; ++ks) {
-        const uint32_t a_hi = base + kOffVhi + ks * kVGroup, a_lo = base + kOffVlo + ks * kVGroup;
+        const uint32_t a_hi = base + kOffIhi + 2 * ks * kIChunk, a_lo = base + kOffIlo + 2 * ks * kIChunk;
         const uint32_t b_hi = base + kOffWhi + 2 * ks * kWChunk, b_lo = base + kOffWlo + 2 * ks * kWChunk;
-        mma(d, sdesc(a_hi, kVGroup, kVChunk), sdesc(b_hi, kWChunk, kWGroup), kId2, ks > 0 ? 1u : 0u);
-        mma(d, sdesc(a_hi, kVGroup, kVChunk), sdesc(b_lo, kWChunk, kWGroup), kId2, 1u);
-        mma(d, sdesc(a_lo, kVGroup, kVChunk), sdesc(b_hi, kWChunk, kWGroup), kId2, 1u);
+        mma(d, sdesc(a_hi, kIChunk, kIGroup), sdesc(b_hi, kWChunk, kWGroup), kId2, ks > 0 ? 1u : 0u);
+        mma(d, sdesc(a_hi, kIChunk, kIGroup), sdesc(b_lo, kWChunk, kWGroup), kId2, 1u);
+        mma(d, sdesc(a_lo, kIChunk, kIGroup), sdesc(b_hi, kWChunk, kWGroup), kId2, 1u);
       }
       commit(x.bar);
     }
     if (rt > 0 && !x.failed) epilogue(rt - 1);
-    if (!restage || rt + 1 == nt2) {
+    if (rt + 1 == nt) {
       wait_mma(x);
       if (x.failed) return;
       epilogue(rt);
-      if (restage) break;
     }
   }
   fence_before();
@@ -459,13 +478,13 @@ __device__ void left_qt(Ctx& x, const float* V, int ldv, const float* Tm, int ld
 
 // ---------------------------------------------------------------- layout probe
 // Diagnostic of the operand layouts (one CTA): stages C (m <= 64 rows x 64
-// columns, ld m) and V (m x 32, ld m) exactly as left_qt does, runs the first
-// GEMM (D1 = C^T V, M = 64) into TMEM columns 0..31 and the second (D2 = V W2
-// with W2 32 x 64, ld 32, M = 128) into columns 64..127, and dumps every TMEM
-// lane: out1 (128 x 32) and out2 (128 x 64), row = lane.  TMEM is zeroed first,
-// so lanes an MMA does not write read 0.  flags bit b swaps the leading and
-// stride byte offsets of: 0 the first GEMM's A, 1 its B, 2 the second GEMM's A,
-// 3 its B.  Every variant reads inside the staged buffers.
+// columns, ld m) and V (m x 32, ld m) as left_qt does and W2 (32 x 64, ld 32),
+// runs the first GEMM (D1 = C^T V, M = 64) into TMEM columns 0..31 and the
+// second (D2 = V W2, M = 64) into columns 64..127, and dumps every TMEM lane:
+// out1 (128 x 32) and out2 (128 x 64), row = lane.  TMEM is zeroed first, so
+// lanes an MMA does not write read 0.  flags bit b swaps the leading and
+// stride byte offsets of: 0 the first GEMM's A, 1 its B, 2 the second GEMM's
+// A, 3 its B.  Every variant reads inside the staged buffers.
 __device__ void probe(Ctx& x, const float* C, const float* V, const float* W2, int m, int flags, float* out1,
                       float* out2) {
   unsigned char* sm = x.sm;
@@ -477,23 +496,25 @@ __device__ void probe(Ctx& x, const float* C, const float* V, const float* W2, i
     for (int i = 0; i < 32; ++i) z[i] = 0.f;
     for (int c0 = 0; c0 < 128; c0 += 32) tmem_st32(x.tmem + ((uint32_t)(32 * warp) << 16) + c0, z);
   }
+  auto put = [&](int off, float v) {
+    const float hi = tf32_hi(v);
+    *reinterpret_cast<float*>(sm + off) = hi;
+    return v - hi;
+  };
   for (int idx = t; idx < 64 * 64; idx += kThreads) {
     const int r = idx & 63, c = idx >> 6;
-    const float v = r < m ? C[r + (size_t)c * m] : 0.f, hi = tf32_hi(v);
-    *reinterpret_cast<float*>(sm + kOffChi + c_off(r, c)) = hi;
-    *reinterpret_cast<float*>(sm + kOffClo + c_off(r, c)) = v - hi;
+    const float v = r < m ? C[r + (size_t)c * m] : 0.f;
+    *reinterpret_cast<float*>(sm + kOffClo + c_off(r, c)) = put(kOffChi + c_off(r, c), v);
   }
-  for (int idx = t; idx < kVRows * 32; idx += kThreads) {
-    const int r = idx & (kVRows - 1), i = idx >> 7;
-    const float v = r < m ? V[r + (size_t)i * m] : 0.f, hi = tf32_hi(v);
-    *reinterpret_cast<float*>(sm + kOffVhi + v_off(r, i)) = hi;
-    *reinterpret_cast<float*>(sm + kOffVlo + v_off(r, i)) = v - hi;
+  for (int idx = t; idx < 64 * 32; idx += kThreads) {
+    const int r = idx & 63, i = idx >> 6;
+    const float v = r < m ? V[r + (size_t)i * m] : 0.f;
+    *reinterpret_cast<float*>(sm + kOffVlo + v_off(r, i)) = put(kOffVhi + v_off(r, i), v);
+    *reinterpret_cast<float*>(sm + kOffIlo + vi_off(r, i)) = put(kOffIhi + vi_off(r, i), v);
   }
   for (int idx = t; idx < 32 * 64; idx += kThreads) {
     const int i = idx & 31, c = idx >> 5;
-    const float v = W2[i + (size_t)c * 32], hi = tf32_hi(v);
-    *reinterpret_cast<float*>(sm + kOffWhi + w_off(c, i)) = hi;
-    *reinterpret_cast<float*>(sm + kOffWlo + w_off(c, i)) = v - hi;
+    *reinterpret_cast<float*>(sm + kOffWlo + w_off(c, i)) = put(kOffWhi + w_off(c, i), W2[i + (size_t)c * 32]);
   }
   fence_smem_async();
   fence_before();
@@ -501,7 +522,7 @@ __device__ void probe(Ctx& x, const float* C, const float* V, const float* W2, i
   auto d = [&](uint32_t a, int lbo, int sbo, bool swap) { return swap ? sdesc(a, sbo, lbo) : sdesc(a, lbo, sbo); };
   if (t == 0) {
     fence_after();
-    constexpr uint32_t kId1 = idesc_tf32(64, 32, 0, 0), kId2 = idesc_tf32(128, 64, 1, 0);
+    constexpr uint32_t kId1 = idesc_tf32(64, 32, 0, 0), kId2 = idesc_tf32(64, 64, 0, 0);
     for (int ks = 0; ks < (m + 7) / 8; ++ks) {
       const uint32_t ah = base + kOffChi + 2 * ks * kCChunk, al = base + kOffClo + 2 * ks * kCChunk;
       const uint32_t bh = base + kOffVhi + 2 * ks * kVChunk, bl = base + kOffVlo + 2 * ks * kVChunk;
@@ -510,11 +531,11 @@ __device__ void probe(Ctx& x, const float* C, const float* V, const float* W2, i
       mma(x.tmem, d(al, kCChunk, kCGroup, flags & 1), d(bh, kVChunk, kVGroup, flags & 2), kId1, 1u);
     }
     for (int ks = 0; ks < 4; ++ks) {
-      const uint32_t ah = base + kOffVhi + ks * kVGroup, al = base + kOffVlo + ks * kVGroup;
+      const uint32_t ah = base + kOffIhi + 2 * ks * kIChunk, al = base + kOffIlo + 2 * ks * kIChunk;
       const uint32_t bh = base + kOffWhi + 2 * ks * kWChunk, bl = base + kOffWlo + 2 * ks * kWChunk;
-      mma(x.tmem + 64, d(ah, kVGroup, kVChunk, flags & 4), d(bh, kWChunk, kWGroup, flags & 8), kId2, ks > 0);
-      mma(x.tmem + 64, d(ah, kVGroup, kVChunk, flags & 4), d(bl, kWChunk, kWGroup, flags & 8), kId2, 1u);
-      mma(x.tmem + 64, d(al, kVGroup, kVChunk, flags & 4), d(bh, kWChunk, kWGroup, flags & 8), kId2, 1u);
+      mma(x.tmem + 64, d(ah, kIChunk, kIGroup, flags & 4), d(bh, kWChunk, kWGroup, flags & 8), kId2, ks > 0);
+      mma(x.tmem + 64, d(ah, kIChunk, kIGroup, flags & 4), d(bl, kWChunk, kWGroup, flags & 8), kId2, 1u);
+      mma(x.tmem + 64, d(al, kIChunk, kIGroup, flags & 4), d(bh, kWChunk, kWGroup, flags & 8), kId2, 1u);
     }
     commit(x.bar);
   }
