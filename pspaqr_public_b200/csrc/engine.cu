@@ -437,7 +437,8 @@ int Tree::factorize() {
       const size_t na = std::min(abase.size(), key.acur + 1);
       key.abase.assign(abase.begin(), abase.begin() + na);
       key.aoff.resize(na);
-      key.sbase.assign(sbase.begin(), sbase.begin() + std::min<size_t>(sbase.size(), 1));
+      // scratch is reset every level: its chunks need only start with those the
+      // recorded level ended with (checked below)
       key.sizes.assign(size_.begin() + Lv.first, size_.begin() + Lv.first + Lv.count);
       key.flags = (fp32_ ? 1 : 0) | (rank_model_ ? 2 : 0) | (rank_log_ ? 4 : 0) | (verbose >= 2 ? 8 : 0);
       auto prefix = [](const std::vector<const char*>& have, const std::vector<const char*>& rec) {

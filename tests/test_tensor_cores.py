@@ -46,7 +46,10 @@ def test_tensor_cores_match_cuda_cores(n, L):
     x = random_reference(n ** 3, 3)
     xa = a.solve_inplace(x.copy())
     xb = b.solve_inplace(x.copy())
-    if np.array_equal(ra, rb):
+    # block by block only while the two float factorizations take the same
+    # pivots: from 32^3 on, rounding flips near-tied pivots of the pivoted QR and
+    # the bases differ while the ranks agree; the backward error judges them
+    if np.array_equal(ra, rb) and n <= 16:
         top = a.level_range(L - 1)[0]
         Ra, Rb = np.triu(a.block(top, top)), np.triu(b.block(top, top))
         assert np.abs(Ra - Rb).max() <= 1e-4 * np.abs(Rb).max()
