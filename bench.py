@@ -2,28 +2,34 @@
 64^3 variable-coefficient diffusion matrix, one B200.
 
 A step is one full time-to-solution run on an assembled tree: ``factorize()``
-followed by left-preconditioned GMRES until the preconditioned residual is
-<= 1e-10 (is.cpp:447-527), with the true ||b - A x|| / ||b|| checked after it.
-Two variants run on the same tree in the same process: the plain FP64 method
-(column-pivoted QR of every interface, left-preconditioned GMRES) and the
-mixed-precision learned-rank method (float factors and preconditioner, learned
-ranks, flexible GMRES in FP64: the headline, ``value``); ``ratio_vs_fp64`` is
-their ratio.
+followed by GMRES until the residual is <= 1e-10, with the true
+||b - A x|| / ||b|| checked after it.  Two variants run on the same tree in the
+same process: the plain FP64 method (column-pivoted QR of every interface,
+left-preconditioned GMRES of is.cpp:447-527) and the mixed-precision
+learned-rank method (float factors whose left block-reflector applies are
+3xTF32 tcgen05 MMAs, learned ranks, flexible GMRES in FP64: the headline,
+``value``); ``ratio_vs_fp64`` is their ratio.
 
   value : device time of the mixed+learned step, inputs resident in HBM (CUDA
           events on the handle's stream, max over ranks), seconds -- lower is
           better.
   e2e   : the same step through the C ABI with host buffers: assemble (matrix
           upload) + factorize + spq_gmres(host b -> host x).
-  roofline : the dominant kernel of the plain factorization (the pivoted QR)
-          against the measured HBM peak.
+  roofline : the tensor-core trailing updates of the headline step (k_update_tc)
+          against the 3xTF32 ceiling derived from the measured bf16 peak;
+          roofline_fp64_rrqr: the plain method's pivoted QR against the measured
+          HBM peak.
+  backward_error : ||A z - u|| / ||u|| with z = M^-1 u for seeded probes, per
+          variant (the factorization's relative backward error).
   cpu_baseline : the CPU oracle (LAPACK restatement of the reference path,
           OpenMP over independent tasks on all host cores) on the same workload.
 
 ``--impl reference`` times that CPU oracle as the reference arm (the reference
 itself cannot be built here: no Eigen, MPI, TaskTorrent or LAPACKE headers).
-With torchrun (N > 1) every rank solves its own replica; the path is not
-sharded across GPUs (replicas only).
+``--config5`` runs BASELINE config 5 (1024^2 convection-diffusion, 16
+right-hand sides solved together) and prints its own line.  With torchrun
+(N > 1) every rank solves its own replica (the subtree sharding plan is in
+pspaqr_public_b200.shard; the factorization itself is not sharded yet).
 """
 from __future__ import annotations
 
@@ -288,6 +294,7 @@ def run_ours(args):
             r["flops"] = t.factor_flops()
             r["level_flops"] = t.level_flops()
             r["rrqr_bytes"] = t.rrqr_bytes()
+            r["tune"] = t.tune_table()
             # the factorization's backward error ||(A P - Q R) z|| / ||Q R z|| in
             # N_PROBES seeded directions (outside the timed steps)
             r["backward_error"] = t.backward_error(N_PROBES, seed=2021).tolist()
@@ -329,12 +336,27 @@ def run_ours(args):
     cnt = head["counts"]
     nint = max(cnt["accepted"] + cnt["fallback"], 1)
     dr = head["ranks"] - res["fp64"]["ranks"]
-    # effective ceiling of the 3xTF32 updates: three kind::tf32 MMAs per
-    # product, TF32 at half the measured bf16 tensor rate
+    # the trailing updates run per level on the tensor cores (3xTF32) or the
+    # CUDA cores, whichever the tuning measured faster; the roofline's ceiling
+    # is that of the kind that ran most of the update flops: three kind::tf32
+    # MMAs per product at half the measured bf16 tensor rate, or cuBLAS SGEMM
+    # (TF32 off) measured in this run
+    tune = head["tune"]
+    on_tc = tune[:, :, 2] == 1
+    lf = head["level_flops"][:, ui]
+    upd_tc_frac = float(lf[on_tc[:, 0]].sum() / max(lf.sum(), 1.0))
     bf16 = peaks.get("bf16_tflops_sustained") or peaks.get("bf16_tflops")
-    tc_peak = bf16 / 2.0 / 3.0 if bf16 else 1590.0 / 2.0 / 3.0
-    tc_src = ("MEASURED_PEAKS.json bf16_tflops_sustained / 2 (TF32 rate) / 3 (MMAs per 3xTF32 product), of measured"
-              if bf16 else "fallback 1590 TFLOP/s bf16 / 2 / 3, of fallback")
+    if upd_tc_frac >= 0.5:
+        upd_bound = "tensor"
+        upd_peak = bf16 / 2.0 / 3.0 if bf16 else 1590.0 / 2.0 / 3.0
+        upd_src = ("MEASURED_PEAKS.json bf16_tflops_sustained / 2 (TF32 rate) / 3 (MMAs per 3xTF32 product), of measured"
+                   if bf16 else "fallback 1590 TFLOP/s bf16 / 2 / 3, of fallback")
+        upd_kernel = "k_update_tc: 3xTF32 tcgen05 trailing updates (the levels tuned to the tensor cores)"
+    else:
+        upd_bound = "fp32"
+        upd_peak = fp32_peak
+        upd_src = "cuBLAS SGEMM 8192^3, TF32 off, measured in this run (MEASURED_PEAKS.json has no FP32 figure)"
+        upd_kernel = "k_update<float>: FP32 trailing updates on the CUDA cores (the levels tuned to them)"
     out = {
         "metric": METRIC,
         "value": step,
@@ -368,14 +390,14 @@ def run_ours(args):
                    "l2": "factor pool (GBs) > L2; 256 MB buffer written before every timed step"},
         "e2e": {"value": e2e, "unit": "s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": 8 * N},
         "gpu_launches": int(np.median(head["launches"])),
-        "roofline": {"bound": "tensor", "achieved": upd_tflops, "peak": tc_peak, "unit": "TFLOP/s",
-                     "frac": upd_tflops / tc_peak,
+        "roofline": {"bound": upd_bound, "achieved": upd_tflops, "peak": upd_peak, "unit": "TFLOP/s",
+                     "frac": upd_tflops / upd_peak if upd_peak else None,
                      "traffic": UPDATE_DRAM_PER_FLOP * upd_flops / max(upd_launches, 1)
                      if UPDATE_DRAM_PER_FLOP else None,
-                     "kernel": "k_update_tc: 3xTF32 tcgen05 trailing updates of the headline step",
+                     "kernel": upd_kernel, "update_flops_on_tensor_cores": upd_tc_frac,
                      "algorithmic_flops": upd_flops, "launches": upd_launches, "duration_s": upd_s,
-                     "per_launch_flops": upd_flops / max(upd_launches, 1), "peak_source": tc_src,
-                     "fp32_simt_sgemm_tflops": fp32_peak},
+                     "per_launch_flops": upd_flops / max(upd_launches, 1), "peak_source": upd_src},
+        "tensor_core_levels": {k: int(on_tc[:, i].sum()) for i, k in enumerate(("updates", "left", "right"))},
         "roofline_fp64_rrqr": {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
                                "frac": achieved / hbm_peak,
                                "traffic": RRQR_DRAM_PER_ALGO_BYTE * rrqr_bytes if RRQR_DRAM_PER_ALGO_BYTE else None,
@@ -392,6 +414,7 @@ def run_ours(args):
         "level_gflop": {k: (head["level_flops"][:, i] / 1e9).round(4).tolist()
                         for i, k in enumerate(ParTree.LEVEL_PHASES[:6])},
         "level_ms_fp64": {k: plt[:, i].round(3).tolist() for i, k in enumerate(ParTree.LEVEL_PHASES)},
+        "tune_ms_tensor_cuda": {k: tune[:, i, :2].round(3).tolist() for i, k in enumerate(("updates", "left", "right"))},
     }
     if rank == 0 and not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline(cp, ri, v, b_host)

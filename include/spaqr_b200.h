@@ -60,14 +60,22 @@ int spq_set_rrqr_work(spq_tree* t, double elems, double fill);
  * pivoted QR of the compression matrices stay in double; bits = 64 (default)
  * is the plain FP64 method.  Takes effect at the next assemble. */
 int spq_set_precision(spq_tree* t, int bits);
-/* Tensor cores of the mixed-precision factorization (no reference counterpart):
- * on = 1 (default) runs the left block-reflector applies of float factors --
- * the trailing updates (the reference's larfb / tpmqrt, ptree.cpp:216-266),
- * the row scaling and the left compression applies (ptree.cpp:1613-1659,
- * 1860-1903) -- as 3xTF32 tcgen05 MMAs with FP32 accumulation; on = 0 runs them
- * in FP32 on the CUDA cores.  No effect on FP64 factors.  Takes effect at the
- * next factorize. */
-int spq_set_tensor_cores(spq_tree* t, int on);
+/* Tensor cores of the mixed-precision factorization (no reference counterpart).
+ * The block-reflector applies of float factors -- the trailing updates (the
+ * reference's larfb / tpmqrt, ptree.cpp:216-266), the row scaling and left
+ * compression applies and the right compression applies (ptree.cpp:1613-1659,
+ * 1860-1903) -- run either as 3xTF32 tcgen05 MMAs with FP32 accumulation or in
+ * FP32 on the CUDA cores.  mode 0 = CUDA cores, 1 = tensor cores, 2 (default) =
+ * tuned: the first float factorization of a partition runs every apply on the
+ * tensor cores, the second on the CUDA cores, and later ones pick per level and
+ * kind of apply the faster of the two measured times (so the first two
+ * factorizations of a partition differ from later ones in rounding).  No
+ * effect on FP64 factors.  Takes effect at the next factorize.
+ * spq_tune_table: per level 9 floats -- for updates, left applies, right
+ * applies: tensor-core ms, CUDA-core ms, choice (1 tensor, 0 CUDA, -1 not
+ * tuned yet). */
+int spq_set_tensor_cores(spq_tree* t, int mode);
+int spq_tune_table(spq_tree* t, float* out);
 /* Diagnostic of the tensor-core operand layouts (no reference counterpart):
  * runs the two GEMMs of one panel apply once, on host inputs C (m x 64,
  * column-major, ld m, m <= 64), V (m x 32, ld m) and W2 (32 x 64, ld 32), and

@@ -127,9 +127,17 @@ int spq_debug_tc_probe(const float* C, const float* V, const float* W2, int m, i
   return e ? -10 : (status ? -12 : 0);
 }
 
-int spq_set_tensor_cores(spq_tree* h, int on) {
-  if (!h || on < 0 || on > 1) return -1;
-  h->t->tensor_cores = on != 0;
+int spq_set_tensor_cores(spq_tree* h, int mode) {
+  if (!h || mode < 0 || mode > 2) return -1;
+  h->t->tensor_cores = mode;
+  return 0;
+}
+
+int spq_tune_table(spq_tree* h, float* out) {
+  if (!h || !out) return -1;
+  std::vector<float> v;
+  h->t->tune_table(v);
+  std::copy(v.begin(), v.end(), out);
   return 0;
 }
 

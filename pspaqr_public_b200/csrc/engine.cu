@@ -103,9 +103,9 @@ void Arena::release() {
 
 // ---------------------------------------------------------------- Tree
 Tree::Tree(int L, int s) : nlevels(L), skip(s) {
-  // SPQ_TENSOR_CORES=0 in the environment starts trees with the float applies
-  // on the CUDA cores (spq_set_tensor_cores changes it per tree)
-  if (const char* e = std::getenv("SPQ_TENSOR_CORES")) tensor_cores = std::atoi(e) != 0;
+  // SPQ_TENSOR_CORES=0 / 1 / 2 in the environment sets the starting mode of
+  // spq_set_tensor_cores (CUDA cores / tensor cores / tuned per level)
+  if (const char* e = std::getenv("SPQ_TENSOR_CORES")) tensor_cores = std::min(std::max(std::atoi(e), 0), 2);
 }
 
 Tree::~Tree() {
@@ -248,6 +248,7 @@ int Tree::partition(int nrows, int ncols, const int* colptr, const int* rowidx, 
   assembled_ = factorized_ = false;
   asm_valid_ = false;
   plans_.clear();
+  tune_runs_ = 0;
   t_partition = wall() - t0;
   if (verbose) printf("Time to partition: %g\n", t_partition);
   return 0;
@@ -394,7 +395,7 @@ static int cluster_for(int ncols) {
 int Tree::factorize() {
   if (!assembled_) return fail(-4, "factorize called before assemble");
   set_factor_fp32(fp32_);
-  set_tensor_cores(fp32_ && tensor_cores);
+  set_tensor_cores(false);
   set_status_word(d_status_);
   if (factorized_) return fail(-4, "factorize called twice; assemble again first");
   clear_status();
@@ -602,6 +603,8 @@ int Tree::factorize() {
       auto* d_ut = static_cast<UpdTask*>(upload(ut.data(), sizeof(UpdTask) * ut.size()));
       auto* d_uo = static_cast<UpdOp*>(upload(uop->data(), sizeof(UpdOp) * uop->size()));
       if (!d_ut || !d_uo) return fail(-11, "out of device memory (update descriptors)");
+      set_tensor_cores(use_tc(lvl, 0));
+      lt_[lvl].kind_tc[0] = tensor_cores_on();
       if (ck(launch_update(d_ut, d_uo, (int)ut.size(), stream_), "update kernel")) return -10;
     }
     cudaEventRecord(ev[1], stream_);
@@ -681,8 +684,11 @@ int Tree::factorize() {
         auto* d_rows = static_cast<EdgeChunk*>(up_vec(rows_scale));
         auto* d_cols = static_cast<EdgeChunk*>(up_vec(cols_scale));
         if (!d_rows || !d_cols) return fail(-11, "out of device memory (scaling)");
-        if (ck(launch_edge(0, d_rows, (int)rows_scale.size(), stream_), "row scaling") ||
-            ck(launch_edge(1, d_cols, (int)cols_scale.size(), stream_), "column scaling"))
+        set_tensor_cores(use_tc(lvl, 1));
+        lt_[lvl].kind_tc[1] = tensor_cores_on();
+        if (ck(launch_edge(0, d_rows, (int)rows_scale.size(), stream_), "row scaling")) return -10;
+        cudaEventRecord(fe[3], stream_);
+        if (ck(launch_edge(1, d_cols, (int)cols_scale.size(), stream_), "column scaling"))
           return -10;
       }
       cudaEventRecord(ev[2], stream_);
@@ -1156,8 +1162,12 @@ int Tree::factorize() {
       }
       if (int rc = build_compress()) return rc;
       cudaEventRecord(fe[2], stream_);
-      if (ck(launch_edge(2, d_right, (int)right.size(), stream_), "right compression") ||
-          ck(launch_edge(0, d_left, (int)left.size(), stream_), "left compression"))
+      set_tensor_cores(use_tc(lvl, 2));
+      lt_[lvl].kind_tc[2] = tensor_cores_on();
+      if (ck(launch_edge(2, d_right, (int)right.size(), stream_), "right compression")) return -10;
+      cudaEventRecord(fe[4], stream_);
+      set_tensor_cores(use_tc(lvl, 1));
+      if (ck(launch_edge(0, d_left, (int)left.size(), stream_), "left compression"))
         return -10;
       cudaEventRecord(ev[3], stream_);
       if (ck(cudaMemcpyAsync(host_rank.data(), d_rank_, sizeof(int) * host_rank.size(), cudaMemcpyDeviceToHost, stream_),
@@ -1312,6 +1322,15 @@ int Tree::factorize() {
     cudaEventElapsedTime(&lt_[lvl].sapp_ms, fe[1], ev[2]);
     cudaEventElapsedTime(&lt_[lvl].rrqr_ms, ev[2], fe[2]);
     cudaEventElapsedTime(&lt_[lvl].capp_ms, fe[2], ev[3]);
+    if (spars) {
+      float a = 0, b = 0, c = 0;
+      cudaEventElapsedTime(&a, fe[1], fe[3]);  // row scaling
+      cudaEventElapsedTime(&b, fe[2], fe[4]);  // right compression
+      cudaEventElapsedTime(&c, fe[4], ev[3]);  // left compression
+      lt_[lvl].kind_ms[1] = a + c;
+      lt_[lvl].kind_ms[2] = b;
+    }
+    lt_[lvl].kind_ms[0] = lt_[lvl].e2_ms;
     scratch_.reset();
     if (verbose)
       printf("%d    elim %.3f ms  scale %.3f ms  spars %.3f ms  merge %.3f ms  (interiors %zu, interfaces %zu)\n", lvl,
@@ -1322,6 +1341,14 @@ int Tree::factorize() {
   for (auto& e : fe) cudaEventDestroy(e);
   for (const LevelTiming& t : lt_)
     for (double f : t.flops) flops_ += f;
+  // tuning of the float applies: the first two factorizations measure each
+  // level's applies on the tensor cores, then on the CUDA cores
+  if (fp32_ && tensor_cores == 2 && tune_runs_ < 2) {
+    tune_ms_[tune_runs_].assign(L, {0.f, 0.f, 0.f});
+    for (int l = 0; l < L; ++l)
+      for (int k = 0; k < 3; ++k) tune_ms_[tune_runs_][l][k] = lt_[l].kind_ms[k];
+    ++tune_runs_;
+  }
   factorized_ = true;
   int rc = build_solve_graph();
   if (rc) return rc;
@@ -1331,6 +1358,27 @@ int Tree::factorize() {
     printf("Time to factorize:  %g\n", t_factorize);
   }
   return 0;
+}
+
+bool Tree::use_tc(int lvl, int kind) const {
+  if (!fp32_ || tensor_cores == 0) return false;
+  if (tensor_cores == 1) return true;
+  if (tune_runs_ < 2) return tune_runs_ == 0;  // measuring: tensor cores first, then CUDA cores
+  return tune_ms_[0][lvl][kind] < tune_ms_[1][lvl][kind];
+}
+
+void Tree::tune_table(std::vector<float>& out) const {
+  const int L = st_.nlevels;
+  out.assign((size_t)L * 9, -1.f);
+  for (int l = 0; l < L; ++l)
+    for (int k = 0; k < 3; ++k) {
+      float* o = out.data() + (size_t)l * 9 + 3 * k;
+      if (tune_runs_ >= 1 && (int)tune_ms_[0].size() == L) o[0] = tune_ms_[0][l][k];
+      if (tune_runs_ >= 2 && (int)tune_ms_[1].size() == L) {
+        o[1] = tune_ms_[1][l][k];
+        o[2] = o[0] < o[1] ? 1.f : 0.f;
+      }
+    }
 }
 
 int Tree::alloc_level_blocks(const std::vector<int>& edges) {

@@ -9,6 +9,7 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <array>
 #include <cstdint>
 #include <string>
 #include <vector>
@@ -91,6 +92,10 @@ struct LevelTiming {
   // applies, pivoted QR / learned ranks, compression applies)
   double flops[6] = {0, 0, 0, 0, 0, 0};
   int ntasks_elim = 0, ntasks_upd = 0, nspars = 0;
+  // the three kinds of tuned applies: trailing updates, left applies (row
+  // scaling + left compression), right compression
+  float kind_ms[3] = {0, 0, 0};
+  bool kind_tc[3] = {false, false, false};  // ran on the tensor cores
 };
 
 class Tree {
@@ -120,10 +125,12 @@ class Tree {
   // 1 = flexible right-preconditioned GMRES, -1 (default) = flexible exactly
   // when the factors are float
   int krylov = -1;
-  // float factors: left block-reflector applies (trailing updates, row
-  // scaling, left compression) on the tensor cores (3xTF32) or on the CUDA
-  // cores
-  bool tensor_cores = true;
+  // float factors: where the block-reflector applies (trailing updates, row
+  // scaling and left compression, right compression) run: 0 = CUDA cores,
+  // 1 = tensor cores (3xTF32), 2 = tuned per level and kind of apply from the
+  // measured times of the first two float factorizations of a partition (the
+  // first on the tensor cores, the second on the CUDA cores)
+  int tensor_cores = 2;
   // cycle budget of every bounded spin wait of the preconditioner apply's
   // forward sweep (takes effect at the next factorize, which captures the
   // apply); a wait that runs out fails the apply with status -12
@@ -140,6 +147,9 @@ class Tree {
   // same sizes and allocator states (LevelPlan)
   bool plan_cache = true;
   long long plan_hits() const { return plan_hits_; }
+  // per level: 3 kinds x (tensor-core ms, CUDA-core ms, chosen: 1 tensor, 0 CUDA,
+  // -1 not tuned yet)
+  void tune_table(std::vector<float>& out) const;
   // learned ranks: the sketch's pivoted QR stops at sketch_tol * tol (the
   // kept rank is then chosen on C itself)
   double sketch_tol = 0.1;
@@ -321,6 +331,11 @@ class Tree {
   int ensure_krylov(size_t doubles);
   std::vector<LevelTiming> lt_;
   std::vector<LevelPlan> plans_;  // per level, cleared by partition
+  // tuning of the float applies (tensor_cores == 2): per level and kind, the
+  // measured milliseconds on the tensor cores [0] and on the CUDA cores [1]
+  std::vector<std::array<float, 3>> tune_ms_[2];
+  int tune_runs_ = 0;  // float factorizations of this partition measured so far
+  bool use_tc(int lvl, int kind) const;
   long long plan_hits_ = 0;       // levels whose lists were reused
   double flops_ = 0;
   double rrqr_bytes_ = 0;

@@ -1308,7 +1308,7 @@ const char* last_launch_name() { return g_last_launch; }
 void set_factor_fp32(bool on) { g_fp32 = on; }
 void set_tensor_cores(bool on) { g_tc = on; }
 void set_status_word(int* status) { g_status = status; }
-bool tensor_cores() { return g_tc; }
+bool tensor_cores_on() { return g_tc; }
 bool factor_fp32() { return g_fp32; }
 void set_last_launch(const char* name) { g_last_launch = name; }
 

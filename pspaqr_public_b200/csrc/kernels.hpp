@@ -24,7 +24,7 @@ bool factor_fp32();
 // scaling, left compression) on the tensor cores (tcgen05, 3xTF32) for the
 // launchers of this thread that follow.
 void set_tensor_cores(bool on);
-bool tensor_cores();
+bool tensor_cores_on();
 // Device status word of the factorization kernels launched by this thread:
 // bit 2 (value 2) a tensor-core wait ran out, 4 a non-finite pivot, 8 a zero
 // pivot in a QR factorization (elimination chains, scaling QR).

@@ -53,6 +53,7 @@ def lib():
             "spq_set_precision": (i32, [vp, i32]),
             "spq_set_krylov": (i32, [vp, i32]),
             "spq_set_tensor_cores": (i32, [vp, i32]),
+            "spq_tune_table": (i32, [vp, pf]),
             "spq_set_spin_limit": (i32, [vp, C.c_longlong]),
             "spq_set_checks": (i32, [vp, i32]),
             "spq_set_plan_cache": (i32, [vp, i32]),
@@ -239,9 +240,17 @@ class ParTree:
         pivoted QR); 64: plain FP64.  Takes effect at the next assemble."""
         self._chk(lib().spq_set_precision(self._h, bits), "set_precision")
 
-    def set_tensor_cores(self, on: bool):
-        """Float factors: left block-reflector applies as 3xTF32 tcgen05 MMAs (default) or FP32 SIMT."""
-        self._chk(lib().spq_set_tensor_cores(self._h, int(bool(on))), "set_tensor_cores")
+    def set_tensor_cores(self, mode):
+        """Float factors' block-reflector applies: 0 / False = CUDA cores, 1 / True =
+        3xTF32 tcgen05 MMAs, 2 = tuned per level from the first two factorizations."""
+        self._chk(lib().spq_set_tensor_cores(self._h, int(mode)), "set_tensor_cores")
+
+    def tune_table(self) -> np.ndarray:
+        """(nlevels, 3, 3): for updates / left applies / right applies: tensor-core ms,
+        CUDA-core ms, choice (1 tensor, 0 CUDA, -1 not tuned yet)."""
+        out = np.zeros(9 * self.nlevels, np.float32)
+        lib().spq_tune_table(self._h, _pf(out))
+        return out.reshape(self.nlevels, 3, 3)
 
     def set_spin_limit(self, cycles: int):
         """Cycle budget of the preconditioner apply's bounded waits (next factorize)."""

@@ -173,6 +173,7 @@ def test_reassembly_is_bit_identical():
     t.set_coords_tensor(16, 3)
     t.partition((cp, ri, scale_columns(cp, v)))
     b = random_reference(16 ** 3, 9)
+    t.set_tensor_cores(1)  # one fixed kind of float apply (the tuned mode measures both first)
     for prec in (64, 32, 64):
         t.set_precision(prec)
         out = []
@@ -203,7 +204,8 @@ def test_reused_plans_are_bit_identical(precision, learned):
 
     def run(cache, tol, reps):
         t = ParTree(6, 0)
-        t.set_tol(tol)
+        t.set_tol(tol[0] if isinstance(tol, list) else tol)
+        t.set_tensor_cores(1)
         t.set_coords_tensor(16, 3)
         t.set_precision(precision)
         t.set_plan_cache(cache)
@@ -234,3 +236,29 @@ def test_reused_plans_are_bit_identical(precision, learned):
     B, x, k, rr, rk = mixed[1]
     B0, x0, k0, rr0, rk0 = fresh3[0]
     assert rk == rk0 and k == k0 and np.array_equal(B, B0) and np.array_equal(x, x0)
+
+
+def test_tuned_applies_pick_the_faster_kind_per_level():
+    """Mode 2 (the default): the first float factorization runs every apply on the
+    tensor cores, the second on the CUDA cores; later ones use, per level and kind
+    of apply, the one measured faster.  Every one of them is a valid factor."""
+    cp, ri, v = _matrix("diff", 16, 3)
+    t = ParTree(6, 0)
+    t.set_tol(1e-2)
+    t.set_coords_tensor(16, 3)
+    t.set_precision(32)
+    t.partition((cp, ri, scale_columns(cp, v)))
+    b = random_reference(16 ** 3, 4)
+    etas = []
+    for _ in range(3):
+        t.assemble()
+        t.factorize()
+        etas.append(t.backward_error(2, seed=5))
+        k, rr = dist_gmres(None, b.copy(), t, 100, 1e-10)
+        assert rr <= 1e-10
+    tab = t.tune_table()
+    measured = tab[:, :, 0] >= 0
+    assert measured.any()
+    for l, k in zip(*np.nonzero(measured)):
+        assert tab[l, k, 2] == (1.0 if tab[l, k, 0] < tab[l, k, 1] else 0.0)
+    assert np.all(np.abs(np.array(etas) / etas[1] - 1) < 0.2)
