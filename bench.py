@@ -261,12 +261,15 @@ def run_ours(args):
 
     from pspaqr_public_b200.tree import load_rank_model
 
-    model = load_rank_model()
+    # the sketch margin calibrated for this tolerance comes with the model when
+    # asked for (--calibrated)
+    model = load_rank_model(tol=W["tol"] if args.calibrated else None)
+    oversample = args.oversample
 
     def set_variant(name):
         # takes effect at the next assemble (every step assembles)
         t.set_precision(32 if name == "mixed+learned" else 64)
-        t.set_rank_model(model if name == "mixed+learned" else None, LEARNED_OVERSAMPLE)
+        t.set_rank_model(model if name == "mixed+learned" else None, oversample)
 
     def ranks():
         cl = t.clusters()
@@ -383,7 +386,7 @@ def run_ours(args):
         "learned": {"interfaces": int(nint), "fallback_rate": cnt["fallback"] / nint,
                     "ranks_within_2": float(np.mean(np.abs(dr) <= 2)) if len(dr) else None,
                     "sketch_columns_per_interface": cnt["sketch_columns"] / nint,
-                    "oversample": LEARNED_OVERSAMPLE},
+                    "oversample": oversample, "margin": float(model.get("margin", 0.0))},
         "partition_s": t_part,
         "config": {"workload": W["name"], "nlevels": W["nlevels"], "tol": W["tol"], "skip": W["skip"],
                    "gmres_tol": W["gmres_tol"], "parallelism": f"replicas x{world}",
@@ -576,6 +579,10 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile", default="", choices=["", "fp64", "mixed+learned"],
                     help="bracket the first timed step of this variant with cudaProfilerStart/Stop")
+    ap.add_argument("--oversample", type=int, default=LEARNED_OVERSAMPLE,
+                    help="sketch columns beyond the predicted rank in the learned-rank variant")
+    ap.add_argument("--calibrated", action="store_true",
+                    help="size the sketches with the rank model's calibrated margin for this tolerance")
     ap.add_argument("--config5", action="store_true",
                     help="the 1024^2 convection-diffusion workload with 16 right-hand sides (its own JSON line)")
     ap.add_argument("--size", type=int, default=64,
