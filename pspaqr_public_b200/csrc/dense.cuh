@@ -824,6 +824,145 @@ __device__ void vec_apply_tpqt(const T* V, int ldv, const T* Tm, int k, T* a, T*
   }
 }
 
+// ---------------------------------------------------------------- staged single-vector applies
+// Asynchronous global -> shared copies (cp.async): 16-byte chunks where the
+// source is 16-byte aligned, single elements at the unaligned head and tail.
+__device__ __forceinline__ void cp_async16(void* sdst, const void* gsrc) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(sdst);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gsrc) : "memory");
+}
+template <typename T>
+__device__ __forceinline__ void cp_async_elem(T* sdst, const T* gsrc) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(sdst);
+  if (sizeof(T) == 8) asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gsrc) : "memory");
+  else asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gsrc) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+
+// Elements of a 16-byte chunk, and the shift that gives a shared copy of
+// g[0, len) the same 16-byte phase as g.
+template <typename T>
+constexpr int kE16 = 16 / (int)sizeof(T);
+template <typename T>
+__device__ __forceinline__ int phase_of(const T* g) {
+  return (int)(((uintptr_t)g & 15u) / sizeof(T));
+}
+
+// One warp copies g[0, len) to d[0, len); d must have g's 16-byte phase.
+template <typename T>
+__device__ __forceinline__ void warp_copy_async(T* d, const T* g, int len, int lane) {
+  int h = (kE16<T> - phase_of(g)) % kE16<T>;
+  if (h > len) h = len;
+  for (int e = lane; e < h; e += 32) cp_async_elem(d + e, g + e);
+  const int nc = (len - h) / kE16<T>;
+  for (int c = lane; c < nc; c += 32) cp_async16(d + h + c * kE16<T>, g + h + c * kE16<T>);
+  for (int e = h + nc * kE16<T> + lane; e < len; e += 32) cp_async_elem(d + e, g + e);
+}
+
+// Shared memory (elements) of vec_apply_staged for m rows: two panel buffers
+// of kNB columns (column stride staged_ld), two T blocks (each with room for
+// a 16-byte phase shift), W and W2.
+template <typename T>
+__host__ __device__ constexpr int staged_ld(int m) {
+  return (m + 2 * kE16<T> - 1) / kE16<T> * kE16<T>;
+}
+template <typename T>
+__host__ __device__ constexpr int staged_tld() {
+  return kNB * kNB + kE16<T>;
+}
+template <typename T>
+__host__ __device__ constexpr size_t staged_elems(int m) {
+  return 2 * (size_t)kNB * staged_ld<T>(m) + 2 * (size_t)staged_tld<T>() + 2 * kNB;
+}
+
+// x (m) <- Q^T x (trans) or Q x for k unit lower trapezoidal reflectors (T in
+// kNB x k layout) with the panels streamed through shared memory: while panel
+// p is applied from one buffer, panel p + 1 (its rows from its diagonal down,
+// and its T block) is copied into the other with cp.async, so a whole panel
+// of loads is in flight instead of a few per thread.  Per panel:
+//   W = V^T x   (a warp per reflector, lanes over rows);
+//   W2 = T^T W (trans) or T W, by warp 0;
+//   x -= V W2   (a thread per row).
+// x in shared memory (m elements); buf: staged_elems<T>(m) elements, 16-byte
+// aligned.  All threads of the CTA call it; it synchronises internally.
+template <typename T>
+__device__ void vec_apply_staged(const T* V, int ldv, const T* Tm, int k, T* x, int m, bool trans, T* buf) {
+  if (k <= 0 || m <= 0) return;
+  __shared__ int s_off[2][kNB];  // element (r, i) of the staged panel at pb[.][s_off[.][i] + r]
+  __shared__ int s_toff[2];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int lds = staged_ld<T>(m);
+  T* const pb0 = buf;
+  T* const tb0 = buf + 2 * (size_t)kNB * lds;
+  T* const W = tb0 + 2 * staged_tld<T>();
+  T* const W2 = W + kNB;
+  const int np = (k + kNB - 1) / kNB;
+  auto j0_of = [&](int s) { return (trans ? s : np - 1 - s) * kNB; };
+  auto stage = [&](int s, int b) {
+    const int j0 = j0_of(s);
+    const int kb = (k - j0) < kNB ? (k - j0) : kNB;
+    T* pb = pb0 + (size_t)b * kNB * lds;
+    for (int i = warp; i < kb; i += kWarps) {
+      const T* g = V + (size_t)(j0 + i) * ldv + j0;
+      const int ph = phase_of(g);
+      warp_copy_async(pb + (size_t)i * lds + ph, g, m - j0, lane);
+      if (lane == 0) s_off[b][i] = i * lds + ph - j0;
+    }
+    if (warp == kWarps - 1) {
+      const T* g = Tm + (size_t)j0 * kNB;
+      const int ph = phase_of(g);
+      warp_copy_async(tb0 + (size_t)b * staged_tld<T>() + ph, g, kNB * kb, lane);
+      if (lane == 0) s_toff[b] = b * staged_tld<T>() + ph;
+    }
+    cp_async_commit();
+  };
+  stage(0, 0);
+  for (int s = 0; s < np; ++s) {
+    const int b = s & 1;
+    const int j0 = j0_of(s);
+    const int kb = (k - j0) < kNB ? (k - j0) : kNB;
+    if (s + 1 < np) {
+      stage(s + 1, b ^ 1);
+      cp_async_wait<1>();
+    } else {
+      cp_async_wait<0>();
+    }
+    __syncthreads();
+    const T* pb = pb0 + (size_t)b * kNB * lds;
+    const T* tp = tb0 + s_toff[b];
+    // W(i) = x(j0 + i) + sum_{r > j0 + i} V(r, i) x(r)
+    for (int i = warp; i < kb; i += kWarps) {
+      const T* col = pb + s_off[b][i];
+      T d = 0.0;
+      for (int r = j0 + i + 1 + lane; r < m; r += 32) d += col[r] * x[r];
+      d = warp_sum(d);
+      if (lane == 0) W[i] = d + x[j0 + i];
+    }
+    __syncthreads();
+    if (warp == 0) {
+      T acc = 0.0;
+      if (lane < kb) {
+        if (trans)
+          for (int l = 0; l <= lane; ++l) acc += tp[l + lane * kNB] * W[l];
+        else
+          for (int l = lane; l < kb; ++l) acc += tp[lane + l * kNB] * W[l];
+      }
+      W2[lane] = acc;
+    }
+    __syncthreads();
+    for (int r = j0 + threadIdx.x; r < m; r += kThreads) {
+      const int lim = (r - j0) < kb ? (r - j0) : kb;
+      T acc = (r - j0) < kb ? W2[r - j0] : (T)0.0;
+#pragma unroll 8
+      for (int i = 0; i < lim; ++i) acc += pb[s_off[b][i] + r] * W2[i];
+      x[r] -= acc;
+    }
+    __syncthreads();
+  }
+}
+
 // C (m <= kNC rows x n) <- C R^{-1}, R upper triangular (n x n), blocked by 32
 // columns: C(:, J) -= C(:, 0:j0) R(0:j0, J) through shared-memory tiles, then
 // the 32 x 32 diagonal block is solved one row per thread.
@@ -937,25 +1076,39 @@ __device__ void trsm_right_upper(const T* R, int ldr, T* C, int ldc, int m, int 
   __syncthreads();
 }
 
-// Upper triangular solve x <- R^{-1} x (n x n), blocked by 32: one warp solves
-// each diagonal block with shuffles, the CTA updates the rows above.
+// Upper triangular solve x <- R^{-1} x (n x n), blocked by 32, bottom block
+// first.  Warp 0 holds the diagonal block in registers (lane i: row i's part
+// on and above the diagonal), loaded while the CTA updates the rows above the
+// previous block, and solves it with shuffles; the CTA then updates the rows
+// above with the solved block.
 template <typename T>
 __device__ void trsv_upper(const T* R, int ldr, T* x, int n, T* xs /*shared >= 32*/) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  T rv[32];
+  auto fetch = [&](int lo, int bs) {
+#pragma unroll
+    for (int j = 0; j < 32; ++j)
+      rv[j] = (j < bs && lane <= j) ? R[(lo + lane) + (size_t)(lo + j) * ldr] : (T)0.0;
+  };
+  if (warp == 0 && n > 0) fetch(n > 32 ? n - 32 : 0, n > 32 ? 32 : n);
   for (int hi = n; hi > 0; hi -= 32) {
     const int lo = hi > 32 ? hi - 32 : 0;
     const int bs = hi - lo;
     if (warp == 0) {
       T xv = lane < bs ? x[lo + lane] : 0.0;
-      for (int j = bs - 1; j >= 0; --j) {
-        if (lane == j) xv = xv / R[(lo + j) + (size_t)(lo + j) * ldr];
-        const T xj = __shfl_sync(0xffffffffu, xv, j);
-        if (lane < j) xv -= R[(lo + lane) + (size_t)(lo + j) * ldr] * xj;
+#pragma unroll
+      for (int j = 31; j >= 0; --j) {
+        if (j < bs) {
+          if (lane == j) xv = xv / rv[j];
+          const T xj = __shfl_sync(0xffffffffu, xv, j);
+          if (lane < j) xv -= rv[j] * xj;
+        }
       }
       if (lane < bs) {
         x[lo + lane] = xv;
         xs[lane] = xv;
       }
+      if (lo > 0) fetch(lo > 32 ? lo - 32 : 0, lo > 32 ? 32 : lo);
     }
     __syncthreads();
     for (int r = threadIdx.x; r < lo; r += kThreads) {

@@ -14,6 +14,8 @@
 #include <algorithm>
 #include <atomic>
 #include <cstdint>
+#include <mutex>
+#include <unordered_map>
 
 #include "dense.cuh"
 #include "kernels.hpp"
@@ -66,16 +68,83 @@ __global__ void k_scatter(int nnz, const double* __restrict__ val, double* const
 // applies the block reflector to its own later panels with the tiled apply
 // (two of its panels per pass).  `lt` holds the owner's tau values, `tg`
 // the global copy, `vb` a reflector tail, `tile` dev::kTileSmem elements.
+//
+// With `pan` (ldp >= the panel's rows; ldp * kNB + kNB * kNB elements, may
+// alias `tile`), the owner copies the panel into shared memory, runs the kb
+// reflector steps and the T factor there and writes the panel back once:
+// the same operations in the same order as on global memory, without a
+// global round trip per step.
 template <typename T>
 __device__ void dist_qr(T* R, int ldr, T* B, int ldb, int m, int n, int unit, T* Tout, T* tg,
-                        T* lt, T* vb, T* red, T* tmp, T* tile, int cs, int* status = nullptr) {
+                        T* lt, T* vb, T* red, T* tmp, T* tile, int cs, int* status = nullptr, T* pan = nullptr,
+                        int ldp = 0) {
   const int rank = crank(cs);
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int gap = (cs - 1) * kNB;  // columns between two panels of one CTA
   for (int j0 = 0; j0 < n; j0 += kNB) {
     const int kb = (n - j0) < kNB ? (n - j0) : kNB;
     const int pend = j0 + kb;
-    if (owns(j0, rank, cs)) {
+    if (owns(j0, rank, cs) && pan) {
+      // panel rows: [j0, m) of R's columns (geqrt) or B's m rows (tpqrt)
+      const int pm = unit ? m - j0 : m;
+      T* pr = pan + (size_t)ldp * kNB;  // tpqrt: R(j0:pend, j0:pend), ld kNB
+      __syncthreads();                  // `pan` may alias the tiled apply's scratch
+      for (int c = warp; c < kb; c += kWarps) {
+        const T* src = unit ? (R + j0 + (size_t)(j0 + c) * ldr) : (B + (size_t)(j0 + c) * ldb);
+        for (int i = lane; i < pm; i += 32) pan[i + (size_t)c * ldp] = __ldcg(src + i);
+      }
+      if (!unit)
+        for (int e = threadIdx.x; e < kb * kb; e += kThreads) {
+          const int r = e % kb, c = e / kb;
+          if (r <= c) pr[r + c * kNB] = __ldcg(R + (j0 + r) + (size_t)(j0 + c) * ldr);
+        }
+      __syncthreads();
+      for (int j = j0; j < pend; ++j) {
+        const int jj = j - j0;
+        const int vlen = unit ? (m - j - 1) : m;
+        T* tail = unit ? (pan + (jj + 1) + (size_t)jj * ldp) : (pan + (size_t)jj * ldp);
+        T* ajj = unit ? (pan + jj + (size_t)jj * ldp) : (pr + jj + jj * kNB);
+        T s = 0.0;
+        for (int i = threadIdx.x; i < vlen; i += kThreads) s += tail[i] * tail[i];
+        s = dev::cta_sum(s, red);
+        const T alpha = *ajj;
+        T beta, scal;
+        const T tj = dev::house(alpha, s, &beta, &scal);
+        if (tj != 0.0)
+          for (int i = threadIdx.x; i < vlen; i += kThreads) tail[i] *= scal;
+        if (threadIdx.x == 0) {
+          *ajj = beta;
+          lt[j] = tj;
+          tg[j] = tj;
+          if (status && !(isfinite(beta) && beta != (T)0)) atomicOr(status, isfinite(beta) ? 8 : 4);
+        }
+        __syncthreads();
+        if (tj != 0.0)
+          for (int k = j + 1 + warp; k < pend; k += kWarps) {
+            const int kk = k - j0;
+            T* rjk = unit ? (pan + jj + (size_t)kk * ldp) : (pr + jj + kk * kNB);
+            T* tk = unit ? (pan + (jj + 1) + (size_t)kk * ldp) : (pan + (size_t)kk * ldp);
+            T d = lane == 0 ? *rjk : 0.0;
+            for (int i = lane; i < vlen; i += 32) d += tail[i] * tk[i];
+            d = dev::warp_sum(d) * tj;
+            if (lane == 0) *rjk -= d;
+            for (int i = lane; i < vlen; i += 32) tk[i] -= tail[i] * d;
+          }
+        __syncthreads();
+      }
+      dev::panel_t(pan, ldp, pm, kb, unit, lt + j0, Tout + (size_t)j0 * kNB, kNB, tmp);
+      for (int c = warp; c < kb; c += kWarps) {
+        T* dst = unit ? (R + j0 + (size_t)(j0 + c) * ldr) : (B + (size_t)(j0 + c) * ldb);
+        for (int i = lane; i < pm; i += 32) dst[i] = pan[i + (size_t)c * ldp];
+      }
+      if (!unit)
+        for (int e = threadIdx.x; e < kb * kb; e += kThreads) {
+          const int r = e % kb, c = e / kb;
+          if (r <= c) R[(j0 + r) + (size_t)(j0 + c) * ldr] = pr[r + c * kNB];
+        }
+      __threadfence();
+      __syncthreads();
+    } else if (owns(j0, rank, cs)) {
       for (int j = j0; j < pend; ++j) {
         const int vlen = unit ? (m - j - 1) : m;
         T* tail = unit ? (R + (j + 1) + (size_t)j * ldr) : (B + (size_t)j * ldb);
@@ -137,7 +206,9 @@ __device__ void dist_qr(T* R, int ldr, T* B, int ldb, int m, int n, int unit, T*
   csync(cs);
 }
 
-template <typename T>
+// kStage: panels factored in shared memory (dist_qr's `pan`, aliasing the
+// tiled apply's scratch; vmax rows).
+template <typename T, bool kStage>
 __global__ void __launch_bounds__(kThreads, 2) k_elim(const ElimTask* __restrict__ tasks, const ElimOut* __restrict__ outs,
                                                    int cs, int vmax, int* status) {
   extern __shared__ __align__(16) unsigned char smraw[];
@@ -148,25 +219,30 @@ __global__ void __launch_bounds__(kThreads, 2) k_elim(const ElimTask* __restrict
   T* lt = tmp + kNB;
   T* vb = lt + t.n;
   T* tile = vb + vmax;
-  dist_qr<T>(as<T>(t.S), t.n, nullptr, 0, t.n, t.n, 1, as<T>(t.T), as<T>(t.tau), lt, vb, red, tmp, tile, cs, status);
+  T* pan = kStage ? tile : nullptr;
+  dist_qr<T>(as<T>(t.S), t.n, nullptr, 0, t.n, t.n, 1, as<T>(t.T), as<T>(t.tau), lt, vb, red, tmp, tile, cs, status,
+             pan, vmax);
   for (int o = t.out_begin; o < t.out_end; ++o) {
     const ElimOut e = outs[o];
     dist_qr<T>(as<T>(t.S), t.n, as<T>(e.B), e.m, e.m, t.n, 0, as<T>(e.T), as<T>(t.tau), lt, vb, red, tmp, tile,
-               cs, status);
+               cs, status, pan, vmax);
   }
 }
 
-template <typename T>
-__global__ void __launch_bounds__(kThreads, 2) k_scale(const ScaleTask* __restrict__ tasks, int cs, int* status) {
+// kStage: panels factored in shared memory (nmax rows), as in k_elim.
+template <typename T, bool kStage>
+__global__ void __launch_bounds__(kThreads, 2) k_scale(const ScaleTask* __restrict__ tasks, int cs, int nmax,
+                                                    int* status) {
   extern __shared__ __align__(16) unsigned char smraw[];
   T* sm = reinterpret_cast<T*>(smraw);
   const ScaleTask t = tasks[blockIdx.x / cs];
   T* red = sm;
   T* tmp = red + kRed;
   T* lt = tmp + kNB;
-  T* vb = lt + t.n;
-  dist_qr<T>(as<T>(t.S), t.n, nullptr, 0, t.n, t.n, 1, as<T>(t.T), as<T>(t.tau), lt, vb, red, tmp, vb + t.n, cs,
-             status);
+  T* vb = lt + nmax;
+  T* tile = vb + nmax;
+  dist_qr<T>(as<T>(t.S), t.n, nullptr, 0, t.n, t.n, 1, as<T>(t.T), as<T>(t.tau), lt, vb, red, tmp, tile, cs,
+             status, kStage ? tile : nullptr, nmax);
 }
 
 // ------------------------------------------------------------ chunked applies
@@ -870,6 +946,9 @@ __global__ void __launch_bounds__(kThreads, 2) k_rrqr(const RrqrTask* __restrict
 // basis Qc = C_sel R^{-1} (column-major, ld m) over the cluster's row blocks:
 // tiles of rt rows, 32-column blocks of R, a blocked update from the solved
 // columns and a triangular solve on the diagonal block.
+// kStage: the QR's panels are factored in shared memory (dist_qr's `pan`,
+// aliasing the basis tiles; mmax rows).
+template <bool kStage>
 __global__ void __launch_bounds__(kThreads, 2) k_selected_qr(const RrqrTask* __restrict__ tasks, int cs, int mmax,
                                                           int nmax, int rt) {
   extern __shared__ double sm[];
@@ -892,7 +971,8 @@ __global__ void __launch_bounds__(kThreads, 2) k_selected_qr(const RrqrTask* __r
     for (int r = lane; r < m; r += 32) t.V[r + (size_t)l * m] = __ldg(C + (size_t)r * ldw + c);
   }
   __syncthreads();
-  dist_qr<double>(t.V, m, nullptr, 0, m, rk, 1, t.T, t.tau, lt, vb, red, tmp, Qt, cs);
+  dist_qr<double>(t.V, m, nullptr, 0, m, rk, 1, t.T, t.tau, lt, vb, red, tmp, Qt, cs, nullptr,
+                  kStage ? Qt : nullptr, mmax);
   // R(l, j) = V[l + j m] for l <= j, written by the owners of column j
   auto R = [&](int l, int j) { return __ldcg(t.V + l + (size_t)j * m); };
   const int rc = (m + cs - 1) / cs;
@@ -987,7 +1067,9 @@ __device__ __forceinline__ void st_release(int* p, int v) {
 // its step, so the order matches the factorization (order_of_trans).  Waits
 // only target lower tickets, which are held by running CTAs, so the sweep
 // cannot deadlock; a wait that exceeds `spin_limit` cycles sets *status = 2.
-template <typename T>
+// kStaged: the interior's own reflectors stream through shared memory
+// (dev::vec_apply_staged), for levels with large interiors.
+template <typename T, bool kStaged>
 __global__ void __launch_bounds__(kThreads, 2) k_fwd_elim(const FwdElimTask* __restrict__ tasks,
                                                        const FwdOut* __restrict__ outs, int ntasks, int* ticket,
                                                        int* status, long long spin_limit, int nmax) {
@@ -1002,12 +1084,13 @@ __global__ void __launch_bounds__(kThreads, 2) k_fwd_elim(const FwdElimTask* __r
   const int ti = s_task;
   if (ti >= ntasks) return;
   const FwdElimTask t = tasks[ti];
-  T* red = sm;
+  T* red = sm + (kStaged ? dev::staged_elems<T>(nmax) : 0);
   T* xc = red + dev::kVecRed;
   T* xn = xc + (nmax > 0 ? nmax : 1);
   for (int i = threadIdx.x; i < t.n; i += kThreads) xc[i] = __ldcg(as<T>(t.x) + i);
   __syncthreads();
-  dev::apply_qt<T>(as<T>(t.S), t.n, as<T>(t.T), t.n, xc, t.n, t.n, 1, red, 2 * kNB);
+  if (kStaged) dev::vec_apply_staged<T>(as<T>(t.S), t.n, as<T>(t.T), t.n, xc, t.n, true, sm);
+  else dev::apply_qt<T>(as<T>(t.S), t.n, as<T>(t.T), t.n, xc, t.n, t.n, 1, red, 2 * kNB);
   for (int o = t.out_begin; o < t.out_end; ++o) {
     const FwdOut e = outs[o];
     if (threadIdx.x == 0) {
@@ -1043,31 +1126,39 @@ __global__ void __launch_bounds__(kThreads, 2) k_fwd_elim(const FwdElimTask* __r
   for (int i = threadIdx.x; i < t.n; i += kThreads) __stcg(as<T>(t.x) + i, xc[i]);
 }
 
-template <typename T>
+// kStaged: the reflector panels stream through shared memory
+// (dev::vec_apply_staged), for levels with large interfaces.
+template <typename T, bool kStaged>
 __global__ void __launch_bounds__(kThreads) k_fwd_spars(const FwdSparsTask* __restrict__ tasks) {
   extern __shared__ __align__(16) unsigned char smraw[];
   T* sm = reinterpret_cast<T*>(smraw);
   const FwdSparsTask t = tasks[blockIdx.x];
-  T* red = sm;
-  T* x = sm + 2 * kNB;
+  T* red = sm + (kStaged ? dev::staged_elems<T>(t.n) : 0);
+  T* x = red + 2 * kNB;
   for (int i = threadIdx.x; i < t.n; i += kThreads) x[i] = as<T>(t.x)[i];
   __syncthreads();
-  dev::apply_qt<T>(as<T>(t.Qs), t.n, as<T>(t.Ts), t.n, x, t.n, t.n, 1, red, 2 * kNB);
-  dev::apply_qt<T>(as<T>(t.V), t.n, as<T>(t.T), *t.rank, x, t.n, t.n, 1, red, 2 * kNB);
+  if (kStaged) {
+    dev::vec_apply_staged<T>(as<T>(t.Qs), t.n, as<T>(t.Ts), t.n, x, t.n, true, sm);
+    dev::vec_apply_staged<T>(as<T>(t.V), t.n, as<T>(t.T), *t.rank, x, t.n, true, sm);
+  } else {
+    dev::apply_qt<T>(as<T>(t.Qs), t.n, as<T>(t.Ts), t.n, x, t.n, t.n, 1, red, 2 * kNB);
+    dev::apply_qt<T>(as<T>(t.V), t.n, as<T>(t.T), *t.rank, x, t.n, t.n, 1, red, 2 * kNB);
+  }
   for (int i = threadIdx.x; i < t.n; i += kThreads) as<T>(t.x)[i] = x[i];
 }
 
-template <typename T>
+template <typename T, bool kStaged>
 __global__ void __launch_bounds__(kThreads) k_bwd_spars(const FwdSparsTask* __restrict__ tasks) {
   extern __shared__ __align__(16) unsigned char smraw[];
   T* sm = reinterpret_cast<T*>(smraw);
   const FwdSparsTask t = tasks[blockIdx.x];
-  T* red = sm;
+  T* red = sm + (kStaged ? dev::staged_elems<T>(t.n) : 0);
   T* xs = red + 2 * kNB;
   T* x = xs + 32;
   for (int i = threadIdx.x; i < t.n; i += kThreads) x[i] = as<T>(t.x)[i];
   __syncthreads();
-  dev::apply_q<T>(as<T>(t.V), t.n, as<T>(t.T), *t.rank, x, t.n, t.n, 1, red, 2 * kNB);
+  if (kStaged) dev::vec_apply_staged<T>(as<T>(t.V), t.n, as<T>(t.T), *t.rank, x, t.n, false, sm);
+  else dev::apply_q<T>(as<T>(t.V), t.n, as<T>(t.T), *t.rank, x, t.n, t.n, 1, red, 2 * kNB);
   dev::trsv_upper<T>(as<T>(t.Qs), t.n, x, t.n, xs);
   for (int i = threadIdx.x; i < t.n; i += kThreads) as<T>(t.x)[i] = x[i];
 }
@@ -1269,10 +1360,20 @@ constexpr size_t kSmemMax = 227 * 1024;
 template <typename K>
 cudaError_t prep(K kern, size_t bytes) {
   if (bytes > kSmemMax) return cudaErrorInvalidValue;
-  // above 48 KB of dynamic plus static shared memory the kernel must opt in;
-  // static shared memory of these kernels stays below 8 KB
-  if (bytes > 40 * 1024) return cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
-  return cudaSuccess;
+  // Above 48 KB of dynamic plus static shared memory the kernel must opt in;
+  // static shared memory of these kernels stays below 8 KB.  The opt-in is
+  // only ever raised: a launch captured into a CUDA graph keeps its size, and
+  // a later, smaller launch of the same kernel must not lower the limit under
+  // it (a graph node relaunched against the lowered limit fails).
+  if (bytes <= 40 * 1024) return cudaSuccess;
+  static std::mutex mu;
+  static std::unordered_map<const void*, size_t> raised;
+  std::lock_guard<std::mutex> lock(mu);
+  size_t& cur = raised[reinterpret_cast<const void*>(kern)];
+  if (bytes <= cur) return cudaSuccess;
+  const cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  if (e == cudaSuccess) cur = bytes;
+  return e;
 }
 
 template <typename... KArgs, typename... Args>
@@ -1332,29 +1433,63 @@ cudaError_t launch_permute(int n, const int* perm, const double* src, double* ds
   return last();
 }
 
+// Shared memory of a dist_qr kernel whose panels are factored in shared
+// memory: `head` bytes, then one region that serves as the tiled apply's
+// scratch and as the panel buffer (rows x kNB plus a kNB x kNB block); 0
+// when that does not fit (the kernel then factors panels in global memory).
+template <typename T>
+size_t staged_panel_bytes(size_t head, int rows) {
+  const size_t panel = ((size_t)rows * kNB + kNB * kNB) * sizeof(T);
+  const size_t region = std::max(smem_bytes(kWcap), panel);
+  return head + region + 1024 <= kSmemMax ? head + region : 0;
+}
+
 cudaError_t launch_elim(const ElimTask* t, const ElimOut* o, int ntasks, int cs, int nmax, int vmax,
                         cudaStream_t st) {
   if (cudaError_t pre = begin("launch_elim")) return pre;
   if (ntasks <= 0) return cudaSuccess;
-  const size_t b = smem_bytes(kRed + kNB + (size_t)nmax + (size_t)std::max(vmax, 1) + kWcap);
+  vmax = std::max(vmax, 1);
+  const size_t head = smem_bytes(kRed + kNB + (size_t)nmax + (size_t)vmax);
   if (g_fp32) {
-    if (cudaError_t e = prep(k_elim<float>, b)) return e;
-    return launch_clustered(k_elim<float>, ntasks, cs, b, st, t, o, cs, vmax, g_status);
+    const size_t bs = staged_panel_bytes<float>(head, vmax);
+    if (bs) {
+      if (cudaError_t e = prep(k_elim<float, true>, bs)) return e;
+      return launch_clustered(k_elim<float, true>, ntasks, cs, bs, st, t, o, cs, vmax, g_status);
+    }
+    if (cudaError_t e = prep(k_elim<float, false>, head + smem_bytes(kWcap))) return e;
+    return launch_clustered(k_elim<float, false>, ntasks, cs, head + smem_bytes(kWcap), st, t, o, cs, vmax,
+                            g_status);
   }
-  if (cudaError_t e = prep(k_elim<double>, b)) return e;
-  return launch_clustered(k_elim<double>, ntasks, cs, b, st, t, o, cs, vmax, g_status);
+  const size_t bs = staged_panel_bytes<double>(head, vmax);
+  if (bs) {
+    if (cudaError_t e = prep(k_elim<double, true>, bs)) return e;
+    return launch_clustered(k_elim<double, true>, ntasks, cs, bs, st, t, o, cs, vmax, g_status);
+  }
+  if (cudaError_t e = prep(k_elim<double, false>, head + smem_bytes(kWcap))) return e;
+  return launch_clustered(k_elim<double, false>, ntasks, cs, head + smem_bytes(kWcap), st, t, o, cs, vmax, g_status);
 }
 
 cudaError_t launch_scale(const ScaleTask* t, int ntasks, int cs, int nmax, cudaStream_t st) {
   if (cudaError_t pre = begin("launch_scale")) return pre;
   if (ntasks <= 0) return cudaSuccess;
-  const size_t b = smem_bytes(kRed + kNB + 2 * (size_t)nmax + kWcap);
+  nmax = std::max(nmax, 1);
+  const size_t head = smem_bytes(kRed + kNB + 2 * (size_t)nmax);
   if (g_fp32) {
-    if (cudaError_t e = prep(k_scale<float>, b)) return e;
-    return launch_clustered(k_scale<float>, ntasks, cs, b, st, t, cs, g_status);
+    const size_t bs = staged_panel_bytes<float>(head, nmax);
+    if (bs) {
+      if (cudaError_t e = prep(k_scale<float, true>, bs)) return e;
+      return launch_clustered(k_scale<float, true>, ntasks, cs, bs, st, t, cs, nmax, g_status);
+    }
+    if (cudaError_t e = prep(k_scale<float, false>, head + smem_bytes(kWcap))) return e;
+    return launch_clustered(k_scale<float, false>, ntasks, cs, head + smem_bytes(kWcap), st, t, cs, nmax, g_status);
   }
-  if (cudaError_t e = prep(k_scale<double>, b)) return e;
-  return launch_clustered(k_scale<double>, ntasks, cs, b, st, t, cs, g_status);
+  const size_t bs = staged_panel_bytes<double>(head, nmax);
+  if (bs) {
+    if (cudaError_t e = prep(k_scale<double, true>, bs)) return e;
+    return launch_clustered(k_scale<double, true>, ntasks, cs, bs, st, t, cs, nmax, g_status);
+  }
+  if (cudaError_t e = prep(k_scale<double, false>, head + smem_bytes(kWcap))) return e;
+  return launch_clustered(k_scale<double, false>, ntasks, cs, head + smem_bytes(kWcap), st, t, cs, nmax, g_status);
 }
 
 cudaError_t launch_update(const UpdTask* t, const UpdOp* o, int ntasks, cudaStream_t st) {
@@ -1487,19 +1622,27 @@ cudaError_t launch_rrqr(const RrqrTask* t, int ntasks, int cs, int mmax, int kma
 
 int selected_qr_rows(int nmax) { return std::max(1, std::min(32, 12288 / (std::max(nmax, 1) + 1))); }
 
-size_t selected_qr_smem(int mmax, int nmax) {
+// stage: with room for the QR's staged panel (0 when that does not fit)
+size_t selected_qr_smem(int mmax, int nmax, bool stage) {
   const int rt = selected_qr_rows(nmax);
-  return smem_bytes(kRed + kNB + (size_t)std::max(nmax, 1) + (size_t)std::max(mmax, 1) +
-                    std::max((size_t)rt * (std::max(nmax, 1) + 1) + 32 * 33, (size_t)kWcap));
+  mmax = std::max(mmax, 1);
+  size_t region = std::max((size_t)rt * (std::max(nmax, 1) + 1) + 32 * 33, (size_t)kWcap);
+  if (stage) region = std::max(region, (size_t)mmax * kNB + kNB * kNB);
+  const size_t b = smem_bytes(kRed + kNB + (size_t)std::max(nmax, 1) + (size_t)mmax + region);
+  return !stage || b + 1024 <= kSmemMax ? b : 0;
 }
 
 cudaError_t launch_selected_qr(const RrqrTask* t, int ntasks, int cs, int mmax, int nmax, cudaStream_t st) {
   if (cudaError_t pre = begin("launch_selected_qr")) return pre;
   if (ntasks <= 0) return cudaSuccess;
-  const size_t b = selected_qr_smem(mmax, nmax);
-  if (cudaError_t e = prep(k_selected_qr, b)) return e;
-  return launch_clustered(k_selected_qr, ntasks, cs, b, st, t, cs, std::max(mmax, 1), std::max(nmax, 1),
-                          selected_qr_rows(nmax));
+  const int mm = std::max(mmax, 1), nn = std::max(nmax, 1), rt = selected_qr_rows(nmax);
+  if (const size_t bs = selected_qr_smem(mmax, nmax, true)) {
+    if (cudaError_t e = prep(k_selected_qr<true>, bs)) return e;
+    return launch_clustered(k_selected_qr<true>, ntasks, cs, bs, st, t, cs, mm, nn, rt);
+  }
+  const size_t b = selected_qr_smem(mmax, nmax, false);
+  if (cudaError_t e = prep(k_selected_qr<false>, b)) return e;
+  return launch_clustered(k_selected_qr<false>, ntasks, cs, b, st, t, cs, mm, nn, rt);
 }
 
 cudaError_t launch_merge(const MergeTask* t, int ntasks, cudaStream_t st) {
@@ -1511,50 +1654,73 @@ cudaError_t launch_merge(const MergeTask* t, int ntasks, cudaStream_t st) {
   return last();
 }
 
+// The staged sweep kernels (reflector panels streamed through shared memory)
+// serve levels whose largest block has at least kStagedMin rows and whose
+// buffers fit; smaller blocks keep more CTAs per SM with the direct loads.
+constexpr int kStagedMin = 256;
+template <typename T>
+bool use_staged(int nmax, size_t other_bytes) {
+  // 1 KB left for the kernels' static shared memory
+  return nmax >= kStagedMin && dev::staged_elems<T>(nmax) * sizeof(T) + other_bytes + 1024 <= kSmemMax;
+}
+
 cudaError_t launch_fwd_elim(const FwdElimTask* t, const FwdOut* o, int ntasks, int nmax, int mmax, int* ticket,
                             int* status, long long spin_limit, cudaStream_t st) {
   if (cudaError_t pre = begin("launch_fwd_elim")) return pre;
   if (ntasks <= 0) return cudaSuccess;
   const size_t b = smem_bytes(dev::kVecRed + (size_t)std::max(nmax, 1) + (size_t)std::max(mmax, 1));
   counted();
+  auto go = [&](auto kern, size_t bytes) -> cudaError_t {
+    if (cudaError_t e = prep(kern, bytes)) return e;
+    kern<<<ntasks, kThreads, bytes, st>>>(t, o, ntasks, ticket, status, spin_limit, nmax);
+    return cudaSuccess;
+  };
+  cudaError_t e;
+  if (g_fp32)
+    e = use_staged<float>(nmax, b) ? go(k_fwd_elim<float, true>, dev::staged_elems<float>(nmax) * sizeof(float) + b)
+                                   : go(k_fwd_elim<float, false>, b);
+  else
+    e = use_staged<double>(nmax, b)
+            ? go(k_fwd_elim<double, true>, dev::staged_elems<double>(nmax) * sizeof(double) + b)
+            : go(k_fwd_elim<double, false>, b);
+  if (e) return e;
+  return last();
+}
+
+// k_fwd_spars / k_bwd_spars over ntasks interfaces of at most nmax rows
+template <bool kFwd>
+cudaError_t launch_spars(const FwdSparsTask* t, int ntasks, int nmax, cudaStream_t st) {
+  const size_t b = smem_bytes(2 * kNB + 32 + (size_t)std::max(nmax, 1));
+  counted();
+  auto go = [&](auto kern, size_t bytes) -> cudaError_t {
+    if (cudaError_t e = prep(kern, bytes)) return e;
+    kern<<<ntasks, kThreads, bytes, st>>>(t);
+    return cudaSuccess;
+  };
+  cudaError_t e;
   if (g_fp32) {
-    if (cudaError_t e = prep(k_fwd_elim<float>, b)) return e;
-    k_fwd_elim<float><<<ntasks, kThreads, b, st>>>(t, o, ntasks, ticket, status, spin_limit, nmax);
+    const size_t bs = dev::staged_elems<float>(nmax) * sizeof(float) + b;
+    if (use_staged<float>(nmax, b)) e = kFwd ? go(k_fwd_spars<float, true>, bs) : go(k_bwd_spars<float, true>, bs);
+    else e = kFwd ? go(k_fwd_spars<float, false>, b) : go(k_bwd_spars<float, false>, b);
   } else {
-    if (cudaError_t e = prep(k_fwd_elim<double>, b)) return e;
-    k_fwd_elim<double><<<ntasks, kThreads, b, st>>>(t, o, ntasks, ticket, status, spin_limit, nmax);
+    const size_t bs = dev::staged_elems<double>(nmax) * sizeof(double) + b;
+    if (use_staged<double>(nmax, b)) e = kFwd ? go(k_fwd_spars<double, true>, bs) : go(k_bwd_spars<double, true>, bs);
+    else e = kFwd ? go(k_fwd_spars<double, false>, b) : go(k_bwd_spars<double, false>, b);
   }
+  if (e) return e;
   return last();
 }
 
 cudaError_t launch_fwd_spars(const FwdSparsTask* t, int ntasks, int nmax, cudaStream_t st) {
   if (cudaError_t pre = begin("launch_fwd_spars")) return pre;
   if (ntasks <= 0) return cudaSuccess;
-  const size_t b = smem_bytes(2 * kNB + (size_t)nmax);
-  counted();
-  if (g_fp32) {
-    if (cudaError_t e = prep(k_fwd_spars<float>, b)) return e;
-    k_fwd_spars<float><<<ntasks, kThreads, b, st>>>(t);
-  } else {
-    if (cudaError_t e = prep(k_fwd_spars<double>, b)) return e;
-    k_fwd_spars<double><<<ntasks, kThreads, b, st>>>(t);
-  }
-  return last();
+  return launch_spars<true>(t, ntasks, nmax, st);
 }
 
 cudaError_t launch_bwd_spars(const FwdSparsTask* t, int ntasks, int nmax, cudaStream_t st) {
   if (cudaError_t pre = begin("launch_bwd_spars")) return pre;
   if (ntasks <= 0) return cudaSuccess;
-  const size_t b = smem_bytes(2 * kNB + 32 + (size_t)nmax);
-  counted();
-  if (g_fp32) {
-    if (cudaError_t e = prep(k_bwd_spars<float>, b)) return e;
-    k_bwd_spars<float><<<ntasks, kThreads, b, st>>>(t);
-  } else {
-    if (cudaError_t e = prep(k_bwd_spars<double>, b)) return e;
-    k_bwd_spars<double><<<ntasks, kThreads, b, st>>>(t);
-  }
-  return last();
+  return launch_spars<false>(t, ntasks, nmax, st);
 }
 
 cudaError_t launch_bwd_elim(const BwdElimTask* t, const BwdIn* in, int ntasks, int nmax, cudaStream_t st) {

@@ -74,7 +74,9 @@ cudaError_t launch_rrqr(const RrqrTask* t, int ntasks, int cs, int mmax, int kma
 // V / T / tau and the orthonormal basis Qc = C_sel R^{-1}; cs-CTA clusters,
 // tasks of at most mmax rows and nmax selected columns.  Uses C, Qc, V, T,
 // tau, colat, rank, m, ldw of the task.
-size_t selected_qr_smem(int mmax, int nmax);
+// Shared memory of k_selected_qr; stage: with room for the QR's panels in
+// shared memory (0 when that does not fit).
+size_t selected_qr_smem(int mmax, int nmax, bool stage);
 cudaError_t launch_selected_qr(const RrqrTask* t, int ntasks, int cs, int mmax, int nmax, cudaStream_t st);
 cudaError_t launch_merge(const MergeTask* t, int ntasks, cudaStream_t st);
 
