@@ -379,9 +379,11 @@ __global__ void k_mlp_adam(float* P, const float* __restrict__ g, float* m1, flo
 
 // ---------------------------------------------------------------- sketch / projection GEMMs
 // 64 x 64 output tile per CTA, k-steps of 32, each thread a 4 x 4 block of
-// outputs at rows ty + 16 a, columns tx + 16 b.  The next k-step's tiles are
-// copied into the other half of a double buffer with cp.async while the
-// current one is multiplied; every output sums its k terms in ascending order.
+// outputs at rows ty + 16 a, columns tx + 16 b.  In the sketch the next
+// k-step's C tile is copied into the other half of a double buffer with
+// cp.async while the current one is multiplied (the projection loads each
+// step's tiles directly: its two tiles in a double buffer would halve the
+// CTAs per SM); every output sums its k terms in ascending order.
 __global__ void __launch_bounds__(kT) k_sketch(const SketchTask* __restrict__ tasks,
                                                const GemmTile* __restrict__ tiles) {
   __shared__ double As[2][kTile][kKStep + 1];      // C(r0 + rr, j0 + jj) at As[.][rr][jj]
@@ -442,68 +444,41 @@ __global__ void __launch_bounds__(kT) k_sketch(const SketchTask* __restrict__ ta
   }
 }
 
-// Shared memory of k_project: double-buffered Q (kTile x (kKStep + 1)) and
-// C (kKStep x kTile) tiles.
-constexpr int kProjA = kTile * (kKStep + 1);
-constexpr int kProjB = kKStep * kTile;
-constexpr size_t kProjSmem = 2 * sizeof(double) * (kProjA + kProjB);
-
 // B(l, j) = sum_r Q(r, l) C(r, j); tile rows l (basis vectors), columns j
 __global__ void __launch_bounds__(kT) k_project(const SketchTask* __restrict__ tasks,
                                                 const GemmTile* __restrict__ tiles) {
-  extern __shared__ __align__(16) double psm_proj[];
-  // Q(k0 + rr, r0 + ll) at As(b)[ll * (kKStep + 1) + rr]; C(k0 + rr, c0 + jj) at Bs(b)[rr * kTile + jj]
-  double* const As0 = psm_proj;
-  double* const Bs0 = psm_proj + 2 * kProjA;
+  __shared__ double As[kKStep][kTile + 1];  // Q(r0 + rr, l0 + ll) at As[rr][ll]
+  __shared__ double Bs[kKStep][kTile + 1];  // C(r0 + rr, j0 + jj) at Bs[rr][jj]
   const GemmTile g = tiles[blockIdx.x];
   const SketchTask t = tasks[g.task];
   const int ell = *t.ell;
   if (g.r0 >= ell) return;
   const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
-  const int nsteps = (t.m + kKStep - 1) / kKStep;
-  auto load = [&](int s, int b) {
-    const int k0 = s * kKStep;
-    double* As = As0 + b * kProjA;
-    double* Bs = Bs0 + b * kProjB;
+  double acc[4][4] = {};
+  for (int k0 = 0; k0 < t.m; k0 += kKStep) {
     for (int e = threadIdx.x; e < kTile * kKStep; e += kT) {
       const int ll = e / kKStep, rr = e % kKStep;
       const int l = g.r0 + ll, r = k0 + rr;
-      if (l < ell && r < t.m) dev::cp_async_elem(As + ll * (kKStep + 1) + rr, t.Qc + (size_t)l * t.m + r);
-      else As[ll * (kKStep + 1) + rr] = 0.0;
+      As[rr][ll] = (l < ell && r < t.m) ? __ldg(t.Qc + (size_t)l * t.m + r) : 0.0;
     }
     for (int e = threadIdx.x; e < kTile * kKStep; e += kT) {
       const int rr = e / kTile, jj = e % kTile;
       const int r = k0 + rr, j = g.c0 + jj;
-      if (r < t.m && j < t.w) dev::cp_async_elem(Bs + rr * kTile + jj, t.C + (size_t)r * t.ldw + j);
-      else Bs[rr * kTile + jj] = 0.0;
-    }
-    dev::cp_async_commit();
-  };
-  double acc[4][4] = {};
-  if (nsteps > 0) load(0, 0);
-  for (int s = 0; s < nsteps; ++s) {
-    const int b = s & 1;
-    if (s + 1 < nsteps) {
-      load(s + 1, b ^ 1);
-      dev::cp_async_wait<1>();
-    } else {
-      dev::cp_async_wait<0>();
+      Bs[rr][jj] = (r < t.m && j < t.w) ? __ldg(t.C + (size_t)r * t.ldw + j) : 0.0;
     }
     __syncthreads();
-    const double* As = As0 + b * kProjA;
-    const double* Bs = Bs0 + b * kProjB;
 #pragma unroll 8
     for (int rr = 0; rr < kKStep; ++rr) {
-      double a[4], bq[4];
+      double a[4], b[4];
 #pragma unroll
       for (int q = 0; q < 4; ++q) {
-        a[q] = As[(ty + 16 * q) * (kKStep + 1) + rr];
-        bq[q] = Bs[rr * kTile + tx + 16 * q];
+        a[q] = As[rr][ty + 16 * q];
+        b[q] = Bs[rr][tx + 16 * q];
       }
 #pragma unroll
       for (int p = 0; p < 4; ++p)
 #pragma unroll
-        for (int q = 0; q < 4; ++q) acc[p][q] += a[p] * bq[q];
+        for (int q = 0; q < 4; ++q) acc[p][q] += a[p] * b[q];
     }
     __syncthreads();
   }
@@ -797,10 +772,7 @@ cudaError_t launch_sketch(const SketchTask* t, const GemmTile* tiles, int ntiles
 cudaError_t launch_project(const SketchTask* t, const GemmTile* tiles, int ntiles, cudaStream_t st) {
   if (cudaError_t e = cudaGetLastError()) return e;
   if (ntiles <= 0) return cudaSuccess;
-  static const cudaError_t attr =
-      cudaFuncSetAttribute(k_project, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kProjSmem);
-  if (attr) return attr;
-  k_project<<<ntiles, kT, kProjSmem, st>>>(t, tiles);
+  k_project<<<ntiles, kT, 0, st>>>(t, tiles);
   return done_launch("launch_project");
 }
 
