@@ -123,6 +123,56 @@ __device__ void panel_t(const T* V, int ldv, int m, int kb, int unit, const T* t
   larft_from_gram(Tm, ldt, kb, tau, tmp);
 }
 
+// panel_t for a panel in shared memory, with T built by one warp: the Gram
+// V^T V of the panel's reflectors goes to sG (kNB x (kNB + 1), shared), then
+// lane i holds row i of T in registers and forms column j as
+//   T(i, j) = -tau_j sum_{l=i}^{j-1} T(i, l) G(l, j),  T(j, j) = tau_j,
+// the sums of larft_from_gram in the same order, without its two barriers
+// and global round trips per column.  Tm is written by warp 0; the caller
+// synchronises before T is read.
+template <typename T>
+__device__ void panel_t_warp(const T* V, int ldv, int m, int kb, int unit, const T* tau, T* Tm, int ldt, T* sG) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  constexpr int kLG = kNB + 1;
+  const int npairs = kb * (kb - 1) / 2;
+  for (int p = warp; p < npairs; p += kWarps) {
+    int l, j;
+    pair_of(p, &l, &j);
+    const T* vl = V + (size_t)l * ldv;
+    const T* vj = V + (size_t)j * ldv;
+    T d = 0.0;
+    if (unit) {
+      d = lane == 0 ? vl[j] : 0.0;
+      for (int i = j + 1 + lane; i < m; i += 32) d += vl[i] * vj[i];
+    } else {
+      for (int i = lane; i < m; i += 32) d += vl[i] * vj[i];
+    }
+    d = warp_sum(d);
+    if (lane == 0) sG[l * kLG + j] = d;
+  }
+  __syncthreads();
+  if (warp == 0) {
+    T t[kNB];
+#pragma unroll
+    for (int j = 0; j < kNB; ++j) t[j] = 0.0;
+#pragma unroll
+    for (int j = 0; j < kNB; ++j) {
+      if (j < kb) {
+        T s = 0.0;
+#pragma unroll
+        for (int l = 0; l < kNB; ++l)
+          if (l < j && l >= lane) s += t[l] * sG[l * kLG + j];
+        const T tj = tau[j];
+        t[j] = lane < j ? -tj * s : (lane == j ? tj : (T)0.0);
+      }
+    }
+    if (lane < kb)
+#pragma unroll
+      for (int j = 0; j < kNB; ++j)
+        if (j < kb) Tm[lane + (size_t)j * ldt] = t[j];
+  }
+}
+
 // ---------------------------------------------------------------- applies
 // C (m x nc) <- (I - V T V^T)^T C for one block of k <= kNB reflectors,
 // V unit lower trapezoidal (m x k), T (k x k, ld ldt).  W: 2*k*nc doubles.

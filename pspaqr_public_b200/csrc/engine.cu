@@ -1150,12 +1150,17 @@ int Tree::factorize() {
         for (auto& e : le) cudaEventDestroy(e);
       }
       if (fp32_ && nsp) {
+        // one CTA per piece of at most kConvPiece elements
+        constexpr long long kConvPiece = 65536;
         std::vector<ConvTask> cv;
+        auto conv = [&](const double* src, double* dst, long long n) {
+          for (long long off = 0; off < n; off += kConvPiece) cv.push_back({src, dst, std::min(kConvPiece, n - off), off});
+        };
         for (size_t q = 0; q < nsp; ++q) {
           const int p = Lv.spars_clusters[q];
           const long long mp = std::max(size_[p], 1);
-          cv.push_back({spV[q], Qsp_[p], mp * mp});
-          cv.push_back({spT[q], Tsp_[p], (long long)NB * mp});
+          conv(spV[q], Qsp_[p], mp * mp);
+          conv(spT[q], Tsp_[p], (long long)NB * mp);
         }
         auto* d_cv = static_cast<ConvTask*>(up_any(cv));
         if (!d_cv || ck(launch_to_f32_batch(d_cv, (int)cv.size(), stream_), "factor conversion")) return -10;
@@ -1275,14 +1280,21 @@ int Tree::factorize() {
         t.roff = rpos_[E.n2];
         t.coff = rpos_[E.n1];
         t.identity = (E.n1 == E.n2 && st_.clusters[E.n1].sparsify) ? 1 : 0;
-        if (t.rows > 0 && t.cols > 0) mt.push_back(t);
+        // one CTA per slab of at most about 16K elements
+        const int slab = std::max(1, 16384 / std::max(t.rows, 1));
+        for (int c0 = 0; t.rows > 0 && c0 < t.cols; c0 += slab) {
+          MergeTask u = t;
+          u.c0 = c0;
+          u.cols = std::min(slab, t.cols - c0);
+          mt.push_back(u);
+        }
       }
       P.merge_valid = true;
       if (check_descriptors) {
         const size_t es = fp32_ ? 4 : 8;
         for (const MergeTask& m : mt)
-          if (!arena_.contains(m.src, es * ((size_t)m.ld_src * (m.cols - 1) + m.rows)) ||
-              !arena_.contains(m.dst, es * ((size_t)m.ld_dst * (m.coff + m.cols - 1) + m.roff + m.rows)))
+          if (!arena_.contains(m.src, es * ((size_t)m.ld_src * (m.c0 + m.cols - 1) + m.rows)) ||
+              !arena_.contains(m.dst, es * ((size_t)m.ld_dst * (m.coff + m.c0 + m.cols - 1) + m.roff + m.rows)))
             return fail(-5, "merge descriptor of level " + std::to_string(lvl) +
                                 " addresses memory outside the block pool; nothing launched");
       }

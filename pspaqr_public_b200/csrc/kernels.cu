@@ -32,6 +32,9 @@ using dev::kThreads;
 using dev::kWarps;
 
 constexpr int kRed = 16;     // reduction scratch (doubles)
+// dist_qr's staged panel beyond its rows x kNB: the tpqrt's R block (kNB x
+// kNB) and the panel's Gram matrix (kNB x (kNB + 1))
+constexpr int kPanExtra = kNB * kNB + kNB * (kNB + 1);
 constexpr int kWcap = dev::kTileSmem;  // shared scratch (doubles) of the tiled block applies
 
 __device__ __forceinline__ void csync(int cs) {
@@ -69,11 +72,10 @@ __global__ void k_scatter(int nnz, const double* __restrict__ val, double* const
 // (two of its panels per pass).  `lt` holds the owner's tau values, `tg`
 // the global copy, `vb` a reflector tail, `tile` dev::kTileSmem elements.
 //
-// With `pan` (ldp >= the panel's rows; ldp * kNB + kNB * kNB elements, may
+// With `pan` (ldp >= the panel's rows; ldp * kNB + kPanExtra elements, may
 // alias `tile`), the owner copies the panel into shared memory, runs the kb
-// reflector steps and the T factor there and writes the panel back once:
-// the same operations in the same order as on global memory, without a
-// global round trip per step.
+// reflector steps and the T factor there (one barrier per reflector, T by
+// one warp) and writes the panel back once.
 template <typename T>
 __device__ void dist_qr(T* R, int ldr, T* B, int ldb, int m, int n, int unit, T* Tout, T* tg,
                         T* lt, T* vb, T* red, T* tmp, T* tile, int cs, int* status = nullptr, T* pan = nullptr,
@@ -88,6 +90,7 @@ __device__ void dist_qr(T* R, int ldr, T* B, int ldb, int m, int n, int unit, T*
       // panel rows: [j0, m) of R's columns (geqrt) or B's m rows (tpqrt)
       const int pm = unit ? m - j0 : m;
       T* pr = pan + (size_t)ldp * kNB;  // tpqrt: R(j0:pend, j0:pend), ld kNB
+      T* sG = pr + kNB * kNB;           // the panel's Gram matrix (panel_t_warp)
       __syncthreads();                  // `pan` may alias the tiled apply's scratch
       for (int c = warp; c < kb; c += kWarps) {
         const T* src = unit ? (R + j0 + (size_t)(j0 + c) * ldr) : (B + (size_t)(j0 + c) * ldb);
@@ -99,40 +102,75 @@ __device__ void dist_qr(T* R, int ldr, T* B, int ldb, int m, int n, int unit, T*
           if (r <= c) pr[r + c * kNB] = __ldcg(R + (j0 + r) + (size_t)(j0 + c) * ldr);
         }
       __syncthreads();
+      // One barrier per reflector.  Every thread forms reflector j from its
+      // alpha and the squared norm of its tail; warp w applies it to columns
+      // j + 1 + w, ... with v = tail * scal formed on the fly, and the warp of
+      // column j + 1 also sums that column's new tail for reflector j + 1.
+      // The scaled tail and beta are stored one step later, when no warp
+      // reads them.
+      __shared__ T s_nrm2[2];
+      T nrm2;
+      {
+        const int vlen = unit ? m - j0 - 1 : m;
+        const T* tail = unit ? pan + 1 : pan;
+        T sq = 0.0;
+        for (int i = threadIdx.x; i < vlen; i += kThreads) sq += tail[i] * tail[i];
+        nrm2 = dev::cta_sum(sq, red);
+      }
+      T* prev_tail = nullptr;
+      T prev_scal = 0.0;
+      int prev_vlen = 0;
+      T* prev_ajj = nullptr;
+      T prev_beta = 0.0;
       for (int j = j0; j < pend; ++j) {
         const int jj = j - j0;
         const int vlen = unit ? (m - j - 1) : m;
         T* tail = unit ? (pan + (jj + 1) + (size_t)jj * ldp) : (pan + (size_t)jj * ldp);
         T* ajj = unit ? (pan + jj + (size_t)jj * ldp) : (pr + jj + jj * kNB);
-        T s = 0.0;
-        for (int i = threadIdx.x; i < vlen; i += kThreads) s += tail[i] * tail[i];
-        s = dev::cta_sum(s, red);
         const T alpha = *ajj;
         T beta, scal;
-        const T tj = dev::house(alpha, s, &beta, &scal);
-        if (tj != 0.0)
-          for (int i = threadIdx.x; i < vlen; i += kThreads) tail[i] *= scal;
+        const T tj = dev::house(alpha, nrm2, &beta, &scal);
+        if (prev_tail)
+          for (int i = threadIdx.x; i < prev_vlen; i += kThreads) prev_tail[i] *= prev_scal;
         if (threadIdx.x == 0) {
-          *ajj = beta;
+          if (prev_ajj) *prev_ajj = prev_beta;
           lt[j] = tj;
           tg[j] = tj;
+          // R(j, j) = 0 or not finite: the triangular solves would break down
           if (status && !(isfinite(beta) && beta != (T)0)) atomicOr(status, isfinite(beta) ? 8 : 4);
         }
-        __syncthreads();
-        if (tj != 0.0)
-          for (int k = j + 1 + warp; k < pend; k += kWarps) {
-            const int kk = k - j0;
-            T* rjk = unit ? (pan + jj + (size_t)kk * ldp) : (pr + jj + kk * kNB);
-            T* tk = unit ? (pan + (jj + 1) + (size_t)kk * ldp) : (pan + (size_t)kk * ldp);
+        for (int k = j + 1 + warp; k < pend; k += kWarps) {
+          const int kk = k - j0;
+          T* rjk = unit ? (pan + jj + (size_t)kk * ldp) : (pr + jj + kk * kNB);
+          T* tk = unit ? (pan + (jj + 1) + (size_t)kk * ldp) : (pan + (size_t)kk * ldp);
+          if (tj != 0.0) {
             T d = lane == 0 ? *rjk : 0.0;
-            for (int i = lane; i < vlen; i += 32) d += tail[i] * tk[i];
+            for (int i = lane; i < vlen; i += 32) d += (tail[i] * scal) * tk[i];
             d = dev::warp_sum(d) * tj;
             if (lane == 0) *rjk -= d;
-            for (int i = lane; i < vlen; i += 32) tk[i] -= tail[i] * d;
+            for (int i = lane; i < vlen; i += 32) tk[i] -= (tail[i] * scal) * d;
           }
+          if (k == j + 1) {  // reflector j + 1's tail: rows below its diagonal
+            T sq = 0.0;
+            for (int i = lane; i < vlen; i += 32)
+              if (!unit || i > 0) sq += tk[i] * tk[i];
+            sq = dev::warp_sum(sq);
+            if (lane == 0) s_nrm2[(j + 1) & 1] = sq;
+          }
+        }
+        prev_tail = tj != 0.0 ? tail : nullptr;
+        prev_scal = scal;
+        prev_vlen = vlen;
+        prev_ajj = ajj;
+        prev_beta = beta;
         __syncthreads();
+        nrm2 = s_nrm2[(j + 1) & 1];
       }
-      dev::panel_t(pan, ldp, pm, kb, unit, lt + j0, Tout + (size_t)j0 * kNB, kNB, tmp);
+      if (prev_tail)
+        for (int i = threadIdx.x; i < prev_vlen; i += kThreads) prev_tail[i] *= prev_scal;
+      if (threadIdx.x == 0 && prev_ajj) *prev_ajj = prev_beta;
+      __syncthreads();
+      dev::panel_t_warp(pan, ldp, pm, kb, unit, lt + j0, Tout + (size_t)j0 * kNB, kNB, sG);
       for (int c = warp; c < kb; c += kWarps) {
         T* dst = unit ? (R + j0 + (size_t)(j0 + c) * ldr) : (B + (size_t)(j0 + c) * ldb);
         for (int i = lane; i < pm; i += 32) dst[i] = pan[i + (size_t)c * ldp];
@@ -1045,7 +1083,7 @@ __global__ void k_merge(const MergeTask* __restrict__ tasks) {
   const T* src = as<T>(t.src);
   T* dst = as<T>(t.dst);
   for (int idx = threadIdx.x; idx < total; idx += blockDim.x) {
-    const int i = idx % t.rows, j = idx / t.rows;
+    const int i = idx % t.rows, j = t.c0 + idx / t.rows;
     const T v = t.identity ? (i == j ? (T)1 : (T)0) : src[i + (size_t)j * t.ld_src];
     dst[(t.roff + i) + (size_t)(t.coff + j) * t.ld_dst] = v;
   }
@@ -1344,7 +1382,7 @@ __global__ void k_to_f64(long long n, const float* __restrict__ src, double* __r
 __global__ void k_to_f32_batch(const ConvTask* __restrict__ tasks) {
   const ConvTask t = tasks[blockIdx.x];
   float* dst = reinterpret_cast<float*>(t.dst);
-  for (long long i = threadIdx.x; i < t.n; i += blockDim.x) dst[i] = (float)t.src[i];
+  for (long long i = t.off + threadIdx.x; i < t.off + t.n; i += blockDim.x) dst[i] = (float)t.src[i];
 }
 
 // ---------------------------------------------------------------- launchers
@@ -1439,7 +1477,7 @@ cudaError_t launch_permute(int n, const int* perm, const double* src, double* ds
 // when that does not fit (the kernel then factors panels in global memory).
 template <typename T>
 size_t staged_panel_bytes(size_t head, int rows) {
-  const size_t panel = ((size_t)rows * kNB + kNB * kNB) * sizeof(T);
+  const size_t panel = ((size_t)rows * kNB + kPanExtra) * sizeof(T);
   const size_t region = std::max(smem_bytes(kWcap), panel);
   return head + region + 1024 <= kSmemMax ? head + region : 0;
 }
@@ -1627,7 +1665,7 @@ size_t selected_qr_smem(int mmax, int nmax, bool stage) {
   const int rt = selected_qr_rows(nmax);
   mmax = std::max(mmax, 1);
   size_t region = std::max((size_t)rt * (std::max(nmax, 1) + 1) + 32 * 33, (size_t)kWcap);
-  if (stage) region = std::max(region, (size_t)mmax * kNB + kNB * kNB);
+  if (stage) region = std::max(region, (size_t)mmax * kNB + kPanExtra);
   const size_t b = smem_bytes(kRed + kNB + (size_t)std::max(nmax, 1) + (size_t)mmax + region);
   return !stage || b + 1024 <= kSmemMax ? b : 0;
 }

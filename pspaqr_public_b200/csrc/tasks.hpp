@@ -96,6 +96,7 @@ struct MergeTask {
   double* dst;
   int ld_src, ld_dst, rows, cols, roff, coff;
   int identity;  // 1: write I_rows (the diagonal block of a sparsified child)
+  int c0;        // first column of this slab of the child block (large blocks are split)
 };
 
 // ----------------------------------------------------------------- solve
@@ -143,6 +144,7 @@ struct ConvTask {
   const double* src;
   double* dst;  // holds floats
   long long n;
+  long long off;  // first element of this piece (large arrays are split)
 };
 
 }  // namespace spq
