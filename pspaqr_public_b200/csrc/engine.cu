@@ -25,6 +25,16 @@ constexpr size_t kAlign = 256;
 constexpr size_t kArenaChunk = size_t(1) << 30;
 // bounded wait of the forward sweep: ~1 s at 2 GHz
 constexpr int kChunk = 64;        // columns (rows) per CTA of the chunked applies
+
+// Row scaling / left compression chunks of the FP32 factorization: those of
+// blocks small enough for the warp-per-chunk kernel first (stable, so a stored
+// plan stays partitioned); returns how many.  The FP64 factorization keeps
+// the tiled kernel (the warp form would spill its registers in FP64).
+static int partition_small_left(std::vector<EdgeChunk>& v, bool fp32) {
+  if (!fp32) return 0;
+  const auto mid = std::stable_partition(v.begin(), v.end(), [](const EdgeChunk& c) { return edge_left_small(c.m); });
+  return (int)(mid - v.begin());
+}
 constexpr int kBigCluster = 8;    // CTAs per task for blocks of >= 8 panels
 constexpr int kRrqrMaxCols = 1024;  // own columns of C per CTA (four per thread)
 // shared memory of a CTA holding its block of C (the sketches of the learned
@@ -681,12 +691,15 @@ int Tree::factorize() {
       }
       lt_[lvl].flops[3] += P.fl_sapp;
       {
+        const int nrows_small = partition_small_left(rows_scale, fp32_);
         auto* d_rows = static_cast<EdgeChunk*>(up_vec(rows_scale));
         auto* d_cols = static_cast<EdgeChunk*>(up_vec(cols_scale));
         if (!d_rows || !d_cols) return fail(-11, "out of device memory (scaling)");
         set_tensor_cores(use_tc(lvl, 1));
         lt_[lvl].kind_tc[1] = tensor_cores_on();
-        if (ck(launch_edge(0, d_rows, (int)rows_scale.size(), stream_), "row scaling")) return -10;
+        if (ck(launch_edge_left_small(d_rows, nrows_small, stream_), "row scaling (small blocks)") ||
+            ck(launch_edge(0, d_rows + nrows_small, (int)rows_scale.size() - nrows_small, stream_), "row scaling"))
+          return -10;
         cudaEventRecord(fe[3], stream_);
         if (ck(launch_edge(1, d_cols, (int)cols_scale.size(), stream_), "column scaling"))
           return -10;
@@ -858,6 +871,7 @@ int Tree::factorize() {
       std::vector<EdgeChunk>& left = P.left;
       EdgeChunk* d_right = nullptr;
       EdgeChunk* d_left = nullptr;
+      int nleft_small = 0;
       bool compress_built = false;
       auto build_compress = [&]() -> int {
         if (compress_built) return 0;
@@ -910,6 +924,7 @@ int Tree::factorize() {
                 return fail(-5, "compression descriptor of level " + std::to_string(lvl) +
                                     " addresses memory outside the block pool; nothing launched");
         }
+        nleft_small = partition_small_left(left, fp32_);
         d_right = static_cast<EdgeChunk*>(up_vec(right));
         d_left = static_cast<EdgeChunk*>(up_vec(left));
         if (!d_right || !d_left) return fail(-11, "out of device memory (compression)");
@@ -1172,7 +1187,8 @@ int Tree::factorize() {
       if (ck(launch_edge(2, d_right, (int)right.size(), stream_), "right compression")) return -10;
       cudaEventRecord(fe[4], stream_);
       set_tensor_cores(use_tc(lvl, 1));
-      if (ck(launch_edge(0, d_left, (int)left.size(), stream_), "left compression"))
+      if (ck(launch_edge_left_small(d_left, nleft_small, stream_), "left compression (small blocks)") ||
+          ck(launch_edge(0, d_left + nleft_small, (int)left.size() - nleft_small, stream_), "left compression"))
         return -10;
       cudaEventRecord(ev[3], stream_);
       if (ck(cudaMemcpyAsync(host_rank.data(), d_rank_, sizeof(int) * host_rank.size(), cudaMemcpyDeviceToHost, stream_),

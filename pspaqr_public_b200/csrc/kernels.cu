@@ -15,6 +15,7 @@
 #include <atomic>
 #include <cstdint>
 #include <mutex>
+#include <type_traits>
 #include <unordered_map>
 
 #include "dense.cuh"
@@ -314,6 +315,122 @@ __global__ void __launch_bounds__(kThreads, 2) k_edge_left(const EdgeChunk* __re
     cnt = min(cnt, lim - t.lo);
   }
   dev::mat_apply_qt<T>(as<T>(t.V), t.ldv, as<T>(t.T), k, as<T>(t.A) + (size_t)t.lo * t.lda, t.lda, t.m, cnt, sm);
+}
+
+// Row scaling / left compression of small blocks, one warp per chunk: m <= 32
+// rows, at most 32 reflectors (one panel), columns in halves of 32.  Lane r
+// holds row r of V in registers and updates row r of C; W = V^T C is formed
+// with lane i as reflector i, reading column i of V and broadcast rows of C
+// from the warp's shared memory; W2 = T^T W likewise (T read by its column);
+// then C -= V W2 on the rows.  No CTA barrier: a CTA of kWarps warps runs
+// kWarps chunks at once (the tiled kernel runs one chunk per CTA through
+// about nine CTA barriers).
+constexpr int kSmallRows = 32;
+constexpr int kSmallLd = 36;  // shared row stride: 16-byte aligned rows
+template <typename T>
+constexpr size_t small_left_smem() {
+  return (size_t)kWarps * 2 * kSmallRows * kSmallLd * sizeof(T);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kThreads, 2) k_edge_left_small(const EdgeChunk* __restrict__ tasks, int ntasks) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  using V4 = typename std::conditional<sizeof(T) == 4, float4, double2>::type;
+  constexpr int kVec = 16 / (int)sizeof(T);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int ti = blockIdx.x * kWarps + warp;
+  if (ti >= ntasks) return;
+  const EdgeChunk t = tasks[ti];
+  const int k = t.kdev ? *t.kdev : t.k;
+  int cnt = t.cnt;
+  if (t.limdev) {
+    const int lim = *t.limdev;
+    if (t.lo >= lim) return;
+    cnt = min(cnt, lim - t.lo);
+  }
+  const int m = t.m;
+  if (k <= 0 || cnt <= 0 || m <= 0) return;
+  T* sV = reinterpret_cast<T*>(smraw) + (size_t)warp * 2 * kSmallRows * kSmallLd;  // sV[r * ld + i] = V(r, i)
+  T* sC = sV + kSmallRows * kSmallLd;  // C, then W, then W2 (row-major, 32 columns)
+  const T* V = as<T>(t.V);
+  const T* Tm = as<T>(t.T);
+  T vrow[kSmallRows];
+#pragma unroll
+  for (int i = 0; i < kSmallRows; ++i) {
+    T v = 0.0;
+    if (lane < m && i < k) v = lane == i ? (T)1.0 : (lane < i ? (T)0.0 : V[lane + (size_t)i * t.ldv]);
+    vrow[i] = v;
+    sV[lane * kSmallLd + i] = v;
+  }
+  for (int h = 0; h < cnt; h += 32) {
+    const int hc = min(32, cnt - h);
+    T* A = as<T>(t.A) + (size_t)(t.lo + h) * t.lda;
+#pragma unroll
+    for (int j = 0; j < 32; ++j) sC[lane * kSmallLd + j] = (lane < m && j < hc) ? A[lane + (size_t)j * t.lda] : (T)0.0;
+    __syncwarp();
+    // W(lane, j) = sum_r V(r, lane) C(r, j)
+    T w[32];
+#pragma unroll
+    for (int j = 0; j < 32; ++j) w[j] = 0.0;
+    for (int r = 0; r < m; ++r) {
+      const T vri = sV[r * kSmallLd + lane];
+      const V4* cr = reinterpret_cast<const V4*>(sC + r * kSmallLd);
+#pragma unroll
+      for (int q = 0; q < 32 / kVec; ++q) {
+        const V4 x = cr[q];
+        const T* xs = reinterpret_cast<const T*>(&x);
+#pragma unroll
+        for (int u = 0; u < kVec; ++u) w[q * kVec + u] += vri * xs[u];
+      }
+    }
+    __syncwarp();
+#pragma unroll
+    for (int j = 0; j < 32; ++j) sC[lane * kSmallLd + j] = w[j];
+    __syncwarp();
+    // W2(lane, j) = sum_{l <= lane} T(l, lane) W(l, j)
+#pragma unroll
+    for (int j = 0; j < 32; ++j) w[j] = 0.0;
+#pragma unroll
+    for (int l = 0; l < kSmallRows; ++l) {
+      if (l < k) {
+        const T tl = (l <= lane && lane < k) ? Tm[l + (size_t)lane * kNB] : (T)0.0;  // T(l, lane)
+        const V4* wl = reinterpret_cast<const V4*>(sC + l * kSmallLd);
+#pragma unroll
+        for (int q = 0; q < 32 / kVec; ++q) {
+          const V4 x = wl[q];
+          const T* xs = reinterpret_cast<const T*>(&x);
+#pragma unroll
+          for (int u = 0; u < kVec; ++u) w[q * kVec + u] += tl * xs[u];
+        }
+      }
+    }
+    __syncwarp();
+#pragma unroll
+    for (int j = 0; j < 32; ++j) sC[lane * kSmallLd + j] = w[j];
+    __syncwarp();
+    // C(lane, j) -= sum_i V(lane, i) W2(i, j)
+#pragma unroll
+    for (int j = 0; j < 32; ++j) w[j] = 0.0;
+#pragma unroll
+    for (int i = 0; i < kSmallRows; ++i) {
+      if (i < k) {
+        const T vi = vrow[i];
+        const V4* wi = reinterpret_cast<const V4*>(sC + i * kSmallLd);
+#pragma unroll
+        for (int q = 0; q < 32 / kVec; ++q) {
+          const V4 x = wi[q];
+          const T* xs = reinterpret_cast<const T*>(&x);
+#pragma unroll
+          for (int u = 0; u < kVec; ++u) w[q * kVec + u] += vi * xs[u];
+        }
+      }
+    }
+    if (lane < m)
+#pragma unroll
+      for (int j = 0; j < 32; ++j)
+        if (j < hc) A[lane + (size_t)j * t.lda] -= w[j];
+    __syncwarp();
+  }
 }
 
 // ------------------------------------------------------------ tensor-core applies (float factors)
@@ -1580,6 +1697,19 @@ cudaError_t launch_edge(int kind, const EdgeChunk* t, int ntasks, cudaStream_t s
   return g_fp32 ? go(k_edge_left<float>, k_edge_trsm<float>, k_edge_right<float>)
                 : go(k_edge_left<double>, k_edge_trsm<double>, k_edge_right<double>);
 }
+
+cudaError_t launch_edge_left_small(const EdgeChunk* t, int ntasks, cudaStream_t st) {
+  if (cudaError_t pre = begin("launch_edge_left_small")) return pre;
+  if (ntasks <= 0) return cudaSuccess;
+  counted();
+  if (!g_fp32) return cudaErrorInvalidValue;  // FP32 factors only
+  const int grid = (ntasks + kWarps - 1) / kWarps;
+  if (cudaError_t e = prep(k_edge_left_small<float>, small_left_smem<float>())) return e;
+  k_edge_left_small<float><<<grid, kThreads, small_left_smem<float>(), st>>>(t, ntasks);
+  return last();
+}
+
+bool edge_left_small(int m) { return m <= kSmallRows; }
 
 cudaError_t launch_tc_probe(const float* C, const float* V, const float* W2, int m, int flags, float* out1,
                             float* out2, int* status, cudaStream_t st) {

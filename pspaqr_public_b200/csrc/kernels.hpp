@@ -79,6 +79,10 @@ cudaError_t launch_rrqr(const RrqrTask* t, int ntasks, int cs, int mmax, int kma
 size_t selected_qr_smem(int mmax, int nmax, bool stage);
 cudaError_t launch_selected_qr(const RrqrTask* t, int ntasks, int cs, int mmax, int nmax, cudaStream_t st);
 cudaError_t launch_merge(const MergeTask* t, int ntasks, cudaStream_t st);
+// Row scaling / left compression (launch_edge kind 0) of FP32 chunks whose
+// blocks have at most 32 rows, one warp per chunk; edge_left_small(m) says which.
+cudaError_t launch_edge_left_small(const EdgeChunk* t, int ntasks, cudaStream_t st);
+bool edge_left_small(int m);
 
 cudaError_t launch_fwd_elim(const FwdElimTask* t, const FwdOut* o, int ntasks, int nmax, int mmax, int* ticket,
                             int* status, long long spin_limit, cudaStream_t st);
