@@ -25,6 +25,7 @@ constexpr size_t kAlign = 256;
 constexpr size_t kArenaChunk = size_t(1) << 30;
 // bounded wait of the forward sweep: ~1 s at 2 GHz
 constexpr int kChunk = 64;        // columns (rows) per CTA of the chunked applies
+constexpr int kUpdSmallMinTasks = 4096;  // small update tasks needed for the team-per-task kernel
 
 // Row scaling / left compression chunks of the FP32 factorization: those of
 // blocks small enough for the warp-per-chunk kernel first (stable, so a stored
@@ -610,12 +611,28 @@ int Tree::factorize() {
                                   " addresses memory outside the block pool; nothing launched");
           }
       }
+      // FP32: tasks whose ops are all small first, for the team-per-task kernel
+      // (stable, so a stored plan stays partitioned)
+      int nut_small = 0;
+      if (fp32_) {
+        const auto mid = std::stable_partition(ut.begin(), ut.end(), [&](const UpdTask& u) {
+          for (int o = u.op_begin; o < u.op_end; ++o)
+            if (!update_op_small(uo[o].k, uo[o].m)) return false;
+          return true;
+        });
+        nut_small = (int)(mid - ut.begin());
+        // a team runs one op chain slower than a CTA does: the team kernel pays
+        // only where there are enough small tasks to fill the GPU many times
+        if (nut_small < kUpdSmallMinTasks) nut_small = 0;
+      }
       auto* d_ut = static_cast<UpdTask*>(upload(ut.data(), sizeof(UpdTask) * ut.size()));
       auto* d_uo = static_cast<UpdOp*>(upload(uop->data(), sizeof(UpdOp) * uop->size()));
       if (!d_ut || !d_uo) return fail(-11, "out of device memory (update descriptors)");
       set_tensor_cores(use_tc(lvl, 0));
       lt_[lvl].kind_tc[0] = tensor_cores_on();
-      if (ck(launch_update(d_ut, d_uo, (int)ut.size(), stream_), "update kernel")) return -10;
+      if (ck(launch_update_small(d_ut, d_uo, nut_small, stream_), "update kernel (small blocks)") ||
+          ck(launch_update(d_ut + nut_small, d_uo, (int)ut.size() - nut_small, stream_), "update kernel"))
+        return -10;
     }
     cudaEventRecord(ev[1], stream_);
     // ---------------- scaling + sparsification

@@ -83,6 +83,11 @@ cudaError_t launch_merge(const MergeTask* t, int ntasks, cudaStream_t st);
 // blocks have at most 32 rows, one warp per chunk; edge_left_small(m) says which.
 cudaError_t launch_edge_left_small(const EdgeChunk* t, int ntasks, cudaStream_t st);
 bool edge_left_small(int m);
+// Trailing updates (FP32 factors) of tasks whose ops all satisfy
+// update_op_small(k, m) (at most 64 reflectors and 64 rows), a 64-thread team
+// per task.
+cudaError_t launch_update_small(const UpdTask* t, const UpdOp* o, int ntasks, cudaStream_t st);
+bool update_op_small(int k, int m);
 
 cudaError_t launch_fwd_elim(const FwdElimTask* t, const FwdOut* o, int ntasks, int nmax, int mmax, int* ticket,
                             int* status, long long spin_limit, cudaStream_t st);
