@@ -382,7 +382,7 @@ __device__ void apply_q_right(const T* V, int ldv, const T* Tm, int k, T* C, int
 // Register-tiled block reflector applies on matrices: rows are streamed
 // through shared memory in tiles of kRT; the left apply keeps two tiles in
 // flight (the next tile's global loads are issued before the current tile's
-// products).  `sm` holds kTileSmem elements.
+// products).  `sm` holds kTileSmem elements (2 kTileSmem for T = float).
 constexpr int kNC = 64;   // columns (rows for right applies) per pass
 constexpr int kRT = 32;   // rows (columns) per shared-memory tile
 // Row strides of the V and C tiles of the left apply: 16-byte aligned rows
@@ -411,6 +411,10 @@ __device__ void tile_left_qt(const T* V, int ldv, const T* Tm, int ldt, int kb, 
                              T* C, int ldc, int m, int nc, T* sm, int cgap = 0) {
   static_assert(kThreads == 256 && kNB == 32 && kNC == 64 && kRT == 32, "tile shapes");
   constexpr int kLV = tile_lv<T>(), kLC = tile_lc<T>();
+  // FP32 callers pass 2 kTileSmem elements (kTileSmem doubles): the partial
+  // sums and W2 then go past the tile buffers
+  constexpr bool kKeep = sizeof(T) == 4;
+  static_assert(!kKeep || 3 * kNB * kNC + kNB * kNC <= kTileSmem, "FP32 park and W2 areas");
   constexpr int kVS = kRT * kLV, kCS = kRT * kLC;
   T* sV0 = sm;               // two [kRT][kLV] tiles of V
   T* sC0 = sV0 + 2 * kVS;    // two [kRT][kLC] tiles of C
@@ -513,10 +517,11 @@ __device__ void tile_left_qt(const T* V, int ldv, const T* Tm, int ldt, int kb, 
       }
       __syncthreads();
     }
-    // sets 1.. park their partial sums in the tile buffers, set 0 adds them in
+    // sets 1.. park their partial sums in the tile buffers (FP32: past them,
+    // so that a single tile stays staged for the update), set 0 adds them in
     // set order
     static_assert((kSets - 1) * kNB * kNC <= 2 * kVS + 2 * kCS, "park area");
-    T* park = sV0;
+    T* park = kKeep ? sm + kTileSmem : sV0;
     if (set > 0)
 #pragma unroll
       for (int a = 0; a < kIW; ++a)
@@ -551,7 +556,7 @@ __device__ void tile_left_qt(const T* V, int ldv, const T* Tm, int ldt, int kb, 
     }
   __syncthreads();
   // ---- W2 = T^T W (T upper triangular: W2(i) = sum_{l <= i} T(l, i) W(l))
-  T* sW2 = sV0;
+  T* sW2 = kKeep ? sm + kTileSmem + (kThreads / ((kNB / 8) * (kNC / 4)) - 1) * kNB * kNC : sV0;
   static_assert(kNB * kNC <= 2 * kVS + 2 * kCS - kNB * (kNB + 1), "W2 and T areas");
   for (int idx = t; idx < kNB * kNC; idx += kThreads) {
     const int i = idx / kNC, c = idx % kNC;
@@ -577,11 +582,13 @@ __device__ void tile_left_qt(const T* V, int ldv, const T* Tm, int ldt, int kb, 
 #pragma unroll
     for (int q = 0; q < kCW; ++q) w2[i][q] = sW2[i * kNC + cq + q];
   __syncthreads();
-  vload(0);
-  cload(0);
-  vstash(0);
-  cstash(0);
-  __syncthreads();
+  if (!(kKeep && ntile == 1)) {  // a single FP32 tile is still staged in buffer 0
+    vload(0);
+    cload(0);
+    vstash(0);
+    cstash(0);
+    __syncthreads();
+  }
   for (int tt = 0; tt < ntile; ++tt) {
     const int b = tt & 1, r0 = tt * kRT;
     const bool more = tt + 1 < ntile;
