@@ -942,10 +942,14 @@ __host__ __device__ constexpr size_t staged_elems(int m) {
 //   W = V^T x   (a warp per reflector, lanes over rows);
 //   W2 = T^T W (trans) or T W, by warp 0;
 //   x -= V W2   (a thread per row).
-// x in shared memory (m elements); buf: staged_elems<T>(m) elements, 16-byte
+// With `a` (pentagonal, trans only): [a (k); x (m)] <- Q^T [a; x] for
+// Q = I - [I; V] T [I; V]^T with V full (m x k), as in vec_apply_tpqt: every
+// panel covers all m rows, W adds a, and a -= W2.
+// x (and a) in shared memory; buf: staged_elems<T>(m) elements, 16-byte
 // aligned.  All threads of the CTA call it; it synchronises internally.
 template <typename T>
-__device__ void vec_apply_staged(const T* V, int ldv, const T* Tm, int k, T* x, int m, bool trans, T* buf) {
+__device__ void vec_apply_staged(const T* V, int ldv, const T* Tm, int k, T* x, int m, bool trans, T* buf,
+                                 T* a = nullptr) {
   if (k <= 0 || m <= 0) return;
   __shared__ int s_off[2][kNB];  // element (r, i) of the staged panel at pb[.][s_off[.][i] + r]
   __shared__ int s_toff[2];
@@ -960,12 +964,13 @@ __device__ void vec_apply_staged(const T* V, int ldv, const T* Tm, int k, T* x, 
   auto stage = [&](int s, int b) {
     const int j0 = j0_of(s);
     const int kb = (k - j0) < kNB ? (k - j0) : kNB;
+    const int rs = a ? 0 : j0;  // first staged row
     T* pb = pb0 + (size_t)b * kNB * lds;
     for (int i = warp; i < kb; i += kWarps) {
-      const T* g = V + (size_t)(j0 + i) * ldv + j0;
+      const T* g = V + (size_t)(j0 + i) * ldv + rs;
       const int ph = phase_of(g);
-      warp_copy_async(pb + (size_t)i * lds + ph, g, m - j0, lane);
-      if (lane == 0) s_off[b][i] = i * lds + ph - j0;
+      warp_copy_async(pb + (size_t)i * lds + ph, g, m - rs, lane);
+      if (lane == 0) s_off[b][i] = i * lds + ph - rs;
     }
     if (warp == kWarps - 1) {
       const T* g = Tm + (size_t)j0 * kNB;
@@ -989,13 +994,13 @@ __device__ void vec_apply_staged(const T* V, int ldv, const T* Tm, int k, T* x, 
     __syncthreads();
     const T* pb = pb0 + (size_t)b * kNB * lds;
     const T* tp = tb0 + s_toff[b];
-    // W(i) = x(j0 + i) + sum_{r > j0 + i} V(r, i) x(r)
+    // W(i) = x(j0 + i) + sum_{r > j0 + i} V(r, i) x(r), or a(j0 + i) + sum_r V(r, i) x(r)
     for (int i = warp; i < kb; i += kWarps) {
       const T* col = pb + s_off[b][i];
       T d = 0.0;
-      for (int r = j0 + i + 1 + lane; r < m; r += 32) d += col[r] * x[r];
+      for (int r = (a ? 0 : j0 + i + 1) + lane; r < m; r += 32) d += col[r] * x[r];
       d = warp_sum(d);
-      if (lane == 0) W[i] = d + x[j0 + i];
+      if (lane == 0) W[i] = d + (a ? a[j0 + i] : x[j0 + i]);
     }
     __syncthreads();
     if (warp == 0) {
@@ -1005,16 +1010,26 @@ __device__ void vec_apply_staged(const T* V, int ldv, const T* Tm, int k, T* x, 
           for (int l = 0; l <= lane; ++l) acc += tp[l + lane * kNB] * W[l];
         else
           for (int l = lane; l < kb; ++l) acc += tp[lane + l * kNB] * W[l];
+        if (a) a[j0 + lane] -= acc;
       }
       W2[lane] = acc;
     }
     __syncthreads();
-    for (int r = j0 + threadIdx.x; r < m; r += kThreads) {
-      const int lim = (r - j0) < kb ? (r - j0) : kb;
-      T acc = (r - j0) < kb ? W2[r - j0] : (T)0.0;
+    if (a) {
+      for (int r = threadIdx.x; r < m; r += kThreads) {
+        T acc = 0.0;
 #pragma unroll 8
-      for (int i = 0; i < lim; ++i) acc += pb[s_off[b][i] + r] * W2[i];
-      x[r] -= acc;
+        for (int i = 0; i < kb; ++i) acc += pb[s_off[b][i] + r] * W2[i];
+        x[r] -= acc;
+      }
+    } else {
+      for (int r = j0 + threadIdx.x; r < m; r += kThreads) {
+        const int lim = (r - j0) < kb ? (r - j0) : kb;
+        T acc = (r - j0) < kb ? W2[r - j0] : (T)0.0;
+#pragma unroll 8
+        for (int i = 0; i < lim; ++i) acc += pb[s_off[b][i] + r] * W2[i];
+        x[r] -= acc;
+      }
     }
     __syncthreads();
   }

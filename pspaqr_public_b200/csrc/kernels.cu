@@ -1365,7 +1365,7 @@ __device__ __forceinline__ void st_release(int* p, int v) {
 template <typename T, bool kStaged>
 __global__ void __launch_bounds__(kThreads, 2) k_fwd_elim(const FwdElimTask* __restrict__ tasks,
                                                        const FwdOut* __restrict__ outs, int ntasks, int* ticket,
-                                                       int* status, long long spin_limit, int nmax) {
+                                                       int* status, long long spin_limit, int nmax, int mmax) {
   extern __shared__ __align__(16) unsigned char smraw[];
   T* sm = reinterpret_cast<T*>(smraw);
   __shared__ int s_task, s_abort;
@@ -1377,7 +1377,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_fwd_elim(const FwdElimTask* __r
   const int ti = s_task;
   if (ti >= ntasks) return;
   const FwdElimTask t = tasks[ti];
-  T* red = sm + (kStaged ? dev::staged_elems<T>(nmax) : 0);
+  T* red = sm + (kStaged ? dev::staged_elems<T>(max(nmax, mmax)) : 0);
   T* xc = red + dev::kVecRed;
   T* xn = xc + (nmax > 0 ? nmax : 1);
   for (int i = threadIdx.x; i < t.n; i += kThreads) xc[i] = __ldcg(as<T>(t.x) + i);
@@ -1408,7 +1408,8 @@ __global__ void __launch_bounds__(kThreads, 2) k_fwd_elim(const FwdElimTask* __r
     if (s_abort) return;
     for (int i = threadIdx.x; i < e.m; i += kThreads) xn[i] = __ldcg(as<T>(e.xn) + i);
     __syncthreads();
-    dev::vec_apply_tpqt<T>(as<T>(e.V), e.m, as<T>(e.T), t.n, xc, xn, e.m, red);
+    if (kStaged) dev::vec_apply_staged<T>(as<T>(e.V), e.m, as<T>(e.T), t.n, xn, e.m, true, sm, xc);
+    else dev::vec_apply_tpqt<T>(as<T>(e.V), e.m, as<T>(e.T), t.n, xc, xn, e.m, red);
     for (int i = threadIdx.x; i < e.m; i += kThreads) __stcg(as<T>(e.xn) + i, xn[i]);
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -1483,6 +1484,26 @@ __global__ void __launch_bounds__(kThreads) k_bwd_elim(const BwdElimTask* __rest
       const T* R = as<T>(e.R);
       const T* xm = as<T>(e.xm);
       int j = warp;
+      if (kR <= 12)  // four columns' loads in flight while the registers allow it
+        for (; j + 3 * kWarps < e.s; j += 4 * kWarps) {
+          const T* c0 = R + (size_t)j * e.ldr;
+          const T* c1 = c0 + (size_t)kWarps * e.ldr;
+          const T* c2 = c1 + (size_t)kWarps * e.ldr;
+          const T* c3 = c2 + (size_t)kWarps * e.ldr;
+          T v0[kR], v1[kR], v2[kR], v3[kR];
+#pragma unroll
+          for (int u = 0; u < kR; ++u) {
+            const int r = lane + 32 * u;
+            const bool ok = u < nrs && r < t.n;
+            v0[u] = ok ? c0[r] : (T)0.0;
+            v1[u] = ok ? c1[r] : (T)0.0;
+            v2[u] = ok ? c2[r] : (T)0.0;
+            v3[u] = ok ? c3[r] : (T)0.0;
+          }
+          const T x0 = xm[j], x1 = xm[j + kWarps], x2 = xm[j + 2 * kWarps], x3 = xm[j + 3 * kWarps];
+#pragma unroll
+          for (int u = 0; u < kR; ++u) y[u] += (v0[u] * x0 + v1[u] * x1) + (v2[u] * x2 + v3[u] * x3);
+        }
       for (; j + kWarps < e.s; j += 2 * kWarps) {
         const T* c0 = R + (size_t)j * e.ldr;
         const T* c1 = c0 + (size_t)kWarps * e.ldr;
@@ -1986,20 +2007,27 @@ cudaError_t launch_fwd_elim(const FwdElimTask* t, const FwdOut* o, int ntasks, i
                             int* status, long long spin_limit, cudaStream_t st) {
   if (cudaError_t pre = begin("launch_fwd_elim")) return pre;
   if (ntasks <= 0) return cudaSuccess;
-  const size_t b = smem_bytes(dev::kVecRed + (size_t)std::max(nmax, 1) + (size_t)std::max(mmax, 1));
+  nmax = std::max(nmax, 1);
+  mmax = std::max(mmax, 1);
+  const size_t b = smem_bytes(dev::kVecRed + (size_t)nmax + (size_t)mmax);
+  const int srows = std::max(nmax, mmax);  // rows of a staged panel: the interior's or a neighbour's
   counted();
   auto go = [&](auto kern, size_t bytes) -> cudaError_t {
     if (cudaError_t e = prep(kern, bytes)) return e;
-    kern<<<ntasks, kThreads, bytes, st>>>(t, o, ntasks, ticket, status, spin_limit, nmax);
+    kern<<<ntasks, kThreads, bytes, st>>>(t, o, ntasks, ticket, status, spin_limit, nmax, mmax);
     return cudaSuccess;
   };
   cudaError_t e;
+  // staged where the interiors themselves are large (the top levels, few
+  // CTAs); large neighbours of small interiors alone do not pay for it
+  const bool big = nmax >= kStagedMin;
   if (g_fp32)
-    e = use_staged<float>(nmax, b) ? go(k_fwd_elim<float, true>, dev::staged_elems<float>(nmax) * sizeof(float) + b)
-                                   : go(k_fwd_elim<float, false>, b);
+    e = big && use_staged<float>(srows, b)
+            ? go(k_fwd_elim<float, true>, dev::staged_elems<float>(srows) * sizeof(float) + b)
+            : go(k_fwd_elim<float, false>, b);
   else
-    e = use_staged<double>(nmax, b)
-            ? go(k_fwd_elim<double, true>, dev::staged_elems<double>(nmax) * sizeof(double) + b)
+    e = big && use_staged<double>(srows, b)
+            ? go(k_fwd_elim<double, true>, dev::staged_elems<double>(srows) * sizeof(double) + b)
             : go(k_fwd_elim<double, false>, b);
   if (e) return e;
   return last();
