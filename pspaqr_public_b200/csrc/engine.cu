@@ -1541,6 +1541,10 @@ int Tree::plan_solve(double* xw, int* turn, std::vector<SolvePlan>& ls) {
     }
     S.nfe = (int)fe.size();
     S.nfs = (int)fs.size();
+    if (fp32_)
+      S.nfs_small = (int)(std::stable_partition(fs.begin(), fs.end(),
+                                                [](const FwdSparsTask& t) { return spars_small(t.n); }) -
+                          fs.begin());
     S.nbe = (int)be.size();
     S.ng = (int)gs.size();
     S.fe = static_cast<FwdElimTask*>(up(fe.data(), sizeof(FwdElimTask) * fe.size()));
@@ -1569,12 +1573,14 @@ int Tree::capture_solve(const std::vector<SolvePlan>& ls, double* xw, int* turn,
   for (int lvl = 0; lvl < L; ++lvl) {
     const SolvePlan& S = ls[lvl];
     cerr = cerr ? cerr : launch_fwd_elim(S.fe, S.fo, S.nfe, S.fe_nmax, S.fe_mmax, tickets + lvl, d_status_, spin_limit, stream_);
-    cerr = cerr ? cerr : launch_fwd_spars(S.fs, S.nfs, S.fs_nmax, stream_);
+    cerr = cerr ? cerr : launch_spars_small(true, S.fs, S.nfs_small, stream_);
+    cerr = cerr ? cerr : launch_fwd_spars(S.fs + S.nfs_small, S.nfs - S.nfs_small, S.fs_nmax, stream_);
     cerr = cerr ? cerr : launch_copy_idx(S.ng, S.gsrc, S.gdst, xw, stream_);
   }
   for (int lvl = L - 1; lvl >= 0; --lvl) {
     const SolvePlan& S = ls[lvl];
-    cerr = cerr ? cerr : launch_bwd_spars(S.fs, S.nfs, S.fs_nmax, stream_);
+    cerr = cerr ? cerr : launch_spars_small(false, S.fs, S.nfs_small, stream_);
+    cerr = cerr ? cerr : launch_bwd_spars(S.fs + S.nfs_small, S.nfs - S.nfs_small, S.fs_nmax, stream_);
     cerr = cerr ? cerr : launch_bwd_elim(S.be, S.bi, S.nbe, S.be_nmax, stream_);
     if (lvl > 0) cerr = cerr ? cerr : launch_copy_idx(ls[lvl - 1].ng, ls[lvl - 1].gdst, ls[lvl - 1].gsrc, xw, stream_);
   }

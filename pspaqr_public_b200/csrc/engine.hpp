@@ -256,6 +256,7 @@ class Tree {
     int nfe = 0, fe_nmax = 1, fe_mmax = 1;
     FwdSparsTask* fs = nullptr;
     int nfs = 0, fs_nmax = 1;
+    int nfs_small = 0;  // FP32: the first nfs_small tasks take the warp-per-interface kernels
     BwdElimTask* be = nullptr;
     BwdIn* bi = nullptr;
     int nbe = 0, be_nmax = 1;

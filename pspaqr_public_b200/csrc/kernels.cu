@@ -1457,6 +1457,87 @@ __global__ void __launch_bounds__(kThreads) k_bwd_spars(const FwdSparsTask* __re
   for (int i = threadIdx.x; i < t.n; i += kThreads) as<T>(t.x)[i] = x[i];
 }
 
+// Forward / backward scaling + sparsification steps of small interfaces (FP32,
+// n <= 32), one warp per interface: lane r holds x(r); each reflector block
+// (a single panel) and its T are staged in the warp's shared memory and the
+// sums run over shuffles.  The CTA kernels spend a 256-thread CTA and three
+// CTA barriers per panel on vectors of this size.
+constexpr int kSpLd = 33;
+constexpr size_t kSparsSmallSmem = (size_t)kWarps * 2 * 32 * kSpLd * sizeof(float);
+
+// Returns lane r's entry of Q^T x (trans) or Q x, Q = I - V T V^T for k <= 32
+// unit lower reflectors of n <= 32 rows (T in kNB x k layout).
+__device__ __forceinline__ float warp_apply_unit(const float* V, int ldv, const float* Tm, int k, float xr, int n,
+                                                 bool trans, float* sV, float* sT, int lane) {
+  for (int i = 0; i < 32; ++i) {
+    float v = 0.0f;
+    if (i < k && lane < n) v = lane == i ? 1.0f : (lane < i ? 0.0f : V[lane + (size_t)i * ldv]);
+    sV[lane * kSpLd + i] = v;                                                         // V(lane, i)
+    sT[lane * kSpLd + i] = (lane <= i && i < k) ? Tm[lane + (size_t)i * kNB] : 0.0f;  // T(lane, i)
+  }
+  __syncwarp();
+  float w = 0.0f;  // W(lane) = sum_r V(r, lane) x(r)
+  for (int r = 0; r < 32; ++r) {
+    const float xb = __shfl_sync(0xffffffffu, xr, r);
+    if (r < n) w += sV[r * kSpLd + lane] * xb;
+  }
+  float w2 = 0.0f;  // W2 = T^T W (trans) or T W
+  for (int l = 0; l < 32; ++l) {
+    const float wl = __shfl_sync(0xffffffffu, w, l);
+    if (trans ? l <= lane : l >= lane) w2 += (trans ? sT[l * kSpLd + lane] : sT[lane * kSpLd + l]) * wl;
+  }
+  if (lane >= k) w2 = 0.0f;
+  float acc = 0.0f;  // (V W2)(lane)
+  for (int i = 0; i < 32; ++i) {
+    const float wi = __shfl_sync(0xffffffffu, w2, i);
+    acc += sV[lane * kSpLd + i] * wi;
+  }
+  __syncwarp();  // the next block overwrites sV / sT
+  return xr - acc;
+}
+
+__global__ void __launch_bounds__(kThreads) k_fwd_spars_small(const FwdSparsTask* __restrict__ tasks, int ntasks) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int ti = blockIdx.x * kWarps + warp;
+  if (ti >= ntasks) return;
+  const FwdSparsTask t = tasks[ti];
+  float* sV = reinterpret_cast<float*>(smraw) + (size_t)warp * 2 * 32 * kSpLd;
+  float* sT = sV + 32 * kSpLd;
+  float* x = as<float>(t.x);
+  const int n = t.n;
+  float xr = lane < n ? x[lane] : 0.0f;
+  xr = warp_apply_unit(as<float>(t.Qs), n, as<float>(t.Ts), n, xr, n, true, sV, sT, lane);
+  xr = warp_apply_unit(as<float>(t.V), n, as<float>(t.T), *t.rank, xr, n, true, sV, sT, lane);
+  if (lane < n) x[lane] = xr;
+}
+
+__global__ void __launch_bounds__(kThreads) k_bwd_spars_small(const FwdSparsTask* __restrict__ tasks, int ntasks) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int ti = blockIdx.x * kWarps + warp;
+  if (ti >= ntasks) return;
+  const FwdSparsTask t = tasks[ti];
+  float* sV = reinterpret_cast<float*>(smraw) + (size_t)warp * 2 * 32 * kSpLd;
+  float* sT = sV + 32 * kSpLd;
+  float* x = as<float>(t.x);
+  const int n = t.n;
+  float xr = lane < n ? x[lane] : 0.0f;
+  xr = warp_apply_unit(as<float>(t.V), n, as<float>(t.T), *t.rank, xr, n, false, sV, sT, lane);
+  // x <- R^{-1} x, R the upper triangle of Qs: the diagonal-block solve of trsv_upper
+  const float* R = as<float>(t.Qs);
+  for (int j = 0; j < 32; ++j) sV[lane * kSpLd + j] = (lane < n && j < n && j >= lane) ? R[lane + (size_t)j * n] : 0.0f;
+  __syncwarp();
+  for (int j = 31; j >= 0; --j) {
+    if (j < n) {
+      if (lane == j) xr = xr / sV[j * kSpLd + j];
+      const float xj = __shfl_sync(0xffffffffu, xr, j);
+      if (lane < j) xr -= sV[lane * kSpLd + j] * xj;
+    }
+  }
+  if (lane < n) x[lane] = xr;
+}
+
 // kBwdRows: rows per lane of the backward GEMV (interiors of <= 32 kBwdRows
 // rows); 0: one thread per row.
 template <typename T, int kBwdRows>
@@ -2056,6 +2137,25 @@ cudaError_t launch_spars(const FwdSparsTask* t, int ntasks, int nmax, cudaStream
   if (e) return e;
   return last();
 }
+
+// The warp-per-interface forms (FP32, n <= 32): kFwd chooses the forward step.
+cudaError_t launch_spars_small(bool fwd, const FwdSparsTask* t, int ntasks, cudaStream_t st) {
+  if (cudaError_t pre = begin("launch_spars_small")) return pre;
+  if (ntasks <= 0) return cudaSuccess;
+  if (!g_fp32) return cudaErrorInvalidValue;  // FP32 factors only
+  counted();
+  const int grid = (ntasks + kWarps - 1) / kWarps;
+  if (fwd) {
+    if (cudaError_t e = prep(k_fwd_spars_small, kSparsSmallSmem)) return e;
+    k_fwd_spars_small<<<grid, kThreads, kSparsSmallSmem, st>>>(t, ntasks);
+  } else {
+    if (cudaError_t e = prep(k_bwd_spars_small, kSparsSmallSmem)) return e;
+    k_bwd_spars_small<<<grid, kThreads, kSparsSmallSmem, st>>>(t, ntasks);
+  }
+  return last();
+}
+
+bool spars_small(int n) { return n <= 32; }
 
 cudaError_t launch_fwd_spars(const FwdSparsTask* t, int ntasks, int nmax, cudaStream_t st) {
   if (cudaError_t pre = begin("launch_fwd_spars")) return pre;

@@ -88,6 +88,10 @@ bool edge_left_small(int m);
 // per task.
 cudaError_t launch_update_small(const UpdTask* t, const UpdOp* o, int ntasks, cudaStream_t st);
 bool update_op_small(int k, int m);
+// Forward (fwd) or backward scaling + sparsification steps of FP32 interfaces
+// with spars_small(n) (at most 32 rows), one warp per interface.
+cudaError_t launch_spars_small(bool fwd, const FwdSparsTask* t, int ntasks, cudaStream_t st);
+bool spars_small(int n);
 
 cudaError_t launch_fwd_elim(const FwdElimTask* t, const FwdOut* o, int ntasks, int nmax, int mmax, int* ticket,
                             int* status, long long spin_limit, cudaStream_t st);
