@@ -1344,8 +1344,15 @@ int Tree::factorize() {
     }
     cudaEventRecord(ev[4], stream_);
     const double h1 = wall();
+    // the status word comes back with the level's synchronisation (staged in
+    // pinned memory), not through a second blocking copy
+    int* h_status = d_status_ ? static_cast<int*>(stage(sizeof(int))) : nullptr;
+    if (h_status) {
+      *h_status = 0;
+      cudaMemcpyAsync(h_status, d_status_, sizeof(int), cudaMemcpyDeviceToHost, stream_);
+    }
     if (ck(cudaStreamSynchronize(stream_), "factorize level")) return -10;
-    if (const int ds = device_status()) {
+    if (const int ds = h_status ? *h_status : device_status()) {
       clear_status();
       if (ds & 2) return fail(-12, "tensor-core MMA wait timed out on the device at level " + std::to_string(lvl));
       return fail(-13, std::string(ds & 4 ? "non-finite" : "zero") + " pivot in the QR factorizations of level " +
