@@ -709,6 +709,11 @@ int Tree::factorize() {
       lt_[lvl].flops[3] += P.fl_sapp;
       {
         const int nrows_small = partition_small_left(rows_scale, fp32_);
+        const int ncols_small =
+            fp32_ ? (int)(std::stable_partition(cols_scale.begin(), cols_scale.end(),
+                                                [](const EdgeChunk& c) { return edge_trsm_small(c.nc, c.cnt); }) -
+                          cols_scale.begin())
+                  : 0;
         auto* d_rows = static_cast<EdgeChunk*>(up_vec(rows_scale));
         auto* d_cols = static_cast<EdgeChunk*>(up_vec(cols_scale));
         if (!d_rows || !d_cols) return fail(-11, "out of device memory (scaling)");
@@ -718,7 +723,8 @@ int Tree::factorize() {
             ck(launch_edge(0, d_rows + nrows_small, (int)rows_scale.size() - nrows_small, stream_), "row scaling"))
           return -10;
         cudaEventRecord(fe[3], stream_);
-        if (ck(launch_edge(1, d_cols, (int)cols_scale.size(), stream_), "column scaling"))
+        if (ck(launch_edge_trsm_small(d_cols, ncols_small, stream_), "column scaling (small blocks)") ||
+            ck(launch_edge(1, d_cols + ncols_small, (int)cols_scale.size() - ncols_small, stream_), "column scaling"))
           return -10;
       }
       cudaEventRecord(ev[2], stream_);

@@ -663,6 +663,53 @@ __global__ void __launch_bounds__(kThreads) k_edge_trsm(const EdgeChunk* __restr
   dev::tile_trsm_right_upper<T>(as<T>(t.V), t.ldv, as<T>(t.A) + t.lo, t.lda, t.cnt, t.nc, sm);
 }
 
+// Column scaling of small blocks (FP32, at most 32 columns, chunks of at most
+// 64 rows), one warp per chunk: lane r holds rows r and r + 32 of C, R sits
+// in the warp's shared memory, and the columns are solved in order,
+// c_j = (c_j - sum_{i<j} c_i R(i, j)) / R(j, j), from broadcast reads; no
+// barrier beyond the warp's.
+constexpr int kTrsmLd = 33;
+__global__ void __launch_bounds__(kThreads, 2) k_edge_trsm_small(const EdgeChunk* __restrict__ tasks, int ntasks) {
+  __shared__ float sRall[kWarps][32 * kTrsmLd];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int ti = blockIdx.x * kWarps + warp;
+  if (ti >= ntasks) return;
+  const EdgeChunk t = tasks[ti];
+  const int n = t.nc, m = t.cnt;
+  float* sR = sRall[warp];  // sR[i * ld + j] = R(i, j)
+  const float* R = as<float>(t.V);
+#pragma unroll
+  for (int j = 0; j < 32; ++j) sR[lane * kTrsmLd + j] = (lane < n && j < n && lane <= j) ? R[lane + (size_t)j * t.ldv] : 0.0f;
+  float* C = as<float>(t.A) + t.lo;
+  float c0[32], c1[32];
+#pragma unroll
+  for (int j = 0; j < 32; ++j) {
+    c0[j] = (j < n && lane < m) ? C[lane + (size_t)j * t.lda] : 0.0f;
+    c1[j] = (j < n && lane + 32 < m) ? C[lane + 32 + (size_t)j * t.lda] : 0.0f;
+  }
+  __syncwarp();
+#pragma unroll
+  for (int j = 0; j < 32; ++j) {
+    if (j < n) {
+      float s0 = c0[j], s1 = c1[j];
+#pragma unroll
+      for (int i = 0; i < j; ++i) {
+        const float rij = sR[i * kTrsmLd + j];
+        s0 -= c0[i] * rij;
+        s1 -= c1[i] * rij;
+      }
+      const float d = sR[j * kTrsmLd + j];
+      c0[j] = s0 / d;
+      c1[j] = s1 / d;
+    }
+  }
+#pragma unroll
+  for (int j = 0; j < 32; ++j) {
+    if (j < n && lane < m) C[lane + (size_t)j * t.lda] = c0[j];
+    if (j < n && lane + 32 < m) C[lane + 32 + (size_t)j * t.lda] = c1[j];
+  }
+}
+
 // right compression: rows [lo, lo+cnt) of A <- A Q
 template <typename T>
 __global__ void __launch_bounds__(kThreads) k_edge_right(const EdgeChunk* __restrict__ tasks) {
@@ -1962,6 +2009,17 @@ cudaError_t launch_edge_left_small(const EdgeChunk* t, int ntasks, cudaStream_t 
 }
 
 bool edge_left_small(int m) { return m <= kSmallRows; }
+
+cudaError_t launch_edge_trsm_small(const EdgeChunk* t, int ntasks, cudaStream_t st) {
+  if (cudaError_t pre = begin("launch_edge_trsm_small")) return pre;
+  if (ntasks <= 0) return cudaSuccess;
+  if (!g_fp32) return cudaErrorInvalidValue;  // FP32 factors only
+  counted();
+  k_edge_trsm_small<<<(ntasks + kWarps - 1) / kWarps, kThreads, 0, st>>>(t, ntasks);
+  return last();
+}
+
+bool edge_trsm_small(int ncols, int rows) { return ncols <= 32 && rows <= 64; }
 
 cudaError_t launch_tc_probe(const float* C, const float* V, const float* W2, int m, int flags, float* out1,
                             float* out2, int* status, cudaStream_t st) {

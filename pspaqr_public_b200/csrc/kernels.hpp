@@ -83,6 +83,10 @@ cudaError_t launch_merge(const MergeTask* t, int ntasks, cudaStream_t st);
 // blocks have at most 32 rows, one warp per chunk; edge_left_small(m) says which.
 cudaError_t launch_edge_left_small(const EdgeChunk* t, int ntasks, cudaStream_t st);
 bool edge_left_small(int m);
+// Column scaling (launch_edge kind 1) of FP32 chunks with edge_trsm_small(nc,
+// cnt) (at most 32 columns and 64 rows), one warp per chunk.
+cudaError_t launch_edge_trsm_small(const EdgeChunk* t, int ntasks, cudaStream_t st);
+bool edge_trsm_small(int ncols, int rows);
 // Trailing updates (FP32 factors) of tasks whose ops all satisfy
 // update_op_small(k, m) (at most 64 reflectors and 64 rows), a 64-thread team
 // per task.
