@@ -894,7 +894,7 @@ int Tree::factorize() {
       std::vector<EdgeChunk>& left = P.left;
       EdgeChunk* d_right = nullptr;
       EdgeChunk* d_left = nullptr;
-      int nleft_small = 0;
+      int nleft_small = 0, nright_small = 0;
       bool compress_built = false;
       auto build_compress = [&]() -> int {
         if (compress_built) return 0;
@@ -948,6 +948,12 @@ int Tree::factorize() {
                                     " addresses memory outside the block pool; nothing launched");
         }
         nleft_small = partition_small_left(left, fp32_);
+        nright_small = fp32_ ? (int)(std::stable_partition(right.begin(), right.end(),
+                                                           [](const EdgeChunk& c) {
+                                                             return edge_trsm_small(c.nc, c.cnt);
+                                                           }) -
+                                     right.begin())
+                             : 0;
         d_right = static_cast<EdgeChunk*>(up_vec(right));
         d_left = static_cast<EdgeChunk*>(up_vec(left));
         if (!d_right || !d_left) return fail(-11, "out of device memory (compression)");
@@ -1207,7 +1213,9 @@ int Tree::factorize() {
       cudaEventRecord(fe[2], stream_);
       set_tensor_cores(use_tc(lvl, 2));
       lt_[lvl].kind_tc[2] = tensor_cores_on();
-      if (ck(launch_edge(2, d_right, (int)right.size(), stream_), "right compression")) return -10;
+      if (ck(launch_edge_right_small(d_right, nright_small, stream_), "right compression (small blocks)") ||
+          ck(launch_edge(2, d_right + nright_small, (int)right.size() - nright_small, stream_), "right compression"))
+        return -10;
       cudaEventRecord(fe[4], stream_);
       set_tensor_cores(use_tc(lvl, 1));
       if (ck(launch_edge_left_small(d_left, nleft_small, stream_), "left compression (small blocks)") ||

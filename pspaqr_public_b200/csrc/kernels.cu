@@ -710,6 +710,74 @@ __global__ void __launch_bounds__(kThreads, 2) k_edge_trsm_small(const EdgeChunk
   }
 }
 
+// Right compression of small blocks (FP32, at most 32 columns, chunks of at
+// most 64 rows), one warp per chunk: C <- C (I - V T V^T), V unit lower
+// (n x k).  Every row is independent: lane r takes rows r and r + 32 in turn
+// and forms W = C(r, :) V, W2 = W T, C(r, :) -= W2 V^T with V and T read as
+// 16-byte broadcasts from the warp's shared memory.
+constexpr int kRightLd = 36;
+constexpr size_t kRightSmallSmem = (size_t)kWarps * 2 * 32 * kRightLd * sizeof(float);
+__global__ void __launch_bounds__(kThreads, 2) k_edge_right_small(const EdgeChunk* __restrict__ tasks, int ntasks) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int ti = blockIdx.x * kWarps + warp;
+  if (ti >= ntasks) return;
+  const EdgeChunk t = tasks[ti];
+  const int n = t.nc, m = t.cnt;
+  const int k = t.kdev ? *t.kdev : t.k;
+  if (k <= 0 || n <= 0 || m <= 0) return;
+  float* sV = reinterpret_cast<float*>(smraw) + (size_t)warp * 2 * 32 * kRightLd;  // sV[j * ld + i] = V(j, i)
+  float* sT = sV + 32 * kRightLd;                                                   // sT[l * ld + i] = T(l, i)
+  const float* V = as<float>(t.V);
+  const float* Tm = as<float>(t.T);
+  for (int i = 0; i < 32; ++i) {
+    float v = 0.0f;
+    if (lane < n && i < k) v = lane == i ? 1.0f : (lane < i ? 0.0f : V[lane + (size_t)i * t.ldv]);
+    sV[lane * kRightLd + i] = v;
+    sT[lane * kRightLd + i] = (lane <= i && i < k) ? Tm[lane + (size_t)i * kNB] : 0.0f;
+  }
+  __syncwarp();
+  float* C = as<float>(t.A) + t.lo;
+  for (int half = 0; half < 2; ++half) {
+    if (32 * half >= m) break;  // uniform over the warp
+    const int r = lane + 32 * half;
+    const bool live = r < m;
+    float w[32];
+#pragma unroll
+    for (int i = 0; i < 32; ++i) w[i] = 0.0f;
+    for (int j = 0; j < n; ++j) {  // W = C(r, :) V
+      const float cj = live ? C[r + (size_t)j * t.lda] : 0.0f;
+      const float4* vr = reinterpret_cast<const float4*>(sV + j * kRightLd);
+#pragma unroll
+      for (int q = 0; q < 8; ++q) {
+        const float4 x = vr[q];
+        w[4 * q] += cj * x.x;
+        w[4 * q + 1] += cj * x.y;
+        w[4 * q + 2] += cj * x.z;
+        w[4 * q + 3] += cj * x.w;
+      }
+    }
+    // W2 = W T in place, columns from the last: W2(i) uses W(l) for l <= i only
+#pragma unroll
+    for (int i = 31; i >= 0; --i) {
+      float sacc = 0.0f;
+#pragma unroll
+      for (int l = 0; l <= i; ++l) sacc += w[l] * sT[l * kRightLd + i];
+      w[i] = sacc;
+    }
+    for (int j = 0; j < n; ++j) {  // C(r, j) -= W2 V(j, :)^T
+      const float4* vr = reinterpret_cast<const float4*>(sV + j * kRightLd);
+      float u = 0.0f;
+#pragma unroll
+      for (int q = 0; q < 8; ++q) {
+        const float4 x = vr[q];
+        u += (w[4 * q] * x.x + w[4 * q + 1] * x.y) + (w[4 * q + 2] * x.z + w[4 * q + 3] * x.w);
+      }
+      if (live) C[r + (size_t)j * t.lda] -= u;
+    }
+  }
+}
+
 // right compression: rows [lo, lo+cnt) of A <- A Q
 template <typename T>
 __global__ void __launch_bounds__(kThreads) k_edge_right(const EdgeChunk* __restrict__ tasks) {
@@ -2020,6 +2088,16 @@ cudaError_t launch_edge_trsm_small(const EdgeChunk* t, int ntasks, cudaStream_t 
 }
 
 bool edge_trsm_small(int ncols, int rows) { return ncols <= 32 && rows <= 64; }
+
+cudaError_t launch_edge_right_small(const EdgeChunk* t, int ntasks, cudaStream_t st) {
+  if (cudaError_t pre = begin("launch_edge_right_small")) return pre;
+  if (ntasks <= 0) return cudaSuccess;
+  if (!g_fp32) return cudaErrorInvalidValue;  // FP32 factors only
+  counted();
+  if (cudaError_t e = prep(k_edge_right_small, kRightSmallSmem)) return e;
+  k_edge_right_small<<<(ntasks + kWarps - 1) / kWarps, kThreads, kRightSmallSmem, st>>>(t, ntasks);
+  return last();
+}
 
 cudaError_t launch_tc_probe(const float* C, const float* V, const float* W2, int m, int flags, float* out1,
                             float* out2, int* status, cudaStream_t st) {

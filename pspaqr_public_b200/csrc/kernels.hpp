@@ -87,6 +87,9 @@ bool edge_left_small(int m);
 // cnt) (at most 32 columns and 64 rows), one warp per chunk.
 cudaError_t launch_edge_trsm_small(const EdgeChunk* t, int ntasks, cudaStream_t st);
 bool edge_trsm_small(int ncols, int rows);
+// Right compression (launch_edge kind 2) of FP32 chunks with
+// edge_trsm_small(nc, cnt), one warp per chunk.
+cudaError_t launch_edge_right_small(const EdgeChunk* t, int ntasks, cudaStream_t st);
 // Trailing updates (FP32 factors) of tasks whose ops all satisfy
 // update_op_small(k, m) (at most 64 reflectors and 64 rows), a 64-thread team
 // per task.
