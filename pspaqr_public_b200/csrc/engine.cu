@@ -26,6 +26,7 @@ constexpr size_t kArenaChunk = size_t(1) << 30;
 // bounded wait of the forward sweep: ~1 s at 2 GHz
 constexpr int kChunk = 64;        // columns (rows) per CTA of the chunked applies
 constexpr int kUpdSmallMinTasks = 4096;  // small update tasks needed for the team-per-task kernel
+constexpr float kTuneMargin = 0.95f;      // tensor cores chosen where at least 5 % faster
 
 // Row scaling / left compression chunks of the FP32 factorization: those of
 // blocks small enough for the warp-per-chunk kernel first (stable, so a stored
@@ -1430,7 +1431,10 @@ bool Tree::use_tc(int lvl, int kind) const {
   if (!fp32_ || tensor_cores == 0) return false;
   if (tensor_cores == 1) return true;
   if (tune_runs_ < 2) return tune_runs_ == 0;  // measuring: tensor cores first, then CUDA cores
-  return tune_ms_[0][lvl][kind] < tune_ms_[1][lvl][kind];
+  // the tensor cores only where they were clearly faster: near-ties (a level
+  // whose two timings differ by a few microseconds) would otherwise flip from
+  // run to run and with them the rounding of the factor
+  return tune_ms_[0][lvl][kind] < kTuneMargin * tune_ms_[1][lvl][kind];
 }
 
 void Tree::tune_table(std::vector<float>& out) const {

@@ -434,139 +434,168 @@ __global__ void __launch_bounds__(kThreads, 2) k_edge_left_small(const EdgeChunk
 }
 
 // Trailing updates of small column chunks (FP32 factors): one team of 64
-// threads per chunk, kTeams teams per CTA, synchronised by their own named
-// barrier.  Every op of the chunk's chain has at most 64 reflectors and 64
-// rows; it is applied panel by panel (32 reflectors) on halves of 32
-// columns.  Per panel and half: thread r stages row r of the panel of V (in
-// registers and shared memory) and of the block it updates; thread t forms
-// W(t mod 32, 16 columns) = V^T C (+ the top block A for a tsqrt step), then
-// W2 = T^T W likewise; thread r updates its row, C(r, :) -= V(r, :) W2.  The
-// tiled kernel runs one chunk per CTA through about nine CTA barriers per
-// op; here 8 chunks share an SM's time.
+// threads per chunk, kTeams teams per 128-thread CTA, synchronised by their
+// own named barrier.  Every op of the chunk's chain has at most 64
+// reflectors and 64 rows.  The ops of one interior c (its geqrt apply, then
+// its tsqrt steps) all update the same block A(c, m): per 32-column half, the
+// team keeps that block in shared memory across the whole run of ops with
+// the same A and brings in only each step's neighbour block B(n, m) and the
+// reflector panels; every panel of an op is applied before B is written back.
+// Per panel: thread r stages row r of the panel of V (registers and shared
+// memory); thread t forms W(t mod 32, 16 columns) = V^T C (+ the top rows of
+// A for a tsqrt step), then W2 = T^T W; thread r updates its row.
 constexpr int kTeam = 64;
-constexpr int kTeams = kThreads / kTeam;
+constexpr int kTeams = 2;  // teams per CTA
+constexpr int kTeamThreads = kTeam * kTeams;
 constexpr int kSmallOp = 64;  // rows, reflectors and columns of an op on the small path
-constexpr size_t kTeamSmem = (size_t)(2 * kSmallOp + kNB) * kSmallLd;  // floats: V panel, C half, W
+// floats per team: A, B, V panel (64 x kSmallLd each), W (32 x kSmallLd), T (32 x 33)
+constexpr size_t kTeamSmem = (size_t)(3 * kSmallOp + kNB) * kSmallLd + kNB * (kNB + 1);
 constexpr size_t kUpdSmallSmem = kTeams * kTeamSmem * sizeof(float);
 
 __device__ __forceinline__ void team_sync(int team) {
   asm volatile("bar.sync %0, %1;" ::"r"(team + 1), "r"(kTeam) : "memory");
 }
 
-__global__ void __launch_bounds__(kThreads, 2) k_update_small(const UpdTask* __restrict__ tasks,
-                                                             const UpdOp* __restrict__ ops, int ntasks) {
+// One panel (reflectors j0 .. j0 + kb) of an op on blocks in shared memory:
+// kind 0: C = sA rows [j0, m) <- Q^T C (V unit lower, rows j0 ..);
+// kind 1: [sA rows j0 .. j0 + kb; sB rows 0 .. m) <- Q^T [.] (V full, m rows).
+__device__ __forceinline__ void team_panel(const UpdOp& op, int j0, int kb, float* sA, float* sB, float* sV,
+                                           float* sW, float* sT, int team, int tl) {
+  const int r0 = op.kind ? 0 : j0;
+  const int nr = op.m - r0;
+  float* sC = op.kind ? sB : sA + (size_t)j0 * kSmallLd;  // rows r0 .. of the block V acts on
+  const float* V = as<float>(op.V);
+  const float* Tm = as<float>(op.T) + (size_t)j0 * kNB;
+  float vrow[kNB];
+#pragma unroll
+  for (int i = 0; i < kNB; ++i) {
+    float v = 0.0f;
+    if (tl < nr && i < kb) {
+      const int r = r0 + tl;
+      v = op.kind ? V[r + (size_t)(j0 + i) * op.ldv]
+                  : (tl == i ? 1.0f : (tl < i ? 0.0f : V[r + (size_t)(j0 + i) * op.ldv]));
+    }
+    vrow[i] = v;
+    sV[tl * kSmallLd + i] = v;
+  }
+  for (int e = tl; e < kNB * kNB; e += kTeam) {  // T transposed: sT[i * 33 + l] = T(l, i)
+    const int l = e % kNB, i = e / kNB;
+    sT[i * (kNB + 1) + l] = (l <= i && i < kb) ? Tm[l + (size_t)i * kNB] : 0.0f;
+  }
+  team_sync(team);
+  const int wi = tl & 31, jc = (tl >> 5) * 16;
+  float w[16];
+#pragma unroll
+  for (int u = 0; u < 16; ++u) w[u] = (op.kind && wi < kb) ? sA[(j0 + wi) * kSmallLd + jc + u] : 0.0f;
+  for (int r = 0; r < nr; ++r) {
+    const float vri = sV[r * kSmallLd + wi];
+    const float4* cr = reinterpret_cast<const float4*>(sC + r * kSmallLd + jc);
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const float4 x = cr[q];
+      w[4 * q] += vri * x.x;
+      w[4 * q + 1] += vri * x.y;
+      w[4 * q + 2] += vri * x.z;
+      w[4 * q + 3] += vri * x.w;
+    }
+  }
+#pragma unroll
+  for (int u = 0; u < 16; ++u) sW[wi * kSmallLd + jc + u] = w[u];
+  team_sync(team);
+#pragma unroll
+  for (int u = 0; u < 16; ++u) w[u] = 0.0f;
+  for (int l = 0; l < kb; ++l) {
+    const float tlw = sT[wi * (kNB + 1) + l];  // T(l, wi); zero unless l <= wi < kb
+    const float4* wl = reinterpret_cast<const float4*>(sW + l * kSmallLd + jc);
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const float4 x = wl[q];
+      w[4 * q] += tlw * x.x;
+      w[4 * q + 1] += tlw * x.y;
+      w[4 * q + 2] += tlw * x.z;
+      w[4 * q + 3] += tlw * x.w;
+    }
+  }
+  team_sync(team);
+#pragma unroll
+  for (int u = 0; u < 16; ++u) sW[wi * kSmallLd + jc + u] = w[u];
+  team_sync(team);
+  if (op.kind)  // the top rows: A(j0 + i, .) -= W2(i, .)
+    for (int e = tl; e < kb * 32; e += kTeam) {
+      const int i = e >> 5, j = e & 31;
+      sA[(j0 + i) * kSmallLd + j] -= sW[i * kSmallLd + j];
+    }
+  if (tl < nr) {  // C(r, .) -= V(r, :) W2
+    float acc[32];
+#pragma unroll
+    for (int j = 0; j < 32; ++j) acc[j] = 0.0f;
+#pragma unroll
+    for (int i = 0; i < kNB; ++i) {
+      if (i < kb) {
+        const float vi = vrow[i];
+        const float4* wr = reinterpret_cast<const float4*>(sW + i * kSmallLd);
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+          const float4 x = wr[q];
+          acc[4 * q] += vi * x.x;
+          acc[4 * q + 1] += vi * x.y;
+          acc[4 * q + 2] += vi * x.z;
+          acc[4 * q + 3] += vi * x.w;
+        }
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < 32; ++j) sC[tl * kSmallLd + j] -= acc[j];
+  }
+  team_sync(team);
+}
+
+__global__ void __launch_bounds__(kTeamThreads, 3) k_update_small(const UpdTask* __restrict__ tasks,
+                                                              const UpdOp* __restrict__ ops, int ntasks) {
   extern __shared__ __align__(16) unsigned char smraw[];
   const int team = threadIdx.x / kTeam, tl = threadIdx.x % kTeam;
   const int ti = blockIdx.x * kTeams + team;
   if (ti >= ntasks) return;  // the whole team
-  float* sV = reinterpret_cast<float*>(smraw) + (size_t)team * kTeamSmem;  // sV[r * ld + i] = V(r0 + r, j0 + i)
-  float* sC = sV + kSmallOp * kSmallLd;                                    // sC[r * ld + j] = C(r0 + r, h + j)
-  float* sW = sC + kSmallOp * kSmallLd;                                    // sW[i * ld + j]: W, then W2
+  float* sA = reinterpret_cast<float*>(smraw) + (size_t)team * kTeamSmem;  // sA[r * ld + j] = A(r, h + j)
+  float* sB = sA + kSmallOp * kSmallLd;                                    // sB[r * ld + j] = B(r, h + j)
+  float* sV = sB + kSmallOp * kSmallLd;
+  float* sW = sV + kSmallOp * kSmallLd;
+  float* sT = sW + kNB * kSmallLd;
   const UpdTask t = tasks[ti];
-  const int wi = tl & 31, jc = (tl >> 5) * 16;  // W phase: reflector wi, columns jc .. jc + 15
-  for (int o = t.op_begin; o < t.op_end; ++o) {
-    const UpdOp op = ops[o];
-    const float* V = as<float>(op.V);
-    const float* Tm = as<float>(op.T);
-    float* A = as<float>(op.A) + (size_t)t.col0 * op.lda;
-    float* Cp = op.kind ? as<float>(op.B) + (size_t)t.col0 * op.ldb : A;  // the block V acts on
-    const int ldc = op.kind ? op.ldb : op.lda;
-    const int k = op.k;
-    for (int h = 0; h < t.ncols; h += 32) {
-      const int hc = min(32, t.ncols - h);
-      for (int j0 = 0; j0 < k; j0 += kNB) {
-        const int kb = min(kNB, k - j0);
-        const int r0 = op.kind ? 0 : j0;  // geqrt panel acts on rows j0.., tsqrt on all of B
-        const int nr = op.m - r0;
-        float vrow[kNB];
+  for (int h = 0; h < t.ncols; h += 32) {
+    const int hc = min(32, t.ncols - h);
+    int o = t.op_begin;
+    while (o < t.op_end) {
+      const double* Aid = ops[o].A;
+      float* A = as<float>(ops[o].A) + (size_t)(t.col0 + h) * ops[o].lda;
+      const int lda = ops[o].lda;
+      const int arows = ops[o].kind ? ops[o].k : ops[o].m;
 #pragma unroll
-        for (int i = 0; i < kNB; ++i) {
-          float v = 0.0f;
-          if (tl < nr && i < kb) {
-            const int r = r0 + tl;
-            v = op.kind ? V[r + (size_t)(j0 + i) * op.ldv]
-                        : (tl == i ? 1.0f : (tl < i ? 0.0f : V[r + (size_t)(j0 + i) * op.ldv]));
-          }
-          vrow[i] = v;
-          sV[tl * kSmallLd + i] = v;
-        }
-#pragma unroll
-        for (int j = 0; j < 32; ++j)
-          sC[tl * kSmallLd + j] = (tl < nr && j < hc) ? Cp[(r0 + tl) + (size_t)(h + j) * ldc] : 0.0f;
-        team_sync(team);
-        // W(wi, jc + u) = sum_r V(r, wi) C(r, jc + u) (+ A(j0 + wi, .) for a tsqrt step)
-        float w[16];
-#pragma unroll
-        for (int u = 0; u < 16; ++u) w[u] = 0.0f;
-        for (int r = 0; r < nr; ++r) {
-          const float vri = sV[r * kSmallLd + wi];
-          const float4* cr = reinterpret_cast<const float4*>(sC + r * kSmallLd + jc);
-#pragma unroll
-          for (int q = 0; q < 4; ++q) {
-            const float4 x = cr[q];
-            w[4 * q] += vri * x.x;
-            w[4 * q + 1] += vri * x.y;
-            w[4 * q + 2] += vri * x.z;
-            w[4 * q + 3] += vri * x.w;
-          }
-        }
-        if (op.kind && wi < kb)
-#pragma unroll
-          for (int u = 0; u < 16; ++u)
-            if (jc + u < hc) w[u] += A[(j0 + wi) + (size_t)(h + jc + u) * op.lda];
-#pragma unroll
-        for (int u = 0; u < 16; ++u) sW[wi * kSmallLd + jc + u] = w[u];
-        team_sync(team);
-        // W2(wi, .) = sum_{l <= wi} T(l, wi) W(l, .)
-#pragma unroll
-        for (int u = 0; u < 16; ++u) w[u] = 0.0f;
-        for (int l = 0; l < kb; ++l) {
-          const float tlw = (l <= wi && wi < kb) ? Tm[(size_t)j0 * kNB + l + (size_t)wi * kNB] : 0.0f;
-          const float4* wl = reinterpret_cast<const float4*>(sW + l * kSmallLd + jc);
-#pragma unroll
-          for (int q = 0; q < 4; ++q) {
-            const float4 x = wl[q];
-            w[4 * q] += tlw * x.x;
-            w[4 * q + 1] += tlw * x.y;
-            w[4 * q + 2] += tlw * x.z;
-            w[4 * q + 3] += tlw * x.w;
-          }
-        }
-        team_sync(team);
-#pragma unroll
-        for (int u = 0; u < 16; ++u) sW[wi * kSmallLd + jc + u] = w[u];
-        team_sync(team);
-        if (op.kind)  // the top block: A(j0 + i, .) -= W2(i, .)
-          for (int e = tl; e < kb * hc; e += kTeam) {
-            const int i = e % kb, j = e / kb;
-            A[(j0 + i) + (size_t)(h + j) * op.lda] -= sW[i * kSmallLd + j];
-          }
-        // C(r, .) -= V(r, :) W2
-        if (tl < nr) {
-          float acc[32];
-#pragma unroll
-          for (int j = 0; j < 32; ++j) acc[j] = 0.0f;
-#pragma unroll
-          for (int i = 0; i < kNB; ++i) {
-            if (i < kb) {
-              const float vi = vrow[i];
-              const float4* wr = reinterpret_cast<const float4*>(sW + i * kSmallLd);
-#pragma unroll
-              for (int q = 0; q < 8; ++q) {
-                const float4 x = wr[q];
-                acc[4 * q] += vi * x.x;
-                acc[4 * q + 1] += vi * x.y;
-                acc[4 * q + 2] += vi * x.z;
-                acc[4 * q + 3] += vi * x.w;
-              }
-            }
-          }
+      for (int j = 0; j < 32; ++j)
+        sA[tl * kSmallLd + j] = (tl < arows && j < hc) ? A[tl + (size_t)j * lda] : 0.0f;
+      team_sync(team);
+      for (; o < t.op_end && ops[o].A == Aid; ++o) {
+        const UpdOp op = ops[o];
+        float* B = nullptr;
+        if (op.kind) {
+          B = as<float>(op.B) + (size_t)(t.col0 + h) * op.ldb;
 #pragma unroll
           for (int j = 0; j < 32; ++j)
-            if (j < hc) Cp[(r0 + tl) + (size_t)(h + j) * ldc] = sC[tl * kSmallLd + j] - acc[j];
+            sB[tl * kSmallLd + j] = (tl < op.m && j < hc) ? B[tl + (size_t)j * op.ldb] : 0.0f;
+          // made visible by the barrier inside team_panel
         }
-        team_sync(team);
+        for (int j0 = 0; j0 < op.k; j0 += kNB) team_panel(op, j0, min(kNB, op.k - j0), sA, sB, sV, sW, sT, team, tl);
+        if (op.kind && tl < op.m)
+#pragma unroll
+          for (int j = 0; j < 32; ++j)
+            if (j < hc) B[tl + (size_t)j * op.ldb] = sB[tl * kSmallLd + j];
+        team_sync(team);  // sB is reused by the next step
       }
+      if (tl < arows)
+#pragma unroll
+        for (int j = 0; j < 32; ++j)
+          if (j < hc) A[tl + (size_t)j * lda] = sA[tl * kSmallLd + j];
+      team_sync(team);  // sA is reused by the next group
     }
   }
 }
@@ -2059,7 +2088,7 @@ cudaError_t launch_update_small(const UpdTask* t, const UpdOp* o, int ntasks, cu
   if (!g_fp32) return cudaErrorInvalidValue;  // FP32 factors only
   counted();
   if (cudaError_t e = prep(k_update_small, kUpdSmallSmem)) return e;
-  k_update_small<<<(ntasks + kTeams - 1) / kTeams, kThreads, kUpdSmallSmem, st>>>(t, o, ntasks);
+  k_update_small<<<(ntasks + kTeams - 1) / kTeams, kTeamThreads, kUpdSmallSmem, st>>>(t, o, ntasks);
   return last();
 }
 

@@ -260,5 +260,6 @@ def test_tuned_applies_pick_the_faster_kind_per_level():
     measured = tab[:, :, 0] >= 0
     assert measured.any()
     for l, k in zip(*np.nonzero(measured)):
-        assert tab[l, k, 2] == (1.0 if tab[l, k, 0] < tab[l, k, 1] else 0.0)
+        # the tensor cores where they were at least 5 % faster, else the CUDA cores
+        assert tab[l, k, 2] == (1.0 if tab[l, k, 0] < np.float32(0.95) * tab[l, k, 1] else 0.0)
     assert np.all(np.abs(np.array(etas) / etas[1] - 1) < 0.2)
