@@ -1446,7 +1446,7 @@ void Tree::tune_table(std::vector<float>& out) const {
       if (tune_runs_ >= 1 && (int)tune_ms_[0].size() == L) o[0] = tune_ms_[0][l][k];
       if (tune_runs_ >= 2 && (int)tune_ms_[1].size() == L) {
         o[1] = tune_ms_[1][l][k];
-        o[2] = o[0] < o[1] ? 1.f : 0.f;
+        o[2] = use_tc(l, k) ? 1.f : 0.f;  // the choice the factorizations make
       }
     }
 }
