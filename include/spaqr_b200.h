@@ -67,10 +67,11 @@ int spq_set_precision(spq_tree* t, int bits);
  * 1860-1903) -- run either as 3xTF32 tcgen05 MMAs with FP32 accumulation or in
  * FP32 on the CUDA cores.  mode 0 = CUDA cores, 1 = tensor cores, 2 (default) =
  * tuned: the first float factorization of a partition runs every apply on the
- * tensor cores, the second on the CUDA cores, and later ones pick per level and
- * kind of apply the faster of the two measured times (so the first two
- * factorizations of a partition differ from later ones in rounding).  No
- * effect on FP64 factors.  Takes effect at the next factorize.
+ * tensor cores, the second on the CUDA cores, and later ones run, per level and
+ * kind of apply, the tensor cores where they measured at least 5 % faster, else
+ * the CUDA cores (so the first two factorizations of a partition differ from
+ * later ones in rounding; the margin keeps near-ties from flipping between
+ * runs).  No effect on FP64 factors.  Takes effect at the next factorize.
  * spq_tune_table: per level 9 floats -- for updates, left applies, right
  * applies: tensor-core ms, CUDA-core ms, choice (1 tensor, 0 CUDA, -1 not
  * tuned yet). */
