@@ -379,15 +379,18 @@ __global__ void k_mlp_adam(float* P, const float* __restrict__ g, float* m1, flo
 
 // ---------------------------------------------------------------- sketch / projection GEMMs
 // 64 x 64 output tile per CTA, k-steps of 32, each thread a 4 x 4 block of
-// outputs at rows ty + 16 a, columns tx + 16 b.  In the sketch the next
+// outputs at rows ty + 16 a (the sketch: rows 4 ty + a), columns tx + 16 b.
+// In the sketch the next
 // k-step's C tile is copied into the other half of a double buffer with
 // cp.async while the current one is multiplied (the projection loads each
 // step's tiles directly: its two tiles in a double buffer would halve the
 // CTAs per SM); every output sums its k terms in ascending order.
 __global__ void __launch_bounds__(kT) k_sketch(const SketchTask* __restrict__ tasks,
                                                const GemmTile* __restrict__ tiles) {
-  __shared__ double As[2][kTile][kKStep + 1];      // C(r0 + rr, j0 + jj) at As[.][rr][jj]
-  __shared__ unsigned long long Ws[2][kKStep];     // signs of Omega(j0 + jj, c0 .. c0 + 63)
+  // C(r0 + rr, j0 + jj) at As[.][jj][rr]: a thread's four consecutive rows are
+  // two 16-byte loads (rows of kTile + 2 doubles keep them 16-byte aligned)
+  __shared__ __align__(16) double As[2][kKStep][kTile + 2];
+  __shared__ unsigned long long Ws[2][kKStep];  // signs of Omega(j0 + jj, c0 .. c0 + 63)
   const GemmTile g = tiles[blockIdx.x];
   const SketchTask t = tasks[g.task];
   const int ell = *t.ell;
@@ -399,8 +402,8 @@ __global__ void __launch_bounds__(kT) k_sketch(const SketchTask* __restrict__ ta
     for (int e = threadIdx.x; e < kTile * kKStep; e += kT) {
       const int rr = e / kKStep, jj = e % kKStep;
       const int r = g.r0 + rr, j = j0 + jj;
-      if (r < t.m && j < t.w) dev::cp_async_elem(&As[b][rr][jj], t.C + (size_t)r * t.ldw + j);
-      else As[b][rr][jj] = 0.0;
+      if (r < t.m && j < t.w) dev::cp_async_elem(&As[b][jj][rr], t.C + (size_t)r * t.ldw + j);
+      else As[b][jj][rr] = 0.0;
     }
     if (threadIdx.x < kKStep) Ws[b][threadIdx.x] = omega_bits(t.seed, j0 + threadIdx.x, g.c0 >> 6);
     dev::cp_async_commit();
@@ -419,12 +422,12 @@ __global__ void __launch_bounds__(kT) k_sketch(const SketchTask* __restrict__ ta
 #pragma unroll 8
     for (int jj = 0; jj < kKStep; ++jj) {
       const unsigned long long w = Ws[b][jj];
-      double a[4], bq[4];
+      const double2 a01 = *reinterpret_cast<const double2*>(&As[b][jj][4 * ty]);
+      const double2 a23 = *reinterpret_cast<const double2*>(&As[b][jj][4 * ty + 2]);
+      const double a[4] = {a01.x, a01.y, a23.x, a23.y};
+      double bq[4];
 #pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        a[q] = As[b][ty + 16 * q][jj];
-        bq[q] = ((w >> (tx + 16 * q)) & 1ull) ? 1.0 : -1.0;
-      }
+      for (int q = 0; q < 4; ++q) bq[q] = ((w >> (tx + 16 * q)) & 1ull) ? 1.0 : -1.0;
 #pragma unroll
       for (int p = 0; p < 4; ++p)
 #pragma unroll
@@ -434,7 +437,7 @@ __global__ void __launch_bounds__(kT) k_sketch(const SketchTask* __restrict__ ta
   }
 #pragma unroll
   for (int p = 0; p < 4; ++p) {
-    const int r = g.r0 + ty + 16 * p;
+    const int r = g.r0 + 4 * ty + p;
     if (r >= t.m) continue;
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
